@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the direct spherical Biot-Savart RK4 step on B200.
+
+Metric: Biot-Savart interactions/s (one interaction = one (target, source)
+pair evaluated; one RK4 step = 4 stages x [nA(nA-1) + (nV + nQ) nA]).
+
+Default workload: Gaussian vortex exp(-16|x-x0|^2) minus its area mean,
+x0 = (22.5N, 0E), icosahedral level 7 (327,680 active panels + 163,842
+vertices), delta = 0.01 for all targets, one RK4 step per timed step, FP32-
+compensated pair arithmetic (the FP64 path is measured beside it).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--config gaussian_l7|rh4_l8|rh4_l4|jet_l6] [--precision fp32c|fp64]
+
+Timing: CUDA events on the library's stream around each step, L2 flushed
+(a 256 MiB write) between timed steps, max over ranks. The reference arm
+(--impl reference) times the CPU FP64 restatement of the reference loops
+(oracle/) on all host cores over a seeded sample of target rows.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOPS_PER_INTERACTION = 22  # dot 5, denominator 1, weight 1, cross 9, accumulate 6
+L2_FLUSH_BYTES = 256 << 20
+
+
+def build_workload(name: str):
+    from thesiscode_b200 import configs
+
+    if name == "gaussian_l7":
+        return configs.gaussian(level=7, delta=0.01, dt=0.01, steps=1)
+    if name == "rh4_l8":
+        return configs.rh4(level=8, delta=0.005, dt=0.01, steps=1)
+    if name == "rh4_l4":
+        return configs.rh4(level=4, delta=0.0, dt=0.01, steps=10)
+    if name == "jet_l6":
+        return configs.jet(level=6, delta=0.02, dt=0.005, steps=20)
+    raise SystemExit(f"unknown config {name}")
+
+
+def workload_config(w, precision, scaling_note):
+    return {"workload": f"{w.name}: {w.meta.get('ic', '')}", "level": w.level, "n_active": w.nA,
+            "n_vertex": w.nV, "n_passive": w.nQ, "delta": w.deltas[0], "omega": w.omega, "dt": w.dt,
+            "rk4_steps_per_step": 1, "arith": precision, "interactions_per_step": w.interactions_per_step(),
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": scaling_note}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks(device: int) -> dict:
+    from thesiscode_b200 import _native as N
+
+    out = {}
+    for key, kind, iters in (("ffma", N.TC_PROBE_FFMA, 65536), ("dfma", N.TC_PROBE_DFMA, 32768)):
+        best = 0.0
+        for _ in range(3):
+            v = ctypes.c_double()
+            N.call("tc_probe_peak", device, kind, iters, ctypes.byref(v))
+            best = max(best, v.value)
+        out[key] = best  # FMA/s
+    return out
+
+
+def stats(ctx, reset=False):
+    from thesiscode_b200 import _native as N
+
+    L, PL, PI = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    ms = ctypes.c_double()
+    N.call("tc_stats", ctx.handle, int(reset), ctypes.byref(L), ctypes.byref(PL), ctypes.byref(PI),
+           ctypes.byref(ms))
+    return L.value, PL.value, PI.value, ms.value
+
+
+def time_device_steps(w, precision, steps, warmup, device, dist_driver=None):
+    """Device-resident timing: state loaded once, `steps` RK4 steps timed one by one."""
+    import torch
+
+    from thesiscode_b200 import _native as N
+    from thesiscode_b200.panel_velocity import Context
+
+    stream = torch.cuda.Stream(device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
+    if dist_driver is None:
+        ctx = Context(device, precision)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_omega(w.omega)
+        ctx.set_deltas(*w.deltas)
+        N.call("tc_rk4_load", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA,
+               N.dptr(w.xV), w.nV, N.dptr(w.xQ) if w.nQ else None, w.nQ, 0)
+
+        def one_step():
+            N.call("tc_rk4_advance", ctx.handle, w.dt, 1, None)
+    else:
+        ctx = dist_driver.ctx
+        dist_driver.bind_stream(stream)
+        dist_driver.load(w)
+
+        def one_step():
+            dist_driver.advance(w.dt, 1)
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            one_step()
+        torch.cuda.synchronize(device)
+        N.call("tc_stats_enable_timing", ctx.handle, 1)
+        stats(ctx, reset=True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        if dist_driver is not None:
+            dist_driver.barrier()
+        torch.cuda.synchronize(device)
+        clocks = ClockSampler(device)
+        clocks.start()
+        t_wall = time.perf_counter()
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            one_step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(device)
+        t_wall = time.perf_counter() - t_wall
+        if dist_driver is not None:
+            dist_driver.barrier()
+        clk = clocks.stop()
+        N.call("tc_stats_enable_timing", ctx.handle, 0)
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        launches, pair_launches, pair_inter, pair_ms = stats(ctx, reset=True)
+    return dict(step_ms=step_ms, total_ms=sum(step_ms), wall_s=t_wall, launches=launches,
+                pair_launches=pair_launches, pair_interactions=pair_inter, pair_ms=pair_ms,
+                clocks=clk, ctx=ctx)
+
+
+def time_e2e(w, precision, steps, device):
+    """End to end through the public host-pointer call tc_rk4_step: pinned host inputs copied
+    in, one fused RK4 step, results (positions, vorticity, kinetic energy) copied out."""
+    import torch
+
+    from thesiscode_b200 import _native as N
+    from thesiscode_b200.panel_velocity import Context
+
+    ctx = Context(device, precision)
+    stream = torch.cuda.Stream(device)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t
+
+    xA, zA, aA, xV = pinned(w.xA), pinned(w.zetaA), pinned(w.areaA), pinned(w.xV)
+    xQ = pinned(w.xQ if w.nQ else np.zeros((0, 3)))
+    ke = pinned(np.zeros(w.nA))
+    tke = np.zeros(1)
+
+    def call():
+        N.call("tc_rk4_step", ctx.handle, *(ctypes.cast(t.data_ptr(), N.dp) for t in (xA, zA, aA)),
+               w.nA, ctypes.cast(xV.data_ptr(), N.dp), w.nV,
+               ctypes.cast(xQ.data_ptr(), N.dp) if w.nQ else None, w.nQ, w.dt, 1, N.dptr(tke),
+               ctypes.cast(ke.data_ptr(), N.dp))
+
+    call()  # warm-up (allocations)
+    times = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        call()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ctx.close()
+    D = 8
+    h2d = (3 * w.nA + 2 * w.nA + 3 * w.nV + 3 * w.nQ) * D
+    d2h = (3 * w.nA + w.nA + 3 * w.nV + 3 * w.nQ + w.nA + 1) * D
+    return dict(ms=sum(times) / len(times), h2d=h2d, d2h=d2h)
+
+
+def sample_rows(w, frac, seed=11):
+    rng = np.random.default_rng(seed)
+    ra = np.sort(rng.choice(w.nA, max(1, int(w.nA * frac)), replace=False)).astype(np.int32)
+    rv = np.sort(rng.choice(w.nV, max(1, int(w.nV * frac)), replace=False)).astype(np.int32)
+    return ra, rv
+
+
+def cpu_baseline(w, frac=1.0 / 64, threads=None):
+    """The CPU FP64 oracle (restated reference loops) on all host cores over a seeded 1/64
+    sample of the target rows of one RK4 stage; returns interactions/s and the sampled sums."""
+    from oracle import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    ra, rv = sample_rows(w, frac)
+    t = time.perf_counter()
+    uA = O.rows(0, ra, None, w.xA, w.zetaA, w.areaA, delta=w.deltas[0], nthreads=threads)
+    uV = O.rows(1, rv, w.xV, w.xA, w.zetaA, w.areaA, delta=w.deltas[1], nthreads=threads)
+    dt = time.perf_counter() - t
+    inter = ra.size * (w.nA - 1) + rv.size * w.nA
+    return dict(value=inter / dt, seconds=dt, cores=threads, rows=(ra, rv), sums=(uA, uV),
+                sample=f"one RK4 stage, seeded 1/{round(1 / frac)} of target rows "
+                       f"({ra.size} active + {rv.size} vertex rows x {w.nA} sources)")
+
+
+def gpu_stage1_errors(w, precision, device, rows, sums):
+    """Max/RMS of |u_gpu - u_oracle| / max|u_oracle| on the sampled rows of stage 1."""
+    from thesiscode_b200 import _native as N
+    from thesiscode_b200.panel_velocity import Context
+
+    ctx = Context(device, precision)
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    dA, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    dV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+    ctx.close()
+    ra, rv = rows
+    diff = np.concatenate([dA[ra] - sums[0], dV[rv] - sums[1]])
+    ref = np.concatenate([sums[0], sums[1]])
+    scale = np.abs(ref).max()
+    return dict(max=float(np.abs(diff).max() / scale),
+                rms=float(np.sqrt((diff ** 2).sum(1).mean()) / scale))
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    device = local
+    torch.cuda.set_device(device)
+    from thesiscode_b200 import _native as N
+
+    N.lib()
+    w = build_workload(args.config)
+    driver = None
+    if world > 1:
+        from thesiscode_b200.dist import DistributedPanelVelocity
+
+        driver = DistributedPanelVelocity(device, args.precision)
+    peaks = measured_peaks(device)
+    main = time_device_steps(w, args.precision, args.steps, args.warmup, device, driver)
+    total_ms = main["total_ms"]
+    if driver is not None:
+        total_ms = driver.max_over_ranks(total_ms)
+    value = w.interactions_per_step() * args.steps / (total_ms * 1e-3)
+    fp_peak = (peaks["ffma"] if args.precision == "fp32c" else peaks["dfma"]) * 2.0
+    pair_flops = FLOPS_PER_INTERACTION * main["pair_interactions"] / max(main["pair_launches"], 1)
+    pair_ms_launch = main["pair_ms"] / max(main["pair_launches"], 1)
+    achieved = pair_flops / (pair_ms_launch * 1e-3)
+    line = {
+        "metric": "Biot-Savart interactions/s (one RK4 step of the direct spherical sum)",
+        "value": value, "unit": "interactions/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+        "dtype": "f32 pairs (compensated, f64 accumulation)" if args.precision == "fp32c" else "f64",
+        "data": "synthetic: analytic vorticity on a generated icosahedral grid (seeded)",
+        "config": workload_config(w, args.precision, f"target-sharded x{world}" if world > 1 else "1 GPU"),
+        "roofline": {"bound": "fp32" if args.precision == "fp32c" else "fp64",
+                     "achieved": achieved / 1e12, "peak": fp_peak / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / fp_peak, "traffic": None,
+                     "kernel": f"pair_{args.precision}_kernel",
+                     "flops_per_interaction": FLOPS_PER_INTERACTION,
+                     "pair_ms_per_launch": pair_ms_launch,
+                     "peak_source": "measured live: CUDA-core FMA probe (tc_probe_peak) x 2 flops"},
+        "gpu_launches": main["launches"],
+        "clocks": main["clocks"],
+    }
+    if rank == 0:
+        if world == 1 and not args.quick:
+            other = "fp64" if args.precision == "fp32c" else "fp32c"
+            o = time_device_steps(w, other, max(1, min(args.steps, 3)), 1, device)
+            o["ctx"].close()
+            line[other] = {"value": w.interactions_per_step() * len(o["step_ms"]) / (o["total_ms"] * 1e-3),
+                           "ms_per_step": o["total_ms"] / len(o["step_ms"])}
+            fast = line["value"] if args.precision == "fp32c" else line[other]["value"]
+            slow = line[other]["value"] if args.precision == "fp32c" else line["value"]
+            line["fp32c_over_fp64"] = fast / slow
+        if not args.quick:
+            e2e = time_e2e(w, args.precision, max(2, min(args.steps, 4)), device)
+            line["e2e"] = {"value": w.interactions_per_step() / (e2e["ms"] * 1e-3), "unit": "interactions/s",
+                           "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                           "ms_per_step": e2e["ms"], "api": "tc_rk4_step (host pointers, pinned)"}
+        if world == 1 and not args.no_cpu:
+            cb = cpu_baseline(w)
+            line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],
+                                    "kind": "port", "sample": cb["sample"], "seconds": cb["seconds"]}
+            line["error_vs_fp64_oracle"] = {
+                p: gpu_stage1_errors(w, p, device, cb["rows"], cb["sums"]) for p in ("fp32c", "fp64")}
+        print(json.dumps(line), flush=True)
+    main["ctx"].close() if driver is None else driver.close()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = build_workload(args.config)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline(w, frac=1.0 / 1024, threads=threads)
+    vals, secs = [], []
+    for _ in range(args.steps):
+        cb = cpu_baseline(w, frac=1.0 / 256, threads=threads)
+        vals.append(cb["value"])
+        secs.append(cb["seconds"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "Biot-Savart interactions/s (one RK4 step of the direct spherical sum)",
+            "value": v, "unit": "interactions/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": w.interactions_per_step() / v * 1e3, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: analytic vorticity on a generated icosahedral grid (seeded)",
+            "config": workload_config(w, "fp64 (CPU)", "host cores"),
+            "cpu_baseline": {"value": v, "unit": "interactions/s", "cores": threads, "kind": "port",
+                             "sample": cb["sample"] + "; each step one such sample, rate extrapolated linearly"},
+            "e2e": {"value": v, "unit": "interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is Fortran+MPI (ifort, mpif90); no Fortran compiler or MPI exists on "
+                    "these machines, so the arm runs the C restatement of its loops (oracle/) on all host "
+                    "threads with the reference's LoadBalance row partition"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="gaussian_l7", choices=["gaussian_l7", "rh4_l8", "rh4_l4", "jet_l6"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error check")
+    ap.add_argument("--quick", action="store_true", help="main measurement only")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

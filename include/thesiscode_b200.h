@@ -1,0 +1,191 @@
+/*
+ * thesiscode_b200.h - C ABI of the B200 (sm_100a) Biot-Savart / RK4 library.
+ *
+ * This is the drop-in boundary for ThesisCode's barotropic-vorticity hot
+ * path: the direct O(N^2) spherical Biot-Savart velocity sum
+ *
+ *     u_i = -1/(4 pi) * sum_{k != i} (x_i x x_k) zeta_k A_k / (1 - x_i.x_k + delta^2)
+ *
+ * evaluated inside the classical RK4 step (PanelVelocityParallel.f90 and
+ * PanelVelocitySerial.f90, VoronoiVelocityParallel.f90 in the reference).
+ *
+ * Conventions (all entry points):
+ *   - reals are IEEE double (Fortran real(kreal) = kind(0.d0), NumberKinds.f90:9),
+ *     integers are int32 (kint = kind(1), NumberKinds.f90:10);
+ *   - a set of n points is stored as the Fortran array x(3,n), column-major,
+ *     i.e. component c of point k is x[3*k + c] (0-based here);
+ *   - index ranges are 0-based and half-open [i0, i1). The reference's
+ *     1-based inclusive [indexStart, indexEnd] maps to i0 = indexStart-1,
+ *     i1 = indexEnd;
+ *   - every call returns TC_OK (0) or a negative status; none aborts or
+ *     prints. tc_last_error() describes the last failure of this thread.
+ *   - entry points named *_device take device pointers and run on the
+ *     context's stream without synchronising; all others take host pointers
+ *     and return after the results are back in host memory.
+ */
+#ifndef THESISCODE_B200_H
+#define THESISCODE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define TC_OK 0
+#define TC_ERR_ARG (-1)       /* bad size, range, pointer or enum value   */
+#define TC_ERR_CUDA (-2)      /* CUDA runtime error (see tc_last_error)   */
+#define TC_ERR_NONFINITE (-3) /* NaN or Inf found in an input or result   */
+#define TC_ERR_TIMEOUT (-4)   /* a bounded device-side wait ran out       */
+#define TC_ERR_STATE (-5)     /* call out of sequence (e.g. no state yet) */
+#define TC_ERR_NOMEM (-6)     /* device or host allocation failed         */
+
+/* ---- arithmetic of the pair sum -------------------------------------- */
+#define TC_FP64 0  /* FP64 throughout; denominator rounded exactly as the
+                      reference's 1 - sum(x_k*x_j) (no contraction)          */
+#define TC_FP32C 1 /* FP32 pair arithmetic on tile-relative offsets with a
+                      cancellation-free denominator, FP64 accumulation of
+                      per-tile FP32 partial sums                              */
+
+/* ---- target classes (the three RHS routines of the reference) ------- */
+#define TC_ACTIVE 0  /* BVEActiveRHS  PanelVelocityParallel.f90:1287-1334:
+                        targets are the sources, self pair excluded,
+                        dVort = -2 Omega u_z, delta = delta_active (0)       */
+#define TC_VERTEX 1  /* BVEPassiveRHS :1337-1373: particles (panel
+                        vertices), delta = delta_vertex (0)                  */
+#define TC_PASSIVE 2 /* BVESmoothVelocity :1376-1412: divided panels,
+                        delta = smooth (0.05 by default, :27)                */
+
+/* ---- throughput probe kinds (tc_probe_peak) --------------------------- */
+#define TC_PROBE_FFMA 0
+#define TC_PROBE_FFMA2 1
+#define TC_PROBE_DFMA 2
+#define TC_PROBE_RCP32 3
+#define TC_PROBE_RCP64 4
+#define TC_PROBE_DDIV 5
+
+typedef struct tc_ctx tc_ctx;
+
+/* ---- library --------------------------------------------------------- */
+const char* tc_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* tc_last_error(void);
+
+/* Measured operations/s of one CUDA-core pipe on `device` (roofline
+ * denominator). No counterpart in the reference (it has no GPU code). */
+int tc_probe_peak(int device, int kind, int iters, double* ops_per_s);
+
+/* ---- device buffers of the RK4 state (tc_rk4_device_buffer) --------- */
+#define TC_BUF_SOURCES 0 /* double4 {x,y,z,zeta*A} per active panel       */
+#define TC_BUF_XA 1      /* x(3,nA) of active panels                      */
+#define TC_BUF_ZETA 2    /* relVort(nA) of active panels                  */
+#define TC_BUF_XV 3      /* x(3,nV) of particles                          */
+#define TC_BUF_XQ 4      /* x(3,nQ) of divided (passive) panels           */
+#define TC_BUF_KE 5      /* kineticEnergy(nA), stage 1 of the last step   */
+
+/* ---- context: the module state of PanelVelocityParallelModule -------- */
+/* Replaces InitializeMPIRK4 (PanelVelocityParallel.f90:126-164) for one
+ * rank: binds a device and the pair arithmetic (TC_FP64 / TC_FP32C). */
+int tc_create(int device, int precision, tc_ctx** out);
+/* FinalizeMPIRK4 (:216-230): frees every device buffer. */
+int tc_destroy(tc_ctx* ctx);
+/* Run on a caller's cudaStream_t (default: the legacy default stream). */
+int tc_set_stream(tc_ctx* ctx, void* cuda_stream);
+int tc_synchronize(tc_ctx* ctx);
+int tc_set_precision(tc_ctx* ctx, int precision);
+int tc_get_precision(tc_ctx* ctx, int* precision);
+/* SetOmega (TracerAndVorticityDistributions.f90:136-139); default 2*pi. */
+int tc_set_omega(tc_ctx* ctx, double omega);
+int tc_get_omega(tc_ctx* ctx, double* omega);
+/* SetSmooth / GetSmooth (PanelVelocityParallel.f90:96-105): delta of the
+ * TC_PASSIVE class (default 0.05, :27). */
+int tc_set_smooth(tc_ctx* ctx, double smooth);
+int tc_get_smooth(tc_ctx* ctx, double* smooth);
+/* delta of each target class (reference: 0, 0, smooth). */
+int tc_set_deltas(tc_ctx* ctx, double delta_active, double delta_vertex, double delta_passive);
+int tc_get_deltas(tc_ctx* ctx, double* delta3);
+
+/* ---- one velocity sum ------------------------------------------------- */
+/* BVEActiveRHS (:1287-1334), BVEPassiveRHS (:1337-1373) or
+ * BVESmoothVelocity (:1376-1412) selected by target_class:
+ *   X(3,m)       targets (NULL or src_x for TC_ACTIVE, then m == n)
+ *   src_x(3,n), vort(n), area(n)   active panels (sources)
+ *   [i0,i1)      target rows computed; dX rows outside are set to 0
+ *   dX(3,m)      velocity, dVort(m) = -2*Omega*dX(3,:) (TC_ACTIVE only,
+ *                nullable)
+ * Host pointers; returns after dX/dVort are written. */
+int tc_bs_velocity(tc_ctx* ctx, int target_class, const double* X, int m, const double* src_x,
+                   const double* vort, const double* area, int n, int i0, int i1, double* dX,
+                   double* dVort);
+/* Same with device pointers, asynchronous on the context's stream. */
+int tc_bs_velocity_device(tc_ctx* ctx, int target_class, const double* X, int m,
+                          const double* src_x, const double* vort, const double* area, int n,
+                          int i0, int i1, double* dX, double* dVort);
+
+/* ---- RK4 (BVERK4, PanelVelocityParallel.f90:435-658) ------------------ */
+/* The drop-in step on host arrays (the gathered active panels, the
+ * particles and the divided panels, GatherPanels order): nsteps classical
+ * RK4 steps of size dt fused on the device; xA, zetaA, xV, xQ are updated
+ * in place (areas frozen, :452). totalKE[nsteps] (nullable) receives each
+ * step's stage-1 kinetic energy 0.5*sum(|u|^2 A) (:495-501),
+ * kineticEnergy[nA] (nullable) the per-panel |u|^2 of the last step. */
+int tc_rk4_step(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int nA, double* xV,
+                int nV, double* xQ, int nQ, double dt, int nsteps, double* totalKE,
+                double* kineticEnergy);
+/* Same with device arrays (totalKE stays a host array). */
+int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int nA,
+                       double* xV, int nV, double* xQ, int nQ, double dt, int nsteps,
+                       double* totalKE, double* kineticEnergy);
+/* Device-resident state: load once (InitRK4 + GatherPanels copy, :236-318),
+ * advance any number of steps, store when the caller needs the arrays. */
+int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA, const double* areaA, int nA,
+                const double* xV, int nV, const double* xQ, int nQ, int on_device);
+int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalKE);
+int tc_rk4_store(tc_ctx* ctx, double* xA, double* zetaA, double* xV, double* xQ,
+                 double* kineticEnergy, int on_device);
+/* ResetRK4 (:321-372): frees the state; call after a remesh changes N. */
+int tc_reset_rk4(tc_ctx* ctx);
+
+/* ---- stage primitives for target-sharded multi-rank runs -------------- */
+/* Pack stage-1 sources of the loaded state into TC_BUF_SOURCES. */
+int tc_rk4_pack_sources(tc_ctx* ctx);
+/* One stage (0..3) for the target rows [a0,a1) x [v0,v1) x [q0,q1)
+ * (LoadBalance ranges, :167-213). Reads every row of TC_BUF_SOURCES, writes
+ * the rows [a0,a1) of the next stage's sources; a rank exchanges those rows
+ * (the reference's per-stage MPI_BCAST loop, :476-489) before the next
+ * stage. total_ke_device (device, nullable): stage-0 0.5*sum(KE*A) of the
+ * rank's active rows. */
+int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int a1, int v0, int v1, int q0,
+                       int q1, double* total_ke_device);
+int tc_rk4_device_buffer(tc_ctx* ctx, int which, void** ptr);
+/* Copy rows [row0, row0+nrows) of an RK4 device buffer (TC_BUF_*) to
+ * (to_buffer = 0) or from (to_buffer = 1) device memory at ptr, on the
+ * context's stream: the exchange unit of a target-sharded run. */
+int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr, int to_buffer);
+
+/* ---- instrumentation (no counterpart in the reference) ----------------- */
+/* Record CUDA events around every pair-kernel launch on the context's
+ * stream (off by default). */
+int tc_stats_enable_timing(tc_ctx* ctx, int on);
+/* Kernels launched, pair-kernel launches, pairs evaluated and summed
+ * pair-kernel event time (ms) since the last reset; reset != 0 zeroes them. */
+int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* pair_launches,
+             long long* pair_interactions, double* pair_ms);
+
+/* ---- icosahedral grid (input generator) ------------------------------- */
+/* PanelMax / ParticleMax / EdgeMax (ParticlesEdgesPanels2.f90:2614-2662)
+ * and the number of leaf panels, 20*4^level. level in [0, 11]. */
+int tc_icos_grid_sizes(int level, int* n_particles, int* n_edges, int* n_panels, int* n_active);
+/* InitIcosTriGrid (:419-645) with DivideTriPanel (:760-1090) and
+ * TriPanelArea (:1727-1802): particle and panel arrays in the reference's
+ * numbering (0-based). Optional outputs may be NULL. */
+int tc_icos_grid(int level, double* particles_x, double* particles_x0, double* panels_x,
+                 double* panels_x0, double* panels_area, int* panels_has_children,
+                 int* panels_vertices, int* panels_nest, int* panels_children);
+/* GatherPanels index maps (:1556-1619), 0-based. */
+int tc_gather_maps(int n, const int* has_children, int* active_map, int n_active,
+                   int* passive_map, int n_passive);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* THESISCODE_B200_H */

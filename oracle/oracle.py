@@ -1,0 +1,154 @@
+"""ctypes wrapper of the CPU FP64 oracle (oracle/bve_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
+the checker and by bench.py's CPU-baseline leg. The product never imports
+it. Parity status: unpinned against a reference binary (the reference is
+Fortran and no Fortran compiler exists here or on the GPU machines); pinned
+by the reference drivers' known answers (tests/test_oracle.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from ctypes import POINTER, c_double, c_int
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+dp = POINTER(c_double)
+ip = POINTER(c_int)
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (gcc -O2 -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        h = ctypes.CDLL(str(LIB))
+        h.or_active_rhs.argtypes = [dp, dp, dp, dp, dp, c_int, c_int, c_int, c_double, c_double]
+        h.or_passive_rhs.argtypes = [dp, dp, c_int, dp, dp, dp, c_int, c_int, c_int]
+        h.or_smooth_velocity.argtypes = [dp, dp, c_int, dp, dp, dp, c_int, c_int, c_int, c_double]
+        h.or_voronoi_velocity.argtypes = [dp, dp, dp, dp, dp, dp, dp, dp, dp, c_int, c_int, c_int,
+                                          c_double]
+        h.or_rows.argtypes = [c_int, ip, c_int, dp, dp, dp, dp, c_int, c_double, dp, c_int]
+        h.or_load_balance.argtypes = [c_int, c_int, ip, ip]
+        h.or_bve_rk4.argtypes = [dp, c_int, dp, dp, dp, c_int, dp, c_int, c_double, c_double,
+                                 c_double, c_double, c_double, dp, dp, dp, c_int]
+        h.or_bve_rk4.restype = c_double
+        h.or_bve_stage.argtypes = [dp, dp, dp, c_int, dp, c_int, dp, c_int, c_double, c_double,
+                                   c_double, c_double, c_int, c_int, c_int, c_int, c_int, c_int,
+                                   dp, dp, dp, dp, c_int]
+        _lib = h
+    return _lib
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(dp)
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def active_rhs(x, vort, area, i0=0, i1=None, omega=2 * np.pi, delta=0.0):
+    """BVEActiveRHS -> (dX (n,3), dVort (n,))."""
+    x, vort, area = _c(x), _c(vort), _c(area)
+    n = x.shape[0]
+    i1 = n if i1 is None else i1
+    dX = np.zeros((n, 3))
+    dV = np.zeros(n)
+    lib().or_active_rhs(_d(dX), _d(dV), _d(x), _d(vort), _d(area), n, i0, i1, omega, delta)
+    return dX, dV
+
+
+def passive_rhs(X, x, vort, area, i0=0, i1=None):
+    """BVEPassiveRHS -> dX (m,3)."""
+    X, x, vort, area = _c(X), _c(x), _c(vort), _c(area)
+    m = X.shape[0]
+    i1 = m if i1 is None else i1
+    dX = np.zeros((m, 3))
+    lib().or_passive_rhs(_d(dX), _d(X), m, _d(x), _d(vort), _d(area), x.shape[0], i0, i1)
+    return dX
+
+
+def smooth_velocity(X, x, vort, area, smooth=0.05, i0=0, i1=None):
+    """BVESmoothVelocity -> dX (m,3)."""
+    X, x, vort, area = _c(X), _c(x), _c(vort), _c(area)
+    m = X.shape[0]
+    i1 = m if i1 is None else i1
+    dX = np.zeros((m, 3))
+    lib().or_smooth_velocity(_d(dX), _d(X), m, _d(x), _d(vort), _d(area), x.shape[0], i0, i1, smooth)
+    return dX
+
+
+def voronoi_velocity(x, y, z, vort, area, i0=0, i1=None, omega=2 * np.pi, dy=None, dz=None):
+    """BVEVelocity (Voronoi SoA) -> (dx, dy, dz, dVort)."""
+    x, y, z, vort, area = map(_c, (x, y, z, vort, area))
+    n = x.shape[0]
+    i1 = n if i1 is None else i1
+    dx = np.zeros(n)
+    dy = np.zeros(n) if dy is None else _c(dy).copy()
+    dz = np.zeros(n) if dz is None else _c(dz).copy()
+    dV = np.zeros(n)
+    lib().or_voronoi_velocity(_d(dx), _d(dy), _d(dz), _d(dV), _d(x), _d(y), _d(z), _d(vort), _d(area),
+                              n, i0, i1, omega)
+    return dx, dy, dz, dV
+
+
+def rows(cls, row_idx, X, x, vort, area, delta=0.0, nthreads=1):
+    """Sums for a list of target rows (cls 0 active / 1 vertex / 2 passive) -> (r,3)."""
+    row_idx = np.ascontiguousarray(row_idx, dtype=np.int32)
+    x, vort, area = _c(x), _c(vort), _c(area)
+    Xc = None if X is None else _c(X)
+    out = np.zeros((row_idx.shape[0], 3))
+    lib().or_rows(int(cls), row_idx.ctypes.data_as(ip), row_idx.shape[0], _d(Xc), _d(x), _d(vort),
+                  _d(area), x.shape[0], delta, _d(out), nthreads)
+    return out
+
+
+def load_balance(n, p):
+    s = np.zeros(p, np.int32)
+    e = np.zeros(p, np.int32)
+    lib().or_load_balance(n, p, s.ctypes.data_as(ip), e.ctypes.data_as(ip))
+    return s, e
+
+
+def bve_rk4(xV, xA, zetaA, areaA, xQ, dt, omega=2 * np.pi, deltas=(0.0, 0.0, 0.05),
+            absVortV=None, nthreads=1):
+    """One BVERK4 step on copies; returns (xV, xA, zetaA, xQ, totalKE, kineticEnergy, relVortV)."""
+    xV, xA, zetaA, areaA, xQ = (_c(a).copy() for a in (xV, xA, zetaA, areaA, xQ))
+    ke = np.zeros(xA.shape[0])
+    rel = None
+    absV = None
+    if absVortV is not None:
+        absV = _c(absVortV)
+        rel = np.zeros(xV.shape[0])
+    tke = lib().or_bve_rk4(_d(xV), xV.shape[0], _d(xA), _d(zetaA), _d(areaA), xA.shape[0], _d(xQ),
+                           xQ.shape[0], dt, omega, deltas[0], deltas[1], deltas[2], _d(absV), _d(rel),
+                           _d(ke), nthreads)
+    return xV, xA, zetaA, xQ, tke, ke, rel
+
+
+def bve_stage(xA, zetaA, areaA, xV, xQ, omega, deltas, ranges, nthreads=1):
+    """One stage's three sums over the given ranges (a0,a1,v0,v1,q0,q1)."""
+    xA, zetaA, areaA, xV, xQ = map(_c, (xA, zetaA, areaA, xV, xQ))
+    nA, nV, nQ = xA.shape[0], xV.shape[0], xQ.shape[0]
+    dXA = np.zeros((nA, 3))
+    dVA = np.zeros(nA)
+    dXV = np.zeros((nV, 3))
+    dXQ = np.zeros((nQ, 3))
+    lib().or_bve_stage(_d(xA), _d(zetaA), _d(areaA), nA, _d(xV), nV, _d(xQ), nQ, omega, deltas[0],
+                       deltas[1], deltas[2], *[int(r) for r in ranges], _d(dXA), _d(dVA), _d(dXV),
+                       _d(dXQ), nthreads)
+    return dXA, dVA, dXV, dXQ

@@ -1,0 +1,212 @@
+"""GPU parity of the Biot-Savart sums and the fused RK4 step (through the C ABI)
+against the FP64 oracle and its committed golden fixtures.
+
+Error metric (as the workload definition states it): max_i |u_gpu - u_ref| /
+max_i |u_ref| (relative to the largest velocity), and the same for RK4
+displacements x_new - x_old.
+Tolerances: FP64 path 1e-12; FP32-compensated path FP32C_TOL (stated bound).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from thesiscode_b200 import _native as N
+from thesiscode_b200 import configs
+from thesiscode_b200.panel_velocity import Context
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+FP64_TOL = 1e-12
+FP32C_TOL = 1e-7  # compensated path; tiles of the icosahedral (quad-tree) target order
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def ctx64(gpu):
+    c = Context(0, "fp64")
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def ctx32(gpu):
+    c = Context(0, "fp32c")
+    yield c
+    c.close()
+
+
+def setup(ctx, omega, deltas):
+    ctx.set_omega(omega)
+    ctx.set_deltas(*deltas)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+def test_three_sums_against_golden(prec, tol, gpu):
+    g = np.load(GOLDEN / "rh4_parity_l2.npz")
+    ctx = Context(0, prec)
+    setup(ctx, float(g["omega"]), tuple(g["deltas"]))
+    i0, i1, v0, v1 = (int(v) for v in g["ranges"])
+    dXA, dVA = ctx.velocity(N.TC_ACTIVE, None, g["xA"], g["zetaA"], g["areaA"], i0, i1)
+    assert rel_err(dXA, g["dXA"]) <= tol
+    assert rel_err(dVA, g["dVA"]) <= tol
+    assert np.all(dXA[:i0] == 0) and np.all(dXA[i1:] == 0)
+    dXV, _ = ctx.velocity(N.TC_VERTEX, g["xV"], g["xA"], g["zetaA"], g["areaA"], v0, v1)
+    assert rel_err(dXV, g["dXV"]) <= tol
+    dXQ, _ = ctx.velocity(N.TC_PASSIVE, g["xQ"], g["xA"], g["zetaA"], g["areaA"])
+    assert rel_err(dXQ, g["dXQ"]) <= tol
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+@pytest.mark.parametrize("level", [4, 5])
+def test_active_and_vertex_sums_full_level(prec, tol, level, gpu):
+    w = configs.rh4(level=level, parity=True)
+    ctx = Context(0, prec)
+    setup(ctx, w.omega, w.deltas)
+    dXA, dVA = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    rows = np.arange(w.nA)
+    ref = O.rows(0, rows, None, w.xA, w.zetaA, w.areaA, nthreads=8)
+    assert rel_err(dXA, ref) <= tol
+    np.testing.assert_allclose(dVA, -2.0 * w.omega * dXA[:, 2], rtol=0, atol=0)
+    dXV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+    refV = O.rows(1, np.arange(w.nV), w.xV, w.xA, w.zetaA, w.areaA, nthreads=8)
+    assert rel_err(dXV, refV) <= tol
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+def test_sampled_rows_level7_with_delta(prec, tol, gpu):
+    """Level 7 (327,680 sources), delta 0.01: 512 seeded target rows per class vs the oracle."""
+    w = configs.gaussian(level=7, delta=0.01)
+    ctx = Context(0, prec)
+    setup(ctx, w.omega, w.deltas)
+    rng = np.random.default_rng(7)
+    rows = np.sort(rng.choice(w.nA, 512, replace=False))
+    dXA, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    ref = O.rows(0, rows, None, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
+    scale = np.abs(dXA).max()
+    assert np.abs(dXA[rows] - ref).max() / scale <= tol
+    rv = np.sort(rng.choice(w.nV, 512, replace=False))
+    dXV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+    refV = O.rows(1, rv, w.xV, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
+    assert np.abs(dXV[rv] - refV).max() / np.abs(dXV).max() <= tol
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+def test_rk4_step_parity_mode_golden(prec, tol, gpu):
+    g = np.load(GOLDEN / "rh4_parity_l2.npz")
+    ctx = Context(0, prec)
+    setup(ctx, float(g["omega"]), tuple(g["deltas"]))
+    xA, zA, xV, xQ = (np.array(g[k]) for k in ("xA", "zetaA", "xV", "xQ"))
+    tke, ke = ctx.rk4_step(xA, zA, np.array(g["areaA"]), xV, xQ, float(g["dt"]), 1)
+    for new, old, ref in ((xA, g["xA"], g["rk_xA"]), (xV, g["xV"], g["rk_xV"]),
+                          (xQ, g["xQ"], g["rk_xQ"]), (zA, g["zetaA"], g["rk_zA"])):
+        assert rel_err(new - old, ref - old) <= tol
+    assert abs(tke[0] - g["rk_tke"]) <= tol * g["rk_tke"]
+    assert rel_err(ke, g["rk_ke"]) <= tol
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+def test_rk4_two_steps_config_mode_golden(prec, tol, gpu):
+    g = np.load(GOLDEN / "gauss_config_l3.npz")
+    ctx = Context(0, prec)
+    setup(ctx, float(g["omega"]), tuple(g["deltas"]))
+    xA, zA, xV = np.array(g["xA"]), np.array(g["zetaA"]), np.array(g["xV"])
+    tke, ke = ctx.rk4_step(xA, zA, np.array(g["areaA"]), xV, np.zeros((0, 3)), float(g["dt"]), 2)
+    assert rel_err(xA - g["xA"], g["rk_xA"] - g["xA"]) <= tol
+    assert rel_err(xV - g["xV"], g["rk_xV"] - g["xV"]) <= tol
+    assert rel_err(zA - g["zetaA"], g["rk_zA"] - g["zetaA"]) <= tol
+    np.testing.assert_allclose(tke, g["rk_tke"], rtol=tol, atol=0)
+    ctx.close()
+
+
+def test_rk4_matches_oracle_level4_parity_mode(ctx64):
+    w = configs.rh4(level=4, parity=True, dt=0.01)
+    setup(ctx64, w.omega, w.deltas)
+    ref = O.bve_rk4(w.xV, w.xA, w.zetaA, w.areaA, w.xQ, w.dt, w.omega, w.deltas, nthreads=8)
+    xA, zA, xV, xQ = w.xA.copy(), w.zetaA.copy(), w.xV.copy(), w.xQ.copy()
+    tke, ke = ctx64.rk4_step(xA, zA, w.areaA, xV, xQ, w.dt, 1)
+    assert rel_err(xA - w.xA, ref[1] - w.xA) <= FP64_TOL
+    assert rel_err(xV - w.xV, ref[0] - w.xV) <= FP64_TOL
+    assert rel_err(xQ - w.xQ, ref[3] - w.xQ) <= FP64_TOL
+    assert abs(tke[0] - ref[4]) <= FP64_TOL * ref[4]
+
+
+def test_solid_body_known_answer_on_gpu(ctx64):
+    w = configs.solid_body(level=5, rotation_rate=2 * np.pi)
+    setup(ctx64, 0.0, (0.0, 0.0, 0.0))
+    dX, dV = ctx64.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    exact = 2 * np.pi * np.stack([-w.xA[:, 1], w.xA[:, 0], np.zeros(w.nA)], 1)
+    assert rel_err(dX, exact) < 3e-3
+    assert np.all(dV == 0)
+
+
+def test_edge_cases(ctx64, ctx32):
+    w = configs.rh4(level=2, parity=True)
+    for ctx in (ctx64, ctx32):
+        setup(ctx, w.omega, w.deltas)
+        # empty target range: all rows zero
+        dX, dV = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA, 5, 5)
+        assert np.all(dX == 0)
+        # no targets
+        dX, _ = ctx.velocity(N.TC_VERTEX, np.zeros((0, 3)), w.xA, w.zetaA, w.areaA)
+        assert dX.shape == (0, 3)
+        # no sources: zero velocity
+        dX, _ = ctx.velocity(N.TC_VERTEX, w.xV, np.zeros((0, 3)), np.zeros(0), np.zeros(0))
+        assert np.all(dX == 0)
+        # one active panel: only the (excluded) self pair
+        dX, dV = ctx.velocity(N.TC_ACTIVE, None, w.xA[:1], w.zetaA[:1], w.areaA[:1])
+        assert np.all(dX == 0) and np.all(np.isfinite(dV))
+        # ragged sizes: 1..3 targets, sources not a multiple of any tile
+        for m in (1, 2, 3, 257, 1031):
+            n = 1 + (m * 7) % w.nA
+            dX, _ = ctx.velocity(N.TC_VERTEX, w.xV[:m % w.nV + 1], w.xA[:n], w.zetaA[:n], w.areaA[:n])
+            ref = O.passive_rhs(w.xV[:m % w.nV + 1], w.xA[:n], w.zetaA[:n], w.areaA[:n])
+            assert rel_err(dX, ref) <= (FP64_TOL if ctx is ctx64 else FP32C_TOL)
+
+
+def test_off_sphere_points(ctx64, ctx32):
+    """RK4 drifts particles off the unit sphere; both paths keep the reference's 1 - x.y."""
+    w = configs.rh4(level=3, parity=True)
+    rng = np.random.default_rng(1)
+    xA = w.xA * (1.0 + 1e-6 * rng.standard_normal((w.nA, 1)))
+    xV = w.xV * (1.0 + 1e-6 * rng.standard_normal((w.nV, 1)))
+    ref = O.passive_rhs(xV, xA, w.zetaA, w.areaA)
+    for ctx, tol in ((ctx64, FP64_TOL), (ctx32, FP32C_TOL)):
+        setup(ctx, w.omega, w.deltas)
+        dX, _ = ctx.velocity(N.TC_VERTEX, xV, xA, w.zetaA, w.areaA)
+        assert rel_err(dX, ref) <= tol
+
+
+def test_deterministic(ctx64, ctx32):
+    w = configs.gaussian(level=5, delta=0.01)
+    for ctx in (ctx64, ctx32):
+        setup(ctx, w.omega, w.deltas)
+        a, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+        b, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+        np.testing.assert_array_equal(a, b)
+
+
+def test_errors_are_reported_not_raised_on_device(ctx64):
+    w = configs.rh4(level=1, parity=True)
+    bad = w.zetaA.copy()
+    bad[3] = np.nan
+    with pytest.raises(N.TcError) as e:
+        ctx64.velocity(N.TC_ACTIVE, None, w.xA, bad, w.areaA)
+    assert e.value.status == N.TC_ERR_NONFINITE
+    with pytest.raises(N.TcError) as e:
+        ctx64.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA, 0, w.nA + 1)
+    assert e.value.status == N.TC_ERR_ARG
+    with pytest.raises(N.TcError) as e:
+        ctx64.velocity(7, w.xV, w.xA, w.zetaA, w.areaA)
+    assert e.value.status == N.TC_ERR_ARG
+    # the context stays usable after each refused call
+    dX, _ = ctx64.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    assert np.all(np.isfinite(dX))

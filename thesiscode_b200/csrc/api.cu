@@ -1,0 +1,524 @@
+// C ABI of libthesiscode_b200: context, parameters, the one-call velocity
+// sums and the device-resident RK4 driver.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "tc_ctx.h"
+
+using tcb::DevBuf;
+using tcb::SegDesc;
+
+namespace {
+
+bool valid_class(int c) { return c == TC_ACTIVE || c == TC_VERTEX || c == TC_PASSIVE; }
+
+int check_finite_host(const double* p, size_t n, const char* what) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) {
+      tc_record_error("non-finite value in %s at index %zu", what, i);
+      return TC_ERR_NONFINITE;
+    }
+  return TC_OK;
+}
+
+int begin(tc_ctx* ctx) {
+  if (!ctx) {
+    tc_record_error("null context");
+    return TC_ERR_ARG;
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+    tc_record_error("cudaSetDevice(%d) failed", ctx->device);
+    return TC_ERR_CUDA;
+  }
+  return TC_OK;
+}
+
+// Shared validation of one velocity call (the size checks of
+// PanelVelocityParallel.f90:1299-1315 / :1348-1361 / :1387-1400, returned
+// as TC_ERR_ARG instead of printed).
+int check_velocity_args(int cls, const double* X, int m, const double* src_x, const double* vort,
+                        const double* area, int n, int i0, int i1, const double* dX) {
+  if (!valid_class(cls)) {
+    tc_record_error("target_class %d is not TC_ACTIVE/TC_VERTEX/TC_PASSIVE", cls);
+    return TC_ERR_ARG;
+  }
+  if (m < 0 || n < 0) {
+    tc_record_error("negative size (m=%d, n=%d)", m, n);
+    return TC_ERR_ARG;
+  }
+  if (cls == TC_ACTIVE && (X != nullptr && X != src_x)) {
+    tc_record_error("TC_ACTIVE targets are the sources: pass X = NULL or X = src_x");
+    return TC_ERR_ARG;
+  }
+  if (cls == TC_ACTIVE && m != n) {
+    tc_record_error("TC_ACTIVE: size mismatch m=%d n=%d", m, n);
+    return TC_ERR_ARG;
+  }
+  if (i0 < 0 || i1 < i0 || i1 > m) {
+    tc_record_error("target range [%d,%d) outside [0,%d)", i0, i1, m);
+    return TC_ERR_ARG;
+  }
+  if ((n > 0 && (!src_x || !vort || !area)) || (m > 0 && !dX) ||
+      (cls != TC_ACTIVE && m > 0 && !X)) {
+    tc_record_error("null array argument");
+    return TC_ERR_ARG;
+  }
+  return TC_OK;
+}
+
+// Device part shared by the host and device entry points.
+int velocity_device(tc_ctx* ctx, int cls, const double* X, int m, const double* src_x,
+                    const double* vort, const double* area, int n, int i0, int i1, double* dX,
+                    double* dVort) {
+  if (cls == TC_ACTIVE) X = src_x;
+  int rc = ctx->scratch[0].ensure((size_t)std::max(n, 1) * sizeof(double4));
+  if (rc) return rc;
+  double4* src = ctx->scratch[0].as<double4>();
+  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
+  SegDesc seg{X, i0, i1, 0, cls == TC_ACTIVE ? 0 : tcb::kNoSelf, ctx->delta[cls] * ctx->delta[cls]};
+  int nch = 0;
+  if ((rc = tcb::launch_pairs(ctx, &seg, 1, src, n, m, &nch))) return rc;
+  return tcb::launch_velocity_epilogue(ctx, X, m, i0, i1, 0, m, nch, dX,
+                                       cls == TC_ACTIVE ? dVort : nullptr);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+extern "C" int tc_create(int device, int precision, tc_ctx** out) {
+  if (!out) return TC_ERR_ARG;
+  *out = nullptr;
+  if (precision != TC_FP64 && precision != TC_FP32C) {
+    tc_record_error("precision %d is not TC_FP64/TC_FP32C", precision);
+    return TC_ERR_ARG;
+  }
+  int rc = tc_set_device_checked(device);
+  if (rc) {
+    tc_record_error("device %d is not available", device);
+    return rc;
+  }
+  tc_ctx* ctx = new (std::nothrow) tc_ctx();
+  if (!ctx) return TC_ERR_NOMEM;
+  ctx->device = device;
+  ctx->precision = precision;
+  if ((rc = tcb::resolve_slots(ctx))) {
+    delete ctx;
+    return rc;
+  }
+  *out = ctx;
+  return TC_OK;
+}
+
+extern "C" int tc_destroy(tc_ctx* ctx) {
+  if (!ctx) return TC_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->partial.release();
+  for (auto& b : ctx->scratch) b.release();
+  tcb::Rk4State& R = ctx->rk;
+  DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV, &R.xiQ,
+                    &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke, &R.keBlocks, &R.totalKE};
+  for (DevBuf* b : bufs) b->release();
+  for (cudaEvent_t e : ctx->pair_events) cudaEventDestroy(e);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TC_OK;
+}
+
+extern "C" int tc_set_stream(tc_ctx* ctx, void* stream) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->own_stream = false;
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  return TC_OK;
+}
+
+extern "C" int tc_synchronize(tc_ctx* ctx) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+extern "C" int tc_set_precision(tc_ctx* ctx, int precision) {
+  if (!ctx) return TC_ERR_ARG;
+  if (precision != TC_FP64 && precision != TC_FP32C) return TC_ERR_ARG;
+  ctx->precision = precision;
+  return TC_OK;
+}
+
+extern "C" int tc_get_precision(tc_ctx* ctx, int* precision) {
+  if (!ctx || !precision) return TC_ERR_ARG;
+  *precision = ctx->precision;
+  return TC_OK;
+}
+
+extern "C" int tc_set_omega(tc_ctx* ctx, double omega) {
+  if (!ctx || !std::isfinite(omega)) return TC_ERR_ARG;
+  ctx->omega = omega;
+  return TC_OK;
+}
+
+extern "C" int tc_get_omega(tc_ctx* ctx, double* omega) {
+  if (!ctx || !omega) return TC_ERR_ARG;
+  *omega = ctx->omega;
+  return TC_OK;
+}
+
+extern "C" int tc_set_smooth(tc_ctx* ctx, double smooth) {
+  if (!ctx || !std::isfinite(smooth)) return TC_ERR_ARG;
+  ctx->delta[TC_PASSIVE] = smooth;
+  return TC_OK;
+}
+
+extern "C" int tc_get_smooth(tc_ctx* ctx, double* smooth) {
+  if (!ctx || !smooth) return TC_ERR_ARG;
+  *smooth = ctx->delta[TC_PASSIVE];
+  return TC_OK;
+}
+
+extern "C" int tc_set_deltas(tc_ctx* ctx, double delta_active, double delta_vertex,
+                             double delta_passive) {
+  if (!ctx || !std::isfinite(delta_active) || !std::isfinite(delta_vertex) ||
+      !std::isfinite(delta_passive))
+    return TC_ERR_ARG;
+  ctx->delta[TC_ACTIVE] = delta_active;
+  ctx->delta[TC_VERTEX] = delta_vertex;
+  ctx->delta[TC_PASSIVE] = delta_passive;
+  return TC_OK;
+}
+
+extern "C" int tc_get_deltas(tc_ctx* ctx, double* delta3) {
+  if (!ctx || !delta3) return TC_ERR_ARG;
+  for (int c = 0; c < 3; ++c) delta3[c] = ctx->delta[c];
+  return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// One velocity sum
+// ---------------------------------------------------------------------------
+extern "C" int tc_bs_velocity_device(tc_ctx* ctx, int target_class, const double* X, int m,
+                                     const double* src_x, const double* vort, const double* area,
+                                     int n, int i0, int i1, double* dX, double* dVort) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if ((rc = check_velocity_args(target_class, X, m, src_x, vort, area, n, i0, i1, dX))) return rc;
+  return velocity_device(ctx, target_class, X, m, src_x, vort, area, n, i0, i1, dX, dVort);
+}
+
+extern "C" int tc_bs_velocity(tc_ctx* ctx, int target_class, const double* X, int m,
+                              const double* src_x, const double* vort, const double* area, int n,
+                              int i0, int i1, double* dX, double* dVort) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if ((rc = check_velocity_args(target_class, X, m, src_x, vort, area, n, i0, i1, dX))) return rc;
+  if ((rc = check_finite_host(src_x, 3 * (size_t)n, "src_x")) ||
+      (rc = check_finite_host(vort, (size_t)n, "vort")) ||
+      (rc = check_finite_host(area, (size_t)n, "area")))
+    return rc;
+  if (target_class != TC_ACTIVE && (rc = check_finite_host(X, 3 * (size_t)m, "X"))) return rc;
+  const size_t nb = (size_t)std::max(n, 1) * sizeof(double);
+  const size_t mb = (size_t)std::max(m, 1) * sizeof(double);
+  if ((rc = ctx->scratch[1].ensure(3 * nb + 2 * nb)) || (rc = ctx->scratch[2].ensure(3 * mb)) ||
+      (rc = ctx->scratch[3].ensure(4 * mb)))
+    return rc;
+  double* d_src = ctx->scratch[1].as<double>();
+  double* d_vort = d_src + 3 * (size_t)std::max(n, 1);
+  double* d_area = d_vort + (size_t)std::max(n, 1);
+  double* d_X = ctx->scratch[2].as<double>();
+  double* d_dX = ctx->scratch[3].as<double>();
+  double* d_dV = d_dX + 3 * (size_t)std::max(m, 1);
+  cudaStream_t s = ctx->stream;
+  TC_CUDA_TRY(cudaMemcpyAsync(d_src, src_x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(d_vort, vort, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(d_area, area, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (target_class != TC_ACTIVE)
+    TC_CUDA_TRY(cudaMemcpyAsync(d_X, X, 3 * (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
+  rc = velocity_device(ctx, target_class, target_class == TC_ACTIVE ? nullptr : d_X, m, d_src,
+                       d_vort, d_area, n, i0, i1, d_dX, d_dV);
+  if (rc) return rc;
+  TC_CUDA_TRY(cudaMemcpyAsync(dX, d_dX, 3 * (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (target_class == TC_ACTIVE && dVort)
+    TC_CUDA_TRY(cudaMemcpyAsync(dVort, d_dV, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_finite_host(dX, 3 * (size_t)m, "dX (result)");
+}
+
+// ---------------------------------------------------------------------------
+// RK4 driver (BVERK4, PanelVelocityParallel.f90:435-658)
+// ---------------------------------------------------------------------------
+namespace {
+
+int rk4_alloc(tc_ctx* ctx, int nA, int nV, int nQ) {
+  tcb::Rk4State& R = ctx->rk;
+  const size_t a = (size_t)std::max(nA, 1), v = (size_t)std::max(nV, 1),
+               q = (size_t)std::max(nQ, 1), D = sizeof(double);
+  int rc;
+  if ((rc = R.x0A.ensure(3 * a * D)) || (rc = R.z0.ensure(a * D)) || (rc = R.areaA.ensure(a * D)) ||
+      (rc = R.x0V.ensure(3 * v * D)) || (rc = R.x0Q.ensure(3 * q * D)) ||
+      (rc = R.xiA.ensure(3 * a * D)) || (rc = R.ziA.ensure(a * D)) ||
+      (rc = R.xiV.ensure(3 * v * D)) || (rc = R.xiQ.ensure(3 * q * D)) ||
+      (rc = R.newA.ensure(3 * a * D)) || (rc = R.newZ.ensure(a * D)) ||
+      (rc = R.newV.ensure(3 * v * D)) || (rc = R.newQ.ensure(3 * q * D)) ||
+      (rc = R.src.ensure(a * sizeof(double4))) || (rc = R.ke.ensure(a * D)))
+    return rc;
+  R.nA = nA;
+  R.nV = nV;
+  R.nQ = nQ;
+  return TC_OK;
+}
+
+int check_rk4_sizes(int nA, int nV, int nQ) {
+  if (nA < 0 || nV < 0 || nQ < 0) {
+    tc_record_error("negative size (nA=%d, nV=%d, nQ=%d)", nA, nV, nQ);
+    return TC_ERR_ARG;
+  }
+  return TC_OK;
+}
+
+}  // namespace
+
+extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
+                           const double* areaA, int nA, const double* xV, int nV,
+                           const double* xQ, int nQ, int on_device) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if ((rc = check_rk4_sizes(nA, nV, nQ))) return rc;
+  if ((nA && (!xA || !zetaA || !areaA)) || (nV && !xV) || (nQ && !xQ)) {
+    tc_record_error("tc_rk4_load: null array argument");
+    return TC_ERR_ARG;
+  }
+  if (!on_device) {
+    if ((rc = check_finite_host(xA, 3 * (size_t)nA, "xA")) ||
+        (rc = check_finite_host(zetaA, (size_t)nA, "zetaA")) ||
+        (rc = check_finite_host(areaA, (size_t)nA, "areaA")) ||
+        (rc = check_finite_host(xV, 3 * (size_t)nV, "xV")) ||
+        (rc = check_finite_host(xQ, 3 * (size_t)nQ, "xQ")))
+      return rc;
+  }
+  if ((rc = rk4_alloc(ctx, nA, nV, nQ))) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const size_t D = sizeof(double);
+  cudaStream_t s = ctx->stream;
+  if (nA) {
+    TC_CUDA_TRY(cudaMemcpyAsync(R.x0A.ptr, xA, 3 * (size_t)nA * D, kind, s));
+    TC_CUDA_TRY(cudaMemcpyAsync(R.z0.ptr, zetaA, (size_t)nA * D, kind, s));
+    TC_CUDA_TRY(cudaMemcpyAsync(R.areaA.ptr, areaA, (size_t)nA * D, kind, s));
+  }
+  if (nV) TC_CUDA_TRY(cudaMemcpyAsync(R.x0V.ptr, xV, 3 * (size_t)nV * D, kind, s));
+  if (nQ) TC_CUDA_TRY(cudaMemcpyAsync(R.x0Q.ptr, xQ, 3 * (size_t)nQ * D, kind, s));
+  R.ready = true;
+  return TC_OK;
+}
+
+extern "C" int tc_rk4_store(tc_ctx* ctx, double* xA, double* zetaA, double* xV, double* xQ,
+                            double* kineticEnergy, int on_device) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  if (!R.ready) {
+    tc_record_error("tc_rk4_store: no RK4 state loaded");
+    return TC_ERR_STATE;
+  }
+  cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t D = sizeof(double);
+  cudaStream_t s = ctx->stream;
+  if (xA && R.nA) TC_CUDA_TRY(cudaMemcpyAsync(xA, R.x0A.ptr, 3 * (size_t)R.nA * D, kind, s));
+  if (zetaA && R.nA) TC_CUDA_TRY(cudaMemcpyAsync(zetaA, R.z0.ptr, (size_t)R.nA * D, kind, s));
+  if (xV && R.nV) TC_CUDA_TRY(cudaMemcpyAsync(xV, R.x0V.ptr, 3 * (size_t)R.nV * D, kind, s));
+  if (xQ && R.nQ) TC_CUDA_TRY(cudaMemcpyAsync(xQ, R.x0Q.ptr, 3 * (size_t)R.nQ * D, kind, s));
+  if (kineticEnergy && R.nA)
+    TC_CUDA_TRY(cudaMemcpyAsync(kineticEnergy, R.ke.ptr, (size_t)R.nA * D, kind, s));
+  if (!on_device) TC_CUDA_TRY(cudaStreamSynchronize(s));
+  return TC_OK;
+}
+
+// One RK4 stage over the given target ranges: the pair sums of all three
+// classes in one launch, then the fused stage epilogue. Sources must be
+// packed in ctx->rk.src (all nA rows) before the call; the epilogue writes
+// the rows [a0,a1) of the next stage's packed sources.
+extern "C" int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int a1, int v0,
+                                  int v1, int q0, int q1, double* total_ke_device) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  if (!R.ready) {
+    tc_record_error("tc_rk4_stage_range: no RK4 state loaded");
+    return TC_ERR_STATE;
+  }
+  if (stage < 0 || stage > 3 || a0 < 0 || a1 < a0 || a1 > R.nA || v0 < 0 || v1 < v0 ||
+      v1 > R.nV || q0 < 0 || q1 < q0 || q1 > R.nQ || !std::isfinite(dt)) {
+    tc_record_error("tc_rk4_stage_range: bad stage or range");
+    return TC_ERR_ARG;
+  }
+  const bool first = stage == 0;
+  SegDesc segs[3] = {
+      {first ? R.x0A.as<double>() : R.xiA.as<double>(), a0, a1, 0, 0,
+       ctx->delta[0] * ctx->delta[0]},
+      {first ? R.x0V.as<double>() : R.xiV.as<double>(), v0, v1, R.nA, tcb::kNoSelf,
+       ctx->delta[1] * ctx->delta[1]},
+      {first ? R.x0Q.as<double>() : R.xiQ.as<double>(), q0, q1, R.nA + R.nV, tcb::kNoSelf,
+       ctx->delta[2] * ctx->delta[2]}};
+  int nch = 0;
+  const int n_out = R.nA + R.nV + R.nQ;
+  if ((rc = tcb::launch_pairs(ctx, segs, 3, R.src.as<double4>(), R.nA, n_out, &nch))) return rc;
+  const int range[6] = {a0, a1, v0, v1, q0, q1};
+  return tcb::launch_stage_epilogue(ctx, stage, dt, range, nch, total_ke_device);
+}
+
+// Packs the sources of stage 1 from the loaded state (x0A, z0, areaA).
+extern "C" int tc_rk4_pack_sources(tc_ctx* ctx) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  if (!R.ready) return TC_ERR_STATE;
+  return tcb::launch_pack(ctx, R.x0A.as<double>(), R.z0.as<double>(), R.areaA.as<double>(), R.nA,
+                          R.src.as<double4>());
+}
+
+extern "C" int tc_rk4_device_buffer(tc_ctx* ctx, int which, void** ptr) {
+  if (!ctx || !ptr) return TC_ERR_ARG;
+  tcb::Rk4State& R = ctx->rk;
+  switch (which) {
+    case TC_BUF_SOURCES: *ptr = R.src.ptr; break;
+    case TC_BUF_XA: *ptr = R.x0A.ptr; break;
+    case TC_BUF_ZETA: *ptr = R.z0.ptr; break;
+    case TC_BUF_XV: *ptr = R.x0V.ptr; break;
+    case TC_BUF_XQ: *ptr = R.x0Q.ptr; break;
+    case TC_BUF_KE: *ptr = R.ke.ptr; break;
+    default: return TC_ERR_ARG;
+  }
+  return R.ready ? TC_OK : TC_ERR_STATE;
+}
+
+// Copy rows [row0, row0+nrows) of one RK4 device buffer to (to_buffer = 0)
+// or from (to_buffer = 1) device memory at `ptr`, on the context's stream.
+// Row sizes: TC_BUF_SOURCES 4 doubles, TC_BUF_XA/XV/XQ 3, TC_BUF_ZETA/KE 1.
+extern "C" int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr,
+                                int to_buffer) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  if (!R.ready) return TC_ERR_STATE;
+  void* base = nullptr;
+  int width = 0, rows = 0;
+  switch (which) {
+    case TC_BUF_SOURCES: base = R.src.ptr; width = 4; rows = R.nA; break;
+    case TC_BUF_XA: base = R.x0A.ptr; width = 3; rows = R.nA; break;
+    case TC_BUF_ZETA: base = R.z0.ptr; width = 1; rows = R.nA; break;
+    case TC_BUF_XV: base = R.x0V.ptr; width = 3; rows = R.nV; break;
+    case TC_BUF_XQ: base = R.x0Q.ptr; width = 3; rows = R.nQ; break;
+    case TC_BUF_KE: base = R.ke.ptr; width = 1; rows = R.nA; break;
+    default: return TC_ERR_ARG;
+  }
+  if (row0 < 0 || nrows < 0 || row0 + nrows > rows || (nrows > 0 && !ptr)) {
+    tc_record_error("tc_rk4_copy_rows: rows [%d,%d) outside [0,%d)", row0, row0 + nrows, rows);
+    return TC_ERR_ARG;
+  }
+  if (nrows == 0) return TC_OK;
+  char* b = static_cast<char*>(base) + (size_t)row0 * width * sizeof(double);
+  size_t bytes = (size_t)nrows * width * sizeof(double);
+  TC_CUDA_TRY(cudaMemcpyAsync(to_buffer ? b : ptr, to_buffer ? ptr : b, bytes,
+                              cudaMemcpyDeviceToDevice, ctx->stream));
+  return TC_OK;
+}
+
+extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalKE) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  if (!R.ready) {
+    tc_record_error("tc_rk4_advance: no RK4 state loaded");
+    return TC_ERR_STATE;
+  }
+  if (nsteps < 0 || !std::isfinite(dt)) return TC_ERR_ARG;
+  if ((rc = R.totalKE.ensure((size_t)std::max(nsteps, 1) * sizeof(double)))) return rc;
+  if ((rc = tc_rk4_pack_sources(ctx))) return rc;
+  for (int step = 0; step < nsteps; ++step)
+    for (int s = 0; s < 4; ++s)
+      if ((rc = tc_rk4_stage_range(ctx, s, dt, 0, R.nA, 0, R.nV, 0, R.nQ,
+                                   s == 0 ? R.totalKE.as<double>() + step : nullptr)))
+        return rc;
+  if (totalKE && nsteps > 0) {
+    TC_CUDA_TRY(cudaMemcpyAsync(totalKE, R.totalKE.ptr, (size_t)nsteps * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  return TC_OK;
+}
+
+// The drop-in BVERK4 call on host arrays: load, nsteps fused steps on the
+// device, store back.
+extern "C" int tc_rk4_step(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int nA,
+                           double* xV, int nV, double* xQ, int nQ, double dt, int nsteps,
+                           double* totalKE, double* kineticEnergy) {
+  int rc = tc_rk4_load(ctx, xA, zetaA, areaA, nA, xV, nV, xQ, nQ, 0);
+  if (rc) return rc;
+  if ((rc = tc_rk4_advance(ctx, dt, nsteps, totalKE))) return rc;
+  if ((rc = tc_rk4_store(ctx, xA, zetaA, xV, xQ, kineticEnergy, 0))) return rc;
+  if ((rc = check_finite_host(xA, 3 * (size_t)nA, "xA (result)"))) return rc;
+  return check_finite_host(zetaA, (size_t)nA, "zetaA (result)");
+}
+
+extern "C" int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA,
+                                  int nA, double* xV, int nV, double* xQ, int nQ, double dt,
+                                  int nsteps, double* totalKE, double* kineticEnergy) {
+  int rc = tc_rk4_load(ctx, xA, zetaA, areaA, nA, xV, nV, xQ, nQ, 1);
+  if (rc) return rc;
+  if ((rc = tc_rk4_advance(ctx, dt, nsteps, totalKE))) return rc;
+  return tc_rk4_store(ctx, xA, zetaA, xV, xQ, kineticEnergy, 1);
+}
+
+// Instrumentation: kernels launched by this context, pair-kernel launches and
+// pair interactions evaluated since the last reset, and (when enabled) the
+// summed CUDA-event time of the pair kernels on the context's stream.
+extern "C" int tc_stats_enable_timing(tc_ctx* ctx, int on) {
+  if (!ctx) return TC_ERR_ARG;
+  ctx->time_pairs = on != 0;
+  return TC_OK;
+}
+
+extern "C" int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* pair_launches,
+                        long long* pair_interactions, double* pair_ms) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!ctx->pair_events.empty()) {
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (size_t j = 0; j + 1 < ctx->pair_events.size(); j += 2) {
+      float ms = 0.f;
+      TC_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->pair_events[j], ctx->pair_events[j + 1]));
+      ctx->pair_ms += ms;
+    }
+    for (cudaEvent_t e : ctx->pair_events) cudaEventDestroy(e);
+    ctx->pair_events.clear();
+  }
+  if (launches) *launches = ctx->launches;
+  if (pair_launches) *pair_launches = ctx->pair_launches;
+  if (pair_interactions) *pair_interactions = ctx->pair_interactions;
+  if (pair_ms) *pair_ms = ctx->pair_ms;
+  if (reset) {
+    ctx->launches = ctx->pair_launches = ctx->pair_interactions = 0;
+    ctx->pair_ms = 0.0;
+  }
+  return TC_OK;
+}
+
+extern "C" int tc_reset_rk4(tc_ctx* ctx) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStreamSynchronize(ctx->stream);
+  tcb::Rk4State& R = ctx->rk;
+  DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV, &R.xiQ,
+                    &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke, &R.keBlocks, &R.totalKE};
+  for (DevBuf* b : bufs) b->release();
+  ctx->partial.release();
+  R.ready = false;
+  R.nA = R.nV = R.nQ = 0;
+  return TC_OK;
+}

@@ -1,0 +1,326 @@
+// Device side of the direct spherical Biot-Savart sum.
+//
+// One interaction (target x_i, source x_k with circulation G_k = zeta_k A_k):
+//     w_ik = G_k / (1 - x_i.x_k + delta^2)
+//     u_i  = -1/(4 pi) * x_i  x  sum_k w_ik (x_k - x_i)
+// which equals the reference's sum_k (x_i x x_k) w_ik (BVEActiveRHS,
+// PanelVelocityParallel.f90:1316-1333) because x_i x x_i = 0; the cross
+// product is taken once per target instead of once per pair.
+//
+// Work decomposition: blockIdx.x = a tile of TB consecutive targets (one of
+// up to three target classes), blockIdx.y = a chunk of consecutive sources.
+// Each CTA streams its source chunk through shared memory in tiles of TS and
+// writes one FP64 partial sum per target and chunk; the stage epilogue adds
+// the chunks in a fixed order, so results are deterministic.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace tcb {
+
+constexpr int kNoSelf = INT32_MIN;
+
+struct TargetSeg {
+  const double* x;  // targets, x[3*i + c]
+  int i0, i1;       // target range [i0, i1) computed by this launch
+  int out_offset;   // partial row of target i is out_offset + i
+  int self_offset;  // source index of target i is i + self_offset (ACTIVE), else kNoSelf
+  double d2;        // delta^2 for this class
+  int tile_begin;   // first blockIdx.x of this segment
+};
+
+struct PairLaunch {
+  TargetSeg seg[3];
+  int nseg;
+  const double4* src;   // packed sources {x, y, z, G}
+  int n;                // number of sources
+  int chunk_len;        // sources per blockIdx.y chunk (multiple of the tile)
+  double* partial;      // partial[(chunk*3 + c)*n_out + row]
+  int n_out;
+};
+
+// ---------------------------------------------------------------------------
+// Reciprocals. The hardware seed (rcp.approx) is refined by Newton-Raphson
+// r <- r + r(1 - d r); two steps take an FP64 seed to full precision. This
+// replaces the IEEE division of the reference (a ~14-DFMA sequence on this
+// GPU) by 4 DFMA; the result is within an ulp of 1/d.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rcp_seed_f64(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  return r;
+}
+
+__device__ __forceinline__ double rcp_newton2(double d) {
+  double r = rcp_seed_f64(d);
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
+__device__ __forceinline__ float rcp_approx_f32(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  return r;
+}
+
+__device__ __forceinline__ const TargetSeg& find_seg(const PairLaunch& P, int tile) {
+  int s = 0;
+  if (P.nseg > 1 && tile >= P.seg[1].tile_begin) s = 1;
+  if (P.nseg > 2 && tile >= P.seg[2].tile_begin) s = 2;
+  return P.seg[s];
+}
+
+// ---------------------------------------------------------------------------
+// FP64 pair kernel. The denominator is rounded exactly as the reference's
+// 1.0 - sum(pointVorts(:,k)*pointVorts(:,j)) [+ smooth*smooth]: three
+// separately rounded products, left-to-right additions, no contraction.
+// ---------------------------------------------------------------------------
+template <int NT, int TPT, int TS>
+__global__ void __launch_bounds__(NT) pair_fp64_kernel(const PairLaunch P) {
+  __shared__ double4 sm[TS];
+  constexpr int TB = NT * TPT;
+  const TargetSeg& G = find_seg(P, blockIdx.x);
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
+  const int i_end = G.i1;
+  const double d2 = G.d2;
+  const bool has_self = G.self_offset != kNoSelf;
+
+  double xi[TPT][3], acc[TPT][3];
+  int self_k[TPT];
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    int i = tile0 + (int)threadIdx.x + t * NT;
+    int ld = i < i_end ? i : tile0;
+    xi[t][0] = G.x[3 * (size_t)ld];
+    xi[t][1] = G.x[3 * (size_t)ld + 1];
+    xi[t][2] = G.x[3 * (size_t)ld + 2];
+    acc[t][0] = acc[t][1] = acc[t][2] = 0.0;
+    self_k[t] = has_self ? i + G.self_offset : -1;
+  }
+  const int self_lo = has_self ? tile0 + G.self_offset : 0;
+  const int self_hi = has_self ? min(tile0 + TB, i_end) + G.self_offset : 0;
+
+  const int c0 = (int)blockIdx.y * P.chunk_len;
+  const int c1 = min(P.n, c0 + P.chunk_len);
+  for (int ts = c0; ts < c1; ts += TS) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < TS; j += NT) {
+      int k = ts + j;
+      sm[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+    __syncthreads();
+    const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
+    if (!diag) {
+#pragma unroll 2
+      for (int j = 0; j < TS; ++j) {
+        const double4 q = sm[j];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+          double s = __dmul_rn(q.x, xi[t][0]);
+          s = __dadd_rn(s, __dmul_rn(q.y, xi[t][1]));
+          s = __dadd_rn(s, __dmul_rn(q.z, xi[t][2]));
+          const double den = __dadd_rn(__dsub_rn(1.0, s), d2);
+          const double w = __dmul_rn(q.w, rcp_newton2(den));
+          acc[t][0] = fma(w, q.x - xi[t][0], acc[t][0]);
+          acc[t][1] = fma(w, q.y - xi[t][1], acc[t][1]);
+          acc[t][2] = fma(w, q.z - xi[t][2], acc[t][2]);
+        }
+      }
+    } else {
+      for (int j = 0; j < TS; ++j) {
+        const double4 q = sm[j];
+        const int k = ts + j;
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+          double s = __dmul_rn(q.x, xi[t][0]);
+          s = __dadd_rn(s, __dmul_rn(q.y, xi[t][1]));
+          s = __dadd_rn(s, __dmul_rn(q.z, xi[t][2]));
+          const double den = __dadd_rn(__dsub_rn(1.0, s), d2);
+          double w = __dmul_rn(q.w, rcp_newton2(den));
+          w = (k == self_k[t]) ? 0.0 : w;
+          acc[t][0] = fma(w, q.x - xi[t][0], acc[t][0]);
+          acc[t][1] = fma(w, q.y - xi[t][1], acc[t][1]);
+          acc[t][2] = fma(w, q.z - xi[t][2], acc[t][2]);
+        }
+      }
+    }
+  }
+  const size_t stride = (size_t)P.n_out;
+  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    int i = tile0 + (int)threadIdx.x + t * NT;
+    if (i < i_end) {
+      out[i] = acc[t][0];
+      out[stride + i] = acc[t][1];
+      out[2 * stride + i] = acc[t][2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32-compensated pair kernel.
+//
+// Each CTA takes the position c of the middle target of its tile as origin.
+// Sources are converted once per CTA and tile from FP64 to FP32 offsets
+// s_k = fl32(x_k - c) (their FP64 difference rounded once), targets likewise
+// t_i = fl32(x_i - c). For spatially coherent target tiles (the icosahedral
+// orderings are quad-tree orders) |s_k|, |t_i| are small for every nearby
+// pair, so d = s_k - t_i carries an absolute error of a few ulps of the tile
+// size instead of ulps of 1. The denominator uses the cancellation-free form
+//     2(1 - x_i.x_k) + 2 delta^2 = |x_k - x_i|^2 + e_i + e_k,
+//     e_i = 1 - |x_i|^2 + 2 delta^2,  e_k = 1 - |x_k|^2
+// (evaluated in FP64 while staging, then rounded to FP32)
+// so near pairs keep full FP32 relative accuracy. Two targets share each
+// f32x2 instruction (FADD2/FFMA2/FMUL2 halve the issue slots; the FP32 pipe
+// stays the bound). Per-target FP32 partial sums are added into FP64
+// accumulators every FLUSH sources.
+// ---------------------------------------------------------------------------
+template <int NT, int NPAIR, int TS, int FLUSH>
+__global__ void __launch_bounds__(NT) pair_fp32c_kernel(const PairLaunch P) {
+  static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
+  __shared__ float4 smA[TS];  // (sx, sx, sy, sy)
+  __shared__ float4 smB[TS];  // (sz, sz, 2G, 2G)
+  __shared__ float2 smC[TS];  // (e, e)
+  constexpr int TPT = 2 * NPAIR;
+  constexpr int TB = NT * TPT;
+  const TargetSeg& G = find_seg(P, blockIdx.x);
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
+  const int i_end = G.i1;
+  const bool has_self = G.self_offset != kNoSelf;
+
+  const int mid = min(tile0 + TB / 2, i_end - 1);
+  const double cx = G.x[3 * (size_t)mid], cy = G.x[3 * (size_t)mid + 1],
+               cz = G.x[3 * (size_t)mid + 2];
+
+  float2 ntx[NPAIR], nty[NPAIR], ntz[NPAIR], ei[NPAIR];
+  float2 fx[NPAIR], fy[NPAIR], fz[NPAIR];
+  double ax[NPAIR][2], ay[NPAIR][2], az[NPAIR][2];
+  int self_k[NPAIR][2];
+#pragma unroll
+  for (int p = 0; p < NPAIR; ++p) {
+    float tv[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int i = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
+      int ld = i < i_end ? i : mid;
+      double x = G.x[3 * (size_t)ld], y = G.x[3 * (size_t)ld + 1], z = G.x[3 * (size_t)ld + 2];
+      tv[h][0] = -(float)(x - cx);
+      tv[h][1] = -(float)(y - cy);
+      tv[h][2] = -(float)(z - cz);
+      tv[h][3] = (float)((1.0 - (x * x + y * y + z * z)) + 2.0 * G.d2);
+      self_k[p][h] = has_self ? i + G.self_offset : -1;
+      ax[p][h] = ay[p][h] = az[p][h] = 0.0;
+    }
+    ntx[p] = make_float2(tv[0][0], tv[1][0]);
+    nty[p] = make_float2(tv[0][1], tv[1][1]);
+    ntz[p] = make_float2(tv[0][2], tv[1][2]);
+    ei[p] = make_float2(tv[0][3], tv[1][3]);
+    fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+  }
+  const int self_lo = has_self ? tile0 + G.self_offset : 0;
+  const int self_hi = has_self ? min(tile0 + TB, i_end) + G.self_offset : 0;
+
+  const int c0 = (int)blockIdx.y * P.chunk_len;
+  const int c1 = min(P.n, c0 + P.chunk_len);
+  for (int ts = c0; ts < c1; ts += TS) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < TS; j += NT) {
+      int k = ts + j;
+      float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f;
+      if (k < c1) {
+        const double4 q = P.src[k];
+        sx = (float)(q.x - cx);
+        sy = (float)(q.y - cy);
+        sz = (float)(q.z - cz);
+        g = (float)(2.0 * q.w);
+        e = (float)(1.0 - (q.x * q.x + q.y * q.y + q.z * q.z));
+      }
+      smA[j] = make_float4(sx, sx, sy, sy);
+      smB[j] = make_float4(sz, sz, g, g);
+      smC[j] = make_float2(e, e);
+    }
+    __syncthreads();
+    const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
+    for (int jf = 0; jf < TS; jf += FLUSH) {
+      if (!diag) {
+#pragma unroll 4
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = smA[j];
+          const float4 b = smB[j];
+          const float2 ee = smC[j];
+          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
+          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
+#pragma unroll
+          for (int p = 0; p < NPAIR; ++p) {
+            const float2 dx = __fadd2_rn(sxx, ntx[p]);
+            const float2 dy = __fadd2_rn(syy, nty[p]);
+            const float2 dz = __fadd2_rn(szz, ntz[p]);
+            float2 D = __fadd2_rn(ee, ei[p]);
+            D = __ffma2_rn(dx, dx, D);
+            D = __ffma2_rn(dy, dy, D);
+            D = __ffma2_rn(dz, dz, D);
+            const float2 r = make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
+            const float2 w = __fmul2_rn(gg, r);
+            fx[p] = __ffma2_rn(w, dx, fx[p]);
+            fy[p] = __ffma2_rn(w, dy, fy[p]);
+            fz[p] = __ffma2_rn(w, dz, fz[p]);
+          }
+        }
+      } else {
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = smA[j];
+          const float4 b = smB[j];
+          const float2 ee = smC[j];
+          const int k = ts + j;
+          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
+          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
+#pragma unroll
+          for (int p = 0; p < NPAIR; ++p) {
+            const float2 dx = __fadd2_rn(sxx, ntx[p]);
+            const float2 dy = __fadd2_rn(syy, nty[p]);
+            const float2 dz = __fadd2_rn(szz, ntz[p]);
+            float2 D = __fadd2_rn(ee, ei[p]);
+            D = __ffma2_rn(dx, dx, D);
+            D = __ffma2_rn(dy, dy, D);
+            D = __ffma2_rn(dz, dz, D);
+            float2 w = __fmul2_rn(gg, make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y)));
+            w.x = (k == self_k[p][0]) ? 0.f : w.x;
+            w.y = (k == self_k[p][1]) ? 0.f : w.y;
+            fx[p] = __ffma2_rn(w, dx, fx[p]);
+            fy[p] = __ffma2_rn(w, dy, fy[p]);
+            fz[p] = __ffma2_rn(w, dz, fz[p]);
+          }
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < NPAIR; ++p) {
+        ax[p][0] += (double)fx[p].x;
+        ax[p][1] += (double)fx[p].y;
+        ay[p][0] += (double)fy[p].x;
+        ay[p][1] += (double)fy[p].y;
+        az[p][0] += (double)fz[p].x;
+        az[p][1] += (double)fz[p].y;
+        fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  const size_t stride = (size_t)P.n_out;
+  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+#pragma unroll
+  for (int p = 0; p < NPAIR; ++p) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int i = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
+      if (i < i_end) {
+        out[i] = ax[p][h];
+        out[stride + i] = ay[p][h];
+        out[2 * stride + i] = az[p][h];
+      }
+    }
+  }
+}
+
+}  // namespace tcb

@@ -1,0 +1,382 @@
+// Host-side launch logic for the pair kernels and the epilogues that turn
+// per-chunk partial sums into velocities and RK4 stage updates.
+#include <algorithm>
+#include <cmath>
+
+#include "tc_ctx.h"
+
+namespace tcb {
+
+// The reference's (-4.0_kreal*PI) (PanelVelocityParallel.f90:1332).
+__constant__ double kMinus4Pi = -4.0 * 3.141592653589793238462643383279502884;
+
+int DevBuf::ensure(size_t need) {
+  if (need <= bytes && ptr) return TC_OK;
+  release();
+  if (need == 0) need = 16;
+  cudaError_t e = cudaMalloc(&ptr, need);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    bytes = 0;
+    tc_record_error("cudaMalloc of %zu bytes failed: %s", need, cudaGetErrorString(e));
+    cudaGetLastError();
+    return TC_ERR_NOMEM;
+  }
+  bytes = need;
+  return TC_OK;
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel instances
+// ---------------------------------------------------------------------------
+constexpr int kNT64 = 256, kTPT64 = 2, kTS64 = 256;
+constexpr int kNT32 = 256, kNPAIR32 = 2, kTS32 = 256, kFLUSH32 = 64;
+
+int resolve_slots(tc_ctx* ctx) {
+  cudaDeviceProp prop;
+  TC_CUDA_TRY(cudaGetDeviceProperties(&prop, ctx->device));
+  ctx->num_sms = prop.multiProcessorCount;
+  int b64 = 0, b32 = 0;
+  TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &b64, pair_fp64_kernel<kNT64, kTPT64, kTS64>, kNT64, 0));
+  TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &b32, pair_fp32c_kernel<kNT32, kNPAIR32, kTS32, kFLUSH32>, kNT32, 0));
+  ctx->slots64 = std::max(1, b64) * ctx->num_sms;
+  ctx->slots32 = std::max(1, b32) * ctx->num_sms;
+  ctx->cfg64 = PairCfg{kNT64, kTPT64, kTS64};
+  ctx->cfg32 = PairCfg{kNT32, 2 * kNPAIR32, kTS32};
+  return TC_OK;
+}
+
+// Number of source chunks: the split that best fills the resident CTA slots
+// (waves of tiles x chunks), never cutting chunks below ctx->min_chunk.
+static int choose_chunks(int tiles, int n, int ts, int slots, int min_chunk, int max_chunks) {
+  int best = 1;
+  double best_eff = 0.0;
+  for (int s = 1; s <= max_chunks; ++s) {
+    int len = (n + s - 1) / s;
+    if (s > 1 && len < min_chunk) break;
+    long long items = (long long)tiles * s;
+    long long waves = (items + slots - 1) / slots;
+    double eff = (double)items / (double)(waves * slots);
+    if (eff > best_eff + 0.02) {
+      best_eff = eff;
+      best = s;
+    }
+    if (eff > 0.97) break;
+  }
+  (void)ts;
+  return best;
+}
+
+int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
+                 int n_out, int* nchunks) {
+  *nchunks = 0;
+  const bool fp64 = ctx->precision == TC_FP64;
+  const PairCfg& cfg = fp64 ? ctx->cfg64 : ctx->cfg32;
+  const int tb = cfg.tb();
+  PairLaunch P{};
+  int tiles = 0, k = 0;
+  for (int s = 0; s < nseg; ++s) {
+    int len = segs[s].i1 - segs[s].i0;
+    if (len <= 0) continue;
+    TargetSeg& g = P.seg[k++];
+    g.x = segs[s].x;
+    g.i0 = segs[s].i0;
+    g.i1 = segs[s].i1;
+    g.out_offset = segs[s].out_offset;
+    g.self_offset = segs[s].self_offset;
+    g.d2 = segs[s].d2;
+    g.tile_begin = tiles;
+    tiles += (len + tb - 1) / tb;
+  }
+  P.nseg = k;
+  if (tiles == 0 || n <= 0) return TC_OK;
+  const int slots = fp64 ? ctx->slots64 : ctx->slots32;
+  int S = choose_chunks(tiles, n, cfg.ts, slots, ctx->min_chunk, ctx->max_chunks);
+  int chunk_len = (n + S - 1) / S;
+  chunk_len = (chunk_len + cfg.ts - 1) / cfg.ts * cfg.ts;
+  S = (n + chunk_len - 1) / chunk_len;
+  int rc = ctx->partial.ensure((size_t)S * 3 * (size_t)n_out * sizeof(double));
+  if (rc) return rc;
+  P.src = src;
+  P.n = n;
+  P.chunk_len = chunk_len;
+  P.partial = ctx->partial.as<double>();
+  P.n_out = n_out;
+  dim3 grid(tiles, S);
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (ctx->time_pairs) {
+    TC_CUDA_TRY(cudaEventCreate(&ev[0]));
+    TC_CUDA_TRY(cudaEventCreate(&ev[1]));
+    TC_CUDA_TRY(cudaEventRecord(ev[0], ctx->stream));
+  }
+  if (fp64)
+    pair_fp64_kernel<kNT64, kTPT64, kTS64><<<grid, kNT64, 0, ctx->stream>>>(P);
+  else
+    pair_fp32c_kernel<kNT32, kNPAIR32, kTS32, kFLUSH32><<<grid, kNT32, 0, ctx->stream>>>(P);
+  TC_CUDA_TRY(cudaGetLastError());
+  if (ctx->time_pairs) {
+    TC_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));
+    ctx->pair_events.push_back(ev[0]);
+    ctx->pair_events.push_back(ev[1]);
+  }
+  ctx->launches += 1;
+  ctx->pair_launches += 1;
+  for (int s = 0; s < P.nseg; ++s)
+    ctx->pair_interactions += (long long)(P.seg[s].i1 - P.seg[s].i0) * n -
+                              (P.seg[s].self_offset != kNoSelf ? (P.seg[s].i1 - P.seg[s].i0) : 0);
+  *nchunks = S;
+  return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Packing: {x, y, z, zeta*area} per source.
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel(const double* __restrict__ x, const double* __restrict__ zeta,
+                            const double* __restrict__ area, int n, double4* __restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[k] = make_double4(x[3 * (size_t)k], x[3 * (size_t)k + 1], x[3 * (size_t)k + 2],
+                        __dmul_rn(zeta[k], area[k]));
+}
+
+int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* area, int n,
+                double4* out) {
+  if (n <= 0) return TC_OK;
+  pack_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(x, zeta, area, n, out);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Shared epilogue math.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reduce_row(const double* __restrict__ partial, int nchunks,
+                                           size_t n_out, size_t row, double T[3]) {
+  T[0] = T[1] = T[2] = 0.0;
+  for (int c = 0; c < nchunks; ++c) {
+    const double* p = partial + (size_t)c * 3 * n_out + row;
+    T[0] += p[0];
+    T[1] += p[n_out];
+    T[2] += p[2 * n_out];
+  }
+}
+
+// u = (x x T) / (-4 pi): the reference divides the summed dX by (-4 pi).
+__device__ __forceinline__ void velocity_from_sum(const double x[3], const double T[3],
+                                                  double u[3]) {
+  u[0] = (x[1] * T[2] - x[2] * T[1]) / kMinus4Pi;
+  u[1] = (x[2] * T[0] - x[0] * T[2]) / kMinus4Pi;
+  u[2] = (x[0] * T[1] - x[1] * T[0]) / kMinus4Pi;
+}
+
+__global__ void velocity_epilogue_kernel(const double* __restrict__ x, int m, int i0, int i1,
+                                         int row_offset, int n_out, int nchunks,
+                                         const double* __restrict__ partial, double m2omega,
+                                         double* __restrict__ dX, double* __restrict__ dVort) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double u[3] = {0.0, 0.0, 0.0};
+  if (i >= i0 && i < i1) {
+    double xi[3] = {x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2]};
+    double T[3];
+    reduce_row(partial, nchunks, (size_t)n_out, (size_t)(row_offset + i), T);
+    velocity_from_sum(xi, T, u);
+  }
+  dX[3 * (size_t)i] = u[0];
+  dX[3 * (size_t)i + 1] = u[1];
+  dX[3 * (size_t)i + 2] = u[2];
+  if (dVort) dVort[i] = m2omega * u[2];
+}
+
+int launch_velocity_epilogue(tc_ctx* ctx, const double* x, int m, int i0, int i1, int row_offset,
+                             int n_out, int nchunks, double* dX, double* dVort) {
+  if (m <= 0) return TC_OK;
+  velocity_epilogue_kernel<<<(m + 255) / 256, 256, 0, ctx->stream>>>(
+      x, m, i0, i1, row_offset, n_out, nchunks, ctx->partial.as<double>(), -2.0 * ctx->omega, dX,
+      dVort);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// RK4 stage epilogue (PanelVelocityParallel.f90:495-516, 545-558, 586-600,
+// 628-656) fused over the three target classes:
+//   k_s    = dt * u_s                         (:503-506)
+//   new   += k_s / 6 or / 3                   (:637-644, evaluated left to right)
+//   input  = x + {1/2, 1/2, 1} * k_s          (next stage's targets/sources)
+//   active: dzeta = (-2 Omega) * u_z, same update for zeta; sources repacked
+//   stage 1: kineticEnergy = u.u, per-block sums of KE*A (:495-501)
+//   stage 4: the state advances to `new`.
+// ---------------------------------------------------------------------------
+struct StageEpi {
+  int stage;
+  double dt, m2omega;
+  int nA, nV, nQ;
+  int a0, a1, v0, v1, q0, q1;
+  int n_out, nchunks;
+  const double* partial;
+  double *x0A, *z0, *x0V, *x0Q;
+  const double* areaA;
+  double *xiA, *ziA, *xiV, *xiQ;
+  double *newA, *newZ, *newV, *newQ;
+  double4* src;
+  double* ke;
+  double* keBlocks;
+};
+
+constexpr int kEpiThreads = 256;
+
+__global__ void __launch_bounds__(kEpiThreads) stage_epilogue_kernel(const StageEpi E) {
+  __shared__ double red[kEpiThreads];
+  const int lenA = E.a1 - E.a0, lenV = E.v1 - E.v0, lenQ = E.q1 - E.q0;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke_area = 0.0;
+  if (r < lenA + lenV + lenQ) {
+    int cls, i;
+    if (r < lenA) {
+      cls = 0;
+      i = E.a0 + r;
+    } else if (r < lenA + lenV) {
+      cls = 1;
+      i = E.v0 + (r - lenA);
+    } else {
+      cls = 2;
+      i = E.q0 + (r - lenA - lenV);
+    }
+    const int row = (cls == 0 ? 0 : cls == 1 ? E.nA : E.nA + E.nV) + i;
+    double* x0 = cls == 0 ? E.x0A : cls == 1 ? E.x0V : E.x0Q;
+    double* xi = cls == 0 ? E.xiA : cls == 1 ? E.xiV : E.xiQ;
+    double* nw = cls == 0 ? E.newA : cls == 1 ? E.newV : E.newQ;
+    const double* xin = E.stage == 0 ? x0 : xi;
+    const size_t b = 3 * (size_t)i;
+    double xs[3] = {xin[b], xin[b + 1], xin[b + 2]};
+    double T[3], u[3];
+    reduce_row(E.partial, E.nchunks, (size_t)E.n_out, (size_t)row, T);
+    velocity_from_sum(xs, T, u);
+    if (cls == 0 && E.stage == 0) {
+      double k2 = __dadd_rn(__dadd_rn(__dmul_rn(u[0], u[0]), __dmul_rn(u[1], u[1])),
+                            __dmul_rn(u[2], u[2]));
+      E.ke[i] = k2;
+      ke_area = k2 * E.areaA[i];
+    }
+    const double div = (E.stage == 0 || E.stage == 3) ? 6.0 : 3.0;
+    const double cnext = E.stage == 2 ? 1.0 : 0.5;
+    double xnext[3];
+    for (int c = 0; c < 3; ++c) {
+      double kc = __dmul_rn(E.dt, u[c]);  // rounded like the reference's dt*stage
+      double base = E.stage == 0 ? x0[b + c] : nw[b + c];
+      double nv = base + kc / div;
+      if (E.stage < 3) {
+        nw[b + c] = nv;
+        xnext[c] = x0[b + c] + (E.stage == 2 ? kc : cnext * kc);
+        xi[b + c] = xnext[c];
+      } else {
+        x0[b + c] = nv;
+        xnext[c] = nv;
+      }
+    }
+    if (cls == 0) {
+      double kz = __dmul_rn(E.dt, __dmul_rn(E.m2omega, u[2]));
+      double zbase = E.stage == 0 ? E.z0[i] : E.newZ[i];
+      double zn = zbase + kz / div;
+      double znext;
+      if (E.stage < 3) {
+        E.newZ[i] = zn;
+        znext = E.z0[i] + (E.stage == 2 ? kz : cnext * kz);
+        E.ziA[i] = znext;
+      } else {
+        E.z0[i] = zn;
+        znext = zn;
+      }
+      E.src[i] = make_double4(xnext[0], xnext[1], xnext[2], znext * E.areaA[i]);
+    }
+  }
+  if (E.stage == 0) {
+    red[threadIdx.x] = ke_area;
+    __syncthreads();
+    for (int s = kEpiThreads / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) E.keBlocks[blockIdx.x] = red[0];
+  }
+}
+
+__global__ void ke_finalize_kernel(const double* __restrict__ blocks, int nblocks,
+                                   double* __restrict__ out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int j = threadIdx.x; j < nblocks; j += 256) s += blocks[j];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = 0.5 * red[0];
+}
+
+int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
+                          double* total_ke) {
+  Rk4State& R = ctx->rk;
+  StageEpi E;
+  E.stage = stage;
+  E.dt = dt;
+  E.m2omega = -2.0 * ctx->omega;
+  E.nA = R.nA;
+  E.nV = R.nV;
+  E.nQ = R.nQ;
+  E.a0 = range[0];
+  E.a1 = range[1];
+  E.v0 = range[2];
+  E.v1 = range[3];
+  E.q0 = range[4];
+  E.q1 = range[5];
+  E.n_out = R.nA + R.nV + R.nQ;
+  E.nchunks = nchunks;
+  E.partial = ctx->partial.as<double>();
+  E.x0A = R.x0A.as<double>();
+  E.z0 = R.z0.as<double>();
+  E.x0V = R.x0V.as<double>();
+  E.x0Q = R.x0Q.as<double>();
+  E.areaA = R.areaA.as<double>();
+  E.xiA = R.xiA.as<double>();
+  E.ziA = R.ziA.as<double>();
+  E.xiV = R.xiV.as<double>();
+  E.xiQ = R.xiQ.as<double>();
+  E.newA = R.newA.as<double>();
+  E.newZ = R.newZ.as<double>();
+  E.newV = R.newV.as<double>();
+  E.newQ = R.newQ.as<double>();
+  E.src = R.src.as<double4>();
+  E.ke = R.ke.as<double>();
+  E.keBlocks = R.keBlocks.as<double>();
+  const int rows = (E.a1 - E.a0) + (E.v1 - E.v0) + (E.q1 - E.q0);
+  const int blocks = std::max(1, (rows + kEpiThreads - 1) / kEpiThreads);
+  if (stage == 0) {
+    int rc = R.keBlocks.ensure((size_t)blocks * sizeof(double));
+    if (rc) return rc;
+    E.keBlocks = R.keBlocks.as<double>();
+  }
+  stage_epilogue_kernel<<<blocks, kEpiThreads, 0, ctx->stream>>>(E);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  if (stage == 0 && total_ke) {
+    ke_finalize_kernel<<<1, 256, 0, ctx->stream>>>(E.keBlocks, blocks, total_ke);
+    TC_CUDA_TRY(cudaGetLastError());
+    ctx->launches += 1;
+  }
+  return TC_OK;
+}
+
+}  // namespace tcb

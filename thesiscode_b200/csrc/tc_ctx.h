@@ -1,0 +1,103 @@
+// The library context: what PanelVelocityParallelModule keeps as module
+// state (`save` variables, PanelVelocityParallel.f90:25-71: smooth, the RK4
+// scratch arrays, kineticEnergy, totalKE) plus the device, stream and
+// launch configuration. Explicit instead of global, so the ABI is reentrant.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <vector>
+
+#include "bs_core.cuh"
+#include "tc_internal.h"
+
+namespace tcb {
+
+// A growable device allocation owned by the context.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need);  // grows (never shrinks); contents are not kept
+  void release();
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Launch shape of one pair-kernel variant.
+struct PairCfg {
+  int nt;     // threads per CTA
+  int tpt;    // targets per thread
+  int ts;     // sources per shared-memory tile
+  int tb() const { return nt * tpt; }
+};
+
+// Target segment as the host describes it before tiles are assigned.
+struct SegDesc {
+  const double* x;
+  int i0, i1;
+  int out_offset;
+  int self_offset;
+  double d2;
+};
+
+// RK4 state and scratch kept on the device between calls (the reference's
+// activePanelsInput/Stage1..4/newActivePanelsX family, :34-71, laid out for
+// the fused stage epilogue: only the running sum of the stages is kept).
+struct Rk4State {
+  int nA = 0, nV = 0, nQ = 0;
+  bool ready = false;
+  DevBuf x0A, z0, areaA, x0V, x0Q;      // state at the start of the step
+  DevBuf xiA, ziA, xiV, xiQ;            // stage inputs (targets / sources)
+  DevBuf newA, newZ, newV, newQ;        // running x + k1/6 + k2/3 + ...
+  DevBuf src;                           // packed sources of the current stage
+  DevBuf ke;                            // kineticEnergy(nA), stage 1
+  DevBuf keBlocks;                      // per-block partial sums of KE*A
+  DevBuf totalKE;                       // one value per step
+};
+
+}  // namespace tcb
+
+struct tc_ctx {
+  int device = 0;
+  int precision = TC_FP64;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+  double omega = 6.283185307179586476925286766559;  // 2*pi, TracerAndVorticityDistributions.f90:34-35
+  double delta[3] = {0.0, 0.0, 0.05};               // ACTIVE, VERTEX, PASSIVE (smooth, :27)
+  tcb::PairCfg cfg64{256, 2, 256};
+  tcb::PairCfg cfg32{256, 4, 256};
+  int min_chunk = 4096;   // smallest source chunk a CTA walks
+  int max_chunks = 64;
+  int slots64 = 0, slots32 = 0;  // resident CTAs per GPU for each kernel
+  tcb::DevBuf partial;    // pair-kernel partial sums
+  tcb::DevBuf scratch[6]; // one-call buffers (velocity entry points)
+  tcb::Rk4State rk;
+  // instrumentation (tc_stats): kernels launched, and CUDA-event time of the
+  // pair kernels when timing is on (events recorded on ctx->stream).
+  long long launches = 0;
+  long long pair_launches = 0;
+  long long pair_interactions = 0;
+  bool time_pairs = false;
+  std::vector<cudaEvent_t> pair_events;  // start/stop pairs, resolved by tc_stats
+  double pair_ms = 0.0;
+};
+
+namespace tcb {
+// Launch the pair kernel of ctx->precision over up to three target segments.
+// Allocates ctx->partial and returns the number of source chunks in *nchunks.
+int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
+                 int n_out, int* nchunks);
+// Pack {x, y, z, zeta*area} for n sources.
+int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* area, int n,
+                double4* out);
+// dX (3*m) and dVort (m, nullable) for rows [i0, i1), zero elsewhere; partial
+// rows are row_offset + i.
+int launch_velocity_epilogue(tc_ctx* ctx, const double* x, int m, int i0, int i1,
+                             int row_offset, int n_out, int nchunks, double* dX, double* dVort);
+// One RK4 stage epilogue over the three classes' ranges.
+// total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
+// stage 0; nchunks is what launch_pairs returned for this stage.
+int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
+                          double* total_ke);
+int resolve_slots(tc_ctx* ctx);
+}  // namespace tcb
