@@ -62,6 +62,7 @@ extern "C" {
 #define TC_PROBE_RCP32 3
 #define TC_PROBE_RCP64 4
 #define TC_PROBE_DDIV 5
+#define TC_PROBE_F2F 6
 
 typedef struct tc_ctx tc_ctx;
 

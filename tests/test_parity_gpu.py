@@ -19,7 +19,11 @@ from thesiscode_b200.panel_velocity import Context
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 FP64_TOL = 1e-12
-FP32C_TOL = 1e-7  # compensated path; tiles of the icosahedral (quad-tree) target order
+# FP32-compensated path, stated bound: 1e-7 from level 6 up (the benchmark sizes; tiles of
+# the quad-tree target order are small against the sphere), 3e-7 on coarser grids, where
+# the FP32 rounding of each pair term (a few ulps) is the floor.
+FP32C_TOL = 3e-7
+FP32C_TOL_FINE = 1e-7
 
 
 def rel_err(a, b):
@@ -79,7 +83,7 @@ def test_active_and_vertex_sums_full_level(prec, tol, level, gpu):
     ctx.close()
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL_FINE)])
 def test_sampled_rows_level7_with_delta(prec, tol, gpu):
     """Level 7 (327,680 sources), delta 0.01: 512 seeded target rows per class vs the oracle."""
     w = configs.gaussian(level=7, delta=0.01)
@@ -108,8 +112,9 @@ def test_rk4_step_parity_mode_golden(prec, tol, gpu):
     for new, old, ref in ((xA, g["xA"], g["rk_xA"]), (xV, g["xV"], g["rk_xV"]),
                           (xQ, g["xQ"], g["rk_xQ"]), (zA, g["zetaA"], g["rk_zA"])):
         assert rel_err(new - old, ref - old) <= tol
-    assert abs(tke[0] - g["rk_tke"]) <= tol * g["rk_tke"]
-    assert rel_err(ke, g["rk_ke"]) <= tol
+    # kinetic energy is quadratic in u: twice the velocity's relative error
+    assert abs(tke[0] - g["rk_tke"]) <= 2 * tol * g["rk_tke"]
+    assert rel_err(ke, g["rk_ke"]) <= 2 * tol
     ctx.close()
 
 
@@ -123,7 +128,7 @@ def test_rk4_two_steps_config_mode_golden(prec, tol, gpu):
     assert rel_err(xA - g["xA"], g["rk_xA"] - g["xA"]) <= tol
     assert rel_err(xV - g["xV"], g["rk_xV"] - g["xV"]) <= tol
     assert rel_err(zA - g["zetaA"], g["rk_zA"] - g["zetaA"]) <= tol
-    np.testing.assert_allclose(tke, g["rk_tke"], rtol=tol, atol=0)
+    np.testing.assert_allclose(tke, g["rk_tke"], rtol=2 * tol, atol=0)
     ctx.close()
 
 

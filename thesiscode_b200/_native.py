@@ -29,7 +29,8 @@ TC_ACTIVE = 0
 TC_VERTEX = 1
 TC_PASSIVE = 2
 # probes
-TC_PROBE_FFMA, TC_PROBE_FFMA2, TC_PROBE_DFMA, TC_PROBE_RCP32, TC_PROBE_RCP64, TC_PROBE_DDIV = range(6)
+(TC_PROBE_FFMA, TC_PROBE_FFMA2, TC_PROBE_DFMA, TC_PROBE_RCP32, TC_PROBE_RCP64, TC_PROBE_DDIV,
+ TC_PROBE_F2F) = range(7)
 # RK4 device buffers
 TC_BUF_SOURCES, TC_BUF_XA, TC_BUF_ZETA, TC_BUF_XV, TC_BUF_XQ, TC_BUF_KE = range(6)
 

@@ -74,9 +74,10 @@ __global__ void probe_rcp32(int iters, float b, float c, float* sink) {
   float a[kChains];
 #pragma unroll
   for (int k = 0; k < kChains; ++k) a[k] = 1.0f + threadIdx.x * 1e-3f + k;
+  // the add keeps ptxas from folding rcp(rcp(x)); MUFU stays the slower pipe
   for (int i = 0; i < iters; ++i) {
 #pragma unroll
-    for (int k = 0; k < kChains; ++k) a[k] = rcp_approx_f32(a[k]);
+    for (int k = 0; k < kChains; ++k) a[k] = rcp_approx_f32(a[k]) + c;
   }
   float s = 0.f;
 #pragma unroll
@@ -98,6 +99,29 @@ __global__ void probe_rcp64(int iters, double b, double c, float* sink) {
   if (sink) sink[blockIdx.x * blockDim.x + threadIdx.x] = (float)(s + b + c);
 }
 
+// FP32 -> FP64 conversions feeding an FP64 add (the flush of FP32 partial
+// sums into FP64 accumulators); counts one conversion per op.
+__global__ void probe_f2f(int iters, float b, float c, float* sink) {
+  double a[kChains];
+  float f[kChains];
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) {
+    a[k] = 0.0;
+    f[k] = threadIdx.x * 1e-3f + k;
+  }
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+      a[k] += (double)f[k];
+      f[k] = f[k] * b;
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) s += a[k];
+  if (sink) sink[blockIdx.x * blockDim.x + threadIdx.x] = (float)s + c;
+}
+
 // IEEE-rounded FP64 division as the compiler emits it for `a / b`.
 __global__ void probe_ddiv(int iters, double b, double c, float* sink) {
   double a[kChains];
@@ -116,10 +140,11 @@ __global__ void probe_ddiv(int iters, double b, double c, float* sink) {
 }  // namespace
 
 // kind: TC_PROBE_FFMA, TC_PROBE_FFMA2, TC_PROBE_DFMA, TC_PROBE_RCP32,
-// TC_PROBE_RCP64, TC_PROBE_DDIV. Returns operations per second (one FMA,
+// TC_PROBE_RCP64, TC_PROBE_DDIV, TC_PROBE_F2F. Returns operations per second (one FMA,
 // one reciprocal or one division = 1 op; FFMA2 counts 2) in *ops_per_s.
 extern "C" int tc_probe_peak(int device, int kind, int iters, double* ops_per_s) {
   if (!ops_per_s || iters <= 0 || iters > (1 << 22)) return TC_ERR_ARG;
+  if (kind < TC_PROBE_FFMA || kind > TC_PROBE_F2F) return TC_ERR_ARG;
   int rc = tc_set_device_checked(device);
   if (rc) return rc;
   cudaDeviceProp prop;
@@ -134,13 +159,13 @@ extern "C" int tc_probe_peak(int device, int kind, int iters, double* ops_per_s)
       case TC_PROBE_FFMA: probe_ffma<<<blocks, threads>>>(it, 0.999999f, 1e-7f, nullptr); break;
       case TC_PROBE_FFMA2: probe_ffma2<<<blocks, threads>>>(it, 0.999999f, 1e-7f, nullptr); break;
       case TC_PROBE_DFMA: probe_dfma<<<blocks, threads>>>(it, 0.999999, 1e-7, nullptr); break;
-      case TC_PROBE_RCP32: probe_rcp32<<<blocks, threads>>>(it, 0.f, 0.f, nullptr); break;
+      case TC_PROBE_RCP32: probe_rcp32<<<blocks, threads>>>(it, 0.f, 1e-7f, nullptr); break;
       case TC_PROBE_RCP64: probe_rcp64<<<blocks, threads>>>(it, 0.0, 0.0, nullptr); break;
       case TC_PROBE_DDIV: probe_ddiv<<<blocks, threads>>>(it, 0.5, 0.75, nullptr); break;
+      case TC_PROBE_F2F: probe_f2f<<<blocks, threads>>>(it, 0.999999f, 0.f, nullptr); break;
       default: break;
     }
   };
-  if (kind < TC_PROBE_FFMA || kind > TC_PROBE_DDIV) return TC_ERR_ARG;
   if (kind == TC_PROBE_FFMA2) per_thread_ops *= 2.0;
   launch(iters / 8 + 1);  // warm-up
   cudaEventRecord(e0);
