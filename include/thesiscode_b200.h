@@ -163,6 +163,15 @@ int tc_rk4_device_buffer(tc_ctx* ctx, int which, void** ptr);
  * context's stream: the exchange unit of a target-sharded run. */
 int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr, int to_buffer);
 
+/* ---- pair-kernel variants (no counterpart in the reference) ------------ */
+/* Number of compiled launch shapes for a precision, and their parameters:
+ * info7 = {threads, targets/thread, sources/tile, FP32 flush length (0 for
+ * FP64), min CTAs/SM, unroll, targets/CTA}. */
+int tc_pair_variant_count(int precision, int* count);
+int tc_pair_variant_info(int precision, int id, int* info7);
+int tc_set_pair_variant(tc_ctx* ctx, int precision, int id);
+int tc_get_pair_variant(tc_ctx* ctx, int precision, int* id);
+
 /* ---- instrumentation (no counterpart in the reference) ----------------- */
 /* Record CUDA events around every pair-kernel launch on the context's
  * stream (off by default). */

@@ -79,6 +79,10 @@ SIGNATURES: dict[str, tuple] = {
                                    c_void_p]),
     "tc_rk4_device_buffer": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     "tc_rk4_copy_rows": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int]),
+    "tc_pair_variant_count": (c_int, [c_int, ip]),
+    "tc_pair_variant_info": (c_int, [c_int, c_int, ip]),
+    "tc_set_pair_variant": (c_int, [c_void_p, c_int, c_int]),
+    "tc_get_pair_variant": (c_int, [c_void_p, c_int, ip]),
     "tc_stats_enable_timing": (c_int, [c_void_p, c_int]),
     "tc_stats": (c_int, [c_void_p, c_int, POINTER(ctypes.c_longlong), POINTER(ctypes.c_longlong),
                          POINTER(ctypes.c_longlong), dp]),

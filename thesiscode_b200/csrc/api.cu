@@ -475,6 +475,33 @@ extern "C" int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const 
   return tc_rk4_store(ctx, xA, zetaA, xV, xQ, kineticEnergy, 1);
 }
 
+// Pair-kernel variants (the launch shapes the autotuner searches).
+extern "C" int tc_pair_variant_count(int precision, int* count) {
+  if (!count || (precision != TC_FP64 && precision != TC_FP32C)) return TC_ERR_ARG;
+  *count = tcb::variant_count(precision);
+  return TC_OK;
+}
+
+extern "C" int tc_pair_variant_info(int precision, int id, int* info7) {
+  const tcb::PairVariant* v = tcb::variant(precision, id);
+  if (!v || !info7) return TC_ERR_ARG;
+  int vals[7] = {v->nt, v->tpt, v->ts, v->flush, v->minb, v->unroll, v->nt * v->tpt};
+  for (int j = 0; j < 7; ++j) info7[j] = vals[j];
+  return TC_OK;
+}
+
+extern "C" int tc_set_pair_variant(tc_ctx* ctx, int precision, int id) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  return tcb::select_variant(ctx, precision, id);
+}
+
+extern "C" int tc_get_pair_variant(tc_ctx* ctx, int precision, int* id) {
+  if (!ctx || !id) return TC_ERR_ARG;
+  *id = precision == TC_FP64 ? ctx->var64 : ctx->var32;
+  return TC_OK;
+}
+
 // Instrumentation: kernels launched by this context, pair-kernel launches and
 // pair interactions evaluated since the last reset, and (when enabled) the
 // summed CUDA-event time of the pair kernels on the context's stream.

@@ -73,18 +73,36 @@ __device__ __forceinline__ const TargetSeg& find_seg(const PairLaunch& P, int ti
 }
 
 // ---------------------------------------------------------------------------
-// FP64 pair kernel. The denominator is rounded exactly as the reference's
-// 1.0 - sum(pointVorts(:,k)*pointVorts(:,j)) [+ smooth*smooth]: three
-// separately rounded products, left-to-right additions, no contraction.
+// FP64 pair kernel.
 // ---------------------------------------------------------------------------
-template <int NT, int TPT, int TS>
-__global__ void __launch_bounds__(NT) pair_fp64_kernel(const PairLaunch P) {
+// FUSED = false: the denominator is rounded exactly like the reference's
+// 1.0 - sum(...) (six separately rounded operations). FUSED = true: the
+// same expression as 1 - x.y + delta^2 in three fused multiply-adds, one
+// rounding instead of six; it differs from the reference's value by the
+// reference's own rounding error in the denominator (a few ulps of x.y).
+template <bool FUSED>
+__device__ __forceinline__ double pair_denominator(const double4& q, const double xi[3], double d2,
+                                                   double one_plus_d2) {
+  if (FUSED) {
+    double s = fma(-q.x, xi[0], one_plus_d2);
+    s = fma(-q.y, xi[1], s);
+    return fma(-q.z, xi[2], s);
+  }
+  double s = __dmul_rn(q.x, xi[0]);
+  s = __dadd_rn(s, __dmul_rn(q.y, xi[1]));
+  s = __dadd_rn(s, __dmul_rn(q.z, xi[2]));
+  return __dadd_rn(__dsub_rn(1.0, s), d2);
+}
+
+template <int NT, int TPT, int TS, int MINB, bool FUSED>
+__global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P) {
   __shared__ double4 sm[TS];
   constexpr int TB = NT * TPT;
   const TargetSeg& G = find_seg(P, blockIdx.x);
   const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
   const int i_end = G.i1;
   const double d2 = G.d2;
+  const double one_plus_d2 = 1.0 + G.d2;
   const bool has_self = G.self_offset != kNoSelf;
 
   double xi[TPT][3], acc[TPT][3];
@@ -118,10 +136,7 @@ __global__ void __launch_bounds__(NT) pair_fp64_kernel(const PairLaunch P) {
         const double4 q = sm[j];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-          double s = __dmul_rn(q.x, xi[t][0]);
-          s = __dadd_rn(s, __dmul_rn(q.y, xi[t][1]));
-          s = __dadd_rn(s, __dmul_rn(q.z, xi[t][2]));
-          const double den = __dadd_rn(__dsub_rn(1.0, s), d2);
+          const double den = pair_denominator<FUSED>(q, xi[t], d2, one_plus_d2);
           const double w = __dmul_rn(q.w, rcp_newton2(den));
           acc[t][0] = fma(w, q.x - xi[t][0], acc[t][0]);
           acc[t][1] = fma(w, q.y - xi[t][1], acc[t][1]);
@@ -134,10 +149,7 @@ __global__ void __launch_bounds__(NT) pair_fp64_kernel(const PairLaunch P) {
         const int k = ts + j;
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-          double s = __dmul_rn(q.x, xi[t][0]);
-          s = __dadd_rn(s, __dmul_rn(q.y, xi[t][1]));
-          s = __dadd_rn(s, __dmul_rn(q.z, xi[t][2]));
-          const double den = __dadd_rn(__dsub_rn(1.0, s), d2);
+          const double den = pair_denominator<FUSED>(q, xi[t], d2, one_plus_d2);
           double w = __dmul_rn(q.w, rcp_newton2(den));
           w = (k == self_k[t]) ? 0.0 : w;
           acc[t][0] = fma(w, q.x - xi[t][0], acc[t][0]);
@@ -178,8 +190,8 @@ __global__ void __launch_bounds__(NT) pair_fp64_kernel(const PairLaunch P) {
 // stays the bound). Per-target FP32 partial sums are added into FP64
 // accumulators every FLUSH sources.
 // ---------------------------------------------------------------------------
-template <int NT, int NPAIR, int TS, int FLUSH>
-__global__ void __launch_bounds__(NT) pair_fp32c_kernel(const PairLaunch P) {
+template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
+__global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
   static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
   __shared__ float4 smA[TS];  // (sx, sx, sy, sy)
   __shared__ float4 smB[TS];  // (sz, sz, 2G, 2G)
@@ -246,7 +258,7 @@ __global__ void __launch_bounds__(NT) pair_fp32c_kernel(const PairLaunch P) {
     const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
     for (int jf = 0; jf < TS; jf += FLUSH) {
       if (!diag) {
-#pragma unroll 4
+#pragma unroll UNROLL
         for (int j = jf; j < jf + FLUSH; ++j) {
           const float4 a = smA[j];
           const float4 b = smB[j];
@@ -319,6 +331,125 @@ __global__ void __launch_bounds__(NT) pair_fp32c_kernel(const PairLaunch P) {
         out[stride + i] = ay[p][h];
         out[2 * stride + i] = az[p][h];
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32-compensated pair kernel, scalar form: the same arithmetic as
+// pair_fp32c_kernel with TPT independent targets per thread and plain FP32
+// instructions (no f32x2 packing); a source is one float4 {sx, sy, sz, 2G}
+// plus one float e in shared memory.
+// ---------------------------------------------------------------------------
+template <int NT, int TPT, int TS, int FLUSH, int MINB, int UNROLL>
+__global__ void __launch_bounds__(NT, MINB) pair_fp32s_kernel(const PairLaunch P) {
+  static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
+  __shared__ float4 smA[TS];  // (sx, sy, sz, 2G)
+  __shared__ float smE[TS];   // e
+  constexpr int TB = NT * TPT;
+  const TargetSeg& G = find_seg(P, blockIdx.x);
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
+  const int i_end = G.i1;
+  const bool has_self = G.self_offset != kNoSelf;
+
+  const int mid = min(tile0 + TB / 2, i_end - 1);
+  const double cx = G.x[3 * (size_t)mid], cy = G.x[3 * (size_t)mid + 1],
+               cz = G.x[3 * (size_t)mid + 2];
+
+  float ntx[TPT], nty[TPT], ntz[TPT], ei[TPT], fx[TPT], fy[TPT], fz[TPT];
+  double ax[TPT], ay[TPT], az[TPT];
+  int self_k[TPT];
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    int i = tile0 + (int)threadIdx.x + t * NT;
+    int ld = i < i_end ? i : mid;
+    double x = G.x[3 * (size_t)ld], y = G.x[3 * (size_t)ld + 1], z = G.x[3 * (size_t)ld + 2];
+    ntx[t] = -(float)(x - cx);
+    nty[t] = -(float)(y - cy);
+    ntz[t] = -(float)(z - cz);
+    ei[t] = (float)((1.0 - (x * x + y * y + z * z)) + 2.0 * G.d2);
+    self_k[t] = has_self ? i + G.self_offset : -1;
+    ax[t] = ay[t] = az[t] = 0.0;
+    fx[t] = fy[t] = fz[t] = 0.f;
+  }
+  const int self_lo = has_self ? tile0 + G.self_offset : 0;
+  const int self_hi = has_self ? min(tile0 + TB, i_end) + G.self_offset : 0;
+
+  const int c0 = (int)blockIdx.y * P.chunk_len;
+  const int c1 = min(P.n, c0 + P.chunk_len);
+  for (int ts = c0; ts < c1; ts += TS) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < TS; j += NT) {
+      int k = ts + j;
+      float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f;
+      if (k < c1) {
+        const double4 q = P.src[k];
+        sx = (float)(q.x - cx);
+        sy = (float)(q.y - cy);
+        sz = (float)(q.z - cz);
+        g = (float)(2.0 * q.w);
+        e = (float)(1.0 - (q.x * q.x + q.y * q.y + q.z * q.z));
+      }
+      smA[j] = make_float4(sx, sy, sz, g);
+      smE[j] = e;
+    }
+    __syncthreads();
+    const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
+    for (int jf = 0; jf < TS; jf += FLUSH) {
+      if (!diag) {
+#pragma unroll UNROLL
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = smA[j];
+          const float e = smE[j];
+#pragma unroll
+          for (int t = 0; t < TPT; ++t) {
+            const float dx = a.x + ntx[t], dy = a.y + nty[t], dz = a.z + ntz[t];
+            float D = fmaf(dx, dx, e + ei[t]);
+            D = fmaf(dy, dy, D);
+            D = fmaf(dz, dz, D);
+            const float w = a.w * rcp_approx_f32(D);
+            fx[t] = fmaf(w, dx, fx[t]);
+            fy[t] = fmaf(w, dy, fy[t]);
+            fz[t] = fmaf(w, dz, fz[t]);
+          }
+        }
+      } else {
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = smA[j];
+          const float e = smE[j];
+          const int k = ts + j;
+#pragma unroll
+          for (int t = 0; t < TPT; ++t) {
+            const float dx = a.x + ntx[t], dy = a.y + nty[t], dz = a.z + ntz[t];
+            float D = fmaf(dx, dx, e + ei[t]);
+            D = fmaf(dy, dy, D);
+            D = fmaf(dz, dz, D);
+            float w = a.w * rcp_approx_f32(D);
+            w = (k == self_k[t]) ? 0.f : w;
+            fx[t] = fmaf(w, dx, fx[t]);
+            fy[t] = fmaf(w, dy, fy[t]);
+            fz[t] = fmaf(w, dz, fz[t]);
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < TPT; ++t) {
+        ax[t] += (double)fx[t];
+        ay[t] += (double)fy[t];
+        az[t] += (double)fz[t];
+        fx[t] = fy[t] = fz[t] = 0.f;
+      }
+    }
+  }
+  const size_t stride = (size_t)P.n_out;
+  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    int i = tile0 + (int)threadIdx.x + t * NT;
+    if (i < i_end) {
+      out[i] = ax[t];
+      out[stride + i] = ay[t];
+      out[2 * stride + i] = az[t];
     }
   }
 }

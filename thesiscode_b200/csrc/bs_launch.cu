@@ -33,25 +33,87 @@ void DevBuf::release() {
 }
 
 // ---------------------------------------------------------------------------
-// Kernel instances
+// Kernel variants: the launch shapes the autotuner chooses from. FP32C
+// variants differ in threads per CTA, target pairs per thread, FP32 partial
+// length before the FP64 flush, minimum resident CTAs (register cap) and
+// source-loop unrolling; FP64 variants in threads and targets per thread.
 // ---------------------------------------------------------------------------
-constexpr int kNT64 = 256, kTPT64 = 2, kTS64 = 256;
-constexpr int kNT32 = 256, kNPAIR32 = 2, kTS32 = 256, kFLUSH32 = 64;
+constexpr int kTS = 256;
+
+template <int NT, int TPT, int MINB, bool FUSED>
+void launch64(dim3 g, cudaStream_t s, const PairLaunch& P) {
+  pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(P);
+}
+template <int NT, int TPT, int FLUSH, int MINB, int UNROLL>
+void launch32s(dim3 g, cudaStream_t s, const PairLaunch& P) {
+  pair_fp32s_kernel<NT, TPT, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(P);
+}
+template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL>
+void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
+  pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(P);
+}
+
+#define V64(NT, TPT, MINB, FUSED)                                                 \
+  PairVariant { TC_FP64, NT, TPT, kTS, FUSED, MINB, 0, launch64<NT, TPT, MINB, FUSED>, \
+                (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED> }
+#define V32S(NT, TPT, FLUSH, MINB, UNROLL)                                               \
+  PairVariant { TC_FP32C, NT, TPT, kTS, FLUSH, MINB, UNROLL,                              \
+                launch32s<NT, TPT, FLUSH, MINB, UNROLL>,                                  \
+                (const void*)pair_fp32s_kernel<NT, TPT, kTS, FLUSH, MINB, UNROLL> }
+#define V32(NT, NPAIR, FLUSH, MINB, UNROLL)                                              \
+  PairVariant { TC_FP32C, NT, 2 * NPAIR, kTS, FLUSH, MINB, UNROLL,                        \
+                launch32<NT, NPAIR, FLUSH, MINB, UNROLL>,                                 \
+                (const void*)pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL> }
+
+// FP64: the `flush` field records the denominator mode (1 = fused, 0 =
+// rounded exactly like the reference).
+const PairVariant kVariants64[] = {
+    V64(256, 2, 5, true),  V64(256, 4, 2, true),  V64(256, 1, 6, true), V64(128, 4, 4, true),
+    V64(256, 2, 5, false), V64(256, 4, 2, false),
+};
+const PairVariant kVariants32[] = {
+    V32(256, 2, 32, 3, 4),  V32(256, 2, 64, 2, 4),  V32(128, 1, 32, 8, 8), V32(256, 2, 16, 2, 4),
+    V32S(256, 4, 32, 2, 4), V32S(256, 8, 32, 1, 2), V32S(128, 8, 32, 2, 4), V32S(256, 4, 16, 2, 4),
+    V32S(256, 6, 32, 2, 2), V32S(128, 4, 32, 4, 4),
+};
+constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
+constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
+
+const PairVariant* variant(int precision, int id) {
+  if (precision == TC_FP64) return (id >= 0 && id < kN64) ? &kVariants64[id] : nullptr;
+  return (id >= 0 && id < kN32) ? &kVariants32[id] : nullptr;
+}
+
+int variant_count(int precision) { return precision == TC_FP64 ? kN64 : kN32; }
+
+int select_variant(tc_ctx* ctx, int precision, int id) {
+  const PairVariant* v = variant(precision, id);
+  if (!v) {
+    tc_record_error("no pair-kernel variant %d for precision %d", id, precision);
+    return TC_ERR_ARG;
+  }
+  int blocks = 0;
+  TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->fn, v->nt, 0));
+  int slots = std::max(1, blocks) * ctx->num_sms;
+  if (precision == TC_FP64) {
+    ctx->var64 = id;
+    ctx->slots64 = slots;
+    ctx->cfg64 = PairCfg{v->nt, v->tpt, v->ts};
+  } else {
+    ctx->var32 = id;
+    ctx->slots32 = slots;
+    ctx->cfg32 = PairCfg{v->nt, v->tpt, v->ts};
+  }
+  return TC_OK;
+}
 
 int resolve_slots(tc_ctx* ctx) {
   cudaDeviceProp prop;
   TC_CUDA_TRY(cudaGetDeviceProperties(&prop, ctx->device));
   ctx->num_sms = prop.multiProcessorCount;
-  int b64 = 0, b32 = 0;
-  TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &b64, pair_fp64_kernel<kNT64, kTPT64, kTS64>, kNT64, 0));
-  TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &b32, pair_fp32c_kernel<kNT32, kNPAIR32, kTS32, kFLUSH32>, kNT32, 0));
-  ctx->slots64 = std::max(1, b64) * ctx->num_sms;
-  ctx->slots32 = std::max(1, b32) * ctx->num_sms;
-  ctx->cfg64 = PairCfg{kNT64, kTPT64, kTS64};
-  ctx->cfg32 = PairCfg{kNT32, 2 * kNPAIR32, kTS32};
-  return TC_OK;
+  int rc = select_variant(ctx, TC_FP64, ctx->var64);
+  if (rc) return rc;
+  return select_variant(ctx, TC_FP32C, ctx->var32);
 }
 
 // Number of source chunks: the split that best fills the resident CTA slots
@@ -117,10 +179,7 @@ int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src,
     TC_CUDA_TRY(cudaEventCreate(&ev[1]));
     TC_CUDA_TRY(cudaEventRecord(ev[0], ctx->stream));
   }
-  if (fp64)
-    pair_fp64_kernel<kNT64, kTPT64, kTS64><<<grid, kNT64, 0, ctx->stream>>>(P);
-  else
-    pair_fp32c_kernel<kNT32, kNPAIR32, kTS32, kFLUSH32><<<grid, kNT32, 0, ctx->stream>>>(P);
+  variant(ctx->precision, fp64 ? ctx->var64 : ctx->var32)->launch(grid, ctx->stream, P);
   TC_CUDA_TRY(cudaGetLastError());
   if (ctx->time_pairs) {
     TC_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));

@@ -30,6 +30,14 @@ struct PairCfg {
   int tb() const { return nt * tpt; }
 };
 
+// One compiled pair-kernel shape.
+struct PairVariant {
+  int precision;
+  int nt, tpt, ts, flush, minb, unroll;
+  void (*launch)(dim3 grid, cudaStream_t stream, const PairLaunch& P);
+  const void* fn;
+};
+
 // Target segment as the host describes it before tiles are assigned.
 struct SegDesc {
   const double* x;
@@ -66,6 +74,7 @@ struct tc_ctx {
   double delta[3] = {0.0, 0.0, 0.05};               // ACTIVE, VERTEX, PASSIVE (smooth, :27)
   tcb::PairCfg cfg64{256, 2, 256};
   tcb::PairCfg cfg32{256, 4, 256};
+  int var64 = 2, var32 = 0;  // pair-kernel variants in use (see kVariants64/32)
   int min_chunk = 4096;   // smallest source chunk a CTA walks
   int max_chunks = 64;
   int slots64 = 0, slots32 = 0;  // resident CTAs per GPU for each kernel
@@ -100,4 +109,7 @@ int launch_velocity_epilogue(tc_ctx* ctx, const double* x, int m, int i0, int i1
 int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
                           double* total_ke);
 int resolve_slots(tc_ctx* ctx);
+const PairVariant* variant(int precision, int id);
+int variant_count(int precision);
+int select_variant(tc_ctx* ctx, int precision, int id);
 }  // namespace tcb
