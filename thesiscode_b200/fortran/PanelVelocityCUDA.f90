@@ -1,0 +1,251 @@
+module PanelVelocityCUDAModule
+!  Drop-in replacement for PanelVelocityParallelModule (PanelVelocityParallel.f90:1-20 in the
+!  reference) on top of the C ABI of libthesiscode_b200 (include/thesiscode_b200.h).
+!  A BVE driver switches by replacing `use PanelVelocityParallelModule` with
+!  `use PanelVelocityCUDAModule`; the public names, argument lists and module state are the same:
+!
+!      BVERK4(aParticles, aPanels, dt, procRank, numProcs)     :435-658
+!      InitializeMPIRK4, FinalizeMPIRK4, LoadBalance           :126-230
+!      ResetRK4, SetSmooth, GetSmooth, ResetArea               :96-120, :321
+!      totalKE, kineticEnergy                                  :25-26
+!
+!  Every rank runs the whole step on its own GPU (the results are identical on all ranks, so the
+!  per-stage MPI_BCAST exchange of the reference is not needed); GatherPanels / ScatterPanels
+!  run on the host as in the reference.
+!
+!  Build: needs the reference's ParticlesEdgesPanelsModule and TracerAndVorticityDistributionModule
+!  and a link against libthesiscode_b200.so, e.g.
+!      gfortran -O2 -c PanelVelocityCUDA.f90 && gfortran ... -L<lib dir> -lthesiscode_b200
+use iso_c_binding
+use NumberKindsModule
+use ParticlesEdgesPanelsModule
+use TracerAndVorticityDistributionModule, only : Omega
+
+implicit none
+
+private
+public totalKE, kineticEnergy
+public BVERK4, ResetRK4, ResetArea, SetSmooth, GetSmooth
+public InitializeMPIRK4, FinalizeMPIRK4, LoadBalance
+public SetPrecisionCUDA
+
+integer(c_int), parameter :: TC_FP64 = 0, TC_FP32C = 1
+
+interface
+  integer(c_int) function tc_create(device, precision, ctx) bind(C, name="tc_create")
+    import :: c_int, c_ptr
+    integer(c_int), value :: device, precision
+    type(c_ptr) :: ctx
+  end function
+  integer(c_int) function tc_destroy(ctx) bind(C, name="tc_destroy")
+    import :: c_int, c_ptr
+    type(c_ptr), value :: ctx
+  end function
+  integer(c_int) function tc_set_omega(ctx, omega) bind(C, name="tc_set_omega")
+    import :: c_int, c_ptr, c_double
+    type(c_ptr), value :: ctx
+    real(c_double), value :: omega
+  end function
+  integer(c_int) function tc_set_deltas(ctx, da, dv, dq) bind(C, name="tc_set_deltas")
+    import :: c_int, c_ptr, c_double
+    type(c_ptr), value :: ctx
+    real(c_double), value :: da, dv, dq
+  end function
+  integer(c_int) function tc_reset_rk4(ctx) bind(C, name="tc_reset_rk4")
+    import :: c_int, c_ptr
+    type(c_ptr), value :: ctx
+  end function
+  integer(c_int) function tc_rk4_step(ctx, xA, zetaA, areaA, nA, xV, nV, xQ, nQ, dt, nsteps, &
+                                      tke, ke) bind(C, name="tc_rk4_step")
+    import :: c_int, c_ptr, c_double
+    type(c_ptr), value :: ctx
+    real(c_double) :: xA(3,*), zetaA(*), areaA(*), xV(3,*), xQ(3,*), tke(*), ke(*)
+    integer(c_int), value :: nA, nV, nQ, nsteps
+    real(c_double), value :: dt
+  end function
+  type(c_ptr) function tc_last_error() bind(C, name="tc_last_error")
+    import :: c_ptr
+  end function
+end interface
+
+real(kreal), allocatable, save :: kineticEnergy(:)
+real(kreal), save :: totalKE = 0.0_kreal
+real(kreal), save :: smooth = 0.05_kreal
+logical(klog), save :: resetAreas = .False.
+logical(klog), save :: rk4IsReady = .False.
+logical(klog), save :: mpiIsReady = .False.
+integer(c_int), save :: precisionMode = TC_FP64
+type(c_ptr), save :: ctx = c_null_ptr
+type(Panels), pointer, save :: activePanels => null(), passivePanels => null()
+integer(kint), allocatable, save :: activeMap(:), passiveMap(:)
+integer(kint), allocatable, save :: particlesIndexStart(:), particlesIndexEnd(:), &
+                                    activePanelsIndexStart(:), activePanelsIndexEnd(:), &
+                                    passivePanelsIndexStart(:), passivePanelsIndexEnd(:)
+
+contains
+
+subroutine SetSmooth(newSmooth)
+  real(kreal), intent(in) :: newSmooth
+  smooth = newSmooth
+end subroutine
+
+function GetSmooth()
+  real(kreal) :: GetSmooth
+  GetSmooth = smooth
+end function
+
+subroutine ResetArea(onOff)
+  logical(klog), intent(in), optional :: onOff
+  if (present(onOff)) then
+    resetAreas = onOff
+  else
+    resetAreas = .True.
+  endif
+end subroutine
+
+subroutine SetPrecisionCUDA(fp32Compensated)
+  ! Selects the FP32-compensated pair arithmetic (.true.) or FP64 (.false., the default).
+  logical(klog), intent(in) :: fp32Compensated
+  if (fp32Compensated) then
+    precisionMode = TC_FP32C
+  else
+    precisionMode = TC_FP64
+  endif
+  if (c_associated(ctx)) call FreeContext()
+end subroutine
+
+subroutine CheckStatus(rc, where)
+  integer(c_int), intent(in) :: rc
+  character(len=*), intent(in) :: where
+  if (rc /= 0) then
+    print *, where, " ERROR : libthesiscode_b200 status ", rc
+    stop
+  endif
+end subroutine
+
+subroutine FreeContext()
+  integer(c_int) :: rc
+  if (c_associated(ctx)) then
+    rc = tc_destroy(ctx)
+    ctx = c_null_ptr
+  endif
+end subroutine
+
+subroutine InitializeMPIRK4(aParticles, aPanels, procRank, numProcs)
+  type(Particles), intent(in) :: aParticles
+  type(Panels), intent(in) :: aPanels
+  integer(kint), intent(in) :: procRank, numProcs
+  integer(c_int) :: rc
+  allocate(particlesIndexStart(0:numProcs-1), particlesIndexEnd(0:numProcs-1))
+  allocate(activePanelsIndexStart(0:numProcs-1), activePanelsIndexEnd(0:numProcs-1))
+  allocate(passivePanelsIndexStart(0:numProcs-1), passivePanelsIndexEnd(0:numProcs-1))
+  mpiIsReady = .True.
+  call LoadBalance(aParticles, aPanels, numProcs)
+  if (.NOT. c_associated(ctx)) then
+    rc = tc_create(0_c_int, precisionMode, ctx)   ! one GPU per rank: device 0 of the rank's view
+    call CheckStatus(rc, "InitializeMPIRK4")
+  endif
+end subroutine
+
+subroutine LoadBalance(aParticles, aPanels, numProcs)
+  ! Same contiguous partition as the reference (:182-204); the GPU step does not need it but
+  ! drivers read the index arrays.
+  type(Particles), intent(in) :: aParticles
+  type(Panels), intent(in) :: aPanels
+  integer(kint), intent(in) :: numProcs
+  integer(kint) :: chunkSize, j
+  chunkSize = aParticles%N / numProcs
+  do j = 0, numProcs - 1
+    particlesIndexStart(j) = j*chunkSize + 1
+    particlesIndexEnd(j) = (j+1)*chunkSize
+  enddo
+  particlesIndexEnd(numProcs-1) = aParticles%N
+  chunkSize = aPanels%N_Active / numProcs
+  do j = 0, numProcs - 1
+    activePanelsIndexStart(j) = j*chunkSize + 1
+    activePanelsIndexEnd(j) = (j+1)*chunkSize
+  enddo
+  activePanelsIndexEnd(numProcs-1) = aPanels%N_Active
+  chunkSize = (aPanels%N - aPanels%N_Active) / numProcs
+  do j = 0, numProcs - 1
+    passivePanelsIndexStart(j) = j*chunkSize + 1
+    passivePanelsIndexEnd(j) = (j+1)*chunkSize
+  enddo
+  passivePanelsIndexEnd(numProcs-1) = aPanels%N - aPanels%N_Active
+end subroutine
+
+subroutine FinalizeMPIRK4()
+  if (rk4IsReady) call ResetRK4()
+  if (allocated(particlesIndexStart)) then
+    deallocate(particlesIndexStart, particlesIndexEnd, activePanelsIndexStart)
+    deallocate(activePanelsIndexEnd, passivePanelsIndexStart, passivePanelsIndexEnd)
+  endif
+  call FreeContext()
+  mpiIsReady = .False.
+end subroutine
+
+subroutine ResetRK4()
+  integer(c_int) :: rc
+  if (allocated(activeMap)) deallocate(activeMap)
+  if (allocated(passiveMap)) deallocate(passiveMap)
+  if (allocated(kineticEnergy)) deallocate(kineticEnergy)
+  if (associated(activePanels)) then
+    call Delete(activePanels)
+    deallocate(activePanels)
+  endif
+  if (associated(passivePanels)) then
+    call Delete(passivePanels)
+    deallocate(passivePanels)
+  endif
+  if (c_associated(ctx)) rc = tc_reset_rk4(ctx)
+  rk4IsReady = .False.
+end subroutine
+
+subroutine InitRK4(aParticles, aPanels)
+  type(Particles), intent(in) :: aParticles
+  type(Panels), intent(in) :: aPanels
+  integer(kint) :: nActive, nPassive
+  nActive = aPanels%N_Active
+  nPassive = aPanels%N - aPanels%N_Active
+  allocate(activePanels, passivePanels)
+  allocate(activeMap(nActive), passiveMap(nPassive), kineticEnergy(nActive))
+  call New(activePanels, nActive, GetPanelKind(aPanels), GetNTracer(aPanels), GetProblemKind(aPanels))
+  call New(passivePanels, nPassive, GetPanelKind(aPanels), GetNTracer(aPanels), GetProblemKind(aPanels))
+  activePanels%N = nActive
+  activePanels%N_Active = nActive
+  passivePanels%N = nPassive
+  rk4IsReady = .True.
+end subroutine
+
+subroutine BVERK4(aParticles, aPanels, dt, procRank, numProcs)
+  type(Particles), intent(inout) :: aParticles
+  type(Panels), intent(inout) :: aPanels
+  real(kreal), intent(in) :: dt
+  integer(kint), intent(in) :: procRank, numProcs
+  integer(c_int) :: rc
+  real(c_double) :: tke(1)
+  if (.NOT. c_associated(ctx)) then
+    rc = tc_create(0_c_int, precisionMode, ctx)
+    call CheckStatus(rc, "BVERK4")
+  endif
+  if (.NOT. rk4IsReady) call InitRK4(aParticles, aPanels)
+  call GatherPanels(aPanels, activePanels, activeMap, passivePanels, passiveMap)
+  rc = tc_set_omega(ctx, real(Omega, c_double))
+  call CheckStatus(rc, "BVERK4 omega")
+  rc = tc_set_deltas(ctx, 0.0_c_double, 0.0_c_double, real(smooth, c_double))
+  call CheckStatus(rc, "BVERK4 smooth")
+  rc = tc_rk4_step(ctx, activePanels%x, activePanels%relVort, activePanels%area, &
+                   int(activePanels%N, c_int), aParticles%x, int(aParticles%N, c_int), &
+                   passivePanels%x, int(passivePanels%N, c_int), real(dt, c_double), 1_c_int, &
+                   tke, kineticEnergy)
+  call CheckStatus(rc, "BVERK4 step")
+  totalKE = tke(1)
+  if (GetNTracer(aPanels) >= 2) activePanels%tracer(:,2) = kineticEnergy
+  ! :651 particles' relative vorticity follows the new latitude
+  aParticles%relVort(1:aParticles%N) = aParticles%absVort(1:aParticles%N) &
+                                       - 2.0_kreal*Omega*aParticles%x(3,1:aParticles%N)
+  call ScatterPanels(aPanels, activePanels, activeMap, passivePanels, passiveMap)
+  if (procRank < 0 .OR. numProcs < 1) print *, "BVERK4 WARNING : bad MPI arguments"
+end subroutine
+
+end module
