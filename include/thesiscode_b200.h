@@ -122,6 +122,19 @@ int tc_bs_velocity_device(tc_ctx* ctx, int target_class, const double* X, int m,
                           const double* src_x, const double* vort, const double* area, int n,
                           int i0, int i1, double* dX, double* dVort);
 
+/* Allocation-free form of tc_bs_velocity_device (no counterpart in the
+ * reference), for callers that cannot let the library allocate device memory
+ * during the call: applications whose device memory is owned by their own
+ * pool, and stepping loops that cannot take cudaMalloc's implicit device
+ * synchronisation. Same arguments and result; the scratch is a 32 MiB array
+ * compiled into the library (held by every GPU that loads it), so
+ * 32*n + 24*m bytes must fit in 32 MiB, else TC_ERR_ARG. The first call on a
+ * device looks the array's address up (make it before any stream capture);
+ * calls share the array, so calls that overlap on the GPU race. */
+int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, const double* X, int m,
+                                  const double* src_x, const double* vort, const double* area,
+                                  int n, int i0, int i1, double* dX, double* dVort);
+
 /* ---- RK4 (BVERK4, PanelVelocityParallel.f90:435-658) ------------------ */
 /* The drop-in step on host arrays (the gathered active panels, the
  * particles and the divided panels, GatherPanels order): nsteps classical

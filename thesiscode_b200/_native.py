@@ -66,6 +66,8 @@ SIGNATURES: dict[str, tuple] = {
     "tc_bs_velocity": (c_int, [c_void_p, c_int, dp, c_int, dp, dp, dp, c_int, c_int, c_int, dp, dp]),
     "tc_bs_velocity_device": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
                                       c_int, c_int, c_int, c_void_p, c_void_p]),
+    "tc_bs_velocity_device_noalloc": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                              c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
     "tc_rk4_step": (c_int, [c_void_p, dp, dp, dp, c_int, dp, c_int, dp, c_int, c_double, c_int, dp, dp]),
     "tc_rk4_step_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
                                    c_void_p, c_int, c_double, c_int, dp, c_void_p]),

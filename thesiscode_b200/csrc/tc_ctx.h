@@ -110,6 +110,13 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
                           double* total_ke);
 int resolve_slots(tc_ctx* ctx);
 const PairVariant* variant(int precision, int id);
+// Kernels defined in bs_launch.cu and also launched from other files.
+__global__ void pack_kernel(const double* __restrict__ x, const double* __restrict__ zeta,
+                            const double* __restrict__ area, int n, double4* __restrict__ out);
+__global__ void velocity_epilogue_kernel(const double* __restrict__ x, int m, int i0, int i1,
+                                         int row_offset, int n_out, int nchunks,
+                                         const double* __restrict__ partial, double m2omega,
+                                         double* __restrict__ dX, double* __restrict__ dVort);
 int variant_count(int precision);
 int select_variant(tc_ctx* ctx, int precision, int id);
 }  // namespace tcb
