@@ -46,6 +46,10 @@ extern "C" {
                       cancellation-free denominator, FP64 accumulation of
                       per-tile FP32 partial sums                              */
 
+/* ---- visiting order of targets in the FP32C pair kernel --------------- */
+#define TC_ORDER_GIVEN 0   /* the caller's order                             */
+#define TC_ORDER_HILBERT 1 /* sorted along a 3-D Hilbert curve (default)     */
+
 /* ---- target classes (the three RHS routines of the reference) ------- */
 #define TC_ACTIVE 0  /* BVEActiveRHS  PanelVelocityParallel.f90:1287-1334:
                         targets are the sources, self pair excluded,
@@ -101,6 +105,11 @@ int tc_get_omega(tc_ctx* ctx, double* omega);
  * TC_PASSIVE class (default 0.05, :27). */
 int tc_set_smooth(tc_ctx* ctx, double smooth);
 int tc_get_smooth(tc_ctx* ctx, double* smooth);
+/* FP32C only: visit targets in the caller's order or along a Hilbert curve
+ * (default; results are returned in the caller's order either way). The
+ * compensated arithmetic is accurate when a CTA's targets are spatially
+ * close; the Hilbert order guarantees that for any input order. */
+int tc_set_target_order(tc_ctx* ctx, int order);
 /* delta of each target class (reference: 0, 0, smooth). */
 int tc_set_deltas(tc_ctx* ctx, double delta_active, double delta_vertex, double delta_passive);
 int tc_get_deltas(tc_ctx* ctx, double* delta3);

@@ -102,6 +102,31 @@ def test_sampled_rows_level7_with_delta(prec, tol, gpu):
     ctx.close()
 
 
+def test_fp32c_coarse_vertices_level7(ctx32):
+    """The first vertices in the reference's numbering belong to the coarse levels and are spread
+    over the whole sphere; the Hilbert visiting order keeps them within the fine-level bound."""
+    w = configs.gaussian(level=7, delta=0.01)
+    setup(ctx32, w.omega, w.deltas)
+    rows = np.arange(2048)
+    dX, _ = ctx32.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+    dA, _ = ctx32.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    ref = O.rows(1, rows, w.xV, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
+    scale = max(np.abs(dX).max(), np.abs(dA).max())
+    assert np.abs(dX[rows] - ref).max() / scale <= FP32C_TOL_FINE
+
+
+def test_fp32c_accuracy_does_not_depend_on_target_order(ctx32):
+    w = configs.gaussian(level=6, delta=0.01)
+    setup(ctx32, w.omega, w.deltas)
+    rng = np.random.default_rng(3)
+    shuffle = rng.permutation(w.nV)
+    xV = np.ascontiguousarray(w.xV[shuffle])
+    dX, _ = ctx32.velocity(N.TC_VERTEX, xV, w.xA, w.zetaA, w.areaA)
+    rows = np.sort(rng.choice(w.nV, 768, replace=False))
+    ref = O.rows(1, rows, xV, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
+    assert np.abs(dX[rows] - ref).max() / np.abs(dX).max() <= FP32C_TOL_FINE
+
+
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
 def test_rk4_step_parity_mode_golden(prec, tol, gpu):
     g = np.load(GOLDEN / "rh4_parity_l2.npz")

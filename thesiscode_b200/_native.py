@@ -24,6 +24,9 @@ TC_ERR_NOMEM = -6
 # precision
 TC_FP64 = 0
 TC_FP32C = 1
+# FP32C target visiting order
+TC_ORDER_GIVEN = 0
+TC_ORDER_HILBERT = 1
 # target classes
 TC_ACTIVE = 0
 TC_VERTEX = 1
@@ -61,6 +64,7 @@ SIGNATURES: dict[str, tuple] = {
     "tc_get_omega": (c_int, [c_void_p, dp]),
     "tc_set_smooth": (c_int, [c_void_p, c_double]),
     "tc_get_smooth": (c_int, [c_void_p, dp]),
+    "tc_set_target_order": (c_int, [c_void_p, c_int]),
     "tc_set_deltas": (c_int, [c_void_p, c_double, c_double, c_double]),
     "tc_get_deltas": (c_int, [c_void_p, dp]),
     "tc_bs_velocity": (c_int, [c_void_p, c_int, dp, c_int, dp, dp, dp, c_int, c_int, c_int, dp, dp]),

@@ -77,10 +77,17 @@ int velocity_device(tc_ctx* ctx, int cls, const double* X, int m, const double* 
   if (rc) return rc;
   double4* src = ctx->scratch[0].as<double4>();
   if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
-  SegDesc seg{X, i0, i1, 0, cls == TC_ACTIVE ? 0 : tcb::kNoSelf, ctx->delta[cls] * ctx->delta[cls]};
+  int* perm = nullptr;
+  if (ctx->precision == TC_FP32C && ctx->target_order == TC_ORDER_HILBERT && i1 > i0) {
+    if ((rc = ctx->scratch[4].ensure((size_t)m * sizeof(int)))) return rc;
+    perm = ctx->scratch[4].as<int>();
+    if ((rc = tcb::compute_order(ctx, X, i0, i1, perm))) return rc;
+  }
+  SegDesc seg{X, perm, i0, i1, 0, cls == TC_ACTIVE ? 0 : tcb::kNoSelf,
+              ctx->delta[cls] * ctx->delta[cls]};
   int nch = 0;
   if ((rc = tcb::launch_pairs(ctx, &seg, 1, src, n, m, &nch))) return rc;
-  return tcb::launch_velocity_epilogue(ctx, X, m, i0, i1, 0, m, nch, dX,
+  return tcb::launch_velocity_epilogue(ctx, X, perm, m, i0, i1, 0, m, nch, dX,
                                        cls == TC_ACTIVE ? dVort : nullptr);
 }
 
@@ -121,8 +128,10 @@ extern "C" int tc_destroy(tc_ctx* ctx) {
   for (auto& b : ctx->scratch) b.release();
   tcb::Rk4State& R = ctx->rk;
   DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV, &R.xiQ,
-                    &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke, &R.keBlocks, &R.totalKE};
+                    &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke, &R.keBlocks, &R.totalKE,
+                    &R.permA, &R.permV, &R.permQ};
   for (DevBuf* b : bufs) b->release();
+  for (auto& b : ctx->order_buf) b.release();
   for (cudaEvent_t e : ctx->pair_events) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -179,6 +188,13 @@ extern "C" int tc_set_smooth(tc_ctx* ctx, double smooth) {
 extern "C" int tc_get_smooth(tc_ctx* ctx, double* smooth) {
   if (!ctx || !smooth) return TC_ERR_ARG;
   *smooth = ctx->delta[TC_PASSIVE];
+  return TC_OK;
+}
+
+extern "C" int tc_set_target_order(tc_ctx* ctx, int order) {
+  if (!ctx || (order != TC_ORDER_GIVEN && order != TC_ORDER_HILBERT)) return TC_ERR_ARG;
+  ctx->target_order = order;
+  ctx->rk.ordered = false;
   return TC_OK;
 }
 
@@ -314,6 +330,7 @@ extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
   if (nV) TC_CUDA_TRY(cudaMemcpyAsync(R.x0V.ptr, xV, 3 * (size_t)nV * D, kind, s));
   if (nQ) TC_CUDA_TRY(cudaMemcpyAsync(R.x0Q.ptr, xQ, 3 * (size_t)nQ * D, kind, s));
   R.ready = true;
+  R.ordered = false;
   return TC_OK;
 }
 
@@ -358,17 +375,36 @@ extern "C" int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int
     return TC_ERR_ARG;
   }
   const bool first = stage == 0;
+  const double* tx[3] = {first ? R.x0A.as<double>() : R.xiA.as<double>(),
+                         first ? R.x0V.as<double>() : R.xiV.as<double>(),
+                         first ? R.x0Q.as<double>() : R.xiQ.as<double>()};
+  const int range[6] = {a0, a1, v0, v1, q0, q1};
+  // FP32C visiting order: computed from the stage-0 positions once per step
+  // (targets move by O(dt) within a step) and whenever the ranges change.
+  const bool want_order = ctx->precision == TC_FP32C && ctx->target_order == TC_ORDER_HILBERT;
+  if (!want_order) {
+    R.ordered = false;
+  } else if (first || !R.ordered || memcmp(range, R.order_range, sizeof(range)) != 0) {
+    tcb::DevBuf* pb[3] = {&R.permA, &R.permV, &R.permQ};
+    const int nn[3] = {R.nA, R.nV, R.nQ};
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = pb[c]->ensure((size_t)std::max(nn[c], 1) * sizeof(int)))) return rc;
+      if ((rc = tcb::compute_order(ctx, tx[c], range[2 * c], range[2 * c + 1], pb[c]->as<int>())))
+        return rc;
+    }
+    memcpy(R.order_range, range, sizeof(range));
+    R.ordered = true;
+  }
+  const bool ord = want_order && R.ordered;
   SegDesc segs[3] = {
-      {first ? R.x0A.as<double>() : R.xiA.as<double>(), a0, a1, 0, 0,
-       ctx->delta[0] * ctx->delta[0]},
-      {first ? R.x0V.as<double>() : R.xiV.as<double>(), v0, v1, R.nA, tcb::kNoSelf,
+      {tx[0], ord ? R.permA.as<int>() : nullptr, a0, a1, 0, 0, ctx->delta[0] * ctx->delta[0]},
+      {tx[1], ord ? R.permV.as<int>() : nullptr, v0, v1, R.nA, tcb::kNoSelf,
        ctx->delta[1] * ctx->delta[1]},
-      {first ? R.x0Q.as<double>() : R.xiQ.as<double>(), q0, q1, R.nA + R.nV, tcb::kNoSelf,
+      {tx[2], ord ? R.permQ.as<int>() : nullptr, q0, q1, R.nA + R.nV, tcb::kNoSelf,
        ctx->delta[2] * ctx->delta[2]}};
   int nch = 0;
   const int n_out = R.nA + R.nV + R.nQ;
   if ((rc = tcb::launch_pairs(ctx, segs, 3, R.src.as<double4>(), R.nA, n_out, &nch))) return rc;
-  const int range[6] = {a0, a1, v0, v1, q0, q1};
   return tcb::launch_stage_epilogue(ctx, stage, dt, range, nch, total_ke_device);
 }
 
@@ -542,10 +578,12 @@ extern "C" int tc_reset_rk4(tc_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   tcb::Rk4State& R = ctx->rk;
   DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV, &R.xiQ,
-                    &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke, &R.keBlocks, &R.totalKE};
+                    &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke, &R.keBlocks, &R.totalKE,
+                    &R.permA, &R.permV, &R.permQ};
   for (DevBuf* b : bufs) b->release();
   ctx->partial.release();
   R.ready = false;
+  R.ordered = false;
   R.nA = R.nV = R.nQ = 0;
   return TC_OK;
 }

@@ -22,6 +22,7 @@ constexpr int kNoSelf = INT32_MIN;
 
 struct TargetSeg {
   const double* x;  // targets, x[3*i + c]
+  const int* perm;  // FP32C: target at position p in [i0,i1) is perm[p] (null: p itself)
   int i0, i1;       // target range [i0, i1) computed by this launch
   int out_offset;   // partial row of target i is out_offset + i
   int self_offset;  // source index of target i is i + self_offset (ACTIVE), else kNoSelf
@@ -178,18 +179,27 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // Each CTA takes the position c of the middle target of its tile as origin.
 // Sources are converted once per CTA and tile from FP64 to FP32 offsets
 // s_k = fl32(x_k - c) (their FP64 difference rounded once), targets likewise
-// t_i = fl32(x_i - c). For spatially coherent target tiles (the icosahedral
-// orderings are quad-tree orders) |s_k|, |t_i| are small for every nearby
-// pair, so d = s_k - t_i carries an absolute error of a few ulps of the tile
-// size instead of ulps of 1. The denominator uses the cancellation-free form
+// t_i = fl32(x_i - c). Targets are visited in a spatially coherent order (a
+// Hilbert order computed by the library, or the caller's order), so a CTA's
+// targets form a compact patch and every nearby pair has small |s_k|, |t_i|:
+// d = s_k - t_i carries an absolute error of a few ulps of the patch size
+// instead of ulps of 1. The denominator uses the cancellation-free form
 //     2(1 - x_i.x_k) + 2 delta^2 = |x_k - x_i|^2 + e_i + e_k,
 //     e_i = 1 - |x_i|^2 + 2 delta^2,  e_k = 1 - |x_k|^2
-// (evaluated in FP64 while staging, then rounded to FP32)
-// so near pairs keep full FP32 relative accuracy. Two targets share each
-// f32x2 instruction (FADD2/FFMA2/FMUL2 halve the issue slots; the FP32 pipe
-// stays the bound). Per-target FP32 partial sums are added into FP64
-// accumulators every FLUSH sources.
+// (evaluated in FP64 once per point, then rounded to FP32), so near pairs
+// keep full FP32 relative accuracy. Two targets share each f32x2 instruction
+// (FADD2/FFMA2/FMUL2 halve the issue slots; the FP32 pipe stays the bound).
+// Per-target FP32 partial sums are added into FP64 accumulators every FLUSH
+// sources.
+//
+// Self pair (TC_ACTIVE, targets are sources): s_k and t_i are rounded from
+// the same double, so d = 0 exactly; e_i carries a +1e-30 bias that keeps
+// D = e_i + e_k away from 0 and from FP32 subnormals (e is either 0 or at
+// least ~1e-17 in magnitude), so w stays finite and w*d adds exactly 0. No
+// per-pair mask is needed.
 // ---------------------------------------------------------------------------
+constexpr float kSelfBias = 1e-30f;
+
 template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
   static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
@@ -201,29 +211,28 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const TargetSeg& G = find_seg(P, blockIdx.x);
   const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
   const int i_end = G.i1;
-  const bool has_self = G.self_offset != kNoSelf;
+  const int* perm = G.perm;
 
-  const int mid = min(tile0 + TB / 2, i_end - 1);
+  const int mid_pos = min(tile0 + TB / 2, i_end - 1);
+  const int mid = perm ? perm[mid_pos] : mid_pos;
   const double cx = G.x[3 * (size_t)mid], cy = G.x[3 * (size_t)mid + 1],
                cz = G.x[3 * (size_t)mid + 2];
 
   float2 ntx[NPAIR], nty[NPAIR], ntz[NPAIR], ei[NPAIR];
   float2 fx[NPAIR], fy[NPAIR], fz[NPAIR];
   double ax[NPAIR][2], ay[NPAIR][2], az[NPAIR][2];
-  int self_k[NPAIR][2];
 #pragma unroll
   for (int p = 0; p < NPAIR; ++p) {
     float tv[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      int i = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
-      int ld = i < i_end ? i : mid;
+      int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
+      int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
       double x = G.x[3 * (size_t)ld], y = G.x[3 * (size_t)ld + 1], z = G.x[3 * (size_t)ld + 2];
       tv[h][0] = -(float)(x - cx);
       tv[h][1] = -(float)(y - cy);
       tv[h][2] = -(float)(z - cz);
-      tv[h][3] = (float)((1.0 - (x * x + y * y + z * z)) + 2.0 * G.d2);
-      self_k[p][h] = has_self ? i + G.self_offset : -1;
+      tv[h][3] = (float)((1.0 - (x * x + y * y + z * z)) + 2.0 * G.d2) + kSelfBias;
       ax[p][h] = ay[p][h] = az[p][h] = 0.0;
     }
     ntx[p] = make_float2(tv[0][0], tv[1][0]);
@@ -232,8 +241,6 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
     ei[p] = make_float2(tv[0][3], tv[1][3]);
     fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
   }
-  const int self_lo = has_self ? tile0 + G.self_offset : 0;
-  const int self_hi = has_self ? min(tile0 + TB, i_end) + G.self_offset : 0;
 
   const int c0 = (int)blockIdx.y * P.chunk_len;
   const int c1 = min(P.n, c0 + P.chunk_len);
@@ -255,56 +262,28 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
       smC[j] = make_float2(e, e);
     }
     __syncthreads();
-    const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
     for (int jf = 0; jf < TS; jf += FLUSH) {
-      if (!diag) {
 #pragma unroll UNROLL
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = smA[j];
-          const float4 b = smB[j];
-          const float2 ee = smC[j];
-          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
+      for (int j = jf; j < jf + FLUSH; ++j) {
+        const float4 a = smA[j];
+        const float4 b = smB[j];
+        const float2 ee = smC[j];
+        const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
+        const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
 #pragma unroll
-          for (int p = 0; p < NPAIR; ++p) {
-            const float2 dx = __fadd2_rn(sxx, ntx[p]);
-            const float2 dy = __fadd2_rn(syy, nty[p]);
-            const float2 dz = __fadd2_rn(szz, ntz[p]);
-            float2 D = __fadd2_rn(ee, ei[p]);
-            D = __ffma2_rn(dx, dx, D);
-            D = __ffma2_rn(dy, dy, D);
-            D = __ffma2_rn(dz, dz, D);
-            const float2 r = make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
-            const float2 w = __fmul2_rn(gg, r);
-            fx[p] = __ffma2_rn(w, dx, fx[p]);
-            fy[p] = __ffma2_rn(w, dy, fy[p]);
-            fz[p] = __ffma2_rn(w, dz, fz[p]);
-          }
-        }
-      } else {
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = smA[j];
-          const float4 b = smB[j];
-          const float2 ee = smC[j];
-          const int k = ts + j;
-          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
-#pragma unroll
-          for (int p = 0; p < NPAIR; ++p) {
-            const float2 dx = __fadd2_rn(sxx, ntx[p]);
-            const float2 dy = __fadd2_rn(syy, nty[p]);
-            const float2 dz = __fadd2_rn(szz, ntz[p]);
-            float2 D = __fadd2_rn(ee, ei[p]);
-            D = __ffma2_rn(dx, dx, D);
-            D = __ffma2_rn(dy, dy, D);
-            D = __ffma2_rn(dz, dz, D);
-            float2 w = __fmul2_rn(gg, make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y)));
-            w.x = (k == self_k[p][0]) ? 0.f : w.x;
-            w.y = (k == self_k[p][1]) ? 0.f : w.y;
-            fx[p] = __ffma2_rn(w, dx, fx[p]);
-            fy[p] = __ffma2_rn(w, dy, fy[p]);
-            fz[p] = __ffma2_rn(w, dz, fz[p]);
-          }
+        for (int p = 0; p < NPAIR; ++p) {
+          const float2 dx = __fadd2_rn(sxx, ntx[p]);
+          const float2 dy = __fadd2_rn(syy, nty[p]);
+          const float2 dz = __fadd2_rn(szz, ntz[p]);
+          float2 D = __fadd2_rn(ee, ei[p]);
+          D = __ffma2_rn(dx, dx, D);
+          D = __ffma2_rn(dy, dy, D);
+          D = __ffma2_rn(dz, dz, D);
+          const float2 r = make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
+          const float2 w = __fmul2_rn(gg, r);
+          fx[p] = __ffma2_rn(w, dx, fx[p]);
+          fy[p] = __ffma2_rn(w, dy, fy[p]);
+          fz[p] = __ffma2_rn(w, dz, fz[p]);
         }
       }
 #pragma unroll
@@ -319,137 +298,19 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
       }
     }
   }
+  // partial rows are indexed by position in the visiting order
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
 #pragma unroll
   for (int p = 0; p < NPAIR; ++p) {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      int i = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
-      if (i < i_end) {
-        out[i] = ax[p][h];
-        out[stride + i] = ay[p][h];
-        out[2 * stride + i] = az[p][h];
+      int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
+      if (pos < i_end) {
+        out[pos] = ax[p][h];
+        out[stride + pos] = ay[p][h];
+        out[2 * stride + pos] = az[p][h];
       }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// FP32-compensated pair kernel, scalar form: the same arithmetic as
-// pair_fp32c_kernel with TPT independent targets per thread and plain FP32
-// instructions (no f32x2 packing); a source is one float4 {sx, sy, sz, 2G}
-// plus one float e in shared memory.
-// ---------------------------------------------------------------------------
-template <int NT, int TPT, int TS, int FLUSH, int MINB, int UNROLL>
-__global__ void __launch_bounds__(NT, MINB) pair_fp32s_kernel(const PairLaunch P) {
-  static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
-  __shared__ float4 smA[TS];  // (sx, sy, sz, 2G)
-  __shared__ float smE[TS];   // e
-  constexpr int TB = NT * TPT;
-  const TargetSeg& G = find_seg(P, blockIdx.x);
-  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
-  const int i_end = G.i1;
-  const bool has_self = G.self_offset != kNoSelf;
-
-  const int mid = min(tile0 + TB / 2, i_end - 1);
-  const double cx = G.x[3 * (size_t)mid], cy = G.x[3 * (size_t)mid + 1],
-               cz = G.x[3 * (size_t)mid + 2];
-
-  float ntx[TPT], nty[TPT], ntz[TPT], ei[TPT], fx[TPT], fy[TPT], fz[TPT];
-  double ax[TPT], ay[TPT], az[TPT];
-  int self_k[TPT];
-#pragma unroll
-  for (int t = 0; t < TPT; ++t) {
-    int i = tile0 + (int)threadIdx.x + t * NT;
-    int ld = i < i_end ? i : mid;
-    double x = G.x[3 * (size_t)ld], y = G.x[3 * (size_t)ld + 1], z = G.x[3 * (size_t)ld + 2];
-    ntx[t] = -(float)(x - cx);
-    nty[t] = -(float)(y - cy);
-    ntz[t] = -(float)(z - cz);
-    ei[t] = (float)((1.0 - (x * x + y * y + z * z)) + 2.0 * G.d2);
-    self_k[t] = has_self ? i + G.self_offset : -1;
-    ax[t] = ay[t] = az[t] = 0.0;
-    fx[t] = fy[t] = fz[t] = 0.f;
-  }
-  const int self_lo = has_self ? tile0 + G.self_offset : 0;
-  const int self_hi = has_self ? min(tile0 + TB, i_end) + G.self_offset : 0;
-
-  const int c0 = (int)blockIdx.y * P.chunk_len;
-  const int c1 = min(P.n, c0 + P.chunk_len);
-  for (int ts = c0; ts < c1; ts += TS) {
-    __syncthreads();
-    for (int j = threadIdx.x; j < TS; j += NT) {
-      int k = ts + j;
-      float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f;
-      if (k < c1) {
-        const double4 q = P.src[k];
-        sx = (float)(q.x - cx);
-        sy = (float)(q.y - cy);
-        sz = (float)(q.z - cz);
-        g = (float)(2.0 * q.w);
-        e = (float)(1.0 - (q.x * q.x + q.y * q.y + q.z * q.z));
-      }
-      smA[j] = make_float4(sx, sy, sz, g);
-      smE[j] = e;
-    }
-    __syncthreads();
-    const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
-    for (int jf = 0; jf < TS; jf += FLUSH) {
-      if (!diag) {
-#pragma unroll UNROLL
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = smA[j];
-          const float e = smE[j];
-#pragma unroll
-          for (int t = 0; t < TPT; ++t) {
-            const float dx = a.x + ntx[t], dy = a.y + nty[t], dz = a.z + ntz[t];
-            float D = fmaf(dx, dx, e + ei[t]);
-            D = fmaf(dy, dy, D);
-            D = fmaf(dz, dz, D);
-            const float w = a.w * rcp_approx_f32(D);
-            fx[t] = fmaf(w, dx, fx[t]);
-            fy[t] = fmaf(w, dy, fy[t]);
-            fz[t] = fmaf(w, dz, fz[t]);
-          }
-        }
-      } else {
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = smA[j];
-          const float e = smE[j];
-          const int k = ts + j;
-#pragma unroll
-          for (int t = 0; t < TPT; ++t) {
-            const float dx = a.x + ntx[t], dy = a.y + nty[t], dz = a.z + ntz[t];
-            float D = fmaf(dx, dx, e + ei[t]);
-            D = fmaf(dy, dy, D);
-            D = fmaf(dz, dz, D);
-            float w = a.w * rcp_approx_f32(D);
-            w = (k == self_k[t]) ? 0.f : w;
-            fx[t] = fmaf(w, dx, fx[t]);
-            fy[t] = fmaf(w, dy, fy[t]);
-            fz[t] = fmaf(w, dz, fz[t]);
-          }
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < TPT; ++t) {
-        ax[t] += (double)fx[t];
-        ay[t] += (double)fy[t];
-        az[t] += (double)fz[t];
-        fx[t] = fy[t] = fz[t] = 0.f;
-      }
-    }
-  }
-  const size_t stride = (size_t)P.n_out;
-  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-#pragma unroll
-  for (int t = 0; t < TPT; ++t) {
-    int i = tile0 + (int)threadIdx.x + t * NT;
-    if (i < i_end) {
-      out[i] = ax[t];
-      out[stride + i] = ay[t];
-      out[2 * stride + i] = az[t];
     }
   }
 }

@@ -44,10 +44,7 @@ template <int NT, int TPT, int MINB, bool FUSED>
 void launch64(dim3 g, cudaStream_t s, const PairLaunch& P) {
   pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(P);
 }
-template <int NT, int TPT, int FLUSH, int MINB, int UNROLL>
-void launch32s(dim3 g, cudaStream_t s, const PairLaunch& P) {
-  pair_fp32s_kernel<NT, TPT, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(P);
-}
+
 template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL>
 void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
   pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(P);
@@ -56,10 +53,6 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
 #define V64(NT, TPT, MINB, FUSED)                                                 \
   PairVariant { TC_FP64, NT, TPT, kTS, FUSED, MINB, 0, launch64<NT, TPT, MINB, FUSED>, \
                 (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED> }
-#define V32S(NT, TPT, FLUSH, MINB, UNROLL)                                               \
-  PairVariant { TC_FP32C, NT, TPT, kTS, FLUSH, MINB, UNROLL,                              \
-                launch32s<NT, TPT, FLUSH, MINB, UNROLL>,                                  \
-                (const void*)pair_fp32s_kernel<NT, TPT, kTS, FLUSH, MINB, UNROLL> }
 #define V32(NT, NPAIR, FLUSH, MINB, UNROLL)                                              \
   PairVariant { TC_FP32C, NT, 2 * NPAIR, kTS, FLUSH, MINB, UNROLL,                        \
                 launch32<NT, NPAIR, FLUSH, MINB, UNROLL>,                                 \
@@ -72,9 +65,8 @@ const PairVariant kVariants64[] = {
     V64(256, 2, 5, false), V64(256, 4, 2, false),
 };
 const PairVariant kVariants32[] = {
-    V32(256, 2, 32, 3, 4),  V32(256, 2, 64, 2, 4),  V32(128, 1, 32, 8, 8), V32(256, 2, 16, 2, 4),
-    V32S(256, 4, 32, 2, 4), V32S(256, 8, 32, 1, 2), V32S(128, 8, 32, 2, 4), V32S(256, 4, 16, 2, 4),
-    V32S(256, 6, 32, 2, 2), V32S(128, 4, 32, 4, 4),
+    V32(256, 2, 32, 3, 4), V32(256, 2, 64, 2, 4), V32(128, 1, 32, 8, 8), V32(256, 2, 16, 2, 4),
+    V32(128, 2, 32, 6, 4), V32(256, 1, 32, 4, 8),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
@@ -150,6 +142,7 @@ int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src,
     if (len <= 0) continue;
     TargetSeg& g = P.seg[k++];
     g.x = segs[s].x;
+    g.perm = fp64 ? nullptr : segs[s].perm;
     g.i0 = segs[s].i0;
     g.i1 = segs[s].i1;
     g.out_offset = segs[s].out_offset;
@@ -237,17 +230,22 @@ __device__ __forceinline__ void velocity_from_sum(const double x[3], const doubl
   u[2] = (x[0] * T[1] - x[1] * T[0]) / kMinus4Pi;
 }
 
-__global__ void velocity_epilogue_kernel(const double* __restrict__ x, int m, int i0, int i1,
-                                         int row_offset, int n_out, int nchunks,
-                                         const double* __restrict__ partial, double m2omega,
-                                         double* __restrict__ dX, double* __restrict__ dVort) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+// Thread p handles partial row p; with a visiting order perm (a permutation
+// of [i0, i1)) that row belongs to target perm[p].
+__global__ void velocity_epilogue_kernel(const double* __restrict__ x, const int* __restrict__ perm,
+                                         int m, int i0, int i1, int row_offset, int n_out,
+                                         int nchunks, const double* __restrict__ partial,
+                                         double m2omega, double* __restrict__ dX,
+                                         double* __restrict__ dVort) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= m) return;
+  const bool in_range = p >= i0 && p < i1;
+  const int i = (in_range && perm) ? perm[p] : p;
   double u[3] = {0.0, 0.0, 0.0};
-  if (i >= i0 && i < i1) {
+  if (in_range) {
     double xi[3] = {x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2]};
     double T[3];
-    reduce_row(partial, nchunks, (size_t)n_out, (size_t)(row_offset + i), T);
+    reduce_row(partial, nchunks, (size_t)n_out, (size_t)(row_offset + p), T);
     velocity_from_sum(xi, T, u);
   }
   dX[3 * (size_t)i] = u[0];
@@ -256,12 +254,12 @@ __global__ void velocity_epilogue_kernel(const double* __restrict__ x, int m, in
   if (dVort) dVort[i] = m2omega * u[2];
 }
 
-int launch_velocity_epilogue(tc_ctx* ctx, const double* x, int m, int i0, int i1, int row_offset,
-                             int n_out, int nchunks, double* dX, double* dVort) {
+int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int m, int i0, int i1,
+                             int row_offset, int n_out, int nchunks, double* dX, double* dVort) {
   if (m <= 0) return TC_OK;
   velocity_epilogue_kernel<<<(m + 255) / 256, 256, 0, ctx->stream>>>(
-      x, m, i0, i1, row_offset, n_out, nchunks, ctx->partial.as<double>(), -2.0 * ctx->omega, dX,
-      dVort);
+      x, ctx->precision == TC_FP64 ? nullptr : perm, m, i0, i1, row_offset, n_out, nchunks,
+      ctx->partial.as<double>(), -2.0 * ctx->omega, dX, dVort);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
   return TC_OK;
@@ -291,6 +289,7 @@ struct StageEpi {
   double4* src;
   double* ke;
   double* keBlocks;
+  const int *permA, *permV, *permQ;  // visiting orders of the three ranges (null: as stored)
 };
 
 constexpr int kEpiThreads = 256;
@@ -301,18 +300,20 @@ __global__ void __launch_bounds__(kEpiThreads) stage_epilogue_kernel(const Stage
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double ke_area = 0.0;
   if (r < lenA + lenV + lenQ) {
-    int cls, i;
+    int cls, pos;
     if (r < lenA) {
       cls = 0;
-      i = E.a0 + r;
+      pos = E.a0 + r;
     } else if (r < lenA + lenV) {
       cls = 1;
-      i = E.v0 + (r - lenA);
+      pos = E.v0 + (r - lenA);
     } else {
       cls = 2;
-      i = E.q0 + (r - lenA - lenV);
+      pos = E.q0 + (r - lenA - lenV);
     }
-    const int row = (cls == 0 ? 0 : cls == 1 ? E.nA : E.nA + E.nV) + i;
+    const int* perm = cls == 0 ? E.permA : cls == 1 ? E.permV : E.permQ;
+    const int i = perm ? perm[pos] : pos;
+    const int row = (cls == 0 ? 0 : cls == 1 ? E.nA : E.nA + E.nV) + pos;
     double* x0 = cls == 0 ? E.x0A : cls == 1 ? E.x0V : E.x0Q;
     double* xi = cls == 0 ? E.xiA : cls == 1 ? E.xiV : E.xiQ;
     double* nw = cls == 0 ? E.newA : cls == 1 ? E.newV : E.newQ;
@@ -420,6 +421,10 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
   E.src = R.src.as<double4>();
   E.ke = R.ke.as<double>();
   E.keBlocks = R.keBlocks.as<double>();
+  const bool ordered = ctx->precision != TC_FP64 && R.ordered;
+  E.permA = ordered ? R.permA.as<int>() : nullptr;
+  E.permV = ordered ? R.permV.as<int>() : nullptr;
+  E.permQ = ordered ? R.permQ.as<int>() : nullptr;
   const int rows = (E.a1 - E.a0) + (E.v1 - E.v0) + (E.q1 - E.q0);
   const int blocks = std::max(1, (rows + kEpiThreads - 1) / kEpiThreads);
   if (stage == 0) {

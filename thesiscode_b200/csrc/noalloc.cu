@@ -142,6 +142,7 @@ extern "C" int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, cons
     nchunks = (n + chunk_len - 1) / chunk_len;
     tcb::PairLaunch P{};
     P.seg[0].x = X;
+    P.seg[0].perm = nullptr;  // targets in the caller's order
     P.seg[0].i0 = i0;
     P.seg[0].i1 = i1;
     P.seg[0].out_offset = 0;
@@ -159,7 +160,7 @@ extern "C" int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, cons
   }
   if (m > 0) {
     tcb::velocity_epilogue_kernel<<<(m + 255) / 256, 256, 0, ctx->stream>>>(
-        X, m, i0, i1, 0, m, nchunks, partial, -2.0 * ctx->omega, dX,
+        X, nullptr, m, i0, i1, 0, m, nchunks, partial, -2.0 * ctx->omega, dX,
         target_class == TC_ACTIVE ? dVort : nullptr);
     TC_CUDA_TRY(cudaGetLastError());
   }

@@ -41,6 +41,7 @@ struct PairVariant {
 // Target segment as the host describes it before tiles are assigned.
 struct SegDesc {
   const double* x;
+  const int* perm;  // visiting order of [i0, i1) (FP32C only; null: as stored)
   int i0, i1;
   int out_offset;
   int self_offset;
@@ -60,6 +61,9 @@ struct Rk4State {
   DevBuf ke;                            // kineticEnergy(nA), stage 1
   DevBuf keBlocks;                      // per-block partial sums of KE*A
   DevBuf totalKE;                       // one value per step
+  DevBuf permA, permV, permQ;           // FP32C visiting orders (Hilbert), per class
+  bool ordered = false;                 // perm* hold orders of the current stage ranges
+  int order_range[6] = {0, 0, 0, 0, 0, 0};
 };
 
 }  // namespace tcb
@@ -74,7 +78,9 @@ struct tc_ctx {
   double delta[3] = {0.0, 0.0, 0.05};               // ACTIVE, VERTEX, PASSIVE (smooth, :27)
   tcb::PairCfg cfg64{256, 2, 256};
   tcb::PairCfg cfg32{256, 4, 256};
-  int var64 = 2, var32 = 0;  // pair-kernel variants in use (see kVariants64/32)
+  int var64 = 2, var32 = 4;  // pair-kernel variants in use (see kVariants64/32)
+  int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
+  tcb::DevBuf order_buf[4];             // keys, sorted keys, indices, sort scratch
   int min_chunk = 4096;   // smallest source chunk a CTA walks
   int max_chunks = 64;
   int slots64 = 0, slots32 = 0;  // resident CTAs per GPU for each kernel
@@ -101,8 +107,10 @@ int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* 
                 double4* out);
 // dX (3*m) and dVort (m, nullable) for rows [i0, i1), zero elsewhere; partial
 // rows are row_offset + i.
-int launch_velocity_epilogue(tc_ctx* ctx, const double* x, int m, int i0, int i1,
+int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int m, int i0, int i1,
                              int row_offset, int n_out, int nchunks, double* dX, double* dVort);
+// perm[i0..i1) <- i0..i1-1 sorted along a Hilbert curve through x[3*i..]
+int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm);
 // One RK4 stage epilogue over the three classes' ranges.
 // total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
 // stage 0; nchunks is what launch_pairs returned for this stage.
@@ -113,10 +121,11 @@ const PairVariant* variant(int precision, int id);
 // Kernels defined in bs_launch.cu and also launched from other files.
 __global__ void pack_kernel(const double* __restrict__ x, const double* __restrict__ zeta,
                             const double* __restrict__ area, int n, double4* __restrict__ out);
-__global__ void velocity_epilogue_kernel(const double* __restrict__ x, int m, int i0, int i1,
-                                         int row_offset, int n_out, int nchunks,
-                                         const double* __restrict__ partial, double m2omega,
-                                         double* __restrict__ dX, double* __restrict__ dVort);
+__global__ void velocity_epilogue_kernel(const double* __restrict__ x, const int* __restrict__ perm,
+                                         int m, int i0, int i1, int row_offset, int n_out,
+                                         int nchunks, const double* __restrict__ partial,
+                                         double m2omega, double* __restrict__ dX,
+                                         double* __restrict__ dVort);
 int variant_count(int precision);
 int select_variant(tc_ctx* ctx, int precision, int id);
 }  // namespace tcb
