@@ -243,6 +243,45 @@ def time_e2e(w, precision, steps, device):
     return dict(ms=sum(times) / len(times), h2d=h2d, d2h=d2h)
 
 
+def time_adjoint(device, level=6, steps=20, ckpt=5):
+    """Adjoint/forward time ratio on the zonal-jet workload (delta 0.02, dt 0.005, FP64): the
+    adjoint call (forward sweep with checkpoints + recomputation + backward) against a forward
+    call over the same steps, both through the host-pointer C ABI."""
+    import torch
+
+    from thesiscode_b200 import _native as N
+    from thesiscode_b200.panel_velocity import Context
+
+    w = build_workload("jet_l6") if level == 6 else None
+    ctx = Context(device, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    J, gz, gx = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
+
+    def fwd():
+        x, z = w.xA.copy(), w.zetaA.copy()
+        ctx.rk4_step(x, z, w.areaA, np.zeros((0, 3)), np.zeros((0, 3)), w.dt, steps)
+
+    def adj():
+        N.call("tc_rk4_adjoint", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt,
+               steps, ckpt, N.TC_J_ENSTROPHY, 0, N.dptr(J), N.dptr(gz), N.dptr(gx))
+
+    fwd()
+    adj()
+    tf, ta = [], []
+    for _ in range(2):
+        t = time.perf_counter()
+        fwd()
+        tf.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        adj()
+        ta.append(time.perf_counter() - t)
+    ctx.close()
+    return {"workload": f"jet level {w.level} ({w.nA} panels), delta 0.02, {steps} RK4 steps dt {w.dt}, "
+                        f"checkpoint every {ckpt}, J = sum zeta^2 A", "forward_s": min(tf), "adjoint_s": min(ta),
+            "adjoint_over_forward": min(ta) / min(tf), "J": float(J[0])}
+
+
 def sample_rows(w, frac, seed=11):
     rng = np.random.default_rng(seed)
     ra = np.sort(rng.choice(w.nA, max(1, int(w.nA * frac)), replace=False)).astype(np.int32)
@@ -346,6 +385,8 @@ def run_ours(args):
             line["e2e"] = {"value": w.interactions_per_step() / (e2e["ms"] * 1e-3), "unit": "interactions/s",
                            "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                            "ms_per_step": e2e["ms"], "api": "tc_rk4_step (host pointers, pinned)"}
+        if world == 1 and not args.quick:
+            line["adjoint"] = time_adjoint(device)
         if world == 1 and not args.no_cpu:
             cb = cpu_baseline(w)
             line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],

@@ -59,6 +59,10 @@ extern "C" {
 #define TC_PASSIVE 2 /* BVESmoothVelocity :1376-1412: divided panels,
                         delta = smooth (0.05 by default, :27)                */
 
+/* ---- end-time functionals of the adjoint ------------------------------ */
+#define TC_J_ENSTROPHY 0 /* J = sum_j zeta_j^2 A_j over the active panels  */
+#define TC_J_PROBE 1     /* J = zeta of one active panel                   */
+
 /* ---- throughput probe kinds (tc_probe_peak) --------------------------- */
 #define TC_PROBE_FFMA 0
 #define TC_PROBE_FFMA2 1
@@ -144,6 +148,25 @@ int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, const double* X
                                   const double* src_x, const double* vort, const double* area,
                                   int n, int i0, int i1, double* dX, double* dVort);
 
+/* ---- Voronoi generators, SoA (VoronoiVelocityParallel.f90) ------------ */
+/* BVEVelocity (:487-515) on x(n), y(n), z(n): rows [i0,i1) summed over all n
+ * sources (unused N_Max slots have vort = area = 0), self excluded. As in the
+ * reference only dx is zeroed first: dy and dz add to what the caller holds,
+ * then all three are divided by (-4 pi) over the whole arrays, and
+ * dVort = -2 Omega dz over all rows (nullable). */
+int tc_bs_velocity_soa(tc_ctx* ctx, const double* x, const double* y, const double* z,
+                       const double* vort, const double* area, int n, int i0, int i1, double* dx,
+                       double* dy, double* dz, double* dVort);
+int tc_bs_velocity_soa_device(tc_ctx* ctx, const double* x, const double* y, const double* z,
+                              const double* vort, const double* area, int n, int i0, int i1,
+                              double* dx, double* dy, double* dz, double* dVort);
+/* Voronoi BVERK4 (:304-478) without the Delaunay/Voronoi rebuild (:480-482,
+ * host-side STRIPACK in the reference): nsteps RK4 steps of the n used
+ * generators, updated in place. */
+int tc_rk4_soa_step(tc_ctx* ctx, double* x, double* y, double* z, double* relVort,
+                    const double* area, int n, double dt, int nsteps, double* totalKE,
+                    double* kineticEnergy);
+
 /* ---- RK4 (BVERK4, PanelVelocityParallel.f90:435-658) ------------------ */
 /* The drop-in step on host arrays (the gathered active panels, the
  * particles and the divided panels, GatherPanels order): nsteps classical
@@ -167,6 +190,18 @@ int tc_rk4_store(tc_ctx* ctx, double* xA, double* zetaA, double* xV, double* xQ,
                  double* kineticEnergy, int on_device);
 /* ResetRK4 (:321-372): frees the state; call after a remesh changes N. */
 int tc_reset_rk4(tc_ctx* ctx);
+
+/* ---- adjoint (no counterpart in the reference) ------------------------- */
+/* Gradient of J(T), T = nsteps*dt, with respect to the initial state of the
+ * active panels, through nsteps RK4 steps of the active panels (the only ones
+ * that feed back; particles and divided panels are passive): the discrete
+ * adjoint of the step (exact gradient of the RK4 map), FP64, state
+ * checkpointed every ckpt_every steps and stage inputs recomputed per
+ * segment. Host arrays: xA0(3,nA), zetaA0, areaA in; J, g_zeta0(nA),
+ * g_x0(3,nA) out. Replaces the context's loaded RK4 state. */
+int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA,
+                   int nA, double dt, int nsteps, int ckpt_every, int functional, int probe,
+                   double* J, double* g_zeta0, double* g_x0);
 
 /* ---- stage primitives for target-sharded multi-rank runs -------------- */
 /* Pack stage-1 sources of the loaded state into TC_BUF_SOURCES. */

@@ -1,0 +1,206 @@
+"""Adjoint of the RK4 Biot-Savart step (tc_rk4_adjoint) on the GPU.
+
+Checked against (1) an FP64 reference gradient: the same RK4 map written in
+torch on the CPU and differentiated by torch.autograd (small grids), and
+(2) centred finite differences (eps = 1e-6) of J through the GPU forward
+step, on seeded entries: vorticities and tangent-plane position
+perturbations (renormalised to the sphere). The adjoint is wrapped in a
+torch.autograd.Function here, in the test harness only.
+"""
+import numpy as np
+import pytest
+import torch
+
+from thesiscode_b200 import _native as N
+from thesiscode_b200 import configs
+from thesiscode_b200.panel_velocity import Context
+
+pytestmark = pytest.mark.gpu
+
+
+def adjoint(ctx, xA, zA, aA, dt, nsteps, ckpt, functional=N.TC_J_ENSTROPHY, probe=0):
+    J = np.zeros(1)
+    gz = np.zeros_like(zA)
+    gx = np.zeros_like(xA)
+    N.call("tc_rk4_adjoint", ctx.handle, N.dptr(np.ascontiguousarray(xA)), N.dptr(np.ascontiguousarray(zA)),
+           N.dptr(np.ascontiguousarray(aA)), xA.shape[0], dt, nsteps, ckpt, functional, probe,
+           N.dptr(J), N.dptr(gz), N.dptr(gx))
+    return J[0], gz, gx
+
+
+class EnstrophyAfterRK4(torch.autograd.Function):
+    """J = sum zeta(T)^2 A through the library's forward and adjoint (test harness only)."""
+
+    @staticmethod
+    def forward(ctx_, x, z, area, lib_ctx, dt, nsteps, ckpt):
+        J, gz, gx = adjoint(lib_ctx, x.detach().numpy(), z.detach().numpy(), area.numpy(), dt, nsteps, ckpt)
+        ctx_.save_for_backward(torch.from_numpy(gx), torch.from_numpy(gz))
+        return torch.tensor(J, dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx_, g):
+        gx, gz = ctx_.saved_tensors
+        return g * gx, g * gz, None, None, None, None, None
+
+
+def torch_rk4_enstrophy(x, z, area, omega, d2, dt, nsteps, probe=None):
+    n = x.shape[0]
+    eye = torch.eye(n, dtype=torch.float64)
+
+    def rhs(x, z):
+        D = 1.0 + d2 - x @ x.T
+        W = (z * area)[None, :] / (D + eye) * (1.0 - eye)
+        S = W @ x
+        u = -torch.cross(x, S, dim=1) / (4.0 * np.pi)
+        return u, -2.0 * omega * u[:, 2]
+
+    for _ in range(nsteps):
+        k1x, k1z = rhs(x, z)
+        k1x, k1z = dt * k1x, dt * k1z
+        k2x, k2z = rhs(x + 0.5 * k1x, z + 0.5 * k1z)
+        k2x, k2z = dt * k2x, dt * k2z
+        k3x, k3z = rhs(x + 0.5 * k2x, z + 0.5 * k2z)
+        k3x, k3z = dt * k3x, dt * k3z
+        k4x, k4z = rhs(x + k3x, z + k3z)
+        k4x, k4z = dt * k4x, dt * k4z
+        x = x + k1x / 6 + k2x / 3 + k3x / 3 + k4x / 6
+        z = z + k1z / 6 + k2z / 3 + k3z / 3 + k4z / 6
+    return (z * z * area).sum() if probe is None else z[probe]
+
+
+def jet(level):
+    return configs.jet(level=level, delta=0.02, dt=0.005, steps=20)
+
+
+def test_adjoint_matches_torch_autograd_fp64(gpu):
+    # a Gaussian vortex: not zonally symmetric, so u_z != 0 and dJ/dx is not roundoff-sized
+    w = configs.gaussian(level=2, delta=0.02, dt=0.01)
+    ctx = Context(0, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    nsteps, ckpt = 6, 4  # a partial last segment too
+    x = torch.tensor(w.xA, requires_grad=True)
+    z = torch.tensor(w.zetaA, requires_grad=True)
+    area = torch.tensor(w.areaA)
+    Jt = torch_rk4_enstrophy(x, z, area, w.omega, w.deltas[0] ** 2, w.dt, nsteps)
+    Jt.backward()
+    x2 = torch.tensor(w.xA, requires_grad=True)
+    z2 = torch.tensor(w.zetaA, requires_grad=True)
+    Jl = EnstrophyAfterRK4.apply(x2, z2, area, ctx, w.dt, nsteps, ckpt)
+    Jl.backward()
+    assert abs(Jl.item() - Jt.item()) <= 1e-12 * abs(Jt.item())
+    gz_ref, gx_ref = z.grad.numpy(), x.grad.numpy()
+    scale = np.abs(gz_ref).max()
+    assert np.abs(z2.grad.numpy() - gz_ref).max() <= 1e-10 * scale
+    # sum zeta^2 A is an invariant of the semi-discrete flow (dJ/dt = -4 Omega sum G_j u_z,j = 0 by
+    # the antisymmetry of the pair term), so dJ/dx is only RK4-truncation sized: compare absolutely
+    assert np.abs(x2.grad.numpy() - gx_ref).max() <= 1e-10 * scale
+    ctx.close()
+
+
+def test_adjoint_probe_gradient_matches_torch_autograd_fp64(gpu):
+    """J = zeta_p(T): its position gradient is O(1), a full check of the position adjoint."""
+    w = configs.gaussian(level=2, delta=0.02, dt=0.01)
+    ctx = Context(0, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    nsteps, ckpt, p = 6, 4, 41
+    x = torch.tensor(w.xA, requires_grad=True)
+    z = torch.tensor(w.zetaA, requires_grad=True)
+    Jt = torch_rk4_enstrophy(x, z, torch.tensor(w.areaA), w.omega, w.deltas[0] ** 2, w.dt, nsteps, probe=p)
+    Jt.backward()
+    J, gz, gx = adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, nsteps, ckpt, N.TC_J_PROBE, p)
+    assert abs(J - Jt.item()) <= 1e-12 * abs(Jt.item())
+    assert np.abs(gx).max() > 1e-3
+    assert np.abs(gx - x.grad.numpy()).max() <= 1e-10 * np.abs(gx).max()
+    assert np.abs(gz - z.grad.numpy()).max() <= 1e-10 * np.abs(gz).max()
+    ctx.close()
+
+
+def test_adjoint_matches_centred_fd(gpu):
+    """32 seeded entries, eps = 1e-6, level 4 jet (delta 0.02), 20 steps, checkpoint every 5.
+    Error measure: |FD - adjoint| / max over all gradient entries <= 1e-6 (for J = sum zeta^2 A the
+    position entries are RK4-truncation sized and FD resolves them only to ulp(J)/eps). The position
+    adjoint is then checked by FD through the probe functional J = zeta_p(T), whose position
+    gradient is O(1)."""
+    w = jet(4)
+    ctx = Context(0, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    nsteps, ckpt, eps = 20, 5, 1e-6
+    J, gz, gx = adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, nsteps, ckpt)
+
+    def final(x, z):
+        x, z = x.copy(), z.copy()
+        ctx.rk4_step(x, z, w.areaA, np.zeros((0, 3)), np.zeros((0, 3)), w.dt, nsteps)
+        return z
+
+    def J_of(x, z):
+        return float(np.sum(final(x, z) ** 2 * w.areaA))
+
+    def tangent_pair(j, t):
+        xp, xm = w.xA.copy(), w.xA.copy()
+        xp[j] = (w.xA[j] + eps * t) / np.linalg.norm(w.xA[j] + eps * t)
+        xm[j] = (w.xA[j] - eps * t) / np.linalg.norm(w.xA[j] - eps * t)
+        return xp, xm
+
+    def tangent(rng, j):
+        t = rng.standard_normal(3)
+        t -= t.dot(w.xA[j]) * w.xA[j]
+        return t / np.linalg.norm(t)
+
+    assert abs(J_of(w.xA, w.zetaA) - J) <= 1e-12 * abs(J)
+    rng = np.random.default_rng(33)
+    picks = rng.choice(w.nA, 32, replace=False)
+    scale = max(np.abs(gz).max(), np.abs(gx).max())
+    for m, j in enumerate(picks):
+        if m % 2 == 0:  # vorticity entry
+            zp, zm = w.zetaA.copy(), w.zetaA.copy()
+            zp[j] += eps
+            zm[j] -= eps
+            fd = (J_of(w.xA, zp) - J_of(w.xA, zm)) / (2 * eps)
+            assert abs(fd - gz[j]) <= 1e-6 * scale, (j, fd, gz[j])
+        else:  # position entry along a tangent direction, renormalised
+            t = tangent(rng, j)
+            xp, xm = tangent_pair(j, t)
+            fd = (J_of(xp, w.zetaA) - J_of(xm, w.zetaA)) / (2 * eps)
+            assert abs(fd - gx[j].dot(t)) <= 1e-6 * scale, (j, fd, gx[j].dot(t))
+    # position adjoint through the probe functional
+    p = int(picks[0])
+    Jp, gzp, gxp = adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, nsteps, ckpt, N.TC_J_PROBE, p)
+    near = np.argsort(np.linalg.norm(w.xA - w.xA[p], axis=1))[:8]  # the panels that move zeta_p most
+    for j in near:
+        t = tangent(rng, j)
+        xp, xm = tangent_pair(j, t)
+        fd = (final(xp, w.zetaA)[p] - final(xm, w.zetaA)[p]) / (2 * eps)
+        assert abs(fd - gxp[j].dot(t)) <= 1e-6 * np.abs(gxp).max(), (j, fd, gxp[j].dot(t))
+    ctx.close()
+
+
+def test_adjoint_probe_functional_and_errors(gpu):
+    w = jet(2)
+    ctx = Context(0, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    J, gz, gx = adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, 3, 2, N.TC_J_PROBE, 17)
+    x, z = w.xA.copy(), w.zetaA.copy()
+    ctx.rk4_step(x, z, w.areaA, np.zeros((0, 3)), np.zeros((0, 3)), w.dt, 3)
+    assert J == z[17]
+    eps = 1e-6
+    zp, zm = w.zetaA.copy(), w.zetaA.copy()
+    zp[17] += eps
+    zm[17] -= eps
+    vals = []
+    for zz in (zp, zm):
+        x, z = w.xA.copy(), zz.copy()
+        ctx.rk4_step(x, z, w.areaA, np.zeros((0, 3)), np.zeros((0, 3)), w.dt, 3)
+        vals.append(z[17])
+    assert abs((vals[0] - vals[1]) / (2 * eps) - gz[17]) <= 1e-6
+    with pytest.raises(N.TcError):
+        adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, 3, 0)  # checkpoint interval 0
+    c32 = Context(0, "fp32c")
+    with pytest.raises(N.TcError) as e:
+        adjoint(c32, w.xA, w.zetaA, w.areaA, w.dt, 3, 2)
+    assert e.value.status == N.TC_ERR_STATE
+    c32.close()
+    ctx.close()

@@ -34,6 +34,9 @@ TC_PASSIVE = 2
 # probes
 (TC_PROBE_FFMA, TC_PROBE_FFMA2, TC_PROBE_DFMA, TC_PROBE_RCP32, TC_PROBE_RCP64, TC_PROBE_DDIV,
  TC_PROBE_F2F) = range(7)
+# adjoint functionals
+TC_J_ENSTROPHY = 0
+TC_J_PROBE = 1
 # RK4 device buffers
 TC_BUF_SOURCES, TC_BUF_XA, TC_BUF_ZETA, TC_BUF_XV, TC_BUF_XQ, TC_BUF_KE = range(6)
 
@@ -72,6 +75,9 @@ SIGNATURES: dict[str, tuple] = {
                                       c_int, c_int, c_int, c_void_p, c_void_p]),
     "tc_bs_velocity_device_noalloc": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
                                               c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "tc_bs_velocity_soa": (c_int, [c_void_p, dp, dp, dp, dp, dp, c_int, c_int, c_int, dp, dp, dp, dp]),
+    "tc_bs_velocity_soa_device": (c_int, [c_void_p] + [c_void_p] * 5 + [c_int] * 3 + [c_void_p] * 4),
+    "tc_rk4_soa_step": (c_int, [c_void_p, dp, dp, dp, dp, dp, c_int, c_double, c_int, dp, dp]),
     "tc_rk4_step": (c_int, [c_void_p, dp, dp, dp, c_int, dp, c_int, dp, c_int, c_double, c_int, dp, dp]),
     "tc_rk4_step_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
                                    c_void_p, c_int, c_double, c_int, dp, c_void_p]),
@@ -84,6 +90,7 @@ SIGNATURES: dict[str, tuple] = {
     "tc_rk4_stage_range": (c_int, [c_void_p, c_int, c_double, c_int, c_int, c_int, c_int, c_int, c_int,
                                    c_void_p]),
     "tc_rk4_device_buffer": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    "tc_rk4_adjoint": (c_int, [c_void_p, dp, dp, dp, c_int, c_double, c_int, c_int, c_int, c_int, dp, dp, dp]),
     "tc_rk4_copy_rows": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int]),
     "tc_pair_variant_count": (c_int, [c_int, ip]),
     "tc_pair_variant_info": (c_int, [c_int, c_int, ip]),

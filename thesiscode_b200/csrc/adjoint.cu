@@ -1,0 +1,450 @@
+// Discrete adjoint of the RK4 Biot-Savart step: the gradient of an end-time
+// functional J(x(T), zeta(T)) with respect to the initial positions and
+// vorticities of the active panels, through nsteps classical RK4 steps
+// (the forward map of BVERK4, PanelVelocityParallel.f90:435-658, restricted
+// to the active panels, which are the only ones that feed back).
+//
+// Vector-Jacobian product of one RHS evaluation. With cotangent (mu_x, mu_z)
+// on (dx/dt, dzeta/dt) = (u, -2 Omega u_z), the cotangent on u is
+// ut_i = mu_x,i + (-2 Omega mu_z,i) z_hat, and for
+//     L = sum_i ut_i . u_i,  u_i = -1/(4 pi) sum_{k != i} G_k (x_i x x_k) / D_ik,
+//     D_ik = 1 + delta^2 - x_i . x_k,  G_k = zeta_k A_k,
+// with v_i = ut_i x x_i and s_ik = x_k . v_i (= ut_i . (x_i x x_k)):
+//     dL/dx_i   = -1/(4 pi) [ S1_i x ut_i + S2_i + G_i (P_i + Q_i) ]
+//     dL/dzeta_k = -A_k/(4 pi) R_k
+//     S1_i = sum_k G_k/D x_k,      S2_i = sum_k G_k s_ik/D^2 x_k     (target side)
+//     P_k  = sum_i v_i/D,          Q_k  = sum_i s_ik/D^2 x_i,
+//     R_k  = sum_i s_ik/D                                            (source side)
+// Both sums are O(N^2) pair loops like the forward one; two kernels compute
+// them in FP64 with the forward kernel's tiling (source tiles in shared
+// memory, targets in registers, per-chunk partial sums reduced in a fixed
+// order). RK4 backward per step, with Y_s the stage inputs and k_s = dt F(Y_s):
+//     lk4 = l'/6,               lY4 = dt J(Y4)^T lk4
+//     lk3 = l'/3 + lY4,         lY3 = dt J(Y3)^T lk3
+//     lk2 = l'/3 + lY3/2,       lY2 = dt J(Y2)^T lk2
+//     lk1 = l'/6 + lY2/2,       lY1 = dt J(Y1)^T lk1
+//     l   = l' + lY1 + lY2 + lY3 + lY4.
+// The state is checkpointed every `ckpt_every` steps on the forward sweep;
+// the backward sweep recomputes each segment's stage inputs from its
+// checkpoint (one extra forward pass in total).
+#include <cmath>
+#include <vector>
+
+#include "tc_ctx.h"
+
+namespace tcb {
+namespace {
+
+constexpr int kAdjNT = 128;
+constexpr int kAdjTS = 128;
+constexpr double kInv4Pi = 0.0795774715459476678844418816862571810;  // 1/(4 pi)
+
+struct AdjLaunch {
+  const double* x;       // positions x[3i+c] (targets and sources: the same panels)
+  const double4* src;    // pass 1: {x, y, z, G}; pass 2: {x, y, z, v_x}
+  const double2* src2;   // pass 2: {v_y, v_z}
+  const double* v;       // pass 1: v_i per target (3 per row)
+  int n;
+  int chunk_len;
+  double one_plus_d2;
+  double* partial;       // [chunk][W][n]
+};
+
+__device__ __forceinline__ double adj_rcp(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
+// Pass 1: per target i, S1 = sum_k G_k/D x_k and S2 = sum_k G_k s_ik/D^2 x_k
+// (6 outputs per row), accumulated on offsets d = x_k - x_i for accuracy:
+// S1 = W1 x_i + sum w1 d, S2 = W2 x_i + sum w2 d.
+__global__ void __launch_bounds__(kAdjNT) adj_target_kernel(const AdjLaunch P) {
+  __shared__ double4 sm[kAdjTS];
+  const int i = blockIdx.x * kAdjNT + threadIdx.x;
+  const int ld = i < P.n ? i : P.n - 1;
+  const double xi0 = P.x[3 * (size_t)ld], xi1 = P.x[3 * (size_t)ld + 1], xi2 = P.x[3 * (size_t)ld + 2];
+  const double v0 = P.v[3 * (size_t)ld], v1 = P.v[3 * (size_t)ld + 1], v2 = P.v[3 * (size_t)ld + 2];
+  double a1x = 0, a1y = 0, a1z = 0, w1s = 0, a2x = 0, a2y = 0, a2z = 0, w2s = 0;
+  const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
+  for (int ts = c0; ts < c1; ts += kAdjTS) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < kAdjTS; j += kAdjNT) {
+      int k = ts + j;
+      sm[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int j = 0; j < kAdjTS; ++j) {
+      const double4 q = sm[j];
+      double D = fma(-q.x, xi0, P.one_plus_d2);
+      D = fma(-q.y, xi1, D);
+      D = fma(-q.z, xi2, D);
+      double r = adj_rcp(D);
+      r = (ts + j == i) ? 0.0 : r;  // self pair (D may be 0: r is then NaN before the select)
+      const double w1 = q.w * r;
+      const double dx = q.x - xi0, dy = q.y - xi1, dz = q.z - xi2;
+      const double s = fma(dx, v0, fma(dy, v1, dz * v2));  // x_k.v_i = d.v_i (x_i.v_i = 0)
+      const double w2 = w1 * s * r;
+      a1x = fma(w1, dx, a1x);
+      a1y = fma(w1, dy, a1y);
+      a1z = fma(w1, dz, a1z);
+      w1s += w1;
+      a2x = fma(w2, dx, a2x);
+      a2y = fma(w2, dy, a2y);
+      a2z = fma(w2, dz, a2z);
+      w2s += w2;
+    }
+  }
+  if (i < P.n) {
+    const size_t n = (size_t)P.n;
+    double* out = P.partial + (size_t)blockIdx.y * 6 * n + i;
+    out[0] = fma(w1s, xi0, a1x);
+    out[n] = fma(w1s, xi1, a1y);
+    out[2 * n] = fma(w1s, xi2, a1z);
+    out[3 * n] = fma(w2s, xi0, a2x);
+    out[4 * n] = fma(w2s, xi1, a2y);
+    out[5 * n] = fma(w2s, xi2, a2z);
+  }
+}
+
+// Pass 2: per panel k (as a source of the forward sum), the transposed sums
+// over the panels i that it acts on: P_k, Q_k (3 each), R_k (7 outputs).
+// Here the thread's row is k and the shared-memory stream is i with {x_i, v_i}.
+__global__ void __launch_bounds__(kAdjNT) adj_source_kernel(const AdjLaunch P) {
+  __shared__ double4 sa[kAdjTS];
+  __shared__ double2 sb[kAdjTS];
+  const int k = blockIdx.x * kAdjNT + threadIdx.x;
+  const int ld = k < P.n ? k : P.n - 1;
+  const double xk0 = P.x[3 * (size_t)ld], xk1 = P.x[3 * (size_t)ld + 1], xk2 = P.x[3 * (size_t)ld + 2];
+  double px = 0, py = 0, pz = 0, qx = 0, qy = 0, qz = 0, rr = 0;
+  const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
+  for (int ts = c0; ts < c1; ts += kAdjTS) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < kAdjTS; j += kAdjNT) {
+      int i = ts + j;
+      sa[j] = i < c1 ? P.src[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sb[j] = i < c1 ? P.src2[i] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int j = 0; j < kAdjTS; ++j) {
+      const double4 a = sa[j];
+      const double2 b = sb[j];
+      double D = fma(-a.x, xk0, P.one_plus_d2);
+      D = fma(-a.y, xk1, D);
+      D = fma(-a.z, xk2, D);
+      double r = adj_rcp(D);
+      r = (ts + j == k) ? 0.0 : r;
+      // s_ik = x_k . v_i = (x_k - x_i) . v_i
+      const double s = fma(xk0 - a.x, a.w, fma(xk1 - a.y, b.x, (xk2 - a.z) * b.y));
+      const double sr = s * r;
+      const double sr2 = sr * r;
+      px = fma(r, a.w, px);
+      py = fma(r, b.x, py);
+      pz = fma(r, b.y, pz);
+      qx = fma(sr2, a.x, qx);
+      qy = fma(sr2, a.y, qy);
+      qz = fma(sr2, a.z, qz);
+      rr += sr;
+    }
+  }
+  if (k < P.n) {
+    const size_t n = (size_t)P.n;
+    double* out = P.partial + (size_t)blockIdx.y * 7 * n + k;
+    out[0] = px;
+    out[n] = py;
+    out[2 * n] = pz;
+    out[3 * n] = qx;
+    out[4 * n] = qy;
+    out[5 * n] = qz;
+    out[6 * n] = rr;
+  }
+}
+
+// v_i = ut_i x x_i with ut_i = mu_x,i + (-2 Omega mu_z,i) z_hat, mu = dt * l_k.
+__global__ void adj_prepare_kernel(const double* __restrict__ x, const double* __restrict__ lkx,
+                                   const double* __restrict__ lkz, const double* __restrict__ zeta,
+                                   const double* __restrict__ area, int n, double dt, double m2omega,
+                                   double* __restrict__ ut, double* __restrict__ v,
+                                   double4* __restrict__ src1, double4* __restrict__ src2a,
+                                   double2* __restrict__ src2b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t b = 3 * (size_t)i;
+  const double u0 = dt * lkx[b], u1 = dt * lkx[b + 1],
+               u2 = dt * lkx[b + 2] + m2omega * (dt * lkz[i]);
+  const double x0 = x[b], x1 = x[b + 1], x2 = x[b + 2];
+  const double v0 = u1 * x2 - u2 * x1, v1 = u2 * x0 - u0 * x2, v2 = u0 * x1 - u1 * x0;
+  ut[b] = u0;
+  ut[b + 1] = u1;
+  ut[b + 2] = u2;
+  v[b] = v0;
+  v[b + 1] = v1;
+  v[b + 2] = v2;
+  src1[i] = make_double4(x0, x1, x2, zeta[i] * area[i]);
+  src2a[i] = make_double4(x0, x1, x2, v0);
+  src2b[i] = make_double2(v1, v2);
+}
+
+// lY_i = J(Y)^T mu: gx (3 per row) and gz (1 per row), written to out_x/out_z.
+__global__ void adj_combine_kernel(const double* __restrict__ x, const double* __restrict__ ut,
+                                   const double* __restrict__ zeta, const double* __restrict__ area,
+                                   int n, const double* __restrict__ p1, int ch1,
+                                   const double* __restrict__ p2, int ch2, double* __restrict__ out_x,
+                                   double* __restrict__ out_z) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t N = (size_t)n, b = 3 * (size_t)i;
+  double s[6] = {0, 0, 0, 0, 0, 0}, t[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int c = 0; c < ch1; ++c)
+    for (int w = 0; w < 6; ++w) s[w] += p1[((size_t)c * 6 + w) * N + i];
+  for (int c = 0; c < ch2; ++c)
+    for (int w = 0; w < 7; ++w) t[w] += p2[((size_t)c * 7 + w) * N + i];
+  const double u0 = ut[b], u1 = ut[b + 1], u2 = ut[b + 2];
+  const double G = zeta[i] * area[i];
+  // S1 x ut + S2 + G (P + Q)
+  const double g0 = (s[1] * u2 - s[2] * u1) + s[3] + G * (t[0] + t[3]);
+  const double g1 = (s[2] * u0 - s[0] * u2) + s[4] + G * (t[1] + t[4]);
+  const double g2 = (s[0] * u1 - s[1] * u0) + s[5] + G * (t[2] + t[5]);
+  out_x[b] = -kInv4Pi * g0;
+  out_x[b + 1] = -kInv4Pi * g1;
+  out_x[b + 2] = -kInv4Pi * g2;
+  out_z[i] = -kInv4Pi * area[i] * t[6];
+}
+
+// Linear combinations of adjoint vectors: y = a*x + b*y (in place on y), n4 = 4*nA
+// values laid out as [3*nA positions | nA vorticities] in one buffer.
+__global__ void axpby_kernel(double a, const double* __restrict__ x, double b, double* __restrict__ y,
+                             size_t n) {
+  size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j < n) y[j] = a * x[j] + b * y[j];
+}
+
+}  // namespace
+}  // namespace tcb
+
+using tcb::DevBuf;
+
+namespace {
+
+struct AdjWork {
+  int nA = 0;
+  size_t n4 = 0;
+  DevBuf ck;        // checkpoints: ncheck x (3nA + nA)
+  DevBuf ys;        // stage inputs of one segment: (steps*4) x (3nA + nA)
+  DevBuf lam, lk, tmp;  // adjoint state, lk, accumulators (4nA each)
+  DevBuf ut, v, s1, s2a, s2b, p1, p2;
+};
+
+int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, double dt,
+                  double* out) {
+  // y and lk, out: [3nA | nA] buffers
+  const int n = W.nA;
+  const double* yx = y;
+  const double* yz = y + 3 * (size_t)n;
+  const double* area = ctx->rk.areaA.as<double>();
+  const int threads = 256, blocks = (n + threads - 1) / threads;
+  tcb::adj_prepare_kernel<<<blocks, threads, 0, ctx->stream>>>(
+      yx, lk, lk + 3 * (size_t)n, yz, area, n, dt, -2.0 * ctx->omega, W.ut.as<double>(),
+      W.v.as<double>(), W.s1.as<double4>(), W.s2a.as<double4>(), W.s2b.as<double2>());
+  TC_CUDA_TRY(cudaGetLastError());
+  const int tiles = (n + tcb::kAdjNT - 1) / tcb::kAdjNT;
+  const int slots = 8 * ctx->num_sms;
+  int S = std::max(1, std::min(32, (2 * slots + tiles - 1) / tiles));
+  int chunk = (n + S - 1) / S;
+  chunk = (chunk + tcb::kAdjTS - 1) / tcb::kAdjTS * tcb::kAdjTS;
+  S = (n + chunk - 1) / chunk;
+  int rc;
+  if ((rc = W.p1.ensure((size_t)S * 6 * n * sizeof(double))) ||
+      (rc = W.p2.ensure((size_t)S * 7 * n * sizeof(double))))
+    return rc;
+  const double d = ctx->delta[TC_ACTIVE];
+  tcb::AdjLaunch P1{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), n, chunk, 1.0 + d * d,
+                    W.p1.as<double>()};
+  tcb::adj_target_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P1);
+  TC_CUDA_TRY(cudaGetLastError());
+  tcb::AdjLaunch P2{yx, W.s2a.as<double4>(), W.s2b.as<double2>(), nullptr, n, chunk, 1.0 + d * d,
+                    W.p2.as<double>()};
+  tcb::adj_source_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P2);
+  TC_CUDA_TRY(cudaGetLastError());
+  tcb::adj_combine_kernel<<<blocks, threads, 0, ctx->stream>>>(
+      yx, W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, W.p2.as<double>(), S, out,
+      out + 3 * (size_t)n);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 4;
+  ctx->pair_launches += 2;
+  ctx->pair_interactions += 2LL * n * (long long)(n - 1);
+  return TC_OK;
+}
+
+int axpby(tc_ctx* ctx, double a, const double* x, double b, double* y, size_t n) {
+  tcb::axpby_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(a, x, b, y, n);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  return TC_OK;
+}
+
+// Copy the RK4 state (x0A, z0) into a [3nA | nA] buffer, or back.
+int state_copy(tc_ctx* ctx, double* buf, bool to_state) {
+  tcb::Rk4State& R = ctx->rk;
+  const size_t b3 = 3 * (size_t)R.nA * sizeof(double), b1 = (size_t)R.nA * sizeof(double);
+  if (to_state) {
+    TC_CUDA_TRY(cudaMemcpyAsync(R.x0A.ptr, buf, b3, cudaMemcpyDeviceToDevice, ctx->stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(R.z0.ptr, buf + 3 * (size_t)R.nA, b1, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+  } else {
+    TC_CUDA_TRY(cudaMemcpyAsync(buf, R.x0A.ptr, b3, cudaMemcpyDeviceToDevice, ctx->stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(buf + 3 * (size_t)R.nA, R.z0.ptr, b1, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+  }
+  return TC_OK;
+}
+
+int stage_input_copy(tc_ctx* ctx, double* buf) {
+  tcb::Rk4State& R = ctx->rk;
+  const size_t b3 = 3 * (size_t)R.nA * sizeof(double), b1 = (size_t)R.nA * sizeof(double);
+  TC_CUDA_TRY(cudaMemcpyAsync(buf, R.xiA.ptr, b3, cudaMemcpyDeviceToDevice, ctx->stream));
+  TC_CUDA_TRY(cudaMemcpyAsync(buf + 3 * (size_t)R.nA, R.ziA.ptr, b1, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+  return TC_OK;
+}
+
+// One forward step of the active panels; when ys != null the four stage
+// inputs are stored there ([4][3nA | nA]).
+int forward_step(tc_ctx* ctx, double dt, double* ys) {
+  tcb::Rk4State& R = ctx->rk;
+  const size_t n4 = 4 * (size_t)R.nA;
+  int rc;
+  if ((rc = tc_rk4_pack_sources(ctx))) return rc;
+  if (ys && (rc = state_copy(ctx, ys, false))) return rc;
+  for (int s = 0; s < 4; ++s) {
+    if ((rc = tc_rk4_stage_range(ctx, s, dt, 0, R.nA, 0, 0, 0, 0, nullptr))) return rc;
+    if (ys && s < 3 && (rc = stage_input_copy(ctx, ys + (size_t)(s + 1) * n4))) return rc;
+  }
+  return TC_OK;
+}
+
+__global__ void enstrophy_seed_kernel(const double* __restrict__ z, const double* __restrict__ area,
+                                      int n, double* __restrict__ lam, double* __restrict__ jblk) {
+  __shared__ double red[256];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double c = 0.0;
+  if (i < n) {
+    lam[i] = 2.0 * z[i] * area[i];
+    c = z[i] * z[i] * area[i];
+  }
+  red[threadIdx.x] = c;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) jblk[blockIdx.x] = red[0];
+}
+
+}  // namespace
+
+// Gradient of J at time nsteps*dt with respect to the initial active-panel
+// state. functional: TC_J_ENSTROPHY (J = sum zeta^2 A) or TC_J_PROBE
+// (J = zeta of panel `probe` at the end). Inputs are host arrays; outputs:
+// J (host scalar), g_zeta0 (nA), g_x0 (3*nA), host arrays.
+extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0,
+                              const double* areaA, int nA, double dt, int nsteps, int ckpt_every,
+                              int functional, int probe, double* J, double* g_zeta0, double* g_x0) {
+  if (!ctx || nA <= 0 || nsteps < 0 || ckpt_every <= 0 || !xA0 || !zetaA0 || !areaA || !J ||
+      !g_zeta0 || !g_x0 || (functional != TC_J_ENSTROPHY && functional != TC_J_PROBE) ||
+      (functional == TC_J_PROBE && (probe < 0 || probe >= nA))) {
+    tc_record_error("tc_rk4_adjoint: bad arguments");
+    return TC_ERR_ARG;
+  }
+  if (ctx->precision != TC_FP64) {
+    tc_record_error("tc_rk4_adjoint: the adjoint runs in FP64 (tc_set_precision(ctx, TC_FP64))");
+    return TC_ERR_STATE;
+  }
+  int rc = tc_rk4_load(ctx, xA0, zetaA0, areaA, nA, nullptr, 0, nullptr, 0, 0);
+  if (rc) return rc;
+  AdjWork W;
+  W.nA = nA;
+  W.n4 = 4 * (size_t)nA;
+  const size_t B = W.n4 * sizeof(double);
+  const int ncheck = (nsteps + ckpt_every - 1) / ckpt_every + 1;
+  if ((rc = W.ck.ensure((size_t)ncheck * B)) || (rc = W.ys.ensure((size_t)ckpt_every * 4 * B)) ||
+      (rc = W.lam.ensure(B)) || (rc = W.lk.ensure(B)) || (rc = W.tmp.ensure(B)) ||
+      (rc = W.ut.ensure(3 * (size_t)nA * sizeof(double))) ||
+      (rc = W.v.ensure(3 * (size_t)nA * sizeof(double))) ||
+      (rc = W.s1.ensure((size_t)nA * sizeof(double4))) ||
+      (rc = W.s2a.ensure((size_t)nA * sizeof(double4))) ||
+      (rc = W.s2b.ensure((size_t)nA * sizeof(double2))))
+    return rc;
+  double* ck = W.ck.as<double>();
+  // forward sweep with checkpoints
+  for (int step = 0; step < nsteps; ++step) {
+    if (step % ckpt_every == 0 && (rc = state_copy(ctx, ck + (size_t)(step / ckpt_every) * W.n4, false)))
+      return rc;
+    if ((rc = forward_step(ctx, dt, nullptr))) return rc;
+  }
+  // seed: l(T) = dJ/dX(T)
+  double* lam = W.lam.as<double>();
+  TC_CUDA_TRY(cudaMemsetAsync(lam, 0, B, ctx->stream));
+  const double* zT = ctx->rk.z0.as<double>();
+  if (functional == TC_J_ENSTROPHY) {
+    const int blocks = (nA + 255) / 256;
+    if ((rc = W.tmp.ensure(std::max(B, (size_t)blocks * sizeof(double))))) return rc;
+    enstrophy_seed_kernel<<<blocks, 256, 0, ctx->stream>>>(zT, ctx->rk.areaA.as<double>(), nA,
+                                                           lam + 3 * (size_t)nA, W.tmp.as<double>());
+    TC_CUDA_TRY(cudaGetLastError());
+    std::vector<double> jb(blocks);
+    TC_CUDA_TRY(cudaMemcpyAsync(jb.data(), W.tmp.ptr, blocks * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    double acc = 0.0;
+    for (double v : jb) acc += v;
+    *J = acc;
+  } else {
+    TC_CUDA_TRY(cudaMemcpyAsync(J, zT + probe, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    const double one = 1.0;
+    TC_CUDA_TRY(cudaMemcpyAsync(lam + 3 * (size_t)nA + probe, &one, sizeof(double),
+                                cudaMemcpyHostToDevice, ctx->stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  // backward sweep, one checkpoint segment at a time
+  double* ys = W.ys.as<double>();
+  double* lk = W.lk.as<double>();
+  double* acc = W.tmp.as<double>();
+  double* ly = nullptr;
+  DevBuf lyb;
+  if ((rc = lyb.ensure(B))) return rc;
+  ly = lyb.as<double>();
+  for (int seg = (nsteps - 1) / ckpt_every; seg >= 0 && nsteps > 0; --seg) {
+    const int s0 = seg * ckpt_every, s1 = std::min(nsteps, s0 + ckpt_every);
+    if ((rc = state_copy(ctx, ck + (size_t)seg * W.n4, true))) return rc;
+    for (int step = s0; step < s1; ++step)
+      if ((rc = forward_step(ctx, dt, ys + (size_t)(step - s0) * 4 * W.n4))) return rc;
+    for (int step = s1 - 1; step >= s0; --step) {
+      const double* Y = ys + (size_t)(step - s0) * 4 * W.n4;
+      // acc = l' (the identity part); lk for stage 4 = l'/6
+      TC_CUDA_TRY(cudaMemcpyAsync(acc, lam, B, cudaMemcpyDeviceToDevice, ctx->stream));
+      const double bcoef[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+      const double ccoef[4] = {0.0, 0.5, 0.5, 1.0};  // Y_s = X + c_s k_{s-1}
+      // lk_4 = l'/6
+      if ((rc = axpby(ctx, bcoef[3], lam, 0.0, lk, W.n4))) return rc;
+      for (int s = 3; s >= 0; --s) {
+        if ((rc = adj_stage_vjp(ctx, W, Y + (size_t)s * W.n4, lk, dt, ly))) return rc;
+        if ((rc = axpby(ctx, 1.0, ly, 1.0, acc, W.n4))) return rc;       // l += lY_s
+        if (s > 0) {                                                     // lk_{s-1} = b l' + c_s lY_s
+          if ((rc = axpby(ctx, bcoef[s - 1], lam, 0.0, lk, W.n4))) return rc;
+          if ((rc = axpby(ctx, ccoef[s], ly, 1.0, lk, W.n4))) return rc;
+        }
+      }
+      TC_CUDA_TRY(cudaMemcpyAsync(lam, acc, B, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+  }
+  TC_CUDA_TRY(cudaMemcpyAsync(g_x0, lam, 3 * (size_t)nA * sizeof(double), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+  TC_CUDA_TRY(cudaMemcpyAsync(g_zeta0, lam + 3 * (size_t)nA, (size_t)nA * sizeof(double),
+                              cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}

@@ -266,6 +266,103 @@ extern "C" int tc_bs_velocity(tc_ctx* ctx, int target_class, const double* X, in
 }
 
 // ---------------------------------------------------------------------------
+// Voronoi SoA sum (BVEVelocity, VoronoiVelocityParallel.f90:487-515)
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void soa_to_aos_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                  const double* __restrict__ z, int n, double* __restrict__ out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  out[3 * (size_t)j] = x[j];
+  out[3 * (size_t)j + 1] = y[j];
+  out[3 * (size_t)j + 2] = z[j];
+}
+
+// BVEVelocity zeroes only dx (:494): dy and dz add to what the caller holds,
+// and the whole arrays are divided by (-4 pi) (:510-512); dVort over all rows.
+__global__ void soa_finish_kernel(const double* __restrict__ u, int n, double m2omega,
+                                  double* __restrict__ dx, double* __restrict__ dy,
+                                  double* __restrict__ dz, double* __restrict__ dVort) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double s = -4.0 * 3.141592653589793238462643383279502884;
+  dx[j] = u[3 * (size_t)j];
+  dy[j] = dy[j] / s + u[3 * (size_t)j + 1];
+  dz[j] = dz[j] / s + u[3 * (size_t)j + 2];
+  if (dVort) dVort[j] = m2omega * dz[j];
+}
+
+}  // namespace
+
+extern "C" int tc_bs_velocity_soa_device(tc_ctx* ctx, const double* x, const double* y,
+                                         const double* z, const double* vort, const double* area,
+                                         int n, int i0, int i1, double* dx, double* dy, double* dz,
+                                         double* dVort) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (n < 0 || i0 < 0 || i1 < i0 || i1 > n) {
+    tc_record_error("tc_bs_velocity_soa: bad size or range (n=%d, [%d,%d))", n, i0, i1);
+    return TC_ERR_ARG;
+  }
+  if (n > 0 && (!x || !y || !z || !vort || !area || !dx || !dy || !dz)) {
+    tc_record_error("tc_bs_velocity_soa: null array argument");
+    return TC_ERR_ARG;
+  }
+  if (n == 0) return TC_OK;
+  if ((rc = ctx->scratch[5].ensure(6 * (size_t)n * sizeof(double)))) return rc;
+  double* aos = ctx->scratch[5].as<double>();
+  double* u = aos + 3 * (size_t)n;
+  soa_to_aos_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(x, y, z, n, aos);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  if ((rc = velocity_device(ctx, TC_ACTIVE, nullptr, n, aos, vort, area, n, i0, i1, u, nullptr)))
+    return rc;
+  soa_finish_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(u, n, -2.0 * ctx->omega, dx, dy, dz,
+                                                               dVort);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  return TC_OK;
+}
+
+extern "C" int tc_bs_velocity_soa(tc_ctx* ctx, const double* x, const double* y, const double* z,
+                                  const double* vort, const double* area, int n, int i0, int i1,
+                                  double* dx, double* dy, double* dz, double* dVort) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!x || !y || !z || !vort || !area || !dx || !dy || !dz))) {
+    tc_record_error("tc_bs_velocity_soa: bad arguments");
+    return TC_ERR_ARG;
+  }
+  const double* in[5] = {x, y, z, vort, area};
+  const char* names[5] = {"x", "y", "z", "vort", "area"};
+  for (int a = 0; a < 5; ++a)
+    if ((rc = check_finite_host(in[a], (size_t)n, names[a]))) return rc;
+  if (n == 0) return TC_OK;
+  const size_t b = (size_t)n * sizeof(double);
+  if ((rc = ctx->scratch[1].ensure(9 * b))) return rc;
+  double* d = ctx->scratch[1].as<double>();
+  cudaStream_t s = ctx->stream;
+  for (int a = 0; a < 5; ++a)
+    TC_CUDA_TRY(cudaMemcpyAsync(d + a * (size_t)n, in[a], b, cudaMemcpyHostToDevice, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(d + 6 * (size_t)n, dy, b, cudaMemcpyHostToDevice, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(d + 7 * (size_t)n, dz, b, cudaMemcpyHostToDevice, s));
+  double* ddx = d + 5 * (size_t)n;
+  double* ddy = d + 6 * (size_t)n;
+  double* ddz = d + 7 * (size_t)n;
+  double* ddv = d + 8 * (size_t)n;
+  if ((rc = tc_bs_velocity_soa_device(ctx, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n,
+                                      d + 4 * (size_t)n, n, i0, i1, ddx, ddy, ddz, ddv)))
+    return rc;
+  TC_CUDA_TRY(cudaMemcpyAsync(dx, ddx, b, cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(dy, ddy, b, cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(dz, ddz, b, cudaMemcpyDeviceToHost, s));
+  if (dVort) TC_CUDA_TRY(cudaMemcpyAsync(dVort, ddv, b, cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_finite_host(dx, (size_t)n, "dx (result)");
+}
+
+// ---------------------------------------------------------------------------
 // RK4 driver (BVERK4, PanelVelocityParallel.f90:435-658)
 // ---------------------------------------------------------------------------
 namespace {
@@ -568,6 +665,36 @@ extern "C" int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* 
   if (reset) {
     ctx->launches = ctx->pair_launches = ctx->pair_interactions = 0;
     ctx->pair_ms = 0.0;
+  }
+  return TC_OK;
+}
+
+// Voronoi BVERK4 (VoronoiVelocityParallel.f90:304-478) on the n used SoA
+// generators, areas frozen for the step; the Delaunay/Voronoi rebuild that
+// follows in the reference (:480-482) stays with the caller. Unused N_Max
+// slots carry zero vorticity and contribute nothing, so they are not passed.
+extern "C" int tc_rk4_soa_step(tc_ctx* ctx, double* x, double* y, double* z, double* relVort,
+                               const double* area, int n, double dt, int nsteps, double* totalKE,
+                               double* kineticEnergy) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!x || !y || !z || !relVort || !area))) {
+    tc_record_error("tc_rk4_soa_step: bad arguments");
+    return TC_ERR_ARG;
+  }
+  std::vector<double> xyz(3 * (size_t)n);
+  for (int j = 0; j < n; ++j) {
+    xyz[3 * (size_t)j] = x[j];
+    xyz[3 * (size_t)j + 1] = y[j];
+    xyz[3 * (size_t)j + 2] = z[j];
+  }
+  if ((rc = tc_rk4_step(ctx, xyz.data(), relVort, area, n, nullptr, 0, nullptr, 0, dt, nsteps,
+                        totalKE, kineticEnergy)))
+    return rc;
+  for (int j = 0; j < n; ++j) {
+    x[j] = xyz[3 * (size_t)j];
+    y[j] = xyz[3 * (size_t)j + 1];
+    z[j] = xyz[3 * (size_t)j + 2];
   }
   return TC_OK;
 }

@@ -16,6 +16,10 @@ namespace tcb {
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
   int ensure(size_t need);  // grows (never shrinks); contents are not kept
   void release();
   template <class T>
