@@ -282,6 +282,31 @@ def time_adjoint(device, level=6, steps=20, ckpt=5):
             "adjoint_over_forward": min(ta) / min(tf), "J": float(J[0])}
 
 
+def time_batch(device, steps=10):
+    """Batched ensemble: 64 Gaussian vortices (seed 4), levels 3-6, 10 RK4 steps each, FP32C,
+    one CUDA-graph launch per call. The first call autotunes and captures; the second is timed
+    end to end (host arrays in and out)."""
+    from thesiscode_b200 import configs
+    from thesiscode_b200.batch import batch_info, batch_rk4
+    from thesiscode_b200.panel_velocity import Context
+
+    ws = configs.batched_gaussians(count=64, seed=4, levels=(3, 4, 5, 6))
+    ctx = Context(device, "fp32c")
+    ctx.set_omega(ws[0].omega)
+    ctx.set_deltas(*ws[0].deltas)
+    batch_rk4(ctx, [w.copy() for w in ws], ws[0].dt, steps)
+    t = time.perf_counter()
+    batch_rk4(ctx, ws, ws[0].dt, steps)
+    dt = time.perf_counter() - t
+    info = batch_info(ctx)
+    ctx.close()
+    inter = steps * sum(w.interactions_per_step() for w in ws)
+    return {"workload": "64 Gaussian vortices (seed 4), icosahedral levels 3-6, beta in [4,20], "
+                        f"{steps} RK4 steps each, FP32C, one CUDA graph", "interactions": inter,
+            "seconds": dt, "value": inter / dt, "unit": "interactions/s",
+            "levels": sorted(set(w.level for w in ws)), "autotuned": info}
+
+
 def sample_rows(w, frac, seed=11):
     rng = np.random.default_rng(seed)
     ra = np.sort(rng.choice(w.nA, max(1, int(w.nA * frac)), replace=False)).astype(np.int32)
@@ -387,6 +412,7 @@ def run_ours(args):
                            "ms_per_step": e2e["ms"], "api": "tc_rk4_step (host pointers, pinned)"}
         if world == 1 and not args.quick:
             line["adjoint"] = time_adjoint(device)
+            line["batched"] = time_batch(device)
         if world == 1 and not args.no_cpu:
             cb = cpu_baseline(w)
             line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],

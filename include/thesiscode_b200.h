@@ -59,6 +59,10 @@ extern "C" {
 #define TC_PASSIVE 2 /* BVESmoothVelocity :1376-1412: divided panels,
                         delta = smooth (0.05 by default, :27)                */
 
+/* ---- batched ensembles (tc_batch_rk4 flags) ---------------------------- */
+#define TC_BATCH_GRAPH 1    /* capture the nsteps steps in one CUDA graph     */
+#define TC_BATCH_AUTOTUNE 2 /* time kernel variants x chunk lengths first     */
+
 /* ---- end-time functionals of the adjoint ------------------------------ */
 #define TC_J_ENSTROPHY 0 /* J = sum_j zeta_j^2 A_j over the active panels  */
 #define TC_J_PROBE 1     /* J = zeta of one active panel                   */
@@ -202,6 +206,22 @@ int tc_reset_rk4(tc_ctx* ctx);
 int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA,
                    int nA, double dt, int nsteps, int ckpt_every, int functional, int probe,
                    double* J, double* g_zeta0, double* g_x0);
+
+/* ---- batched ensembles (no counterpart in the reference) --------------- */
+/* `count` independent particle sets stored back to back (host arrays):
+ * instance b owns active rows [sum_{c<b} nA[c], +nA[b]) of xA(3,*), zetaA,
+ * areaA and vertex rows [sum_{c<b} nV[c], +nV[b]) of xV(3,*); each evolves
+ * as its own BVERK4 (its active panels are its only sources) for nsteps
+ * steps, updated in place. totalKE[nsteps*count] (step-major) receives each
+ * instance's stage-1 kinetic energy. The pair work of all instances runs in
+ * one persistent launch per stage; TC_BATCH_GRAPH replays all steps as one
+ * CUDA graph, TC_BATCH_AUTOTUNE times the kernel variants and source-chunk
+ * lengths on the batch first (cached per batch shape). */
+int tc_batch_rk4(tc_ctx* ctx, int count, const int* nA, const int* nV, double* xA, double* zetaA,
+                 const double* areaA, double* xV, double dt, int nsteps, double* totalKE,
+                 int flags);
+/* Variant, source-chunk length and work-item count of the last batch. */
+int tc_batch_info(tc_ctx* ctx, int* variant, int* chunk_len, int* n_items);
 
 /* ---- stage primitives for target-sharded multi-rank runs -------------- */
 /* Pack stage-1 sources of the loaded state into TC_BUF_SOURCES. */

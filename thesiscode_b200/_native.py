@@ -34,6 +34,9 @@ TC_PASSIVE = 2
 # probes
 (TC_PROBE_FFMA, TC_PROBE_FFMA2, TC_PROBE_DFMA, TC_PROBE_RCP32, TC_PROBE_RCP64, TC_PROBE_DDIV,
  TC_PROBE_F2F) = range(7)
+# batched ensembles
+TC_BATCH_GRAPH = 1
+TC_BATCH_AUTOTUNE = 2
 # adjoint functionals
 TC_J_ENSTROPHY = 0
 TC_J_PROBE = 1
@@ -90,6 +93,8 @@ SIGNATURES: dict[str, tuple] = {
     "tc_rk4_stage_range": (c_int, [c_void_p, c_int, c_double, c_int, c_int, c_int, c_int, c_int, c_int,
                                    c_void_p]),
     "tc_rk4_device_buffer": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    "tc_batch_rk4": (c_int, [c_void_p, c_int, ip, ip, dp, dp, dp, dp, c_double, c_int, dp, c_int]),
+    "tc_batch_info": (c_int, [c_void_p, ip, ip, ip]),
     "tc_rk4_adjoint": (c_int, [c_void_p, dp, dp, dp, c_int, c_double, c_int, c_int, c_int, c_int, dp, dp, dp]),
     "tc_rk4_copy_rows": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int]),
     "tc_pair_variant_count": (c_int, [c_int, ip]),

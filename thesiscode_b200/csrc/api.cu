@@ -132,6 +132,7 @@ extern "C" int tc_destroy(tc_ctx* ctx) {
                     &R.permA, &R.permV, &R.permQ};
   for (DevBuf* b : bufs) b->release();
   for (auto& b : ctx->order_buf) b.release();
+  tc_batch_free(ctx);
   for (cudaEvent_t e : ctx->pair_events) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -95,16 +95,18 @@ __device__ __forceinline__ double pair_denominator(const double4& q, const doubl
   return __dadd_rn(__dsub_rn(1.0, s), d2);
 }
 
-template <int NT, int TPT, int TS, int MINB, bool FUSED>
-__global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P) {
-  __shared__ double4 sm[TS];
+// One work unit: the targets at positions [tile0, min(tile0 + NT*TPT, i_end))
+// of x against the sources [c0, c1); FP64 sums written to out[pos],
+// out[stride + pos], out[2*stride + pos]. Targets whose source index is
+// i + self_offset (self_offset != kNoSelf) skip themselves.
+template <int NT, int TPT, int TS, bool FUSED>
+__device__ __forceinline__ void fp64_unit(const double* __restrict__ x, int tile0, int i_end,
+                                          int self_offset, double d2,
+                                          const double4* __restrict__ src, int c0, int c1,
+                                          double* __restrict__ out, size_t stride, double4* sm) {
   constexpr int TB = NT * TPT;
-  const TargetSeg& G = find_seg(P, blockIdx.x);
-  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
-  const int i_end = G.i1;
-  const double d2 = G.d2;
-  const double one_plus_d2 = 1.0 + G.d2;
-  const bool has_self = G.self_offset != kNoSelf;
+  const double one_plus_d2 = 1.0 + d2;
+  const bool has_self = self_offset != kNoSelf;
 
   double xi[TPT][3], acc[TPT][3];
   int self_k[TPT];
@@ -112,22 +114,20 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
   for (int t = 0; t < TPT; ++t) {
     int i = tile0 + (int)threadIdx.x + t * NT;
     int ld = i < i_end ? i : tile0;
-    xi[t][0] = G.x[3 * (size_t)ld];
-    xi[t][1] = G.x[3 * (size_t)ld + 1];
-    xi[t][2] = G.x[3 * (size_t)ld + 2];
+    xi[t][0] = x[3 * (size_t)ld];
+    xi[t][1] = x[3 * (size_t)ld + 1];
+    xi[t][2] = x[3 * (size_t)ld + 2];
     acc[t][0] = acc[t][1] = acc[t][2] = 0.0;
-    self_k[t] = has_self ? i + G.self_offset : -1;
+    self_k[t] = has_self ? i + self_offset : -1;
   }
-  const int self_lo = has_self ? tile0 + G.self_offset : 0;
-  const int self_hi = has_self ? min(tile0 + TB, i_end) + G.self_offset : 0;
+  const int self_lo = has_self ? tile0 + self_offset : 0;
+  const int self_hi = has_self ? min(tile0 + TB, i_end) + self_offset : 0;
 
-  const int c0 = (int)blockIdx.y * P.chunk_len;
-  const int c1 = min(P.n, c0 + P.chunk_len);
   for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
     for (int j = threadIdx.x; j < TS; j += NT) {
       int k = ts + j;
-      sm[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sm[j] = k < c1 ? src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
     }
     __syncthreads();
     const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
@@ -160,8 +160,6 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
       }
     }
   }
-  const size_t stride = (size_t)P.n_out;
-  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
 #pragma unroll
   for (int t = 0; t < TPT; ++t) {
     int i = tile0 + (int)threadIdx.x + t * NT;
@@ -171,6 +169,19 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
       out[2 * stride + i] = acc[t][2];
     }
   }
+}
+
+template <int NT, int TPT, int TS, int MINB, bool FUSED>
+__global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P) {
+  __shared__ double4 sm[TS];
+  const TargetSeg& G = find_seg(P, blockIdx.x);
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * TPT);
+  const int c0 = (int)blockIdx.y * P.chunk_len;
+  const int c1 = min(P.n, c0 + P.chunk_len);
+  const size_t stride = (size_t)P.n_out;
+  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+  fp64_unit<NT, TPT, TS, FUSED>(G.x, tile0, G.i1, G.self_offset, G.d2, P.src, c0, c1, out, stride,
+                                sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -200,23 +211,21 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // ---------------------------------------------------------------------------
 constexpr float kSelfBias = 1e-30f;
 
-template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
-__global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
+// One work unit (targets at visiting positions [tile0, min(tile0 + NT*2*NPAIR,
+// i_end)) against sources [c0, c1)); shared memory smA/smB/smC of TS entries.
+template <int NT, int NPAIR, int TS, int FLUSH, int UNROLL>
+__device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const int* __restrict__ perm,
+                                           int tile0, int i_end, double d2,
+                                           const double4* __restrict__ src, int c0, int c1,
+                                           double* __restrict__ out, size_t stride, float4* smA,
+                                           float4* smB, float2* smC) {
   static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
-  __shared__ float4 smA[TS];  // (sx, sx, sy, sy)
-  __shared__ float4 smB[TS];  // (sz, sz, 2G, 2G)
-  __shared__ float2 smC[TS];  // (e, e)
   constexpr int TPT = 2 * NPAIR;
   constexpr int TB = NT * TPT;
-  const TargetSeg& G = find_seg(P, blockIdx.x);
-  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * TB;
-  const int i_end = G.i1;
-  const int* perm = G.perm;
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
   const int mid = perm ? perm[mid_pos] : mid_pos;
-  const double cx = G.x[3 * (size_t)mid], cy = G.x[3 * (size_t)mid + 1],
-               cz = G.x[3 * (size_t)mid + 2];
+  const double cx = x[3 * (size_t)mid], cy = x[3 * (size_t)mid + 1], cz = x[3 * (size_t)mid + 2];
 
   float2 ntx[NPAIR], nty[NPAIR], ntz[NPAIR], ei[NPAIR];
   float2 fx[NPAIR], fy[NPAIR], fz[NPAIR];
@@ -228,11 +237,11 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
     for (int h = 0; h < 2; ++h) {
       int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
       int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
-      double x = G.x[3 * (size_t)ld], y = G.x[3 * (size_t)ld + 1], z = G.x[3 * (size_t)ld + 2];
-      tv[h][0] = -(float)(x - cx);
-      tv[h][1] = -(float)(y - cy);
-      tv[h][2] = -(float)(z - cz);
-      tv[h][3] = (float)((1.0 - (x * x + y * y + z * z)) + 2.0 * G.d2) + kSelfBias;
+      double px = x[3 * (size_t)ld], py = x[3 * (size_t)ld + 1], pz = x[3 * (size_t)ld + 2];
+      tv[h][0] = -(float)(px - cx);
+      tv[h][1] = -(float)(py - cy);
+      tv[h][2] = -(float)(pz - cz);
+      tv[h][3] = (float)((1.0 - (px * px + py * py + pz * pz)) + 2.0 * d2) + kSelfBias;
       ax[p][h] = ay[p][h] = az[p][h] = 0.0;
     }
     ntx[p] = make_float2(tv[0][0], tv[1][0]);
@@ -242,15 +251,13 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
     fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
   }
 
-  const int c0 = (int)blockIdx.y * P.chunk_len;
-  const int c1 = min(P.n, c0 + P.chunk_len);
   for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
     for (int j = threadIdx.x; j < TS; j += NT) {
       int k = ts + j;
       float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f;
       if (k < c1) {
-        const double4 q = P.src[k];
+        const double4 q = src[k];
         sx = (float)(q.x - cx);
         sy = (float)(q.y - cy);
         sz = (float)(q.z - cz);
@@ -299,8 +306,6 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
     }
   }
   // partial rows are indexed by position in the visiting order
-  const size_t stride = (size_t)P.n_out;
-  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
 #pragma unroll
   for (int p = 0; p < NPAIR; ++p) {
 #pragma unroll
@@ -312,6 +317,90 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
         out[2 * stride + pos] = az[p][h];
       }
     }
+  }
+}
+
+
+template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
+__global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
+  __shared__ float4 smA[TS];  // (sx, sx, sy, sy)
+  __shared__ float4 smB[TS];  // (sz, sz, 2G, 2G)
+  __shared__ float2 smC[TS];  // (e, e)
+  const TargetSeg& G = find_seg(P, blockIdx.x);
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * 2 * NPAIR);
+  const int c0 = (int)blockIdx.y * P.chunk_len;
+  const int c1 = min(P.n, c0 + P.chunk_len);
+  const size_t stride = (size_t)P.n_out;
+  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+  fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
+                                           stride, smA, smB, smC);
+}
+
+// ---------------------------------------------------------------------------
+// Batched (ensemble) form: many independent particle sets concatenated in one
+// RK4 state. A work item is (target tile of one class of one instance, one
+// chunk of that instance's sources); a persistent grid of one wave of CTAs
+// takes items from an atomic counter until none is left (no CTA ever waits
+// on another). Items are queued longest first, so the uneven instance sizes
+// even out across the SMs.
+// ---------------------------------------------------------------------------
+struct BatchSeg {
+  const double* x;   // target positions of the class (concatenated instances)
+  const int* perm;   // FP32C visiting order (null: as stored)
+  int out_offset;    // partial row of target position p is out_offset + p
+  int self_offset;   // TC_ACTIVE: source index of target i is i + self_offset
+  double d2;
+};
+
+struct BatchItem {
+  int seg;           // index into the segment table
+  int tile0, i1;     // target positions [tile0, min(tile0 + TB, i1))
+  int c0, c1;        // sources [c0, c1) (absolute rows of the packed sources)
+  int chunk;         // chunk index within the instance (partial slab)
+};
+
+struct BatchLaunch {
+  const BatchItem* items;
+  int n_items;
+  int* counter;      // zeroed before each launch
+  const BatchSeg* segs;
+  const double4* src;
+  double* partial;   // partial[(chunk*3 + c)*stride + row]
+  size_t stride;
+};
+
+__device__ __forceinline__ int next_item(int* counter, int* slot) {
+  __syncthreads();  // every thread is done with the previous item's slot value
+  if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+  __syncthreads();
+  return *slot;
+}
+
+template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
+__global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
+  __shared__ float4 smA[TS];
+  __shared__ float4 smB[TS];
+  __shared__ float2 smC[TS];
+  __shared__ int slot;
+  for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
+    const BatchItem I = B.items[it];
+    const BatchSeg S = B.segs[I.seg];
+    double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+    fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1,
+                                             out, B.stride, smA, smB, smC);
+  }
+}
+
+template <int NT, int TPT, int TS, int MINB, bool FUSED>
+__global__ void __launch_bounds__(NT, MINB) pair_fp64_batch_kernel(const BatchLaunch B) {
+  __shared__ double4 sm[TS];
+  __shared__ int slot;
+  for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
+    const BatchItem I = B.items[it];
+    const BatchSeg S = B.segs[I.seg];
+    double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+    fp64_unit<NT, TPT, TS, FUSED>(S.x, I.tile0, I.i1, S.self_offset, S.d2, B.src, I.c0, I.c1, out,
+                                  B.stride, sm);
   }
 }
 

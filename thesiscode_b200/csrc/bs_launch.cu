@@ -44,6 +44,14 @@ template <int NT, int TPT, int MINB, bool FUSED>
 void launch64(dim3 g, cudaStream_t s, const PairLaunch& P) {
   pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(P);
 }
+template <int NT, int TPT, int MINB, bool FUSED>
+void launch64b(int g, cudaStream_t s, const BatchLaunch& B) {
+  pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(B);
+}
+template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL>
+void launch32b(int g, cudaStream_t s, const BatchLaunch& B) {
+  pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(B);
+}
 
 template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL>
 void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
@@ -52,11 +60,15 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
 
 #define V64(NT, TPT, MINB, FUSED)                                                 \
   PairVariant { TC_FP64, NT, TPT, kTS, FUSED, MINB, 0, launch64<NT, TPT, MINB, FUSED>, \
-                (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED> }
+                (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED>,               \
+                launch64b<NT, TPT, MINB, FUSED>,                                         \
+                (const void*)pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED> }
 #define V32(NT, NPAIR, FLUSH, MINB, UNROLL)                                              \
   PairVariant { TC_FP32C, NT, 2 * NPAIR, kTS, FLUSH, MINB, UNROLL,                        \
                 launch32<NT, NPAIR, FLUSH, MINB, UNROLL>,                                 \
-                (const void*)pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL> }
+                (const void*)pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL>,      \
+                launch32b<NT, NPAIR, FLUSH, MINB, UNROLL>,                                \
+                (const void*)pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL> }
 
 // FP64: the `flush` field records the denominator mode (1 = fused, 0 =
 // rounded exactly like the reference).
@@ -290,6 +302,7 @@ struct StageEpi {
   double* ke;
   double* keBlocks;
   const int *permA, *permV, *permQ;  // visiting orders of the three ranges (null: as stored)
+  const int* row_nchunks;            // batched runs: chunks of each partial row (null: nchunks)
 };
 
 constexpr int kEpiThreads = 256;
@@ -321,7 +334,8 @@ __global__ void __launch_bounds__(kEpiThreads) stage_epilogue_kernel(const Stage
     const size_t b = 3 * (size_t)i;
     double xs[3] = {xin[b], xin[b + 1], xin[b + 2]};
     double T[3], u[3];
-    reduce_row(E.partial, E.nchunks, (size_t)E.n_out, (size_t)row, T);
+    reduce_row(E.partial, E.row_nchunks ? E.row_nchunks[row] : E.nchunks, (size_t)E.n_out,
+               (size_t)row, T);
     velocity_from_sum(xs, T, u);
     if (cls == 0 && E.stage == 0) {
       double k2 = __dadd_rn(__dadd_rn(__dmul_rn(u[0], u[0]), __dmul_rn(u[1], u[1])),
@@ -387,9 +401,10 @@ __global__ void ke_finalize_kernel(const double* __restrict__ blocks, int nblock
 }
 
 int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
-                          double* total_ke) {
+                          double* total_ke, const int* row_nchunks, const double* partial) {
   Rk4State& R = ctx->rk;
   StageEpi E;
+  E.row_nchunks = row_nchunks;
   E.stage = stage;
   E.dt = dt;
   E.m2omega = -2.0 * ctx->omega;
@@ -404,7 +419,7 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
   E.q1 = range[5];
   E.n_out = R.nA + R.nV + R.nQ;
   E.nchunks = nchunks;
-  E.partial = ctx->partial.as<double>();
+  E.partial = partial ? partial : ctx->partial.as<double>();
   E.x0A = R.x0A.as<double>();
   E.z0 = R.z0.as<double>();
   E.x0V = R.x0V.as<double>();

@@ -40,6 +40,8 @@ struct PairVariant {
   int nt, tpt, ts, flush, minb, unroll;
   void (*launch)(dim3 grid, cudaStream_t stream, const PairLaunch& P);
   const void* fn;
+  void (*launch_batch)(int grid, cudaStream_t stream, const BatchLaunch& B);
+  const void* fn_batch;
 };
 
 // Target segment as the host describes it before tiles are assigned.
@@ -72,6 +74,9 @@ struct Rk4State {
 
 }  // namespace tcb
 
+struct tc_batch_plan;            // batched-ensemble plan (batch.cu)
+void tc_batch_free(tc_ctx* ctx);
+
 struct tc_ctx {
   int device = 0;
   int precision = TC_FP64;
@@ -99,6 +104,7 @@ struct tc_ctx {
   bool time_pairs = false;
   std::vector<cudaEvent_t> pair_events;  // start/stop pairs, resolved by tc_stats
   double pair_ms = 0.0;
+  tc_batch_plan* batch = nullptr;
 };
 
 namespace tcb {
@@ -119,7 +125,8 @@ int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm);
 // total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
 // stage 0; nchunks is what launch_pairs returned for this stage.
 int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
-                          double* total_ke);
+                          double* total_ke, const int* row_nchunks = nullptr,
+                          const double* partial = nullptr);
 int resolve_slots(tc_ctx* ctx);
 const PairVariant* variant(int precision, int id);
 // Kernels defined in bs_launch.cu and also launched from other files.
