@@ -244,42 +244,51 @@ def time_e2e(w, precision, steps, device):
 
 
 def time_adjoint(device, level=6, steps=20, ckpt=5):
-    """Adjoint/forward time ratio on the zonal-jet workload (delta 0.02, dt 0.005, FP64): the
-    adjoint call (forward sweep with checkpoints + recomputation + backward) against a forward
-    call over the same steps, both through the host-pointer C ABI."""
+    """Adjoint/forward time ratio on the zonal-jet workload (level 6, delta 0.02, dt 0.005, FP64,
+    J = sum zeta^2 A). The adjoint's phases are CUDA-event timed inside the library (forward sweep
+    with checkpoints, recomputation of checkpoint segments, backward sweep); the forward reference
+    is the same steps through tc_rk4_advance on device-resident state."""
     import torch
 
     from thesiscode_b200 import _native as N
     from thesiscode_b200.panel_velocity import Context
 
-    w = build_workload("jet_l6") if level == 6 else None
+    w = build_workload("jet_l6")
     ctx = Context(device, "fp64")
+    stream = torch.cuda.Stream(device)
+    ctx.set_stream(stream.cuda_stream)
     ctx.set_omega(w.omega)
     ctx.set_deltas(*w.deltas)
     J, gz, gx = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
+    out = {"workload": f"jet level {w.level} ({w.nA} panels), delta 0.02, {steps} RK4 steps dt {w.dt}, "
+                       "J = sum zeta^2 A, FP64"}
 
-    def fwd():
-        x, z = w.xA.copy(), w.zetaA.copy()
-        ctx.rk4_step(x, z, w.areaA, np.zeros((0, 3)), np.zeros((0, 3)), w.dt, steps)
+    def fwd_ms():
+        N.call("tc_rk4_load", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, None, 0,
+               None, 0, 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N.call("tc_rk4_advance", ctx.handle, w.dt, steps, None)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
 
-    def adj():
-        N.call("tc_rk4_adjoint", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt,
-               steps, ckpt, N.TC_J_ENSTROPHY, 0, N.dptr(J), N.dptr(gz), N.dptr(gx))
-
-    fwd()
-    adj()
-    tf, ta = [], []
-    for _ in range(2):
-        t = time.perf_counter()
-        fwd()
-        tf.append(time.perf_counter() - t)
-        t = time.perf_counter()
-        adj()
-        ta.append(time.perf_counter() - t)
+    fwd_ms()
+    tf = min(fwd_ms() for _ in range(2))
+    out["forward_ms"] = tf
+    for name, ck in (("checkpoint_every_5", ckpt), ("stage_inputs_kept", steps)):
+        ph = np.zeros(3)
+        for _ in range(2):
+            N.call("tc_rk4_adjoint", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt,
+                   steps, ck, N.TC_J_ENSTROPHY, 0, N.dptr(J), N.dptr(gz), N.dptr(gx))
+        N.call("tc_adjoint_phase_ms", ctx.handle, N.dptr(ph))
+        out[name] = {"checkpoint_every": ck, "forward_sweep_ms": ph[0], "recompute_ms": ph[1],
+                     "backward_ms": ph[2],
+                     "adjoint_over_forward": (ph[1] + ph[2]) / tf,
+                     "gradient_over_forward": (ph[0] + ph[1] + ph[2]) / tf}
+    out["J"] = float(J[0])
     ctx.close()
-    return {"workload": f"jet level {w.level} ({w.nA} panels), delta 0.02, {steps} RK4 steps dt {w.dt}, "
-                        f"checkpoint every {ckpt}, J = sum zeta^2 A", "forward_s": min(tf), "adjoint_s": min(ta),
-            "adjoint_over_forward": min(ta) / min(tf), "J": float(J[0])}
+    return out
 
 
 def time_batch(device, steps=10):

@@ -206,6 +206,16 @@ int tc_reset_rk4(tc_ctx* ctx);
 int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA,
                    int nA, double dt, int nsteps, int ckpt_every, int functional, int probe,
                    double* J, double* g_zeta0, double* g_x0);
+/* How each stage's vector-Jacobian product visits the pairs: 3 = one
+ * row-major pass computing both sides' row sums (the default), 0 = two
+ * passes (target side, transposed source side), 1 and 2 = one pass with
+ * in-block column reductions (256 threads x 2 targets, or 128 x 4). All
+ * modes give the same gradient to rounding. */
+int tc_set_adjoint_mode(tc_ctx* ctx, int mode);
+/* Device time (ms) of the last tc_rk4_adjoint call: ms3[0] forward sweep
+ * with checkpoints, ms3[1] recomputation of checkpoint segments, ms3[2]
+ * backward sweep. */
+int tc_adjoint_phase_ms(tc_ctx* ctx, double* ms3);
 
 /* ---- batched ensembles (no counterpart in the reference) --------------- */
 /* `count` independent particle sets stored back to back (host arrays):

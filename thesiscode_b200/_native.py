@@ -71,6 +71,8 @@ SIGNATURES: dict[str, tuple] = {
     "tc_set_smooth": (c_int, [c_void_p, c_double]),
     "tc_get_smooth": (c_int, [c_void_p, dp]),
     "tc_set_target_order": (c_int, [c_void_p, c_int]),
+    "tc_set_adjoint_mode": (c_int, [c_void_p, c_int]),
+    "tc_adjoint_phase_ms": (c_int, [c_void_p, dp]),
     "tc_set_deltas": (c_int, [c_void_p, c_double, c_double, c_double]),
     "tc_get_deltas": (c_int, [c_void_p, dp]),
     "tc_bs_velocity": (c_int, [c_void_p, c_int, dp, c_int, dp, dp, dp, c_int, c_int, c_int, dp, dp]),

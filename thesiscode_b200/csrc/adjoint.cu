@@ -44,6 +44,7 @@ struct AdjLaunch {
   const double4* src;    // pass 1: {x, y, z, G}; pass 2: {x, y, z, v_x}
   const double2* src2;   // pass 2: {v_y, v_z}
   const double* v;       // pass 1: v_i per target (3 per row)
+  const double4* src2_4; // row pass: {v_x, v_y, v_z, 0}
   int n;
   int chunk_len;
   double one_plus_d2;
@@ -60,15 +61,14 @@ __device__ __forceinline__ double adj_rcp(double d) {
 }
 
 // Pass 1: per target i, S1 = sum_k G_k/D x_k and S2 = sum_k G_k s_ik/D^2 x_k
-// (6 outputs per row), accumulated on offsets d = x_k - x_i for accuracy:
-// S1 = W1 x_i + sum w1 d, S2 = W2 x_i + sum w2 d.
+// (6 outputs per row).
 __global__ void __launch_bounds__(kAdjNT) adj_target_kernel(const AdjLaunch P) {
   __shared__ double4 sm[kAdjTS];
   const int i = blockIdx.x * kAdjNT + threadIdx.x;
   const int ld = i < P.n ? i : P.n - 1;
   const double xi0 = P.x[3 * (size_t)ld], xi1 = P.x[3 * (size_t)ld + 1], xi2 = P.x[3 * (size_t)ld + 2];
   const double v0 = P.v[3 * (size_t)ld], v1 = P.v[3 * (size_t)ld + 1], v2 = P.v[3 * (size_t)ld + 2];
-  double a1x = 0, a1y = 0, a1z = 0, w1s = 0, a2x = 0, a2y = 0, a2z = 0, w2s = 0;
+  double a1x = 0, a1y = 0, a1z = 0, a2x = 0, a2y = 0, a2z = 0;
   const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
   for (int ts = c0; ts < c1; ts += kAdjTS) {
     __syncthreads();
@@ -85,28 +85,25 @@ __global__ void __launch_bounds__(kAdjNT) adj_target_kernel(const AdjLaunch P) {
       double r = adj_rcp(D);
       r = (ts + j == i) ? 0.0 : r;  // self pair (D may be 0: r is then NaN before the select)
       const double w1 = q.w * r;
-      const double dx = q.x - xi0, dy = q.y - xi1, dz = q.z - xi2;
-      const double s = fma(dx, v0, fma(dy, v1, dz * v2));  // x_k.v_i = d.v_i (x_i.v_i = 0)
+      const double s = fma(q.x, v0, fma(q.y, v1, q.z * v2));  // s_ik = x_k . v_i
       const double w2 = w1 * s * r;
-      a1x = fma(w1, dx, a1x);
-      a1y = fma(w1, dy, a1y);
-      a1z = fma(w1, dz, a1z);
-      w1s += w1;
-      a2x = fma(w2, dx, a2x);
-      a2y = fma(w2, dy, a2y);
-      a2z = fma(w2, dz, a2z);
-      w2s += w2;
+      a1x = fma(w1, q.x, a1x);
+      a1y = fma(w1, q.y, a1y);
+      a1z = fma(w1, q.z, a1z);
+      a2x = fma(w2, q.x, a2x);
+      a2y = fma(w2, q.y, a2y);
+      a2z = fma(w2, q.z, a2z);
     }
   }
   if (i < P.n) {
     const size_t n = (size_t)P.n;
     double* out = P.partial + (size_t)blockIdx.y * 6 * n + i;
-    out[0] = fma(w1s, xi0, a1x);
-    out[n] = fma(w1s, xi1, a1y);
-    out[2 * n] = fma(w1s, xi2, a1z);
-    out[3 * n] = fma(w2s, xi0, a2x);
-    out[4 * n] = fma(w2s, xi1, a2y);
-    out[5 * n] = fma(w2s, xi2, a2z);
+    out[0] = a1x;
+    out[n] = a1y;
+    out[2 * n] = a1z;
+    out[3 * n] = a2x;
+    out[4 * n] = a2y;
+    out[5 * n] = a2z;
   }
 }
 
@@ -137,8 +134,8 @@ __global__ void __launch_bounds__(kAdjNT) adj_source_kernel(const AdjLaunch P) {
       D = fma(-a.z, xk2, D);
       double r = adj_rcp(D);
       r = (ts + j == k) ? 0.0 : r;
-      // s_ik = x_k . v_i = (x_k - x_i) . v_i
-      const double s = fma(xk0 - a.x, a.w, fma(xk1 - a.y, b.x, (xk2 - a.z) * b.y));
+      // s_ik = x_k . v_i
+      const double s = fma(xk0, a.w, fma(xk1, b.x, xk2 * b.y));
       const double sr = s * r;
       const double sr2 = sr * r;
       px = fma(r, a.w, px);
@@ -163,13 +160,199 @@ __global__ void __launch_bounds__(kAdjNT) adj_source_kernel(const AdjLaunch P) {
   }
 }
 
+// Fused pass: one visit of each pair (i, k) feeds both sides. Rows (targets
+// i) keep S1 = sum_k G_k/D x_k and S2 = sum_k G_k s/D^2 x_k in registers;
+// columns (sources k) get P, Q, R summed over the CTA's targets: per source,
+// across the thread's targets, then the warp (shuffles), then the warps
+// (shared memory); one column partial per (target tile, source) goes to
+// colpart[(tile*7 + c)*n + k]. Every (tile, k) slot is written exactly once,
+// so the combine is a fixed-order sum: deterministic, no atomics.
+
+struct AdjFused {
+  const double* x;       // positions of the panels (rows and columns)
+  const double4* src;    // {x, y, z, G} per panel
+  const double* v;       // v_i per row
+  int n;
+  int chunk_len;
+  double one_plus_d2;
+  double* rowpart;       // [chunk][6][n]
+  double* colpart;       // [tile][7][n]
+};
+
+// LEVELS shuffle steps leave 32 >> LEVELS partial sums per warp and source.
+template <int kFNT, int kFTPT, int LEVELS, int kFTS>
+__global__ void __launch_bounds__(kFNT) adj_fused_kernel(const AdjFused P) {
+  constexpr int kFWARPS = kFNT / 32;
+  constexpr int kPARTS = 32 >> LEVELS;
+  __shared__ double4 sm[kFTS];
+  __shared__ double red[kFWARPS * kPARTS][kFTS][7];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tile0 = blockIdx.x * (kFNT * kFTPT);
+  double xi[kFTPT][3], vi[kFTPT][3], s1[kFTPT][3], s2[kFTPT][3];
+  int row[kFTPT];
+  bool valid[kFTPT];
+#pragma unroll
+  for (int t = 0; t < kFTPT; ++t) {
+    row[t] = tile0 + (int)threadIdx.x + t * kFNT;
+    valid[t] = row[t] < P.n;
+    const int ld = valid[t] ? row[t] : P.n - 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      xi[t][c] = P.x[3 * (size_t)ld + c];
+      vi[t][c] = P.v[3 * (size_t)ld + c];
+      s1[t][c] = s2[t][c] = 0.0;
+    }
+  }
+  const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
+  const size_t N = (size_t)P.n;
+  for (int ts = c0; ts < c1; ts += kFTS) {
+    __syncthreads();  // previous tile's sm and red are consumed
+    for (int j = threadIdx.x; j < kFTS; j += kFNT) {
+      int k = ts + j;
+      sm[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int j = 0; j < kFTS; ++j) {
+      const double4 q = sm[j];
+      const int k = ts + j;
+      double pk[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int t = 0; t < kFTPT; ++t) {
+        double D = fma(-q.x, xi[t][0], P.one_plus_d2);
+        D = fma(-q.y, xi[t][1], D);
+        D = fma(-q.z, xi[t][2], D);
+        double r = adj_rcp(D);
+        r = (valid[t] && k != row[t] && k < c1) ? r : 0.0;  // self pair, padded rows and sources
+        const double s = fma(q.x, vi[t][0], fma(q.y, vi[t][1], q.z * vi[t][2]));
+        const double w1 = q.w * r;
+        const double sr = s * r;
+        const double w2 = w1 * sr;
+        const double sr2 = sr * r;
+        s1[t][0] = fma(w1, q.x, s1[t][0]);
+        s1[t][1] = fma(w1, q.y, s1[t][1]);
+        s1[t][2] = fma(w1, q.z, s1[t][2]);
+        s2[t][0] = fma(w2, q.x, s2[t][0]);
+        s2[t][1] = fma(w2, q.y, s2[t][1]);
+        s2[t][2] = fma(w2, q.z, s2[t][2]);
+        pk[0] = fma(r, vi[t][0], pk[0]);
+        pk[1] = fma(r, vi[t][1], pk[1]);
+        pk[2] = fma(r, vi[t][2], pk[2]);
+        pk[3] = fma(sr2, xi[t][0], pk[3]);
+        pk[4] = fma(sr2, xi[t][1], pk[4]);
+        pk[5] = fma(sr2, xi[t][2], pk[5]);
+        pk[6] += sr;
+      }
+#pragma unroll
+      for (int c = 0; c < 7; ++c) {
+#pragma unroll
+        for (int o = 16; o >= kPARTS; o >>= 1) pk[c] += __shfl_down_sync(0xffffffffu, pk[c], o);
+      }
+      if (lane < kPARTS)
+#pragma unroll
+        for (int c = 0; c < 7; ++c) red[warp * kPARTS + lane][j][c] = pk[c];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kFTS * 7; idx += kFNT) {
+      const int j = idx / 7, c = idx - 7 * j, k = ts + j;
+      if (k < c1) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < kFWARPS * kPARTS; ++w) acc += red[w][j][c];
+        P.colpart[((size_t)blockIdx.x * 7 + c) * N + k] = acc;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < kFTPT; ++t)
+    if (valid[t]) {
+      double* out = P.rowpart + (size_t)blockIdx.y * 6 * N + row[t];
+      out[0] = s1[t][0];
+      out[N] = s1[t][1];
+      out[2 * N] = s1[t][2];
+      out[3 * N] = s2[t][0];
+      out[4 * N] = s2[t][1];
+      out[5 * N] = s2[t][2];
+    }
+}
+
+// Row-major single pass. The source-side sums of panel k are sums over the
+// panels j it acts on, for fixed k - row sums like the target side - and
+// D_ij = D_ji, so one visit of each ordered pair (i, j) gives row i all 13
+// quantities with s_ij = x_j . v_i and s_ji = x_i . v_j:
+//     S1 += G_j r x_j, S2 += G_j s_ij r^2 x_j, P += r v_j, Q += s_ji r^2 x_j,
+//     R += s_ji r        (r = 1/D_ij, 31 FP64 operations per pair)
+// with no reduction across threads. Rows: rowpart[(chunk*13 + c)*n + i].
+constexpr int kRNT = 128, kRTS = 128;
+
+__global__ void __launch_bounds__(kRNT) adj_row_kernel(const AdjLaunch P) {
+  __shared__ double4 sa[kRTS];  // {x_j, G_j}
+  __shared__ double4 sb[kRTS];  // {v_j, 0}
+  const int i = blockIdx.x * kRNT + threadIdx.x;
+  const int ld = i < P.n ? i : P.n - 1;
+  const double xi0 = P.x[3 * (size_t)ld], xi1 = P.x[3 * (size_t)ld + 1], xi2 = P.x[3 * (size_t)ld + 2];
+  const double v0 = P.v[3 * (size_t)ld], v1 = P.v[3 * (size_t)ld + 1], v2 = P.v[3 * (size_t)ld + 2];
+  double a[13];
+#pragma unroll
+  for (int c = 0; c < 13; ++c) a[c] = 0.0;
+  const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
+  for (int ts = c0; ts < c1; ts += kRTS) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < kRTS; j += kRNT) {
+      int k = ts + j;
+      sa[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      if (k < c1) {
+        const double4 q = P.src2_4[k];
+        sb[j] = q;
+      } else {
+        sb[j] = make_double4(0.0, 0.0, 0.0, 0.0);
+      }
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int j = 0; j < kRTS; ++j) {
+      const double4 q = sa[j];
+      const double4 w = sb[j];
+      double D = fma(-q.x, xi0, P.one_plus_d2);
+      D = fma(-q.y, xi1, D);
+      D = fma(-q.z, xi2, D);
+      double r = adj_rcp(D);
+      r = (ts + j == i) ? 0.0 : r;
+      const double sij = fma(q.x, v0, fma(q.y, v1, q.z * v2));
+      const double sji = fma(xi0, w.x, fma(xi1, w.y, xi2 * w.z));
+      const double w1 = q.w * r;
+      const double w2 = w1 * sij * r;
+      const double sr = sji * r;
+      const double sr2 = sr * r;
+      a[0] = fma(w1, q.x, a[0]);
+      a[1] = fma(w1, q.y, a[1]);
+      a[2] = fma(w1, q.z, a[2]);
+      a[3] = fma(w2, q.x, a[3]);
+      a[4] = fma(w2, q.y, a[4]);
+      a[5] = fma(w2, q.z, a[5]);
+      a[6] = fma(r, w.x, a[6]);
+      a[7] = fma(r, w.y, a[7]);
+      a[8] = fma(r, w.z, a[8]);
+      a[9] = fma(sr2, q.x, a[9]);
+      a[10] = fma(sr2, q.y, a[10]);
+      a[11] = fma(sr2, q.z, a[11]);
+      a[12] += sr;
+    }
+  }
+  if (i < P.n) {
+    const size_t n = (size_t)P.n;
+    double* out = P.partial + (size_t)blockIdx.y * 13 * n + i;
+#pragma unroll
+    for (int c = 0; c < 13; ++c) out[c * n] = a[c];
+  }
+}
+
 // v_i = ut_i x x_i with ut_i = mu_x,i + (-2 Omega mu_z,i) z_hat, mu = dt * l_k.
 __global__ void adj_prepare_kernel(const double* __restrict__ x, const double* __restrict__ lkx,
                                    const double* __restrict__ lkz, const double* __restrict__ zeta,
                                    const double* __restrict__ area, int n, double dt, double m2omega,
                                    double* __restrict__ ut, double* __restrict__ v,
                                    double4* __restrict__ src1, double4* __restrict__ src2a,
-                                   double2* __restrict__ src2b) {
+                                   double2* __restrict__ src2b, double4* __restrict__ vrow) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t b = 3 * (size_t)i;
@@ -186,22 +369,25 @@ __global__ void adj_prepare_kernel(const double* __restrict__ x, const double* _
   src1[i] = make_double4(x0, x1, x2, zeta[i] * area[i]);
   src2a[i] = make_double4(x0, x1, x2, v0);
   src2b[i] = make_double2(v1, v2);
+  vrow[i] = make_double4(v0, v1, v2, 0.0);
 }
 
 // lY_i = J(Y)^T mu: gx (3 per row) and gz (1 per row), written to out_x/out_z.
+// p1: chunks of `st1` rows each, the first 6 = (S1, S2); p2: chunks of `st2`
+// rows each, the first 7 = (P, Q, R).
 __global__ void adj_combine_kernel(const double* __restrict__ x, const double* __restrict__ ut,
                                    const double* __restrict__ zeta, const double* __restrict__ area,
-                                   int n, const double* __restrict__ p1, int ch1,
-                                   const double* __restrict__ p2, int ch2, double* __restrict__ out_x,
-                                   double* __restrict__ out_z) {
+                                   int n, const double* __restrict__ p1, int ch1, int st1,
+                                   const double* __restrict__ p2, int ch2, int st2,
+                                   double* __restrict__ out_x, double* __restrict__ out_z) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t N = (size_t)n, b = 3 * (size_t)i;
   double s[6] = {0, 0, 0, 0, 0, 0}, t[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int c = 0; c < ch1; ++c)
-    for (int w = 0; w < 6; ++w) s[w] += p1[((size_t)c * 6 + w) * N + i];
+    for (int w = 0; w < 6; ++w) s[w] += p1[((size_t)c * st1 + w) * N + i];
   for (int c = 0; c < ch2; ++c)
-    for (int w = 0; w < 7; ++w) t[w] += p2[((size_t)c * 7 + w) * N + i];
+    for (int w = 0; w < 7; ++w) t[w] += p2[((size_t)c * st2 + w) * N + i];
   const double u0 = ut[b], u1 = ut[b + 1], u2 = ut[b + 2];
   const double G = zeta[i] * area[i];
   // S1 x ut + S2 + G (P + Q)
@@ -235,7 +421,7 @@ struct AdjWork {
   DevBuf ck;        // checkpoints: ncheck x (3nA + nA)
   DevBuf ys;        // stage inputs of one segment: (steps*4) x (3nA + nA)
   DevBuf lam, lk, tmp;  // adjoint state, lk, accumulators (4nA each)
-  DevBuf ut, v, s1, s2a, s2b, p1, p2;
+  DevBuf ut, v, s1, s2a, s2b, vrow, p1, p2;
 };
 
 int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, double dt,
@@ -248,34 +434,85 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
   const int threads = 256, blocks = (n + threads - 1) / threads;
   tcb::adj_prepare_kernel<<<blocks, threads, 0, ctx->stream>>>(
       yx, lk, lk + 3 * (size_t)n, yz, area, n, dt, -2.0 * ctx->omega, W.ut.as<double>(),
-      W.v.as<double>(), W.s1.as<double4>(), W.s2a.as<double4>(), W.s2b.as<double2>());
+      W.v.as<double>(), W.s1.as<double4>(), W.s2a.as<double4>(), W.s2b.as<double2>(),
+      W.vrow.as<double4>());
   TC_CUDA_TRY(cudaGetLastError());
-  const int tiles = (n + tcb::kAdjNT - 1) / tcb::kAdjNT;
-  const int slots = 8 * ctx->num_sms;
-  int S = std::max(1, std::min(32, (2 * slots + tiles - 1) / tiles));
-  int chunk = (n + S - 1) / S;
-  chunk = (chunk + tcb::kAdjTS - 1) / tcb::kAdjTS * tcb::kAdjTS;
-  S = (n + chunk - 1) / chunk;
   int rc;
-  if ((rc = W.p1.ensure((size_t)S * 6 * n * sizeof(double))) ||
-      (rc = W.p2.ensure((size_t)S * 7 * n * sizeof(double))))
-    return rc;
   const double d = ctx->delta[TC_ACTIVE];
-  tcb::AdjLaunch P1{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), n, chunk, 1.0 + d * d,
-                    W.p1.as<double>()};
-  tcb::adj_target_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P1);
-  TC_CUDA_TRY(cudaGetLastError());
-  tcb::AdjLaunch P2{yx, W.s2a.as<double4>(), W.s2b.as<double2>(), nullptr, n, chunk, 1.0 + d * d,
-                    W.p2.as<double>()};
-  tcb::adj_source_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P2);
-  TC_CUDA_TRY(cudaGetLastError());
+  // 3: row-major single pass (default); 0: two passes; 1, 2: fused with column reductions
+  const int mode = ctx->adj_mode;
+  const int ftb = mode == 1 ? 512 : 512;
+  const int ftiles = (n + ftb - 1) / ftb;
+  const size_t col_bytes = (size_t)ftiles * 7 * n * sizeof(double);
+  int S, S2, st1 = 6, st2 = 7;
+  const double* p2ptr = nullptr;
+  if (mode == 3) {
+    const int tiles = (n + tcb::kRNT - 1) / tcb::kRNT;
+    const int slots = 4 * ctx->num_sms;
+    S = std::max(1, std::min(32, (2 * slots + tiles - 1) / tiles));
+    int chunk = (n + S - 1) / S;
+    chunk = (chunk + tcb::kRTS - 1) / tcb::kRTS * tcb::kRTS;
+    S = (n + chunk - 1) / chunk;
+    S2 = S;
+    st1 = st2 = 13;
+    if ((rc = W.p1.ensure((size_t)S * 13 * n * sizeof(double)))) return rc;
+    tcb::AdjLaunch R{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), W.vrow.as<double4>(), n,
+                     chunk, 1.0 + d * d, W.p1.as<double>()};
+    tcb::adj_row_kernel<<<dim3(tiles, S), tcb::kRNT, 0, ctx->stream>>>(R);
+    TC_CUDA_TRY(cudaGetLastError());
+    p2ptr = W.p1.as<double>() + 6 * (size_t)n;
+    ctx->launches += 1;
+    ctx->pair_launches += 1;
+    ctx->pair_interactions += (long long)n * (long long)(n - 1);
+  } else if (mode != 0 && col_bytes <= (size_t(16) << 30)) {
+    // fused pass: rows and columns from one visit of each pair
+    const int slots = 2 * ctx->num_sms;
+    S = std::max(1, std::min(16, (2 * slots + ftiles - 1) / ftiles));
+    int chunk = (n + S - 1) / S;
+    chunk = (chunk + 63) / 64 * 64;  // a multiple of both variants' shared-memory tile
+    S = (n + chunk - 1) / chunk;
+    S2 = ftiles;
+    if ((rc = W.p1.ensure((size_t)S * 6 * n * sizeof(double))) || (rc = W.p2.ensure(col_bytes)))
+      return rc;
+    tcb::AdjFused F{yx, W.s1.as<double4>(), W.v.as<double>(), n, chunk, 1.0 + d * d,
+                    W.p1.as<double>(), W.p2.as<double>()};
+    if (mode == 1)
+      tcb::adj_fused_kernel<256, 2, 5, 64><<<dim3(ftiles, S), 256, 0, ctx->stream>>>(F);
+    else
+      tcb::adj_fused_kernel<128, 4, 3, 32><<<dim3(ftiles, S), 128, 0, ctx->stream>>>(F);
+    TC_CUDA_TRY(cudaGetLastError());
+    ctx->launches += 1;
+    ctx->pair_launches += 1;
+    ctx->pair_interactions += (long long)n * (long long)(n - 1);
+  } else {
+    // two passes (target side, then the transposed source side)
+    const int tiles = (n + tcb::kAdjNT - 1) / tcb::kAdjNT;
+    const int slots = 8 * ctx->num_sms;
+    S = std::max(1, std::min(32, (2 * slots + tiles - 1) / tiles));
+    int chunk = (n + S - 1) / S;
+    chunk = (chunk + tcb::kAdjTS - 1) / tcb::kAdjTS * tcb::kAdjTS;
+    S = (n + chunk - 1) / chunk;
+    S2 = S;
+    if ((rc = W.p1.ensure((size_t)S * 6 * n * sizeof(double))) ||
+        (rc = W.p2.ensure((size_t)S * 7 * n * sizeof(double))))
+      return rc;
+    tcb::AdjLaunch P1{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), nullptr, n, chunk,
+                      1.0 + d * d, W.p1.as<double>()};
+    tcb::adj_target_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P1);
+    TC_CUDA_TRY(cudaGetLastError());
+    tcb::AdjLaunch P2{yx, W.s2a.as<double4>(), W.s2b.as<double2>(), nullptr, nullptr, n, chunk,
+                      1.0 + d * d, W.p2.as<double>()};
+    tcb::adj_source_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P2);
+    TC_CUDA_TRY(cudaGetLastError());
+    ctx->launches += 2;
+    ctx->pair_launches += 2;
+    ctx->pair_interactions += 2LL * n * (long long)(n - 1);
+  }
   tcb::adj_combine_kernel<<<blocks, threads, 0, ctx->stream>>>(
-      yx, W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, W.p2.as<double>(), S, out,
-      out + 3 * (size_t)n);
+      yx, W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, st1,
+      p2ptr ? p2ptr : W.p2.as<double>(), S2, st2, out, out + 3 * (size_t)n);
   TC_CUDA_TRY(cudaGetLastError());
-  ctx->launches += 4;
-  ctx->pair_launches += 2;
-  ctx->pair_interactions += 2LL * n * (long long)(n - 1);
+  ctx->launches += 2;
   return TC_OK;
 }
 
@@ -350,6 +587,15 @@ __global__ void enstrophy_seed_kernel(const double* __restrict__ z, const double
 // state. functional: TC_J_ENSTROPHY (J = sum zeta^2 A) or TC_J_PROBE
 // (J = zeta of panel `probe` at the end). Inputs are host arrays; outputs:
 // J (host scalar), g_zeta0 (nA), g_x0 (3*nA), host arrays.
+// Device time (ms) of the last adjoint call's phases: the forward sweep with
+// checkpoints, the recomputation of checkpoint segments, and the backward
+// sweep (vector-Jacobian products and combinations).
+extern "C" int tc_adjoint_phase_ms(tc_ctx* ctx, double* ms3) {
+  if (!ctx || !ms3) return TC_ERR_ARG;
+  for (int k = 0; k < 3; ++k) ms3[k] = ctx->adj_ms[k];
+  return TC_OK;
+}
+
 extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0,
                               const double* areaA, int nA, double dt, int nsteps, int ckpt_every,
                               int functional, int probe, double* J, double* g_zeta0, double* g_x0) {
@@ -376,15 +622,33 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
       (rc = W.v.ensure(3 * (size_t)nA * sizeof(double))) ||
       (rc = W.s1.ensure((size_t)nA * sizeof(double4))) ||
       (rc = W.s2a.ensure((size_t)nA * sizeof(double4))) ||
-      (rc = W.s2b.ensure((size_t)nA * sizeof(double2))))
+      (rc = W.s2b.ensure((size_t)nA * sizeof(double2))) ||
+      (rc = W.vrow.ensure((size_t)nA * sizeof(double4))))
     return rc;
   double* ck = W.ck.as<double>();
-  // forward sweep with checkpoints
+  double* ys = W.ys.as<double>();
+  // phase timing: forward sweep, recomputation, backward (CUDA events on the stream)
+  cudaEvent_t ev[4];
+  for (auto& e : ev) TC_CUDA_TRY(cudaEventCreate(&e));
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int k = 0; k < 4; ++k) cudaEventDestroy(e[k]);
+    }
+  } ev_guard{ev};
+  float recompute_ms = 0.f;
+  TC_CUDA_TRY(cudaEventRecord(ev[0], ctx->stream));
+  // forward sweep with checkpoints; the last segment's stage inputs are kept
+  // as they are computed, so that segment needs no recomputation
+  const int last_seg = nsteps > 0 ? (nsteps - 1) / ckpt_every : 0;
   for (int step = 0; step < nsteps; ++step) {
     if (step % ckpt_every == 0 && (rc = state_copy(ctx, ck + (size_t)(step / ckpt_every) * W.n4, false)))
       return rc;
-    if ((rc = forward_step(ctx, dt, nullptr))) return rc;
+    const int seg = step / ckpt_every;
+    double* rec = seg == last_seg ? ys + (size_t)(step - seg * ckpt_every) * 4 * W.n4 : nullptr;
+    if ((rc = forward_step(ctx, dt, rec))) return rc;
   }
+  TC_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));
   // seed: l(T) = dJ/dX(T)
   double* lam = W.lam.as<double>();
   TC_CUDA_TRY(cudaMemsetAsync(lam, 0, B, ctx->stream));
@@ -410,7 +674,6 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
     TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   }
   // backward sweep, one checkpoint segment at a time
-  double* ys = W.ys.as<double>();
   double* lk = W.lk.as<double>();
   double* acc = W.tmp.as<double>();
   double* ly = nullptr;
@@ -419,9 +682,17 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
   ly = lyb.as<double>();
   for (int seg = (nsteps - 1) / ckpt_every; seg >= 0 && nsteps > 0; --seg) {
     const int s0 = seg * ckpt_every, s1 = std::min(nsteps, s0 + ckpt_every);
-    if ((rc = state_copy(ctx, ck + (size_t)seg * W.n4, true))) return rc;
-    for (int step = s0; step < s1; ++step)
-      if ((rc = forward_step(ctx, dt, ys + (size_t)(step - s0) * 4 * W.n4))) return rc;
+    if (seg != last_seg) {
+      TC_CUDA_TRY(cudaEventRecord(ev[2], ctx->stream));
+      if ((rc = state_copy(ctx, ck + (size_t)seg * W.n4, true))) return rc;
+      for (int step = s0; step < s1; ++step)
+        if ((rc = forward_step(ctx, dt, ys + (size_t)(step - s0) * 4 * W.n4))) return rc;
+      TC_CUDA_TRY(cudaEventRecord(ev[3], ctx->stream));
+      TC_CUDA_TRY(cudaEventSynchronize(ev[3]));
+      float ms = 0.f;
+      TC_CUDA_TRY(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+      recompute_ms += ms;
+    }
     for (int step = s1 - 1; step >= s0; --step) {
       const double* Y = ys + (size_t)(step - s0) * 4 * W.n4;
       // acc = l' (the identity part); lk for stage 4 = l'/6
@@ -441,6 +712,14 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
       TC_CUDA_TRY(cudaMemcpyAsync(lam, acc, B, cudaMemcpyDeviceToDevice, ctx->stream));
     }
   }
+  TC_CUDA_TRY(cudaEventRecord(ev[2], ctx->stream));
+  TC_CUDA_TRY(cudaEventSynchronize(ev[2]));
+  float fwd_ms = 0.f, total_ms = 0.f;
+  TC_CUDA_TRY(cudaEventElapsedTime(&fwd_ms, ev[0], ev[1]));
+  TC_CUDA_TRY(cudaEventElapsedTime(&total_ms, ev[0], ev[2]));
+  ctx->adj_ms[0] = fwd_ms;
+  ctx->adj_ms[1] = recompute_ms;
+  ctx->adj_ms[2] = total_ms - fwd_ms - recompute_ms;
   TC_CUDA_TRY(cudaMemcpyAsync(g_x0, lam, 3 * (size_t)nA * sizeof(double), cudaMemcpyDeviceToHost,
                               ctx->stream));
   TC_CUDA_TRY(cudaMemcpyAsync(g_zeta0, lam + 3 * (size_t)nA, (size_t)nA * sizeof(double),

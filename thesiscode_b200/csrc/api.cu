@@ -192,6 +192,12 @@ extern "C" int tc_get_smooth(tc_ctx* ctx, double* smooth) {
   return TC_OK;
 }
 
+extern "C" int tc_set_adjoint_mode(tc_ctx* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 3) return TC_ERR_ARG;
+  ctx->adj_mode = mode;
+  return TC_OK;
+}
+
 extern "C" int tc_set_target_order(tc_ctx* ctx, int order) {
   if (!ctx || (order != TC_ORDER_GIVEN && order != TC_ORDER_HILBERT)) return TC_ERR_ARG;
   ctx->target_order = order;

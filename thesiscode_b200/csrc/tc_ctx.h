@@ -89,6 +89,8 @@ struct tc_ctx {
   tcb::PairCfg cfg32{256, 4, 256};
   int var64 = 2, var32 = 4;  // pair-kernel variants in use (see kVariants64/32)
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
+  double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
+  int adj_mode = 3;  // adjoint VJP: 3 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
   tcb::DevBuf order_buf[4];             // keys, sorted keys, indices, sort scratch
   int min_chunk = 4096;   // smallest source chunk a CTA walks
   int max_chunks = 64;
