@@ -37,6 +37,9 @@ sys.path.insert(0, str(ROOT))
 
 FLOPS_PER_INTERACTION = 22  # dot 5, denominator 1, weight 1, cross 9, accumulate 6
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) of one FP32C pair launch on the level-7 Gaussian workload, from an
+# ncu capture of `bench.py --quick --no-cpu --steps 2` (dram__bytes_read.sum + dram__bytes_write.sum)
+PAIR_FP32C_L7_DRAM_BYTES = 28.07e6 + 42.58e6
 
 
 def build_workload(name: str):
@@ -396,7 +399,9 @@ def run_ours(args):
         "config": workload_config(w, args.precision, f"target-sharded x{world}" if world > 1 else "1 GPU"),
         "roofline": {"bound": "fp32" if args.precision == "fp32c" else "fp64",
                      "achieved": achieved / 1e12, "peak": fp_peak / 1e12, "unit": "TFLOP/s",
-                     "frac": achieved / fp_peak, "traffic": None,
+                     "frac": achieved / fp_peak,
+                     "traffic": PAIR_FP32C_L7_DRAM_BYTES if (args.precision == "fp32c" and
+                                                              args.config == "gaussian_l7") else None,
                      "kernel": f"pair_{args.precision}_kernel",
                      "flops_per_interaction": FLOPS_PER_INTERACTION,
                      "pair_ms_per_launch": pair_ms_launch,

@@ -448,8 +448,22 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
   const double* p2ptr = nullptr;
   if (mode == 3) {
     const int tiles = (n + tcb::kRNT - 1) / tcb::kRNT;
-    const int slots = 4 * ctx->num_sms;
-    S = std::max(1, std::min(32, (2 * slots + tiles - 1) / tiles));
+    int per_sm = 0;
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tcb::adj_row_kernel,
+                                                              tcb::kRNT, 0));
+    const int slots = std::max(1, per_sm) * ctx->num_sms;
+    // whole waves: the chunk count that best fills tiles x chunks into the resident slots
+    S = 1;
+    double best = 0.0;
+    for (int c = 1; c <= 32; ++c) {
+      if (c > 1 && (n + c - 1) / c < 1024) break;
+      const long long items = (long long)tiles * c, waves = (items + slots - 1) / slots;
+      const double eff = (double)items / (double)(waves * slots);
+      if (eff > best + 0.02) {
+        best = eff;
+        S = c;
+      }
+    }
     int chunk = (n + S - 1) / S;
     chunk = (chunk + tcb::kRTS - 1) / tcb::kRTS * tcb::kRTS;
     S = (n + chunk - 1) / chunk;

@@ -1,10 +1,11 @@
 """One launch of the pair kernels on a workload of a chosen size, for profilers.
 
-    python -m thesiscode_b200.profile_case --precision fp32c --level 6 [--what velocity|rk4]
+    python -m thesiscode_b200.profile_case --precision fp32c --level 6 [--what velocity|rk4|adjoint]
 
 `velocity` runs one TC_ACTIVE and one TC_VERTEX sum (two pair-kernel launches);
-`rk4` runs one fused RK4 step (four pair-kernel launches). The Gaussian-vortex
-workload with delta 0.01 is used at every level.
+`rk4` runs one fused RK4 step (four pair-kernel launches); `adjoint` runs the
+FP64 adjoint of two RK4 steps (eight vector-Jacobian pair launches). The
+Gaussian-vortex workload with delta 0.01 is used at every level.
 """
 from __future__ import annotations
 
@@ -19,7 +20,7 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--level", type=int, default=6)
-    ap.add_argument("--what", default="velocity", choices=["velocity", "rk4"])
+    ap.add_argument("--what", default="velocity", choices=["velocity", "rk4", "adjoint"])
     a = ap.parse_args()
     w = configs.gaussian(level=a.level, delta=0.01)
     ctx = Context(0, a.precision)
@@ -28,8 +29,14 @@ def main() -> None:
     if a.what == "velocity":
         ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
         ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
-    else:
+    elif a.what == "rk4":
         ctx.rk4_step(w.xA.copy(), w.zetaA.copy(), w.areaA, w.xV.copy(), w.xQ.copy(), w.dt, 1)
+    else:
+        import numpy as np
+
+        J, gz, gx = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
+        N.call("tc_rk4_adjoint", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt, 2, 2,
+               N.TC_J_ENSTROPHY, 0, N.dptr(J), N.dptr(gz), N.dptr(gx))
     ctx.synchronize()
     ctx.close()
     print(f"profile_case {a.precision} level {a.level} {a.what}: ok")
