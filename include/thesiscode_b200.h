@@ -185,6 +185,19 @@ int tc_rk4_step(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int
 int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int nA,
                        double* xV, int nV, double* xQ, int nQ, double dt, int nsteps,
                        double* totalKE, double* kineticEnergy);
+/* StratosphereRK4 (PanelVelocityParallel.f90:661-919): nsteps forced RK4
+ * steps from time t. Positions of the three classes advance like tc_rk4_step;
+ * the active vorticity is not integrated: each stage's source vorticity is
+ * absVortA - 2 Omega z - F(x, t_s) with the Juckes forcing F
+ * (TracerAndVorticityDistributions.f90:1213-1221) at t_s = t, t + dt/2,
+ * t + dt/2, t + dt (:690-694, :752-755, :800-803, :847-850). On return
+ * relVortA[nA] and relVortV[nV] (nullable; relVortV needs absVortV) hold
+ * absVort - 2 Omega z - F(x, t + nsteps dt) at the new positions (:908-915).
+ * totalKE / kineticEnergy as for tc_rk4_step. Step k starts at t + k dt. */
+int tc_strat_rk4_step(tc_ctx* ctx, double* xA, const double* absVortA, double* relVortA,
+                      const double* areaA, int nA, double* xV, const double* absVortV,
+                      double* relVortV, int nV, double* xQ, int nQ, double t, double dt,
+                      int nsteps, double* totalKE, double* kineticEnergy);
 /* Device-resident state: load once (InitRK4 + GatherPanels copy, :236-318),
  * advance any number of steps, store when the caller needs the arrays. */
 int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA, const double* areaA, int nA,
@@ -206,11 +219,14 @@ int tc_reset_rk4(tc_ctx* ctx);
 int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA,
                    int nA, double dt, int nsteps, int ckpt_every, int functional, int probe,
                    double* J, double* g_zeta0, double* g_x0);
-/* How each stage's vector-Jacobian product visits the pairs: 3 = one
- * row-major pass computing both sides' row sums (the default), 0 = two
+/* How each stage's vector-Jacobian product visits the pairs: 3 to 6 = one
+ * row-major pass computing both sides' row sums (3: one row per thread,
+ * 4: two rows per thread; 5 and 6: the same with a one-step Newton
+ * reciprocal, relative error the square of the rcp.approx.f64 seed's), 0 = two
  * passes (target side, transposed source side), 1 and 2 = one pass with
- * in-block column reductions (256 threads x 2 targets, or 128 x 4). All
- * modes give the same gradient to rounding. */
+ * in-block column reductions (256 threads x 2 targets, or 128 x 4). Default 5.
+ * Modes 0-4 give the same gradient to FP64 rounding; 5 and 6 differ from them
+ * by the seed's squared error (below 1e-13 of the gradient's scale). */
 int tc_set_adjoint_mode(tc_ctx* ctx, int mode);
 /* Device time (ms) of the last tc_rk4_adjoint call: ms3[0] forward sweep
  * with checkpoints, ms3[1] recomputation of checkpoint segments, ms3[2]
@@ -252,10 +268,12 @@ int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr, int
 
 /* ---- pair-kernel variants (no counterpart in the reference) ------------ */
 /* Number of compiled launch shapes for a precision, and their parameters:
- * info7 = {threads, targets/thread, sources/tile, FP32 flush length (0 for
- * FP64), min CTAs/SM, unroll, targets/CTA}. */
+ * info8 = {threads, targets/thread, sources/tile, FP32 flush length (FP64:
+ * 1 fused denominator, 0 rounded like the reference), min CTAs/SM, unroll,
+ * targets/CTA, form (FP32C: bit 0 far-field expansion for well-separated
+ * source tiles, bit 1 one reciprocal per two targets; FP64: 0)}. */
 int tc_pair_variant_count(int precision, int* count);
-int tc_pair_variant_info(int precision, int id, int* info7);
+int tc_pair_variant_info(int precision, int id, int* info8);
 int tc_set_pair_variant(tc_ctx* ctx, int precision, int id);
 int tc_get_pair_variant(tc_ctx* ctx, int precision, int* id);
 

@@ -77,6 +77,20 @@ void or_bve_stage(const double* xA, const double* zetaA, const double* areaA, in
                   int v1, int q0, int q1,
                   double* dXA, double* dVortA, double* dXV, double* dXQ, int nthreads);
 
+/* Juckes forcing F(x, t) and its time factor A(t),
+ * TracerAndVorticityDistributions.f90:1213-1221, :550-566 (strat_oracle.c). */
+double or_juckes_forcing(const double* xyz, double t);
+double or_juckes_a(double t);
+
+/* StratosphereRK4, PanelVelocityParallel.f90:661-919, with one rank: one
+ * forced RK4 step from time t (strat_oracle.c). Positions are updated in
+ * place; relVortA / relVortV (nullable) receive absVort - 2 Omega z - F(x, t+dt)
+ * at the new positions. Returns totalKE of stage 1. */
+double or_strat_rk4(double* xV, int nV, double* xA, const double* absVortA, double* relVortA,
+                    const double* areaA, int nA, double* xQ, int nQ, const double* absVortV,
+                    double* relVortV, double t, double dt, double omega, double deltaA,
+                    double deltaV, double deltaQ, double* kineticEnergy, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,4 +1,4 @@
-"""ctypes wrapper of the CPU FP64 oracle (oracle/bve_oracle.c).
+"""ctypes wrapper of the CPU FP64 oracle (oracle/bve_oracle.c, oracle/strat_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
 the checker and by bench.py's CPU-baseline leg. The product never imports
@@ -49,6 +49,13 @@ def lib():
         h.or_bve_stage.argtypes = [dp, dp, dp, c_int, dp, c_int, dp, c_int, c_double, c_double,
                                    c_double, c_double, c_int, c_int, c_int, c_int, c_int, c_int,
                                    dp, dp, dp, dp, c_int]
+        h.or_juckes_forcing.argtypes = [dp, c_double]
+        h.or_juckes_forcing.restype = c_double
+        h.or_juckes_a.argtypes = [c_double]
+        h.or_juckes_a.restype = c_double
+        h.or_strat_rk4.argtypes = [dp, c_int, dp, dp, dp, dp, c_int, dp, c_int, dp, dp, c_double,
+                                   c_double, c_double, c_double, c_double, c_double, dp, c_int]
+        h.or_strat_rk4.restype = c_double
         _lib = h
     return _lib
 
@@ -152,3 +159,27 @@ def bve_stage(xA, zetaA, areaA, xV, xQ, omega, deltas, ranges, nthreads=1):
                        deltas[1], deltas[2], *[int(r) for r in ranges], _d(dXA), _d(dVA), _d(dXV),
                        _d(dXQ), nthreads)
     return dXA, dVA, dXV, dXQ
+
+
+def juckes_forcing(x, t):
+    """Juckes forcing F(x, t) at each row of x (n,3)."""
+    x = _c(np.atleast_2d(x))
+    return np.array([lib().or_juckes_forcing(_d(np.ascontiguousarray(r)), float(t)) for r in x])
+
+
+def strat_rk4(xV, xA, absVortA, areaA, xQ, t, dt, omega=2 * np.pi, deltas=(0.0, 0.0, 0.05),
+              absVortV=None, nthreads=1):
+    """One StratosphereRK4 step from time t on copies; returns
+    (xV, xA, relVortA, xQ, totalKE, kineticEnergy, relVortV)."""
+    xV, xA, absA, areaA, xQ = (_c(a).copy() for a in (xV, xA, absVortA, areaA, xQ))
+    nA = xA.shape[0]
+    ke = np.zeros(nA)
+    relA = np.zeros(nA)
+    relV = absV = None
+    if absVortV is not None:
+        absV = _c(absVortV)
+        relV = np.zeros(xV.shape[0])
+    tke = lib().or_strat_rk4(_d(xV), xV.shape[0], _d(xA), _d(absA), _d(relA), _d(areaA), nA, _d(xQ),
+                             xQ.shape[0], _d(absV), _d(relV), t, dt, omega, deltas[0], deltas[1],
+                             deltas[2], _d(ke), nthreads)
+    return xV, xA, relA, xQ, tke, ke, relV

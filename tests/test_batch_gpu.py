@@ -10,7 +10,7 @@ from thesiscode_b200.batch import batch_info, batch_rk4
 from thesiscode_b200.panel_velocity import Context
 
 pytestmark = pytest.mark.gpu
-TOL = {"fp64": 1e-12, "fp32c": 3e-7}
+TOL = {"fp64": 1e-12, "fp32c": 5e-7}  # levels 1-3: the coarse-grid FP32C bound
 
 
 def small_batch(seed=4):

@@ -173,3 +173,50 @@ def test_ics_reference_vs_benchmark_formulas():
     cfg = ics.rh4_config(x)
     zonal = 2.0 * (np.pi / 7.0) * x[:, 2]
     np.testing.assert_allclose(cfg - zonal, -(np.pi / 7.0) * (ref - zonal), atol=1e-12)
+
+
+def test_juckes_forcing_time_window_and_hemisphere():
+    """Juckes_A (TracerAndVorticityDistributions.f90:550-566) ramps over [0, 4), holds 1 on
+    [4, 11), ramps down over [11, 15) and is 0 outside; B(lat) = 0 for lat <= 0 (:600-611)."""
+    lib = O.lib()
+    assert lib.or_juckes_a(-0.5) == 0.0 and lib.or_juckes_a(0.0) == 0.0
+    assert abs(lib.or_juckes_a(2.0) - 0.5) < 1e-15
+    assert lib.or_juckes_a(4.0) == 1.0 and lib.or_juckes_a(10.99) == 1.0
+    assert abs(lib.or_juckes_a(13.0) - 0.5) < 1e-15
+    assert lib.or_juckes_a(15.0) == 0.0 and lib.or_juckes_a(30.0) == 0.0
+    south = ics.sphere_point(np.deg2rad(-30.0), 1.0)
+    assert O.juckes_forcing(south, 5.0)[0] == 0.0
+    lat, lon = np.deg2rad(50.0), 0.3
+    q = np.tan(np.pi / 3) ** 2 / np.tan(lat) ** 2
+    expect = 0.3 * 4 * np.pi * q * np.exp(1 - q) * np.cos(lon)
+    got = O.juckes_forcing(ics.sphere_point(lat, lon), 5.0)[0]
+    assert abs(got - expect) <= 1e-14 * abs(expect)
+
+
+def test_stratosphere_step_without_forcing_is_the_bve_step():
+    """With the forcing off (t >= 15) StratosphereRK4 rebuilds zeta = absVort - 2 Omega z at each
+    stage input, which is exactly what BVERK4's integrated zeta is (both are linear in the same
+    stage increments): the two steps agree to rounding."""
+    w = configs.stratosphere(level=3, dt=0.01)
+    absA, absV = w.meta["absVortA"], w.meta["absVortV"]
+    zA = absA - 2.0 * w.omega * w.xA[:, 2]
+    bve = O.bve_rk4(w.xV, w.xA, zA, w.areaA, w.xQ, w.dt, w.omega, w.deltas, absVortV=absV, nthreads=4)
+    st = O.strat_rk4(w.xV, w.xA, absA, w.areaA, w.xQ, 20.0, w.dt, w.omega, w.deltas, absVortV=absV,
+                     nthreads=4)
+    disp = np.abs(bve[1] - w.xA).max()
+    assert np.abs(st[1] - bve[1]).max() <= 1e-12 * disp
+    assert np.abs(st[0] - bve[0]).max() <= 1e-12 * disp
+    assert np.abs(st[2] - bve[2]).max() <= 1e-12 * np.abs(zA).max()
+    assert np.abs(st[6] - bve[6]).max() <= 1e-12 * np.abs(zA).max()
+    assert abs(st[4] - bve[4]) <= 1e-13 * bve[4]
+
+
+def test_stratosphere_forcing_changes_the_flow():
+    w = configs.stratosphere(level=3, dt=0.01)
+    absA = w.meta["absVortA"]
+    on = O.strat_rk4(w.xV, w.xA, absA, w.areaA, w.xQ, 5.0, w.dt, w.omega, w.deltas, nthreads=4)
+    off = O.strat_rk4(w.xV, w.xA, absA, w.areaA, w.xQ, 20.0, w.dt, w.omega, w.deltas, nthreads=4)
+    F = O.juckes_forcing(on[1], 5.0 + w.dt)
+    assert np.abs(F).max() > 0.1
+    # relVort difference at the new time is the forcing (positions differ by O(dt))
+    assert np.abs((off[2] - on[2]) - F).max() < 0.05 * np.abs(F).max()

@@ -20,8 +20,12 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 FP64_TOL = 1e-12
 # FP32-compensated path, stated bound: 1e-7 from level 6 up (the benchmark sizes; tiles of
-# the quad-tree target order are small against the sphere), 3e-7 on coarser grids, where
-# the FP32 rounding of each pair term (a few ulps) is the floor.
+# the Hilbert target order are small against the sphere), 3e-7 at levels 4-5 and 5e-7 at
+# levels <= 3 (<= 1,280 panels), where one tile spans much of the sphere and the FP32
+# rounding of each pair term relative to the tile origin (a few ulps) is the floor; it
+# moves between 2e-7 and 4e-7 with the tile shape. Scaled to the largest value of the
+# compared quantity (dVort = -2 Omega u_z scales with max |u_z|, not max |u|).
+FP32C_TOL_COARSE = 5e-7
 FP32C_TOL = 3e-7
 FP32C_TOL_FINE = 1e-7
 
@@ -49,7 +53,7 @@ def setup(ctx, omega, deltas):
     ctx.set_deltas(*deltas)
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL_COARSE)])
 def test_three_sums_against_golden(prec, tol, gpu):
     g = np.load(GOLDEN / "rh4_parity_l2.npz")
     ctx = Context(0, prec)
@@ -127,7 +131,7 @@ def test_fp32c_accuracy_does_not_depend_on_target_order(ctx32):
     assert np.abs(dX[rows] - ref).max() / np.abs(dX).max() <= FP32C_TOL_FINE
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL_COARSE)])
 def test_rk4_step_parity_mode_golden(prec, tol, gpu):
     g = np.load(GOLDEN / "rh4_parity_l2.npz")
     ctx = Context(0, prec)
@@ -143,7 +147,7 @@ def test_rk4_step_parity_mode_golden(prec, tol, gpu):
     ctx.close()
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL)])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL_COARSE)])
 def test_rk4_two_steps_config_mode_golden(prec, tol, gpu):
     g = np.load(GOLDEN / "gauss_config_l3.npz")
     ctx = Context(0, prec)
@@ -199,7 +203,7 @@ def test_edge_cases(ctx64, ctx32):
             n = 1 + (m * 7) % w.nA
             dX, _ = ctx.velocity(N.TC_VERTEX, w.xV[:m % w.nV + 1], w.xA[:n], w.zetaA[:n], w.areaA[:n])
             ref = O.passive_rhs(w.xV[:m % w.nV + 1], w.xA[:n], w.zetaA[:n], w.areaA[:n])
-            assert rel_err(dX, ref) <= (FP64_TOL if ctx is ctx64 else FP32C_TOL)
+            assert rel_err(dX, ref) <= (FP64_TOL if ctx is ctx64 else FP32C_TOL_COARSE)
 
 
 def test_off_sphere_points(ctx64, ctx32):
@@ -209,7 +213,7 @@ def test_off_sphere_points(ctx64, ctx32):
     xA = w.xA * (1.0 + 1e-6 * rng.standard_normal((w.nA, 1)))
     xV = w.xV * (1.0 + 1e-6 * rng.standard_normal((w.nV, 1)))
     ref = O.passive_rhs(xV, xA, w.zetaA, w.areaA)
-    for ctx, tol in ((ctx64, FP64_TOL), (ctx32, FP32C_TOL)):
+    for ctx, tol in ((ctx64, FP64_TOL), (ctx32, FP32C_TOL_COARSE)):
         setup(ctx, w.omega, w.deltas)
         dX, _ = ctx.velocity(N.TC_VERTEX, xV, xA, w.zetaA, w.areaA)
         assert rel_err(dX, ref) <= tol
@@ -240,3 +244,33 @@ def test_errors_are_reported_not_raised_on_device(ctx64):
     # the context stays usable after each refused call
     dX, _ = ctx64.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
     assert np.all(np.isfinite(dX))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_every_pair_variant_matches_oracle(gpu, precision):
+    """Every compiled launch shape (threads, targets per thread, flush length, register cap,
+    FP32C far-field form and paired reciprocal) gives the oracle's sums within the path's
+    tolerance, on a level-5 Gaussian (sampled rows) in its Hilbert visiting order."""
+    import ctypes
+    w = configs.gaussian(level=5, delta=0.01)
+    pid = N.TC_FP64 if precision == "fp64" else N.TC_FP32C
+    tol = FP64_TOL if precision == "fp64" else FP32C_TOL
+    rng = np.random.default_rng(11)
+    ra = np.sort(rng.choice(w.nA, 256, replace=False))
+    rv = np.sort(rng.choice(w.nV, 256, replace=False))
+    refA = O.rows(0, ra, None, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
+    refV = O.rows(1, rv, w.xV, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
+    scale = max(np.abs(refA).max(), np.abs(refV).max())
+    cnt = ctypes.c_int()
+    N.call("tc_pair_variant_count", pid, ctypes.byref(cnt))
+    assert cnt.value >= 6
+    for v in range(cnt.value):
+        ctx = Context(0, precision)
+        ctx.set_omega(w.omega)
+        ctx.set_deltas(*w.deltas)
+        N.call("tc_set_pair_variant", ctx.handle, pid, v)
+        dA, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+        dV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+        err = max(np.abs(dA[ra] - refA).max(), np.abs(dV[rv] - refV).max()) / scale
+        assert err <= tol, (v, err)
+        ctx.close()

@@ -12,7 +12,7 @@ from thesiscode_b200.voronoi_velocity import BVERK4, BVEVelocity, VorPanels
 
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
-TOL = {"fp64": 1e-12, "fp32c": 3e-7}
+TOL = {"fp64": 1e-12, "fp32c": 5e-7}  # levels 2-3: the coarse-grid FP32C bound
 
 
 def rel(a, b):

@@ -100,6 +100,24 @@ def solid_body(level=3, rotation_rate=2.0 * np.pi, dt=0.01, steps=1) -> Workload
                     (0.0, 0.0, 0.0), dt, steps, dict(rotation_rate=rotation_rate))
 
 
+def stratosphere(level=4, dt=0.01, steps=1, t0=5.0, Omega=2.0 * np.pi, parity=True) -> Workload:
+    """Forced stratosphere model (InitStratosphere, TracerAndVorticityDistributions.f90:793-824;
+    StratosphereRK4, PanelVelocityParallel.f90:661-919): relVort = StratosphereRelVortX - gaussConst,
+    absVort = relVort + 2 Omega z at panels and vertices; meta holds absVortA, absVortV and the start
+    time t0 (the Juckes forcing is fully on for 4 <= t < 11)."""
+    parts, pans, maps, xA, aA, xQ = _grid(level)
+    g = ics.stratosphere_rel_vort(xA)
+    gc = ics.remove_area_mean(g, aA)
+    zA = g - gc
+    xV = parts.x.copy()
+    absA = zA + 2.0 * Omega * xA[:, 2]
+    absV = ics.stratosphere_rel_vort(xV) - gc + 2.0 * Omega * xV[:, 2]
+    deltas = (0.0, 0.0, 0.05)
+    xQ = xQ if parity else np.zeros((0, 3))
+    return Workload(f"stratosphere_l{level}", level, xA, zA, aA, xV, xQ, Omega, deltas, dt, steps,
+                    dict(ic="StratosphereRelVortX - gaussConst", absVortA=absA, absVortV=absV, t0=t0))
+
+
 def batched_gaussians(count=64, seed=4, levels=(3, 4, 5, 6), dt=0.01, steps=10,
                       Omega=2.0 * np.pi, delta=0.0) -> list[Workload]:
     """Config 4: independent Gaussian vortices, level ~ U{3..6}, centre uniform on the sphere,

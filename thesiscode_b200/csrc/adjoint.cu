@@ -277,73 +277,123 @@ __global__ void __launch_bounds__(kFNT) adj_fused_kernel(const AdjFused P) {
 
 // Row-major single pass. The source-side sums of panel k are sums over the
 // panels j it acts on, for fixed k - row sums like the target side - and
-// D_ij = D_ji, so one visit of each ordered pair (i, j) gives row i all 13
-// quantities with s_ij = x_j . v_i and s_ji = x_i . v_j:
-//     S1 += G_j r x_j, S2 += G_j s_ij r^2 x_j, P += r v_j, Q += s_ji r^2 x_j,
-//     R += s_ji r        (r = 1/D_ij, 31 FP64 operations per pair)
-// with no reduction across threads. Rows: rowpart[(chunk*13 + c)*n + i].
-constexpr int kRNT = 128, kRTS = 128;
+// D_ij = D_ji, so one visit of each ordered pair (i, j) gives row i every sum
+// it needs, with s_ij = x_j . v_i and s_ji = x_i . v_j. Q_i enters dL/dx_i only
+// as G_i Q_i, next to S2_i, and both weight x_j, so they share one accumulator:
+//     S1 += G_j r x_j,  C += (G_j s_ij + G_i s_ji) r^2 x_j  (= S2 + G_i Q),
+//     P  += r v_j,      R += s_ji r                          (r = 1/D_ij)
+// 10 accumulators per row and 24 FP64 operations per pair besides the
+// reciprocal: rcp.approx.f64 seed + NEWTON Newton-Raphson steps
+// r <- r + r (1 - D r) of 2 FMA each (2 steps: full FP64; 1 step: the seed's
+// error squared). TPT rows per thread share each source's shared-memory loads.
+// No reduction across threads. Rows: partial[(chunk*10 + c)*n + i].
+constexpr int kRNT = 128, kRTS = 128, kRowSums = 10;
 
+template <int NEWTON>
+__device__ __forceinline__ double adj_rcp_n(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+#pragma unroll
+  for (int k = 0; k < NEWTON; ++k) r = fma(r, fma(-d, r, 1.0), r);
+  return r;
+}
+
+template <int TPT, int NEWTON, int UNROLL>
 __global__ void __launch_bounds__(kRNT) adj_row_kernel(const AdjLaunch P) {
   __shared__ double4 sa[kRTS];  // {x_j, G_j}
   __shared__ double4 sb[kRTS];  // {v_j, 0}
-  const int i = blockIdx.x * kRNT + threadIdx.x;
-  const int ld = i < P.n ? i : P.n - 1;
-  const double xi0 = P.x[3 * (size_t)ld], xi1 = P.x[3 * (size_t)ld + 1], xi2 = P.x[3 * (size_t)ld + 2];
-  const double v0 = P.v[3 * (size_t)ld], v1 = P.v[3 * (size_t)ld + 1], v2 = P.v[3 * (size_t)ld + 2];
-  double a[13];
+  int row[TPT];
+  double x0[TPT], x1[TPT], x2[TPT], v0[TPT], v1[TPT], v2[TPT], gi[TPT];
+  double a[TPT][kRowSums];
 #pragma unroll
-  for (int c = 0; c < 13; ++c) a[c] = 0.0;
+  for (int t = 0; t < TPT; ++t) {
+    row[t] = (blockIdx.x * TPT + t) * kRNT + threadIdx.x;
+    const int ld = row[t] < P.n ? row[t] : P.n - 1;
+    const double4 q = P.src[ld];
+    const double4 w = P.src2_4[ld];
+    x0[t] = q.x;
+    x1[t] = q.y;
+    x2[t] = q.z;
+    gi[t] = q.w;
+    v0[t] = w.x;
+    v1[t] = w.y;
+    v2[t] = w.z;
+#pragma unroll
+    for (int c = 0; c < kRowSums; ++c) a[t][c] = 0.0;
+  }
   const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
   for (int ts = c0; ts < c1; ts += kRTS) {
     __syncthreads();
     for (int j = threadIdx.x; j < kRTS; j += kRNT) {
-      int k = ts + j;
+      const int k = ts + j;
       sa[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
-      if (k < c1) {
-        const double4 q = P.src2_4[k];
-        sb[j] = q;
-      } else {
-        sb[j] = make_double4(0.0, 0.0, 0.0, 0.0);
-      }
+      sb[j] = k < c1 ? P.src2_4[k] : make_double4(0.0, 0.0, 0.0, 0.0);
     }
     __syncthreads();
-#pragma unroll 2
+#pragma unroll UNROLL
     for (int j = 0; j < kRTS; ++j) {
       const double4 q = sa[j];
       const double4 w = sb[j];
-      double D = fma(-q.x, xi0, P.one_plus_d2);
-      D = fma(-q.y, xi1, D);
-      D = fma(-q.z, xi2, D);
-      double r = adj_rcp(D);
-      r = (ts + j == i) ? 0.0 : r;
-      const double sij = fma(q.x, v0, fma(q.y, v1, q.z * v2));
-      const double sji = fma(xi0, w.x, fma(xi1, w.y, xi2 * w.z));
-      const double w1 = q.w * r;
-      const double w2 = w1 * sij * r;
-      const double sr = sji * r;
-      const double sr2 = sr * r;
-      a[0] = fma(w1, q.x, a[0]);
-      a[1] = fma(w1, q.y, a[1]);
-      a[2] = fma(w1, q.z, a[2]);
-      a[3] = fma(w2, q.x, a[3]);
-      a[4] = fma(w2, q.y, a[4]);
-      a[5] = fma(w2, q.z, a[5]);
-      a[6] = fma(r, w.x, a[6]);
-      a[7] = fma(r, w.y, a[7]);
-      a[8] = fma(r, w.z, a[8]);
-      a[9] = fma(sr2, q.x, a[9]);
-      a[10] = fma(sr2, q.y, a[10]);
-      a[11] = fma(sr2, q.z, a[11]);
-      a[12] += sr;
+#pragma unroll
+      for (int t = 0; t < TPT; ++t) {
+        double D = fma(-q.x, x0[t], P.one_plus_d2);
+        D = fma(-q.y, x1[t], D);
+        D = fma(-q.z, x2[t], D);
+        double r = adj_rcp_n<NEWTON>(D);
+        r = (ts + j == row[t]) ? 0.0 : r;  // k == i: no self term (zero-padded sources give r*0)
+        const double sij = fma(q.x, v0[t], fma(q.y, v1[t], q.z * v2[t]));
+        const double sji = fma(x0[t], w.x, fma(x1[t], w.y, x2[t] * w.z));
+        const double c = fma(q.w, sij, gi[t] * sji) * (r * r);
+        const double w1 = q.w * r;
+        a[t][0] = fma(w1, q.x, a[t][0]);
+        a[t][1] = fma(w1, q.y, a[t][1]);
+        a[t][2] = fma(w1, q.z, a[t][2]);
+        a[t][3] = fma(c, q.x, a[t][3]);
+        a[t][4] = fma(c, q.y, a[t][4]);
+        a[t][5] = fma(c, q.z, a[t][5]);
+        a[t][6] = fma(r, w.x, a[t][6]);
+        a[t][7] = fma(r, w.y, a[t][7]);
+        a[t][8] = fma(r, w.z, a[t][8]);
+        a[t][9] = fma(sji, r, a[t][9]);
+      }
     }
   }
-  if (i < P.n) {
-    const size_t n = (size_t)P.n;
-    double* out = P.partial + (size_t)blockIdx.y * 13 * n + i;
+  const size_t n = (size_t)P.n;
 #pragma unroll
-    for (int c = 0; c < 13; ++c) out[c * n] = a[c];
+  for (int t = 0; t < TPT; ++t) {
+    if (row[t] < P.n) {
+      double* out = P.partial + (size_t)blockIdx.y * kRowSums * n + row[t];
+#pragma unroll
+      for (int c = 0; c < kRowSums; ++c) out[c * n] = a[t][c];
+    }
   }
+}
+
+// Row-pass combination: g_x = -(S1 x ut + C + G P)/(4 pi), g_zeta = -A R/(4 pi),
+// from `chunks` partial blocks of kRowSums rows each, added in chunk order.
+__global__ void adj_combine_row_kernel(const double* __restrict__ ut,
+                                       const double* __restrict__ zeta,
+                                       const double* __restrict__ area, int n,
+                                       const double* __restrict__ p, int chunks,
+                                       double* __restrict__ out_x, double* __restrict__ out_z) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t N = (size_t)n, b = 3 * (size_t)i;
+  double s[kRowSums];
+#pragma unroll
+  for (int w = 0; w < kRowSums; ++w) s[w] = 0.0;
+  for (int c = 0; c < chunks; ++c)
+#pragma unroll
+    for (int w = 0; w < kRowSums; ++w) s[w] += p[((size_t)c * kRowSums + w) * N + i];
+  const double u0 = ut[b], u1 = ut[b + 1], u2 = ut[b + 2];
+  const double G = zeta[i] * area[i];
+  const double g0 = (s[1] * u2 - s[2] * u1) + s[3] + G * s[6];
+  const double g1 = (s[2] * u0 - s[0] * u2) + s[4] + G * s[7];
+  const double g2 = (s[0] * u1 - s[1] * u0) + s[5] + G * s[8];
+  out_x[b] = -kInv4Pi * g0;
+  out_x[b + 1] = -kInv4Pi * g1;
+  out_x[b + 2] = -kInv4Pi * g2;
+  out_z[i] = -kInv4Pi * area[i] * s[9];
 }
 
 // v_i = ut_i x x_i with ut_i = mu_x,i + (-2 Omega mu_z,i) z_hat, mu = dt * l_k.
@@ -446,11 +496,19 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
   const size_t col_bytes = (size_t)ftiles * 7 * n * sizeof(double);
   int S, S2, st1 = 6, st2 = 7;
   const double* p2ptr = nullptr;
-  if (mode == 3) {
-    const int tiles = (n + tcb::kRNT - 1) / tcb::kRNT;
+  if (mode >= 3) {
+    // row pass: mode 3 one row per thread, 4 two rows per thread (both full FP64
+    // reciprocals); 5 and 6 the same with one Newton step
+    const int tpt = (mode == 4 || mode == 6) ? 2 : 1;
+    const int newton = mode <= 4 ? 2 : 1;
+    const void* fn = tpt == 1 ? (newton == 2 ? (const void*)tcb::adj_row_kernel<1, 2, 2>
+                                             : (const void*)tcb::adj_row_kernel<1, 1, 2>)
+                              : (newton == 2 ? (const void*)tcb::adj_row_kernel<2, 2, 1>
+                                             : (const void*)tcb::adj_row_kernel<2, 1, 1>);
+    const int rows_per_cta = tcb::kRNT * tpt;
+    const int tiles = (n + rows_per_cta - 1) / rows_per_cta;
     int per_sm = 0;
-    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tcb::adj_row_kernel,
-                                                              tcb::kRNT, 0));
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tcb::kRNT, 0));
     const int slots = std::max(1, per_sm) * ctx->num_sms;
     // whole waves: the chunk count that best fills tiles x chunks into the resident slots
     S = 1;
@@ -467,17 +525,26 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
     int chunk = (n + S - 1) / S;
     chunk = (chunk + tcb::kRTS - 1) / tcb::kRTS * tcb::kRTS;
     S = (n + chunk - 1) / chunk;
-    S2 = S;
-    st1 = st2 = 13;
-    if ((rc = W.p1.ensure((size_t)S * 13 * n * sizeof(double)))) return rc;
+    if ((rc = W.p1.ensure((size_t)S * tcb::kRowSums * n * sizeof(double)))) return rc;
     tcb::AdjLaunch R{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), W.vrow.as<double4>(), n,
                      chunk, 1.0 + d * d, W.p1.as<double>()};
-    tcb::adj_row_kernel<<<dim3(tiles, S), tcb::kRNT, 0, ctx->stream>>>(R);
+    const dim3 grid(tiles, S);
+    if (tpt == 1 && newton == 2)
+      tcb::adj_row_kernel<1, 2, 2><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
+    else if (tpt == 1)
+      tcb::adj_row_kernel<1, 1, 2><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
+    else if (newton == 2)
+      tcb::adj_row_kernel<2, 2, 1><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
+    else
+      tcb::adj_row_kernel<2, 1, 1><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
     TC_CUDA_TRY(cudaGetLastError());
-    p2ptr = W.p1.as<double>() + 6 * (size_t)n;
-    ctx->launches += 1;
+    tcb::adj_combine_row_kernel<<<blocks, threads, 0, ctx->stream>>>(
+        W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, out, out + 3 * (size_t)n);
+    TC_CUDA_TRY(cudaGetLastError());
+    ctx->launches += 3;
     ctx->pair_launches += 1;
     ctx->pair_interactions += (long long)n * (long long)(n - 1);
+    return TC_OK;
   } else if (mode != 0 && col_bytes <= (size_t(16) << 30)) {
     // fused pass: rows and columns from one visit of each pair
     const int slots = 2 * ctx->num_sms;

@@ -76,13 +76,13 @@ int velocity_device(tc_ctx* ctx, int cls, const double* X, int m, const double* 
   int rc = ctx->scratch[0].ensure((size_t)std::max(n, 1) * sizeof(double4));
   if (rc) return rc;
   double4* src = ctx->scratch[0].as<double4>();
-  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
   int* perm = nullptr;
   if (ctx->precision == TC_FP32C && ctx->target_order == TC_ORDER_HILBERT && i1 > i0) {
     if ((rc = ctx->scratch[4].ensure((size_t)m * sizeof(int)))) return rc;
     perm = ctx->scratch[4].as<int>();
     if ((rc = tcb::compute_order(ctx, X, i0, i1, perm))) return rc;
   }
+  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
   SegDesc seg{X, perm, i0, i1, 0, cls == TC_ACTIVE ? 0 : tcb::kNoSelf,
               ctx->delta[cls] * ctx->delta[cls]};
   int nch = 0;
@@ -193,7 +193,7 @@ extern "C" int tc_get_smooth(tc_ctx* ctx, double* smooth) {
 }
 
 extern "C" int tc_set_adjoint_mode(tc_ctx* ctx, int mode) {
-  if (!ctx || mode < 0 || mode > 3) return TC_ERR_ARG;
+  if (!ctx || mode < 0 || mode > 6) return TC_ERR_ARG;
   ctx->adj_mode = mode;
   return TC_OK;
 }
@@ -435,6 +435,7 @@ extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
   if (nQ) TC_CUDA_TRY(cudaMemcpyAsync(R.x0Q.ptr, xQ, 3 * (size_t)nQ * D, kind, s));
   R.ready = true;
   R.ordered = false;
+  R.strat = false;
   return TC_OK;
 }
 
@@ -509,7 +510,9 @@ extern "C" int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int
   int nch = 0;
   const int n_out = R.nA + R.nV + R.nQ;
   if ((rc = tcb::launch_pairs(ctx, segs, 3, R.src.as<double4>(), R.nA, n_out, &nch))) return rc;
-  return tcb::launch_stage_epilogue(ctx, stage, dt, range, nch, total_ke_device);
+  if ((rc = tcb::launch_stage_epilogue(ctx, stage, dt, range, nch, total_ke_device))) return rc;
+  if (stage == 3 && R.strat) ++R.step;
+  return TC_OK;
 }
 
 // Packs the sources of stage 1 from the loaded state (x0A, z0, areaA).
@@ -518,6 +521,7 @@ extern "C" int tc_rk4_pack_sources(tc_ctx* ctx) {
   if (rc) return rc;
   tcb::Rk4State& R = ctx->rk;
   if (!R.ready) return TC_ERR_STATE;
+  if (R.strat) return tcb::launch_pack_strat(ctx, R.t0 + (double)R.step * R.strat_dt);
   return tcb::launch_pack(ctx, R.x0A.as<double>(), R.z0.as<double>(), R.areaA.as<double>(), R.nA,
                           R.src.as<double4>());
 }
@@ -615,6 +619,53 @@ extern "C" int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const 
   return tc_rk4_store(ctx, xA, zetaA, xV, xQ, kineticEnergy, 1);
 }
 
+// StratosphereRK4 (PanelVelocityParallel.f90:661-919) on host arrays: nsteps
+// forced steps from time t, fused on the device like tc_rk4_step. Each stage's
+// source vorticity is absVortA - 2 Omega z - F(x, t_stage) (Juckes forcing F);
+// on return relVortA / relVortV (nullable) hold absVort - 2 Omega z - F(x, T),
+// T = t + nsteps dt, at the new positions (:908-915), and totalKE[nsteps] the
+// stage-1 kinetic energy of each step.
+extern "C" int tc_strat_rk4_step(tc_ctx* ctx, double* xA, const double* absVortA,
+                                 double* relVortA, const double* areaA, int nA, double* xV,
+                                 const double* absVortV, double* relVortV, int nV, double* xQ,
+                                 int nQ, double t, double dt, int nsteps, double* totalKE,
+                                 double* kineticEnergy) {
+  if (!ctx || nsteps < 0 || !std::isfinite(t) || !std::isfinite(dt) || (nA && !absVortA) ||
+      (relVortV && nV && !absVortV)) {
+    tc_record_error("tc_strat_rk4_step: bad arguments");
+    return TC_ERR_ARG;
+  }
+  int rc = check_finite_host(absVortA, (size_t)nA, "absVortA");
+  if (rc || (absVortV && (rc = check_finite_host(absVortV, (size_t)nV, "absVortV")))) return rc;
+  if ((rc = tc_rk4_load(ctx, xA, absVortA, areaA, nA, xV, nV, xQ, nQ, 0))) return rc;
+  tcb::Rk4State& R = ctx->rk;
+  const size_t D = sizeof(double);
+  if ((rc = R.absA.ensure((size_t)std::max(nA, 1) * D)) ||
+      (rc = R.absV.ensure((size_t)std::max(nV, 1) * D)))
+    return rc;
+  if (nA) TC_CUDA_TRY(cudaMemcpyAsync(R.absA.ptr, absVortA, nA * D, cudaMemcpyHostToDevice, ctx->stream));
+  if (nV && absVortV)
+    TC_CUDA_TRY(cudaMemcpyAsync(R.absV.ptr, absVortV, nV * D, cudaMemcpyHostToDevice, ctx->stream));
+  R.strat = true;
+  R.t0 = t;
+  R.step = 0;
+  R.strat_dt = dt;
+  // (advance packs the stage-1 sources first, which also sets relVortA at t)
+  if ((rc = tc_rk4_advance(ctx, dt, nsteps, totalKE))) return rc;
+  if ((rc = tc_rk4_store(ctx, xA, relVortA, xV, xQ, kineticEnergy, 0))) return rc;
+  if (relVortV && nV) {
+    tcb::DevBuf out;
+    if ((rc = out.ensure(nV * D))) return rc;
+    if ((rc = tcb::launch_strat_rel_vort(ctx, R.absV.as<double>(), R.x0V.as<double>(), nV,
+                                         R.t0 + (double)R.step * dt, out.as<double>())))
+      return rc;
+    TC_CUDA_TRY(cudaMemcpyAsync(relVortV, out.ptr, nV * D, cudaMemcpyDeviceToHost, ctx->stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  if ((rc = check_finite_host(xA, 3 * (size_t)nA, "xA (result)"))) return rc;
+  return relVortA ? check_finite_host(relVortA, (size_t)nA, "relVortA (result)") : TC_OK;
+}
+
 // Pair-kernel variants (the launch shapes the autotuner searches).
 extern "C" int tc_pair_variant_count(int precision, int* count) {
   if (!count || (precision != TC_FP64 && precision != TC_FP32C)) return TC_ERR_ARG;
@@ -622,11 +673,11 @@ extern "C" int tc_pair_variant_count(int precision, int* count) {
   return TC_OK;
 }
 
-extern "C" int tc_pair_variant_info(int precision, int id, int* info7) {
+extern "C" int tc_pair_variant_info(int precision, int id, int* info8) {
   const tcb::PairVariant* v = tcb::variant(precision, id);
-  if (!v || !info7) return TC_ERR_ARG;
-  int vals[7] = {v->nt, v->tpt, v->ts, v->flush, v->minb, v->unroll, v->nt * v->tpt};
-  for (int j = 0; j < 7; ++j) info7[j] = vals[j];
+  if (!v || !info8) return TC_ERR_ARG;
+  int vals[8] = {v->nt, v->tpt, v->ts, v->flush, v->minb, v->unroll, v->nt * v->tpt, v->form};
+  for (int j = 0; j < 8; ++j) info8[j] = vals[j];
   return TC_OK;
 }
 

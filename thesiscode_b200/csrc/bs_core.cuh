@@ -211,106 +211,235 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // ---------------------------------------------------------------------------
 constexpr float kSelfBias = 1e-30f;
 
+// Far-field form (FM bit 0). For a source tile whose every source lies
+// farther than kFarRatio times the CTA's target radius rho (the largest
+// |t_i| of the CTA) from the origin, the denominator is expanded as
+//     D/2 = A_k + B_i + s_k.nt_i,   A_k = (|s_k|^2 + e_k)/2,
+//     B_i = (|t_i|^2 + e_i)/2,      nt_i = -t_i
+// (A_k and B_i from FP64, rounded once), and the sum as
+//     sum w (s_k - t_i) = sum w s_k + nt_i sum w,
+// so the three offset subtractions leave the pair loop: 9 FP32 operations
+// per pair instead of 11. With |s| > 3 rho, D >= (|s| - rho)^2 >= 4|s|^2/9,
+// so each rounding of the expansion costs at most a few ulps of D, as in the
+// near form; the self pair never qualifies (|s_self| = |t_self| <= rho).
+// Paired reciprocal (FM bit 1): the two targets of an f32x2 lane pair share
+// one MUFU reciprocal q = 1/(D_a D_b): 1/D_a = q D_b, 1/D_b = q D_a.
+constexpr float kFarRatio2 = 9.0f;  // kFarRatio = 3
+
+template <bool PR>
+__device__ __forceinline__ float2 rcp_pair(float2 D) {
+  if (PR) {
+    const float q = rcp_approx_f32(__fmul_rn(D.x, D.y));
+    return __fmul2_rn(make_float2(q, q), make_float2(D.y, D.x));
+  }
+  return make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
+}
+
+__device__ __forceinline__ float norm2_f32(float a, float b, float c) {
+  return __fmaf_rn(c, c, __fmaf_rn(b, b, __fmul_rn(a, a)));
+}
+
+// min (max) of a non-negative float over the CTA: one warp reduction, one
+// entry per warp in red[]; the caller synchronises before combine_*.
+__device__ __forceinline__ void warp_store_min(float v, unsigned* red) {
+  const unsigned m = __reduce_min_sync(0xffffffffu, __float_as_uint(v));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+}
+__device__ __forceinline__ void warp_store_max(float v, unsigned* red) {
+  const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(v));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+}
+template <int NW>
+__device__ __forceinline__ float combine_min(const unsigned* red) {
+  unsigned m = red[0];
+#pragma unroll
+  for (int w = 1; w < NW; ++w) m = min(m, red[w]);
+  return __uint_as_float(m);
+}
+template <int NW>
+__device__ __forceinline__ float combine_max(const unsigned* red) {
+  unsigned m = red[0];
+#pragma unroll
+  for (int w = 1; w < NW; ++w) m = max(m, red[w]);
+  return __uint_as_float(m);
+}
+
+// Shared memory of one FP32C unit.
+template <int NT, int TS>
+struct Fp32cSmem {
+  float4 a[TS];           // (sx, sx, sy, sy)
+  float4 b[TS];           // (sz, sz, 2G, 2G)
+  float2 e[TS];           // near form: (e_k, e_k)
+  float2 h[TS];           // far form: (A_k, A_k)
+  unsigned tmin[NT / 32]; // per-warp min of |s_k|^2 over the tile
+  unsigned rho[NT / 32];  // per-warp max of |t_i|^2 over the CTA's targets
+};
+
 // One work unit (targets at visiting positions [tile0, min(tile0 + NT*2*NPAIR,
-// i_end)) against sources [c0, c1)); shared memory smA/smB/smC of TS entries.
-template <int NT, int NPAIR, int TS, int FLUSH, int UNROLL>
+// i_end)) against sources [c0, c1)).
+template <int NT, int NPAIR, int TS, int FLUSH, int UNROLL, int FM>
 __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                            int tile0, int i_end, double d2,
                                            const double4* __restrict__ src, int c0, int c1,
-                                           double* __restrict__ out, size_t stride, float4* smA,
-                                           float4* smB, float2* smC) {
+                                           double* __restrict__ out, size_t stride,
+                                           Fp32cSmem<NT, TS>& sm) {
   static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
+  static_assert(NT % 32 == 0, "whole warps");
   constexpr int TPT = 2 * NPAIR;
   constexpr int TB = NT * TPT;
+  constexpr bool FAR = (FM & 1) != 0;
+  constexpr bool PR = (FM & 2) != 0;
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
   const int mid = perm ? perm[mid_pos] : mid_pos;
   const double cx = x[3 * (size_t)mid], cy = x[3 * (size_t)mid + 1], cz = x[3 * (size_t)mid + 2];
 
-  float2 ntx[NPAIR], nty[NPAIR], ntz[NPAIR], ei[NPAIR];
-  float2 fx[NPAIR], fy[NPAIR], fz[NPAIR];
-  double ax[NPAIR][2], ay[NPAIR][2], az[NPAIR][2];
+  float2 ntx[NPAIR], nty[NPAIR], ntz[NPAIR], ei[NPAIR], bh[NPAIR];
+  float2 fx[NPAIR], fy[NPAIR], fz[NPAIR], fw[NPAIR];
+  double ax[NPAIR][2], ay[NPAIR][2], az[NPAIR][2], aw[NPAIR][2];
+  float rho2 = 0.f;
 #pragma unroll
   for (int p = 0; p < NPAIR; ++p) {
-    float tv[2][4];
+    float tv[2][5];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
       int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
       double px = x[3 * (size_t)ld], py = x[3 * (size_t)ld + 1], pz = x[3 * (size_t)ld + 2];
-      tv[h][0] = -(float)(px - cx);
-      tv[h][1] = -(float)(py - cy);
-      tv[h][2] = -(float)(pz - cz);
-      tv[h][3] = (float)((1.0 - (px * px + py * py + pz * pz)) + 2.0 * d2) + kSelfBias;
-      ax[p][h] = ay[p][h] = az[p][h] = 0.0;
+      const float tx = (float)(px - cx), ty = (float)(py - cy), tz = (float)(pz - cz);
+      const double E = (1.0 - (px * px + py * py + pz * pz)) + 2.0 * d2;
+      tv[h][0] = -tx;
+      tv[h][1] = -ty;
+      tv[h][2] = -tz;
+      tv[h][3] = (float)E + kSelfBias;
+      const float t2 = norm2_f32(tx, ty, tz);
+      tv[h][4] = (float)(0.5 * ((double)t2 + E));
+      rho2 = fmaxf(rho2, t2);
+      ax[p][h] = ay[p][h] = az[p][h] = aw[p][h] = 0.0;
     }
     ntx[p] = make_float2(tv[0][0], tv[1][0]);
     nty[p] = make_float2(tv[0][1], tv[1][1]);
     ntz[p] = make_float2(tv[0][2], tv[1][2]);
     ei[p] = make_float2(tv[0][3], tv[1][3]);
-    fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+    bh[p] = make_float2(tv[0][4], tv[1][4]);
+    fx[p] = fy[p] = fz[p] = fw[p] = make_float2(0.f, 0.f);
   }
+  if (FAR) warp_store_max(rho2, sm.rho);
 
   for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
+    float smin = __int_as_float(0x7f800000);  // +inf
     for (int j = threadIdx.x; j < TS; j += NT) {
       int k = ts + j;
-      float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f;
+      float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f, ah = 1.f;
       if (k < c1) {
         const double4 q = src[k];
         sx = (float)(q.x - cx);
         sy = (float)(q.y - cy);
         sz = (float)(q.z - cz);
         g = (float)(2.0 * q.w);
-        e = (float)(1.0 - (q.x * q.x + q.y * q.y + q.z * q.z));
-      }
-      smA[j] = make_float4(sx, sx, sy, sy);
-      smB[j] = make_float4(sz, sz, g, g);
-      smC[j] = make_float2(e, e);
-    }
-    __syncthreads();
-    for (int jf = 0; jf < TS; jf += FLUSH) {
-#pragma unroll UNROLL
-      for (int j = jf; j < jf + FLUSH; ++j) {
-        const float4 a = smA[j];
-        const float4 b = smB[j];
-        const float2 ee = smC[j];
-        const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-        const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
-#pragma unroll
-        for (int p = 0; p < NPAIR; ++p) {
-          const float2 dx = __fadd2_rn(sxx, ntx[p]);
-          const float2 dy = __fadd2_rn(syy, nty[p]);
-          const float2 dz = __fadd2_rn(szz, ntz[p]);
-          float2 D = __fadd2_rn(ee, ei[p]);
-          D = __ffma2_rn(dx, dx, D);
-          D = __ffma2_rn(dy, dy, D);
-          D = __ffma2_rn(dz, dz, D);
-          const float2 r = make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
-          const float2 w = __fmul2_rn(gg, r);
-          fx[p] = __ffma2_rn(w, dx, fx[p]);
-          fy[p] = __ffma2_rn(w, dy, fy[p]);
-          fz[p] = __ffma2_rn(w, dz, fz[p]);
+        const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
+        e = (float)ek;
+        if (FAR) {
+          const float s2 = norm2_f32(sx, sy, sz);
+          ah = (float)(0.5 * ((double)s2 + ek));
+          smin = fminf(smin, s2);
         }
       }
+      sm.a[j] = make_float4(sx, sx, sy, sy);
+      sm.b[j] = make_float4(sz, sz, g, g);
+      sm.e[j] = make_float2(e, e);
+      if (FAR) sm.h[j] = make_float2(ah, ah);
+    }
+    if (FAR) warp_store_min(smin, sm.tmin);
+    __syncthreads();
+    // strict: with rho = 0 (one target position) no tile is far
+    const bool far = FAR && combine_min<NT / 32>(sm.tmin) > kFarRatio2 * combine_max<NT / 32>(sm.rho);
+    if (far) {
+      for (int jf = 0; jf < TS; jf += FLUSH) {
+#pragma unroll UNROLL
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = sm.a[j];
+          const float4 b = sm.b[j];
+          const float2 ah = sm.h[j];
+          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
+          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
 #pragma unroll
-      for (int p = 0; p < NPAIR; ++p) {
-        ax[p][0] += (double)fx[p].x;
-        ax[p][1] += (double)fx[p].y;
-        ay[p][0] += (double)fy[p].x;
-        ay[p][1] += (double)fy[p].y;
-        az[p][0] += (double)fz[p].x;
-        az[p][1] += (double)fz[p].y;
-        fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+          for (int p = 0; p < NPAIR; ++p) {
+            float2 D = __fadd2_rn(ah, bh[p]);
+            D = __ffma2_rn(sxx, ntx[p], D);
+            D = __ffma2_rn(syy, nty[p], D);
+            D = __ffma2_rn(szz, ntz[p], D);
+            const float2 w = __fmul2_rn(gg, rcp_pair<PR>(D));  // 2 w: D/2 above
+            fx[p] = __ffma2_rn(w, sxx, fx[p]);
+            fy[p] = __ffma2_rn(w, syy, fy[p]);
+            fz[p] = __ffma2_rn(w, szz, fz[p]);
+            fw[p] = __fadd2_rn(fw[p], w);
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < NPAIR; ++p) {
+          ax[p][0] = fma(0.5, (double)fx[p].x, ax[p][0]);
+          ax[p][1] = fma(0.5, (double)fx[p].y, ax[p][1]);
+          ay[p][0] = fma(0.5, (double)fy[p].x, ay[p][0]);
+          ay[p][1] = fma(0.5, (double)fy[p].y, ay[p][1]);
+          az[p][0] = fma(0.5, (double)fz[p].x, az[p][0]);
+          az[p][1] = fma(0.5, (double)fz[p].y, az[p][1]);
+          aw[p][0] = fma(0.5, (double)fw[p].x, aw[p][0]);
+          aw[p][1] = fma(0.5, (double)fw[p].y, aw[p][1]);
+          fx[p] = fy[p] = fz[p] = fw[p] = make_float2(0.f, 0.f);
+        }
+      }
+    } else {
+      for (int jf = 0; jf < TS; jf += FLUSH) {
+#pragma unroll UNROLL
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = sm.a[j];
+          const float4 b = sm.b[j];
+          const float2 ee = sm.e[j];
+          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
+          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
+#pragma unroll
+          for (int p = 0; p < NPAIR; ++p) {
+            const float2 dx = __fadd2_rn(sxx, ntx[p]);
+            const float2 dy = __fadd2_rn(syy, nty[p]);
+            const float2 dz = __fadd2_rn(szz, ntz[p]);
+            float2 D = __fadd2_rn(ee, ei[p]);
+            D = __ffma2_rn(dx, dx, D);
+            D = __ffma2_rn(dy, dy, D);
+            D = __ffma2_rn(dz, dz, D);
+            const float2 w = __fmul2_rn(gg, rcp_pair<PR>(D));
+            fx[p] = __ffma2_rn(w, dx, fx[p]);
+            fy[p] = __ffma2_rn(w, dy, fy[p]);
+            fz[p] = __ffma2_rn(w, dz, fz[p]);
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < NPAIR; ++p) {
+          ax[p][0] += (double)fx[p].x;
+          ax[p][1] += (double)fx[p].y;
+          ay[p][0] += (double)fy[p].x;
+          ay[p][1] += (double)fy[p].y;
+          az[p][0] += (double)fz[p].x;
+          az[p][1] += (double)fz[p].y;
+          fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+        }
       }
     }
   }
-  // partial rows are indexed by position in the visiting order
+  // far tiles: + nt_i sum w; partial rows are indexed by position in the visiting order
 #pragma unroll
   for (int p = 0; p < NPAIR; ++p) {
+    const float ntxs[2] = {ntx[p].x, ntx[p].y}, ntys[2] = {nty[p].x, nty[p].y},
+                ntzs[2] = {ntz[p].x, ntz[p].y};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
+      if (FAR) {
+        ax[p][h] = fma((double)ntxs[h], aw[p][h], ax[p][h]);
+        ay[p][h] = fma((double)ntys[h], aw[p][h], ay[p][h]);
+        az[p][h] = fma((double)ntzs[h], aw[p][h], az[p][h]);
+      }
       if (pos < i_end) {
         out[pos] = ax[p][h];
         out[stride + pos] = ay[p][h];
@@ -321,19 +450,17 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 }
 
 
-template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
+template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
-  __shared__ float4 smA[TS];  // (sx, sx, sy, sy)
-  __shared__ float4 smB[TS];  // (sz, sz, 2G, 2G)
-  __shared__ float2 smC[TS];  // (e, e)
+  __shared__ Fp32cSmem<NT, TS> sm;
   const TargetSeg& G = find_seg(P, blockIdx.x);
   const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * 2 * NPAIR);
   const int c0 = (int)blockIdx.y * P.chunk_len;
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-  fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
-                                           stride, smA, smB, smC);
+  fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
+                                               stride, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -376,18 +503,16 @@ __device__ __forceinline__ int next_item(int* counter, int* slot) {
   return *slot;
 }
 
-template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL>
+template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
-  __shared__ float4 smA[TS];
-  __shared__ float4 smB[TS];
-  __shared__ float2 smC[TS];
+  __shared__ Fp32cSmem<NT, TS> sm;
   __shared__ int slot;
   for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
     const BatchItem I = B.items[it];
     const BatchSeg S = B.segs[I.seg];
     double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1,
-                                             out, B.stride, smA, smB, smC);
+    fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0,
+                                                 I.c1, out, B.stride, sm);
   }
 }
 

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "strat.cuh"
 #include "tc_ctx.h"
 
 namespace tcb {
@@ -48,27 +49,27 @@ template <int NT, int TPT, int MINB, bool FUSED>
 void launch64b(int g, cudaStream_t s, const BatchLaunch& B) {
   pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(B);
 }
-template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL>
+template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL, int FM>
 void launch32b(int g, cudaStream_t s, const BatchLaunch& B) {
-  pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(B);
+  pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(B);
 }
 
-template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL>
+template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL, int FM>
 void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
-  pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL><<<g, NT, 0, s>>>(P);
+  pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(P);
 }
 
 #define V64(NT, TPT, MINB, FUSED)                                                 \
   PairVariant { TC_FP64, NT, TPT, kTS, FUSED, MINB, 0, launch64<NT, TPT, MINB, FUSED>, \
                 (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED>,               \
                 launch64b<NT, TPT, MINB, FUSED>,                                         \
-                (const void*)pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED> }
-#define V32(NT, NPAIR, FLUSH, MINB, UNROLL)                                              \
-  PairVariant { TC_FP32C, NT, 2 * NPAIR, kTS, FLUSH, MINB, UNROLL,                        \
-                launch32<NT, NPAIR, FLUSH, MINB, UNROLL>,                                 \
-                (const void*)pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL>,      \
-                launch32b<NT, NPAIR, FLUSH, MINB, UNROLL>,                                \
-                (const void*)pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL> }
+                (const void*)pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED>, 0 }
+#define V32(NT, NPAIR, FLUSH, MINB, UNROLL, FM)                                             \
+  PairVariant { TC_FP32C, NT, 2 * NPAIR, kTS, FLUSH, MINB, UNROLL,                           \
+                launch32<NT, NPAIR, FLUSH, MINB, UNROLL, FM>,                                \
+                (const void*)pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM>,     \
+                launch32b<NT, NPAIR, FLUSH, MINB, UNROLL, FM>,                               \
+                (const void*)pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM>, FM }
 
 // FP64: the `flush` field records the denominator mode (1 = fused, 0 =
 // rounded exactly like the reference).
@@ -76,9 +77,15 @@ const PairVariant kVariants64[] = {
     V64(256, 2, 5, true),  V64(256, 4, 2, true),  V64(256, 1, 6, true), V64(128, 4, 4, true),
     V64(256, 2, 5, false), V64(256, 4, 2, false),
 };
+// FP32C: the last field selects the far-field form (1), the paired
+// reciprocal (2), or both (3).
 const PairVariant kVariants32[] = {
-    V32(256, 2, 32, 3, 4), V32(256, 2, 64, 2, 4), V32(128, 1, 32, 8, 8), V32(256, 2, 16, 2, 4),
-    V32(128, 2, 32, 6, 4), V32(256, 1, 32, 4, 8),
+    V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
+    V32(256, 2, 16, 2, 4, 0), V32(128, 2, 32, 6, 4, 0), V32(256, 1, 32, 4, 8, 0),
+    V32(128, 2, 32, 5, 4, 1), V32(128, 2, 32, 5, 4, 3), V32(256, 2, 32, 2, 4, 1),
+    V32(256, 2, 32, 2, 4, 3), V32(128, 1, 32, 8, 8, 1), V32(128, 1, 32, 8, 8, 3),
+    V32(128, 2, 32, 6, 4, 2), V32(128, 2, 32, 4, 4, 1), V32(128, 2, 32, 4, 4, 3),
+    V32(128, 1, 32, 6, 8, 1), V32(128, 1, 32, 8, 16, 1), V32(256, 1, 32, 4, 8, 1),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
@@ -211,6 +218,49 @@ __global__ void pack_kernel(const double* __restrict__ x, const double* __restri
                         __dmul_rn(zeta[k], area[k]));
 }
 
+// Forced model: stage-1 sources from the absolute vorticity at time t; the
+// relative vorticity is also written to z0 (it is the state's zeta at t).
+__global__ void pack_strat_kernel(const double* __restrict__ x, const double* __restrict__ absv,
+                                  const double* __restrict__ area, int n, double two_omega,
+                                  double t, double* __restrict__ zeta, double4* __restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double px = x[3 * (size_t)k], py = x[3 * (size_t)k + 1], pz = x[3 * (size_t)k + 2];
+  const double z = strat_rel_vort(absv[k], two_omega, px, py, pz, t);
+  zeta[k] = z;
+  out[k] = make_double4(px, py, pz, __dmul_rn(z, area[k]));
+}
+
+__global__ void strat_rel_vort_kernel(const double* __restrict__ absv,
+                                      const double* __restrict__ x, int n, double two_omega,
+                                      double t, double* __restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[k] = strat_rel_vort(absv[k], two_omega, x[3 * (size_t)k], x[3 * (size_t)k + 1],
+                          x[3 * (size_t)k + 2], t);
+}
+
+int launch_pack_strat(tc_ctx* ctx, double t) {
+  Rk4State& R = ctx->rk;
+  if (R.nA <= 0) return TC_OK;
+  pack_strat_kernel<<<(R.nA + 255) / 256, 256, 0, ctx->stream>>>(
+      R.x0A.as<double>(), R.absA.as<double>(), R.areaA.as<double>(), R.nA, 2.0 * ctx->omega, t,
+      R.z0.as<double>(), R.src.as<double4>());
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  return TC_OK;
+}
+
+int launch_strat_rel_vort(tc_ctx* ctx, const double* abs_vort, const double* x, int n, double t,
+                          double* out) {
+  if (n <= 0) return TC_OK;
+  strat_rel_vort_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(abs_vort, x, n,
+                                                                  2.0 * ctx->omega, t, out);
+  TC_CUDA_TRY(cudaGetLastError());
+  ctx->launches += 1;
+  return TC_OK;
+}
+
 int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* area, int n,
                 double4* out) {
   if (n <= 0) return TC_OK;
@@ -303,6 +353,8 @@ struct StageEpi {
   double* keBlocks;
   const int *permA, *permV, *permQ;  // visiting orders of the three ranges (null: as stored)
   const int* row_nchunks;            // batched runs: chunks of each partial row (null: nchunks)
+  const double* absA;                // forced model: absolute vorticity (null: BVE)
+  double two_omega, t_next;          // forced model: 2 Omega, time of the next stage input
 };
 
 constexpr int kEpiThreads = 256;
@@ -359,7 +411,17 @@ __global__ void __launch_bounds__(kEpiThreads) stage_epilogue_kernel(const Stage
         xnext[c] = nv;
       }
     }
-    if (cls == 0) {
+    if (cls == 0 && E.absA) {
+      // forced model (PanelVelocityParallel.f90:752-755, :800-803, :847-850, :908-911): the
+      // vorticity is not integrated; the next input is rebuilt from absVort at t_next
+      const double znext =
+          strat_rel_vort(E.absA[i], E.two_omega, xnext[0], xnext[1], xnext[2], E.t_next);
+      if (E.stage < 3)
+        E.ziA[i] = znext;
+      else
+        E.z0[i] = znext;
+      E.src[i] = make_double4(xnext[0], xnext[1], xnext[2], znext * E.areaA[i]);
+    } else if (cls == 0) {
       double kz = __dmul_rn(E.dt, __dmul_rn(E.m2omega, u[2]));
       double zbase = E.stage == 0 ? E.z0[i] : E.newZ[i];
       double zn = zbase + kz / div;
@@ -440,6 +502,12 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
   E.permA = ordered ? R.permA.as<int>() : nullptr;
   E.permV = ordered ? R.permV.as<int>() : nullptr;
   E.permQ = ordered ? R.permQ.as<int>() : nullptr;
+  E.absA = R.strat ? R.absA.as<double>() : nullptr;
+  E.two_omega = 2.0 * ctx->omega;
+  // stage inputs at t, t + dt/2, t + dt/2, t + dt; after stage 4 the next step's t
+  const double t_step = R.t0 + (double)R.step * dt;
+  E.t_next = stage < 2 ? t_step + 0.5 * dt
+                       : (stage == 2 ? t_step + dt : R.t0 + (double)(R.step + 1) * dt);
   const int rows = (E.a1 - E.a0) + (E.v1 - E.v0) + (E.q1 - E.q0);
   const int blocks = std::max(1, (rows + kEpiThreads - 1) / kEpiThreads);
   if (stage == 0) {

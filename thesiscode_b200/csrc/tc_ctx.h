@@ -42,6 +42,7 @@ struct PairVariant {
   const void* fn;
   void (*launch_batch)(int grid, cudaStream_t stream, const BatchLaunch& B);
   const void* fn_batch;
+  int form;  // FP32C: bit 0 far-field form, bit 1 paired reciprocal; FP64: 0
 };
 
 // Target segment as the host describes it before tiles are assigned.
@@ -70,6 +71,12 @@ struct Rk4State {
   DevBuf permA, permV, permQ;           // FP32C visiting orders (Hilbert), per class
   bool ordered = false;                 // perm* hold orders of the current stage ranges
   int order_range[6] = {0, 0, 0, 0, 0, 0};
+  // forced (stratosphere) model: source vorticity rebuilt each stage from absA
+  bool strat = false;
+  DevBuf absA, absV;                    // absolute vorticity of panels and vertices
+  double t0 = 0.0;                      // time at the start of step 0
+  double strat_dt = 0.0;                // step length of the forced run
+  long long step = 0;                   // steps completed since t0
 };
 
 }  // namespace tcb
@@ -87,10 +94,10 @@ struct tc_ctx {
   double delta[3] = {0.0, 0.0, 0.05};               // ACTIVE, VERTEX, PASSIVE (smooth, :27)
   tcb::PairCfg cfg64{256, 2, 256};
   tcb::PairCfg cfg32{256, 4, 256};
-  int var64 = 2, var32 = 4;  // pair-kernel variants in use (see kVariants64/32)
+  int var64 = 2, var32 = 15;  // pair-kernel variants in use (see kVariants64/32)
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
-  int adj_mode = 3;  // adjoint VJP: 3 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
+  int adj_mode = 5;  // adjoint VJP: 3-6 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
   tcb::DevBuf order_buf[4];             // keys, sorted keys, indices, sort scratch
   int min_chunk = 4096;   // smallest source chunk a CTA walks
   int max_chunks = 64;
@@ -115,6 +122,9 @@ namespace tcb {
 int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
                  int n_out, int* nchunks);
 // Pack {x, y, z, zeta*area} for n sources.
+int launch_pack_strat(tc_ctx* ctx, double t);
+int launch_strat_rel_vort(tc_ctx* ctx, const double* abs_vort, const double* x, int n, double t,
+                          double* out);
 int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* area, int n,
                 double4* out);
 // dX (3*m) and dVort (m, nullable) for rows [i0, i1), zero elsewhere; partial

@@ -90,6 +90,15 @@ def jet_reference(x, theta0=PI / 4.0, beta=12.0, perturb_amp=0.025, perturb_wave
     return 300.0 * np.sin(lat - theta_p) * np.exp(-2.0 * beta * beta * (1.0 - np.cos(lat - theta_p)))
 
 
+def stratosphere_rel_vort(x, beta=1.5, th0=15.0 * PI / 32.0):
+    """StratosphereRelVortX (TracerAndVorticityDistributions.f90:1203-1211): the polar-vortex
+    relative vorticity of the forced stratosphere model (before the Gauss constant is removed)."""
+    lat = latitude(x)
+    return -PI * (np.cos(lat) * (-2.0 * beta * beta * (np.cos(th0) * np.sin(lat) - np.sin(th0) * np.cos(lat)))
+                  - np.sin(lat)) * np.exp(-2.0 * beta * beta * (1.0 - np.cos(th0) * np.cos(lat)
+                                                                 - np.sin(th0) * np.sin(lat)))
+
+
 def solid_body(x, rotation_rate):
     """InitSolidBody / SolidBodyX (TracerAndVorticityDistributions.f90:1246-1268): 2 w z.
     With Omega = 0 the exact velocity is u = w z_hat x x (solidBody.f90:296-300)."""

@@ -123,6 +123,24 @@ class Context:
                N.dptr(tke), N.dptr(ke))
         return tke[:nsteps], ke
 
+    def strat_rk4_step(self, xA, absVortA, areaA, xV, xQ, t: float, dt: float, nsteps: int = 1,
+                       absVortV=None):
+        """nsteps forced (stratosphere) RK4 steps from time t on host arrays (positions updated in
+        place). Returns (relVortA, relVortV or None, totalKE per step, kineticEnergy)."""
+        for a in (xA, areaA, xV, xQ):
+            if not (a.dtype == np.float64 and a.flags.c_contiguous):
+                raise TypeError("RK4 arrays must be C-contiguous float64")
+        absA = np.ascontiguousarray(absVortA, dtype=np.float64)
+        absV = None if absVortV is None else np.ascontiguousarray(absVortV, dtype=np.float64)
+        relA = np.zeros(xA.shape[0])
+        relV = None if absV is None else np.zeros(xV.shape[0])
+        tke = np.zeros(max(nsteps, 1))
+        ke = np.zeros(xA.shape[0])
+        N.call("tc_strat_rk4_step", self.handle, N.dptr(xA), N.dptr(absA), N.dptr(relA), N.dptr(areaA),
+               xA.shape[0], N.dptr(xV), N.dptr(absV), N.dptr(relV), xV.shape[0], N.dptr(xQ), xQ.shape[0],
+               float(t), float(dt), int(nsteps), N.dptr(tke), N.dptr(ke))
+        return relA, relV, tke[:nsteps], ke
+
     def reset_rk4(self) -> None:
         N.call("tc_reset_rk4", self.handle)
 
@@ -206,6 +224,29 @@ class PanelVelocity:
         scatter_panels(aPanels, maps, xA, zA, xQ)
 
 
+    def StratosphereRK4(self, aParticles: Particles, aPanels: Panels, t: float, dt: float,
+                        procRank: int = 0, numProcs: int = 1) -> None:
+        """One forced RK4 step from time t (PanelVelocityParallel.f90:661-919): positions advance,
+        the relative vorticity of panels and particles is rebuilt from absVort, the rotation and
+        the Juckes forcing at t + dt (:908-915)."""
+        if numProcs != 1:
+            raise ValueError("PanelVelocity runs one rank")
+        if self._maps is None:
+            self._maps = gather_panels(aPanels)[0]
+        maps, xA, _, aA, xQ = gather_panels(aPanels, self._maps)
+        absA = np.ascontiguousarray(aPanels.absVort[maps.active])
+        xV = np.ascontiguousarray(aParticles.x)
+        relA, relV, tke, ke = self.ctx.strat_rk4_step(xA, absA, aA, xV, xQ, t, dt, 1,
+                                                      absVortV=aParticles.absVort)
+        self.totalKE = float(tke[0])
+        self.kineticEnergy = ke
+        aParticles.x[:] = xV
+        aParticles.relVort[:] = relV
+        if aPanels.tracer.shape[1] >= 2:
+            aPanels.tracer[maps.active, 1] = ke
+        scatter_panels(aPanels, maps, xA, relA, xQ)
+
+
 _default: PanelVelocity | None = None
 
 
@@ -218,6 +259,10 @@ def _state() -> PanelVelocity:
 
 def BVERK4(aParticles, aPanels, dt, procRank=0, numProcs=1):
     _state().BVERK4(aParticles, aPanels, dt, procRank, numProcs)
+
+
+def StratosphereRK4(aParticles, aPanels, t, dt, procRank=0, numProcs=1):
+    _state().StratosphereRK4(aParticles, aPanels, t, dt, procRank, numProcs)
 
 
 def InitializeMPIRK4(aParticles, aPanels, procRank=0, numProcs=1):
