@@ -146,6 +146,8 @@ def _worker(rank, world, port, out_dir, mode):
         if mode == "fail" and rank == 1:
             raise RuntimeError("injected failure on rank 1 before its first collective")
         w = configs.rh4(level=2, parity=True, dt=0.01)
+        if mode == "short" and rank == 1:  # a rank whose active-panel arrays lost their last rows
+            w.xA, w.zetaA, w.areaA = w.xA[:-7], w.zetaA[:-7], w.areaA[:-7]
         drv = DistributedPanelVelocity(backend=OracleBackend())
         drv.load(w)
         drv.advance(w.dt, 2)
@@ -155,7 +157,7 @@ def _worker(rank, world, port, out_dir, mode):
         Path(out_dir, f"rank{rank}.err").write_text(f"{type(e).__name__}: {e}\n{traceback.format_exc()}")
     finally:
         try:
-            if mode != "fail":
+            if mode == "ok" or mode == "short":
                 dist.destroy_process_group()
         except Exception:
             pass
@@ -205,3 +207,11 @@ def test_failed_rank_surfaces_as_error_not_hang(tmp_path, native_built):
     assert "injected failure" in e1
     e0 = tmp_path / "rank0.err"
     assert e0.exists(), "rank 0 finished although its peer never joined the collective"
+
+
+def test_short_buffer_on_one_rank_is_an_error_on_every_rank(tmp_path, native_built):
+    _spawn("short", tmp_path)
+    for r in range(2):
+        e = tmp_path / f"rank{r}.err"
+        assert e.exists(), f"rank {r} ran on with mismatched sizes"
+        assert "ranks disagree on (nA, nV, nQ)" in e.read_text()

@@ -136,7 +136,16 @@ class DistributedPanelVelocity:
         return float(t.item())
 
     def load(self, w) -> None:
-        """Every rank loads the full state (replicated data, as in the reference)."""
+        """Every rank loads the full state (replicated data, as in the reference). The ranks
+        first agree on the sizes: a rank whose arrays are short (or long) makes every rank raise
+        ValueError here, before any stage exchange could wait on mismatched messages."""
+        sizes = self.backend.empty(1, 3)
+        sizes[0, 0], sizes[0, 1], sizes[0, 2] = float(w.nA), float(w.nV), float(w.nQ)
+        seen = [self.backend.empty(1, 3) for _ in range(self.world)]
+        self.dist.all_gather(seen, sizes, group=self.group)
+        got = [tuple(int(v) for v in t.reshape(-1).tolist()) for t in seen]
+        if any(g != got[0] for g in got):
+            raise ValueError(f"ranks disagree on (nA, nV, nQ): {got}")
         self.w = w
         self.nA, self.nV, self.nQ = w.nA, w.nV, w.nQ
         self.ranges = Ranges(load_balance(w.nA, self.world), load_balance(w.nV, self.world),
