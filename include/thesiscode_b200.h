@@ -185,6 +185,12 @@ int tc_rk4_step(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int
 int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int nA,
                        double* xV, int nV, double* xQ, int nQ, double dt, int nsteps,
                        double* totalKE, double* kineticEnergy);
+/* tc_rk4_advance replays steps 1..nsteps-1 from a CUDA graph (captured once
+ * per shape, step, parameters and buffer addresses) when a step is small
+ * enough for launch overhead to matter: mode 0 never, 1 (default) when a step
+ * has at most 4.1e10 interactions (level 6) and nsteps >= 3, 2 always (nsteps
+ * >= 3). Results are bitwise those of the launch-by-launch path. */
+int tc_set_rk4_graphs(tc_ctx* ctx, int mode);
 /* StratosphereRK4 (PanelVelocityParallel.f90:661-919): nsteps forced RK4
  * steps from time t. Positions of the three classes advance like tc_rk4_step;
  * the active vorticity is not integrated: each stage's source vorticity is

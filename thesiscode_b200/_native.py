@@ -84,6 +84,7 @@ SIGNATURES: dict[str, tuple] = {
     "tc_bs_velocity_soa_device": (c_int, [c_void_p] + [c_void_p] * 5 + [c_int] * 3 + [c_void_p] * 4),
     "tc_rk4_soa_step": (c_int, [c_void_p, dp, dp, dp, dp, dp, c_int, c_double, c_int, dp, dp]),
     "tc_rk4_step": (c_int, [c_void_p, dp, dp, dp, c_int, dp, c_int, dp, c_int, c_double, c_int, dp, dp]),
+    "tc_set_rk4_graphs": (c_int, [c_void_p, c_int]),
     "tc_strat_rk4_step": (c_int, [c_void_p, dp, dp, dp, dp, c_int, dp, dp, dp, c_int, dp, c_int,
                                   c_double, c_double, c_int, dp, dp]),
     "tc_rk4_step_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,

@@ -1,6 +1,7 @@
 // C ABI of libthesiscode_b200: context, parameters, the one-call velocity
 // sums and the device-resident RK4 driver.
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -133,6 +134,7 @@ extern "C" int tc_destroy(tc_ctx* ctx) {
   for (DevBuf* b : bufs) b->release();
   for (auto& b : ctx->order_buf) b.release();
   tc_batch_free(ctx);
+  tc_advance_graph_free(ctx);
   for (cudaEvent_t e : ctx->pair_events) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -573,6 +575,130 @@ extern "C" int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, voi
   return TC_OK;
 }
 
+// Launch-bound small problems: steps 1..nsteps-1 of tc_rk4_advance are
+// captured once into a CUDA graph (after step 0 has sized every buffer) and
+// replayed as one launch while the shape, the step, the parameters and every
+// buffer address stay the same. The graph runs on a private non-blocking
+// stream ordered after and before the context's stream by events (the legacy
+// NULL stream cannot be captured).
+struct tc_advance_graph {
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  std::vector<uint64_t> key;  // shape, dt, steps, parameters and buffer addresses at capture
+  long long launches = 0, pair_launches = 0, pair_interactions = 0;
+  ~tc_advance_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+void tc_advance_graph_free(tc_ctx* ctx) {
+  delete ctx->agraph;
+  ctx->agraph = nullptr;
+}
+
+extern "C" int tc_set_rk4_graphs(tc_ctx* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 2) return TC_ERR_ARG;
+  ctx->rk4_graphs = mode;
+  return TC_OK;
+}
+
+namespace {
+
+constexpr int kCaptureFailed = 1;  // advance_graph: no graph, nothing launched
+
+int advance_steps(tc_ctx* ctx, double dt, int first, int last) {
+  tcb::Rk4State& R = ctx->rk;
+  for (int step = first; step < last; ++step)
+    for (int s = 0; s < 4; ++s) {
+      int rc = tc_rk4_stage_range(ctx, s, dt, 0, R.nA, 0, R.nV, 0, R.nQ,
+                                  s == 0 ? R.totalKE.as<double>() + step : nullptr);
+      if (rc) return rc;
+    }
+  return TC_OK;
+}
+
+uint64_t bits(double v) {
+  uint64_t u;
+  memcpy(&u, &v, sizeof(u));
+  return u;
+}
+
+std::vector<uint64_t> graph_key(tc_ctx* ctx, double dt, int nsteps) {
+  tcb::Rk4State& R = ctx->rk;
+  std::vector<uint64_t> k = {(uint64_t)R.nA, (uint64_t)R.nV, (uint64_t)R.nQ, bits(dt),
+                             (uint64_t)nsteps, (uint64_t)ctx->precision, (uint64_t)ctx->var64,
+                             (uint64_t)ctx->var32, (uint64_t)ctx->target_order, bits(ctx->omega),
+                             bits(ctx->delta[0]), bits(ctx->delta[1]), bits(ctx->delta[2])};
+  const tcb::DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV,
+                               &R.xiQ, &R.newA, &R.newZ, &R.newV, &R.newQ, &R.src, &R.ke,
+                               &R.keBlocks, &R.totalKE, &R.permA, &R.permV, &R.permQ,
+                               &ctx->partial, &ctx->order_buf[0], &ctx->order_buf[1],
+                               &ctx->order_buf[2], &ctx->order_buf[3]};
+  for (const tcb::DevBuf* b : bufs) k.push_back((uint64_t)(uintptr_t)b->ptr);
+  return k;
+}
+
+int advance_graph(tc_ctx* ctx, double dt, int nsteps) {
+  if (!ctx->agraph) ctx->agraph = new (std::nothrow) tc_advance_graph();
+  if (!ctx->agraph) return TC_ERR_NOMEM;
+  tc_advance_graph& G = *ctx->agraph;
+  if (!G.stream) {
+    TC_CUDA_TRY(cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&G.ev[0], cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&G.ev[1], cudaEventDisableTiming));
+  }
+  const std::vector<uint64_t> key = graph_key(ctx, dt, nsteps);
+  if (!G.exec || G.key != key) {
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G.exec = nullptr;
+    const cudaStream_t user = ctx->stream;
+    const long long l0 = ctx->launches, p0 = ctx->pair_launches, i0 = ctx->pair_interactions;
+    ctx->stream = G.stream;
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeThreadLocal);
+    int rc = ce == cudaSuccess ? advance_steps(ctx, dt, 1, nsteps) : TC_ERR_CUDA;
+    if (ce == cudaSuccess) ce = cudaStreamEndCapture(G.stream, &g);
+    ctx->stream = user;
+    if (rc || ce != cudaSuccess) {
+      // capture failed before anything ran: undo the counters and let the caller
+      // run the steps without a graph
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      ctx->launches = l0;
+      ctx->pair_launches = p0;
+      ctx->pair_interactions = i0;
+      return kCaptureFailed;
+    }
+    ce = cudaGraphInstantiate(&G.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      G.exec = nullptr;
+      tc_record_error("RK4 graph instantiation failed: %s", cudaGetErrorString(ce));
+      return TC_ERR_CUDA;
+    }
+    G.key = key;
+    G.launches = ctx->launches - l0;
+    G.pair_launches = ctx->pair_launches - p0;
+    G.pair_interactions = ctx->pair_interactions - i0;
+  } else {
+    ctx->launches += G.launches;
+    ctx->pair_launches += G.pair_launches;
+    ctx->pair_interactions += G.pair_interactions;
+  }
+  TC_CUDA_TRY(cudaEventRecord(G.ev[0], ctx->stream));
+  TC_CUDA_TRY(cudaStreamWaitEvent(G.stream, G.ev[0], 0));
+  TC_CUDA_TRY(cudaGraphLaunch(G.exec, G.stream));
+  TC_CUDA_TRY(cudaEventRecord(G.ev[1], G.stream));
+  TC_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, G.ev[1], 0));
+  return TC_OK;
+}
+
+}  // namespace
+
 extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalKE) {
   int rc = begin(ctx);
   if (rc) return rc;
@@ -584,11 +710,22 @@ extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalK
   if (nsteps < 0 || !std::isfinite(dt)) return TC_ERR_ARG;
   if ((rc = R.totalKE.ensure((size_t)std::max(nsteps, 1) * sizeof(double)))) return rc;
   if ((rc = tc_rk4_pack_sources(ctx))) return rc;
-  for (int step = 0; step < nsteps; ++step)
-    for (int s = 0; s < 4; ++s)
-      if ((rc = tc_rk4_stage_range(ctx, s, dt, 0, R.nA, 0, R.nV, 0, R.nQ,
-                                   s == 0 ? R.totalKE.as<double>() + step : nullptr)))
-        return rc;
+  // graphs: not for forced runs (their stage times are host arguments of each
+  // launch) nor while pair kernels are timed one by one
+  const double per_step = 4.0 * ((double)R.nA * R.nA + (double)(R.nV + R.nQ) * R.nA);
+  const bool graph = nsteps >= 3 && !R.strat && !ctx->time_pairs &&
+                     (ctx->rk4_graphs == 2 || (ctx->rk4_graphs == 1 && per_step <= 4.1e10));
+  if (graph) {
+    if ((rc = advance_steps(ctx, dt, 0, 1))) return rc;
+    rc = advance_graph(ctx, dt, nsteps);
+    if (rc == kCaptureFailed) {
+      ctx->rk4_graphs = 0;  // this context runs its steps one launch at a time from now on
+      rc = advance_steps(ctx, dt, 1, nsteps);
+    }
+    if (rc) return rc;
+  } else if ((rc = advance_steps(ctx, dt, 0, nsteps))) {
+    return rc;
+  }
   if (totalKE && nsteps > 0) {
     TC_CUDA_TRY(cudaMemcpyAsync(totalKE, R.totalKE.ptr, (size_t)nsteps * sizeof(double),
                                 cudaMemcpyDeviceToHost, ctx->stream));
@@ -767,6 +904,7 @@ extern "C" int tc_reset_rk4(tc_ctx* ctx) {
                     &R.permA, &R.permV, &R.permQ};
   for (DevBuf* b : bufs) b->release();
   ctx->partial.release();
+  tc_advance_graph_free(ctx);
   R.ready = false;
   R.ordered = false;
   R.nA = R.nV = R.nQ = 0;

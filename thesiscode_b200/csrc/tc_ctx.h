@@ -82,6 +82,8 @@ struct Rk4State {
 }  // namespace tcb
 
 struct tc_batch_plan;            // batched-ensemble plan (batch.cu)
+struct tc_advance_graph;         // captured RK4 steps of tc_rk4_advance (api.cu)
+void tc_advance_graph_free(tc_ctx* ctx);
 void tc_batch_free(tc_ctx* ctx);
 
 struct tc_ctx {
@@ -99,7 +101,7 @@ struct tc_ctx {
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
   int adj_mode = 5;  // adjoint VJP: 3-6 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
   tcb::DevBuf order_buf[4];             // keys, sorted keys, indices, sort scratch
-  int min_chunk = 4096;   // smallest source chunk a CTA walks
+  int min_chunk = 256;    // smallest source chunk a CTA walks (one shared-memory tile)
   int max_chunks = 64;
   int slots64 = 0, slots32 = 0;  // resident CTAs per GPU for each kernel
   tcb::DevBuf partial;    // pair-kernel partial sums
@@ -114,6 +116,8 @@ struct tc_ctx {
   std::vector<cudaEvent_t> pair_events;  // start/stop pairs, resolved by tc_stats
   double pair_ms = 0.0;
   tc_batch_plan* batch = nullptr;
+  tc_advance_graph* agraph = nullptr;
+  int rk4_graphs = 1;  // tc_rk4_advance graph replay: 0 never, 1 small problems, 2 always
 };
 
 namespace tcb {

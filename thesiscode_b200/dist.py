@@ -106,12 +106,16 @@ class LibBackend:
 class DistributedPanelVelocity:
     """BVERK4 over torch.distributed ranks with target sharding and a per-stage all-gather."""
 
-    def __init__(self, device: int = 0, precision="fp32c", backend=None, group=None):
-        import torch.distributed as dist
+    def __init__(self, device: int = 0, precision="fp32c", backend=None, group=None, comm=None):
+        """comm: the collective layer (torch.distributed by default; any object with its
+        get_rank / get_world_size / all_gather / all_reduce / barrier / ReduceOp)."""
+        if comm is None:
+            import torch.distributed as comm
 
+            if not comm.is_initialized():
+                comm.init_process_group("nccl")
+        dist = comm
         self.dist = dist
-        if not dist.is_initialized():
-            dist.init_process_group("nccl")
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
