@@ -1,11 +1,15 @@
 """One launch of the pair kernels on a workload of a chosen size, for profilers.
 
-    python -m thesiscode_b200.profile_case --precision fp32c --level 6 [--what velocity|rk4|adjoint]
+    python -m thesiscode_b200.profile_case --precision fp32c --level 6 \
+        [--what velocity|rk4|adjoint|batch|strat]
 
 `velocity` runs one TC_ACTIVE and one TC_VERTEX sum (two pair-kernel launches);
 `rk4` runs one fused RK4 step (four pair-kernel launches); `adjoint` runs the
-FP64 adjoint of two RK4 steps (eight vector-Jacobian pair launches). The
-Gaussian-vortex workload with delta 0.01 is used at every level.
+FP64 adjoint of two RK4 steps (eight vector-Jacobian pair launches); `batch`
+runs one RK4 step of the 64-instance Gaussian ensemble (levels 3 to `--level`)
+without autotuning or graph (four persistent batch-kernel launches); `strat`
+runs one forced stratosphere RK4 step (parity mode). The Gaussian-vortex
+workload with delta 0.01 is used at every level for the first three.
 """
 from __future__ import annotations
 
@@ -20,8 +24,27 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--level", type=int, default=6)
-    ap.add_argument("--what", default="velocity", choices=["velocity", "rk4", "adjoint"])
+    ap.add_argument("--what", default="velocity", choices=["velocity", "rk4", "adjoint", "batch", "strat"])
     a = ap.parse_args()
+    if a.what in ("batch", "strat"):
+        ctx = Context(0, a.precision)
+        if a.what == "batch":
+            from .batch import batch_rk4
+
+            ws = configs.batched_gaussians(count=64, seed=4, levels=tuple(range(3, a.level + 1)))
+            ctx.set_omega(ws[0].omega)
+            ctx.set_deltas(*ws[0].deltas)
+            batch_rk4(ctx, ws, ws[0].dt, 1, graph=False, autotune=False)
+        else:
+            w = configs.stratosphere(level=a.level, dt=0.01)
+            ctx.set_omega(w.omega)
+            ctx.set_deltas(*w.deltas)
+            ctx.strat_rk4_step(w.xA.copy(), w.meta["absVortA"], w.areaA, w.xV.copy(), w.xQ.copy(),
+                               w.meta["t0"], w.dt, 1, absVortV=w.meta["absVortV"])
+        ctx.synchronize()
+        ctx.close()
+        print(f"profile_case {a.precision} level {a.level} {a.what}: ok")
+        return
     w = configs.gaussian(level=a.level, delta=0.01)
     ctx = Context(0, a.precision)
     ctx.set_omega(w.omega)
