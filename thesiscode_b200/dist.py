@@ -109,11 +109,16 @@ class DistributedPanelVelocity:
     def __init__(self, device: int = 0, precision="fp32c", backend=None, group=None, comm=None):
         """comm: the collective layer (torch.distributed by default; any object with its
         get_rank / get_world_size / all_gather / all_reduce / barrier / ReduceOp)."""
+        self._owns_group = False
         if comm is None:
+            from datetime import timedelta
+
             import torch.distributed as comm
 
             if not comm.is_initialized():
-                comm.init_process_group("nccl")
+                # a short timeout: a rank that dies makes the others' next collective fail
+                comm.init_process_group("nccl", timeout=timedelta(seconds=180))
+                self._owns_group = True
         dist = comm
         self.dist = dist
         self.group = group
@@ -205,3 +210,6 @@ class DistributedPanelVelocity:
 
     def close(self) -> None:
         self.backend.close()
+        if self._owns_group:
+            self.dist.destroy_process_group()
+            self._owns_group = False
