@@ -225,6 +225,14 @@ int tc_reset_rk4(tc_ctx* ctx);
 int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA,
                    int nA, double dt, int nsteps, int ckpt_every, int functional, int probe,
                    double* J, double* g_zeta0, double* g_x0);
+/* Vector-Jacobian product of the whole trajectory: given cotangents gT_x[3nA]
+ * and gT_zeta[nA] (either nullable, not both) on the state after nsteps RK4
+ * steps, g_x0 / g_zeta0 = (d state(T) / d state(0))^T applied to them, and J =
+ * gT_x . x(T) + gT_zeta . zeta(T). Same checkpointing and errors as
+ * tc_rk4_adjoint (no reference counterpart). */
+int tc_rk4_vjp(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA, int nA,
+               double dt, int nsteps, int ckpt_every, const double* gT_x, const double* gT_zeta,
+               double* J, double* g_zeta0, double* g_x0);
 /* How each stage's vector-Jacobian product visits the pairs: 3 to 6 = one
  * row-major pass computing both sides' row sums (3: one row per thread,
  * 4: two rows per thread; 5 and 6: the same with a one-step Newton

@@ -43,6 +43,32 @@ class EnstrophyAfterRK4(torch.autograd.Function):
         return g * gx, g * gz, None, None, None, None, None
 
 
+def torch_rk4_state(x, z, area, omega, d2, dt, nsteps):
+    """The RK4 map of the active panels in torch FP64 (test harness): (x(T), zeta(T))."""
+    n = x.shape[0]
+    eye = torch.eye(n, dtype=torch.float64)
+
+    def rhs(x, z):
+        D = 1.0 + d2 - x @ x.T
+        W = (z * area)[None, :] / (D + eye) * (1.0 - eye)
+        S = W @ x
+        u = -torch.cross(x, S, dim=1) / (4.0 * np.pi)
+        return u, -2.0 * omega * u[:, 2]
+
+    for _ in range(nsteps):
+        k1x, k1z = rhs(x, z)
+        k1x, k1z = dt * k1x, dt * k1z
+        k2x, k2z = rhs(x + 0.5 * k1x, z + 0.5 * k1z)
+        k2x, k2z = dt * k2x, dt * k2z
+        k3x, k3z = rhs(x + 0.5 * k2x, z + 0.5 * k2z)
+        k3x, k3z = dt * k3x, dt * k3z
+        k4x, k4z = rhs(x + k3x, z + k3z)
+        k4x, k4z = dt * k4x, dt * k4z
+        x = x + k1x / 6 + k2x / 3 + k3x / 3 + k4x / 6
+        z = z + k1z / 6 + k2z / 3 + k3z / 3 + k4z / 6
+    return x, z
+
+
 def torch_rk4_enstrophy(x, z, area, omega, d2, dt, nsteps, probe=None):
     n = x.shape[0]
     eye = torch.eye(n, dtype=torch.float64)
@@ -203,4 +229,43 @@ def test_adjoint_probe_functional_and_errors(gpu):
         adjoint(c32, w.xA, w.zetaA, w.areaA, w.dt, 3, 2)
     assert e.value.status == N.TC_ERR_STATE
     c32.close()
+    ctx.close()
+
+
+def test_trajectory_vjp_matches_torch_autograd_fp64(gpu):
+    """tc_rk4_vjp with seeded random cotangents on both x(T) and zeta(T) against
+    torch.autograd.grad of the same RK4 map with those grad_outputs."""
+    w = configs.gaussian(level=2, delta=0.02, dt=0.01)
+    ctx = Context(0, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    nsteps, ckpt = 5, 2
+    rng = np.random.default_rng(8)
+    gTx = rng.standard_normal((w.nA, 3))
+    gTz = rng.standard_normal(w.nA)
+    x = torch.tensor(w.xA, requires_grad=True)
+    z = torch.tensor(w.zetaA, requires_grad=True)
+    xT, zT = torch_rk4_state(x, z, torch.tensor(w.areaA), w.omega, w.deltas[0] ** 2, w.dt, nsteps)
+    gx_ref, gz_ref = torch.autograd.grad((xT, zT), (x, z), (torch.tensor(gTx), torch.tensor(gTz)))
+    J_ref = float((xT.detach() * torch.tensor(gTx)).sum() + (zT.detach() * torch.tensor(gTz)).sum())
+    J, gz, gx = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
+    N.call("tc_rk4_vjp", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt, nsteps,
+           ckpt, N.dptr(gTx), N.dptr(gTz), N.dptr(J), N.dptr(gz), N.dptr(gx))
+    assert abs(J[0] - J_ref) <= 1e-12 * abs(J_ref)
+    assert np.abs(gx - gx_ref.numpy()).max() <= 1e-10 * np.abs(gx_ref.numpy()).max()
+    assert np.abs(gz - gz_ref.numpy()).max() <= 1e-10 * np.abs(gz_ref.numpy()).max()
+    # the zeta-only cotangent equals the enstrophy adjoint's seed 2 zeta A: same gradient
+    Jz, gz2, gx2 = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
+    zfin = w.zetaA.copy()
+    xfin = w.xA.copy()
+    ctx.rk4_step(xfin, zfin, w.areaA, np.zeros((0, 3)), np.zeros((0, 3)), w.dt, nsteps)
+    seed = 2.0 * zfin * w.areaA
+    N.call("tc_rk4_vjp", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt, nsteps,
+           ckpt, None, N.dptr(seed), N.dptr(Jz), N.dptr(gz2), N.dptr(gx2))
+    Je, gze, gxe = adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, nsteps, ckpt)
+    assert np.abs(gz2 - gze).max() <= 1e-12 * np.abs(gze).max()
+    assert np.abs(gx2 - gxe).max() <= 1e-12 * np.abs(gze).max()
+    with pytest.raises(N.TcError):
+        N.call("tc_rk4_vjp", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, w.dt,
+               nsteps, ckpt, None, None, N.dptr(Jz), N.dptr(gz2), N.dptr(gx2))
     ctx.close()

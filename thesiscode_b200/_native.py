@@ -85,6 +85,7 @@ SIGNATURES: dict[str, tuple] = {
     "tc_rk4_soa_step": (c_int, [c_void_p, dp, dp, dp, dp, dp, c_int, c_double, c_int, dp, dp]),
     "tc_rk4_step": (c_int, [c_void_p, dp, dp, dp, c_int, dp, c_int, dp, c_int, c_double, c_int, dp, dp]),
     "tc_set_rk4_graphs": (c_int, [c_void_p, c_int]),
+    "tc_rk4_vjp": (c_int, [c_void_p, dp, dp, dp, c_int, c_double, c_int, c_int, dp, dp, dp, dp, dp]),
     "tc_strat_rk4_step": (c_int, [c_void_p, dp, dp, dp, dp, c_int, dp, dp, dp, c_int, dp, c_int,
                                   c_double, c_double, c_int, dp, dp]),
     "tc_rk4_step_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,

@@ -664,10 +664,6 @@ __global__ void enstrophy_seed_kernel(const double* __restrict__ z, const double
 
 }  // namespace
 
-// Gradient of J at time nsteps*dt with respect to the initial active-panel
-// state. functional: TC_J_ENSTROPHY (J = sum zeta^2 A) or TC_J_PROBE
-// (J = zeta of panel `probe` at the end). Inputs are host arrays; outputs:
-// J (host scalar), g_zeta0 (nA), g_x0 (3*nA), host arrays.
 // Device time (ms) of the last adjoint call's phases: the forward sweep with
 // checkpoints, the recomputation of checkpoint segments, and the backward
 // sweep (vector-Jacobian products and combinations).
@@ -677,15 +673,19 @@ extern "C" int tc_adjoint_phase_ms(tc_ctx* ctx, double* ms3) {
   return TC_OK;
 }
 
-extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0,
-                              const double* areaA, int nA, double dt, int nsteps, int ckpt_every,
-                              int functional, int probe, double* J, double* g_zeta0, double* g_x0) {
-  if (!ctx || nA <= 0 || nsteps < 0 || ckpt_every <= 0 || !xA0 || !zetaA0 || !areaA || !J ||
-      !g_zeta0 || !g_x0 || (functional != TC_J_ENSTROPHY && functional != TC_J_PROBE) ||
-      (functional == TC_J_PROBE && (probe < 0 || probe >= nA))) {
-    tc_record_error("tc_rk4_adjoint: bad arguments");
-    return TC_ERR_ARG;
-  }
+namespace {
+
+constexpr int kCotangent = -1;  // adjoint_impl: seed with caller-given cotangents
+
+// Gradient of J at time nsteps*dt with respect to the initial active-panel
+// state. functional: TC_J_ENSTROPHY (J = sum zeta^2 A), TC_J_PROBE (J = zeta
+// of panel `probe` at the end) or kCotangent (J = gT_x . x(T) + gT_zeta . zeta(T),
+// a vector-Jacobian product of the whole trajectory). Inputs are host arrays;
+// outputs: J (host scalar), g_zeta0 (nA), g_x0 (3*nA), host arrays.
+int adjoint_impl(tc_ctx* ctx, const double* xA0, const double* zetaA0, const double* areaA,
+                 int nA, double dt, int nsteps, int ckpt_every, int functional, int probe,
+                 const double* gT_x, const double* gT_zeta, double* J, double* g_zeta0,
+                 double* g_x0) {
   if (ctx->precision != TC_FP64) {
     tc_record_error("tc_rk4_adjoint: the adjoint runs in FP64 (tc_set_precision(ctx, TC_FP64))");
     return TC_ERR_STATE;
@@ -747,12 +747,32 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
     double acc = 0.0;
     for (double v : jb) acc += v;
     *J = acc;
-  } else {
+  } else if (functional == TC_J_PROBE) {
     TC_CUDA_TRY(cudaMemcpyAsync(J, zT + probe, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     const double one = 1.0;
     TC_CUDA_TRY(cudaMemcpyAsync(lam + 3 * (size_t)nA + probe, &one, sizeof(double),
                                 cudaMemcpyHostToDevice, ctx->stream));
     TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  } else {
+    // the caller's cotangents; J = their dot product with the final state (on the host)
+    std::vector<double> xT(3 * (size_t)nA), zTh(nA);
+    TC_CUDA_TRY(cudaMemcpyAsync(xT.data(), ctx->rk.x0A.ptr, 3 * (size_t)nA * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(zTh.data(), zT, (size_t)nA * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    if (gT_x)
+      TC_CUDA_TRY(cudaMemcpyAsync(lam, gT_x, 3 * (size_t)nA * sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    if (gT_zeta)
+      TC_CUDA_TRY(cudaMemcpyAsync(lam + 3 * (size_t)nA, gT_zeta, (size_t)nA * sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    double acc = 0.0;
+    if (gT_x)
+      for (size_t k = 0; k < 3 * (size_t)nA; ++k) acc += gT_x[k] * xT[k];
+    if (gT_zeta)
+      for (int k = 0; k < nA; ++k) acc += gT_zeta[k] * zTh[k];
+    *J = acc;
   }
   // backward sweep, one checkpoint segment at a time
   double* lk = W.lk.as<double>();
@@ -807,4 +827,32 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
                               cudaMemcpyDeviceToHost, ctx->stream));
   TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return TC_OK;
+}
+
+}  // namespace
+
+extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zetaA0,
+                              const double* areaA, int nA, double dt, int nsteps, int ckpt_every,
+                              int functional, int probe, double* J, double* g_zeta0, double* g_x0) {
+  if (!ctx || nA <= 0 || nsteps < 0 || ckpt_every <= 0 || !xA0 || !zetaA0 || !areaA || !J ||
+      !g_zeta0 || !g_x0 || (functional != TC_J_ENSTROPHY && functional != TC_J_PROBE) ||
+      (functional == TC_J_PROBE && (probe < 0 || probe >= nA))) {
+    tc_record_error("tc_rk4_adjoint: bad arguments");
+    return TC_ERR_ARG;
+  }
+  return adjoint_impl(ctx, xA0, zetaA0, areaA, nA, dt, nsteps, ckpt_every, functional, probe,
+                      nullptr, nullptr, J, g_zeta0, g_x0);
+}
+
+extern "C" int tc_rk4_vjp(tc_ctx* ctx, const double* xA0, const double* zetaA0,
+                          const double* areaA, int nA, double dt, int nsteps, int ckpt_every,
+                          const double* gT_x, const double* gT_zeta, double* J, double* g_zeta0,
+                          double* g_x0) {
+  if (!ctx || nA <= 0 || nsteps < 0 || ckpt_every <= 0 || !xA0 || !zetaA0 || !areaA || !J ||
+      !g_zeta0 || !g_x0 || (!gT_x && !gT_zeta)) {
+    tc_record_error("tc_rk4_vjp: bad arguments");
+    return TC_ERR_ARG;
+  }
+  return adjoint_impl(ctx, xA0, zetaA0, areaA, nA, dt, nsteps, ckpt_every, kCotangent, 0, gT_x,
+                      gT_zeta, J, g_zeta0, g_x0);
 }
