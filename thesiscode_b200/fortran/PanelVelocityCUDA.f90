@@ -5,6 +5,7 @@ module PanelVelocityCUDAModule
 !  `use PanelVelocityCUDAModule`; the public names, argument lists and module state are the same:
 !
 !      BVERK4(aParticles, aPanels, dt, procRank, numProcs)     :435-658
+!      StratosphereRK4(aParticles, aPanels, t, dt, procRank, numProcs)  :661-919
 !      InitializeMPIRK4, FinalizeMPIRK4, LoadBalance           :126-230
 !      ResetRK4, SetSmooth, GetSmooth, ResetArea               :96-120, :321
 !      totalKE, kineticEnergy                                  :25-26
@@ -25,7 +26,7 @@ implicit none
 
 private
 public totalKE, kineticEnergy
-public BVERK4, ResetRK4, ResetArea, SetSmooth, GetSmooth
+public BVERK4, StratosphereRK4, ResetRK4, ResetArea, SetSmooth, GetSmooth
 public InitializeMPIRK4, FinalizeMPIRK4, LoadBalance
 public SetPrecisionCUDA
 
@@ -62,6 +63,16 @@ interface
     real(c_double) :: xA(3,*), zetaA(*), areaA(*), xV(3,*), xQ(3,*), tke(*), ke(*)
     integer(c_int), value :: nA, nV, nQ, nsteps
     real(c_double), value :: dt
+  end function
+  integer(c_int) function tc_strat_rk4_step(ctx, xA, absVortA, relVortA, areaA, nA, xV, &
+                                            absVortV, relVortV, nV, xQ, nQ, t, dt, nsteps, &
+                                            tke, ke) bind(C, name="tc_strat_rk4_step")
+    import :: c_int, c_ptr, c_double
+    type(c_ptr), value :: ctx
+    real(c_double) :: xA(3,*), absVortA(*), relVortA(*), areaA(*), xV(3,*), absVortV(*), &
+                      relVortV(*), xQ(3,*), tke(*), ke(*)
+    integer(c_int), value :: nA, nV, nQ, nsteps
+    real(c_double), value :: t, dt
   end function
   type(c_ptr) function tc_last_error() bind(C, name="tc_last_error")
     import :: c_ptr
@@ -246,6 +257,37 @@ subroutine BVERK4(aParticles, aPanels, dt, procRank, numProcs)
                                        - 2.0_kreal*Omega*aParticles%x(3,1:aParticles%N)
   call ScatterPanels(aPanels, activePanels, activeMap, passivePanels, passiveMap)
   if (procRank < 0 .OR. numProcs < 1) print *, "BVERK4 WARNING : bad MPI arguments"
+end subroutine
+
+subroutine StratosphereRK4(aParticles, aPanels, t, dt, procRank, numProcs)
+  ! Forced model (:661-919): positions advance; the relative vorticity of panels and particles
+  ! is rebuilt from absVort, the rotation and the Juckes forcing at t + dt (:908-915).
+  type(Particles), intent(inout) :: aParticles
+  type(Panels), intent(inout) :: aPanels
+  real(kreal), intent(in) :: t, dt
+  integer(kint), intent(in) :: procRank, numProcs
+  integer(c_int) :: rc
+  real(c_double) :: tke(1)
+  if (.NOT. c_associated(ctx)) then
+    rc = tc_create(0_c_int, precisionMode, ctx)
+    call CheckStatus(rc, "StratosphereRK4")
+  endif
+  if (.NOT. rk4IsReady) call InitRK4(aParticles, aPanels)
+  call GatherPanels(aPanels, activePanels, activeMap, passivePanels, passiveMap)
+  rc = tc_set_omega(ctx, real(Omega, c_double))
+  call CheckStatus(rc, "StratosphereRK4 omega")
+  rc = tc_set_deltas(ctx, 0.0_c_double, 0.0_c_double, real(smooth, c_double))
+  call CheckStatus(rc, "StratosphereRK4 smooth")
+  rc = tc_strat_rk4_step(ctx, activePanels%x, activePanels%absVort, activePanels%relVort, &
+                         activePanels%area, int(activePanels%N, c_int), aParticles%x, &
+                         aParticles%absVort, aParticles%relVort, int(aParticles%N, c_int), &
+                         passivePanels%x, int(passivePanels%N, c_int), real(t, c_double), &
+                         real(dt, c_double), 1_c_int, tke, kineticEnergy)
+  call CheckStatus(rc, "StratosphereRK4 step")
+  totalKE = tke(1)
+  if (GetNTracer(aPanels) >= 2) activePanels%tracer(:,2) = kineticEnergy
+  call ScatterPanels(aPanels, activePanels, activeMap, passivePanels, passiveMap)
+  if (procRank < 0 .OR. numProcs < 1) print *, "StratosphereRK4 WARNING : bad MPI arguments"
 end subroutine
 
 end module
