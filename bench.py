@@ -436,6 +436,9 @@ def run_ours(args):
                      "pair_ms_per_launch": pair_ms_launch,
                      "peak_source": "measured live: CUDA-core FMA probe (tc_probe_peak) x 2 flops"},
         "gpu_launches": main["launches"],
+        "gpu_launches_note": "the library's own kernels (pack, Hilbert keys, pair, stage epilogue, KE finalize); "
+                             "each FP32C step also runs two CUB radix sorts (6 kernels each on this "
+                             "toolkit: histogram, exclusive sum, 4 onesweep passes)",
         "clocks": main["clocks"],
     }
     e2e_dist = None
