@@ -86,6 +86,9 @@ const PairVariant kVariants32[] = {
     V32(256, 2, 32, 2, 4, 3), V32(128, 1, 32, 8, 8, 1), V32(128, 1, 32, 8, 8, 3),
     V32(128, 2, 32, 6, 4, 2), V32(128, 2, 32, 4, 4, 1), V32(128, 2, 32, 4, 4, 3),
     V32(128, 1, 32, 6, 8, 1), V32(128, 1, 32, 8, 16, 1), V32(256, 1, 32, 4, 8, 1),
+    V32(64, 1, 32, 12, 8, 1), V32(128, 1, 64, 6, 8, 1), V32(128, 1, 32, 7, 8, 1),
+    V32(256, 1, 32, 3, 8, 1), V32(128, 1, 128, 6, 8, 1), V32(128, 1, 64, 8, 8, 1),
+    V32(128, 1, 64, 6, 16, 1),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
