@@ -1,7 +1,7 @@
 /*
  * bve_oracle.c - CPU FP64 restatement of the reference's Biot-Savart sums and
- * RK4 driver. TEST INFRASTRUCTURE ONLY (parity checker and timed CPU
- * baseline); see bve_oracle.h for the parity status ("parity unpinned"
+ * RK4 driver. TEST INFRASTRUCTURE ONLY (the parity tests' reference values and
+ * the timed CPU baseline); see bve_oracle.h for the parity status ("parity unpinned"
  * against a reference binary: no Fortran compiler is available).
  *
  * Every arithmetic expression keeps the reference's operand order so that a

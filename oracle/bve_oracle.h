@@ -1,10 +1,10 @@
 /*
  * bve_oracle.h - CPU FP64 restatement of ThesisCode's Biot-Savart / RK4 hot
- * path. TEST INFRASTRUCTURE ONLY: the parity checker for the CUDA library and
- * the CPU baseline of the benchmark. Nothing in the product links or calls it.
+ * path. TEST INFRASTRUCTURE ONLY: the reference values of the CUDA library's
+ * parity tests and the CPU baseline of the benchmark. Nothing in the product links or calls it.
  *
  * Parity status: the reference is Fortran (ifort/Open MPI) and no Fortran
- * compiler exists on the build or GPU machines, so this restatement is
+ * compiler is available to build it, so this restatement is
  * "parity unpinned" against a reference binary. It is pinned instead by the
  * known answers the reference's own validation drivers check (solid-body
  * rotation, RK4 time-step convergence, invariants; see tests/test_oracle.py)

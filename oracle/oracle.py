@@ -1,9 +1,9 @@
 """ctypes wrapper of the CPU FP64 oracle (oracle/bve_oracle.c, oracle/strat_oracle.c).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
-the checker and by bench.py's CPU-baseline leg. The product never imports
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the entry module's smoke() to
+verify one GPU step, and by bench.py's CPU-baseline leg. The product never imports
 it. Parity status: unpinned against a reference binary (the reference is
-Fortran and no Fortran compiler exists here or on the GPU machines); pinned
+Fortran and no Fortran compiler is available to build it); pinned
 by the reference drivers' known answers (tests/test_oracle.py).
 """
 from __future__ import annotations

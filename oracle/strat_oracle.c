@@ -1,5 +1,5 @@
 /* CPU FP64 oracle of the forced (stratosphere) RK4 step - TEST
- * INFRASTRUCTURE ONLY, used by tests/ as the checker.
+ * INFRASTRUCTURE ONLY, the reference values of the forced step's tests.
  *
  * StratosphereRK4, PanelVelocityParallel.f90:661-919, with one rank: the
  * positions of all three target classes advance by classical RK4 like

@@ -4,8 +4,8 @@ The reference ships no golden vectors and cannot be compiled here (Fortran,
 no compiler), so the fixtures are outputs of the CPU FP64 oracle
 (oracle/bve_oracle.c, a line-by-line restatement of the reference loops) on
 small seeded inputs. They freeze the oracle (tests/test_oracle.py checks it
-reproduces them bit for bit) and give the GPU parity tests a checker that
-needs no oracle build on the GPU machine.
+reproduces them bit for bit) and give the GPU parity tests reference values
+that need no oracle build where the GPU tests run.
 
 Run from the repository root:  python tests/golden/make_golden.py
 """

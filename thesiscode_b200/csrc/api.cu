@@ -708,6 +708,11 @@ extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalK
     return TC_ERR_STATE;
   }
   if (nsteps < 0 || !std::isfinite(dt)) return TC_ERR_ARG;
+  if (R.strat && dt != R.strat_dt) {  // forced run continued with another step: rebase its clock
+    R.t0 += (double)R.step * R.strat_dt;
+    R.step = 0;
+    R.strat_dt = dt;
+  }
   if ((rc = R.totalKE.ensure((size_t)std::max(nsteps, 1) * sizeof(double)))) return rc;
   if ((rc = tc_rk4_pack_sources(ctx))) return rc;
   // graphs: not for forced runs (their stage times are host arguments of each
