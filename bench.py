@@ -335,7 +335,9 @@ def time_batch(device, steps=10):
     ctx = Context(device, "fp32c")
     ctx.set_omega(ws[0].omega)
     ctx.set_deltas(*ws[0].deltas)
+    t = time.perf_counter()
     batch_rk4(ctx, [w.copy() for w in ws], ws[0].dt, steps)
+    first = time.perf_counter() - t
     t = time.perf_counter()
     batch_rk4(ctx, ws, ws[0].dt, steps)
     dt = time.perf_counter() - t
@@ -345,6 +347,7 @@ def time_batch(device, steps=10):
     return {"workload": "64 Gaussian vortices (seed 4), icosahedral levels 3-6, beta in [4,20], "
                         f"{steps} RK4 steps each, FP32C, one CUDA graph", "interactions": inter,
             "seconds": dt, "value": inter / dt, "unit": "interactions/s",
+            "first_call_seconds": first,
             "levels": sorted(set(w.level for w in ws)), "autotuned": info}
 
 
