@@ -44,7 +44,6 @@ struct AdjLaunch {
   const double4* src;    // pass 1: {x, y, z, G}; pass 2: {x, y, z, v_x}
   const double2* src2;   // pass 2: {v_y, v_z}
   const double* v;       // pass 1: v_i per target (3 per row)
-  const double4* src2_4; // row pass: {v_x, v_y, v_z, 0}
   int n;
   int chunk_len;
   double one_plus_d2;
@@ -279,15 +278,26 @@ __global__ void __launch_bounds__(kFNT) adj_fused_kernel(const AdjFused P) {
 // panels j it acts on, for fixed k - row sums like the target side - and
 // D_ij = D_ji, so one visit of each ordered pair (i, j) gives row i every sum
 // it needs, with s_ij = x_j . v_i and s_ji = x_i . v_j. Q_i enters dL/dx_i only
-// as G_i Q_i, next to S2_i, and both weight x_j, so they share one accumulator:
-//     S1 += G_j r x_j,  C += (G_j s_ij + G_i s_ji) r^2 x_j  (= S2 + G_i Q),
-//     P  += r v_j,      R += s_ji r                          (r = 1/D_ij)
-// 10 accumulators per row and 24 FP64 operations per pair besides the
+// as G_i Q_i, next to S2_i, and both weight x_j, so they share one accumulator;
+// R_i = sum_j s_ji r = x_i . P_i needs none:
+//     S1 += r (G_j x_j),  C += ((G_j x_j).v_i + (G_i x_i).v_j) r^2 x_j  (= S2 + G_i Q),
+//     P  += r v_j                                          (r = 1/D_ij)
+// 9 accumulators per row and 20 FP64 operations per pair besides the
 // reciprocal: rcp.approx.f64 seed + NEWTON Newton-Raphson steps
 // r <- r + r (1 - D r) of 2 FMA each (2 steps: full FP64; 1 step: the seed's
 // error squared). TPT rows per thread share each source's shared-memory loads.
-// No reduction across threads. Rows: partial[(chunk*10 + c)*n + i].
-constexpr int kRNT = 128, kRTS = 128, kRowSums = 10;
+// No reduction across threads. Rows: partial[(chunk*9 + c)*n + i].
+constexpr int kRNT = 128, kRTS = 128, kRowSums = 9;
+
+struct RowLaunch {
+  const double4* ra;  // {x, y, z, G x} per panel
+  const double4* rb;  // {G y, G z, v_x, v_y}
+  const double* rc;   // v_z
+  int n;
+  int chunk_len;
+  double one_plus_d2;
+  double* partial;    // [chunk][kRowSums][n]
+};
 
 template <int NEWTON>
 __device__ __forceinline__ double adj_rcp_n(double d) {
@@ -299,25 +309,28 @@ __device__ __forceinline__ double adj_rcp_n(double d) {
 }
 
 template <int TPT, int NEWTON, int UNROLL>
-__global__ void __launch_bounds__(kRNT) adj_row_kernel(const AdjLaunch P) {
-  __shared__ double4 sa[kRTS];  // {x_j, G_j}
-  __shared__ double4 sb[kRTS];  // {v_j, 0}
+__global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
+  __shared__ double4 sa[kRTS];  // {x_j, G_j x_j}
+  __shared__ double4 sb[kRTS];  // {G_j y_j, G_j z_j, v_j,x, v_j,y}
+  __shared__ double sc[kRTS];   // v_j,z
   int row[TPT];
-  double x0[TPT], x1[TPT], x2[TPT], v0[TPT], v1[TPT], v2[TPT], gi[TPT];
+  double x0[TPT], x1[TPT], x2[TPT], g0[TPT], g1[TPT], g2[TPT], v0[TPT], v1[TPT], v2[TPT];
   double a[TPT][kRowSums];
 #pragma unroll
   for (int t = 0; t < TPT; ++t) {
     row[t] = (blockIdx.x * TPT + t) * kRNT + threadIdx.x;
     const int ld = row[t] < P.n ? row[t] : P.n - 1;
-    const double4 q = P.src[ld];
-    const double4 w = P.src2_4[ld];
+    const double4 q = P.ra[ld];
+    const double4 w = P.rb[ld];
     x0[t] = q.x;
     x1[t] = q.y;
     x2[t] = q.z;
-    gi[t] = q.w;
-    v0[t] = w.x;
-    v1[t] = w.y;
-    v2[t] = w.z;
+    g0[t] = q.w;
+    g1[t] = w.x;
+    g2[t] = w.y;
+    v0[t] = w.z;
+    v1[t] = w.w;
+    v2[t] = P.rc[ld];
 #pragma unroll
     for (int c = 0; c < kRowSums; ++c) a[t][c] = 0.0;
   }
@@ -326,14 +339,16 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const AdjLaunch P) {
     __syncthreads();
     for (int j = threadIdx.x; j < kRTS; j += kRNT) {
       const int k = ts + j;
-      sa[j] = k < c1 ? P.src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
-      sb[j] = k < c1 ? P.src2_4[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sa[j] = k < c1 ? P.ra[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sb[j] = k < c1 ? P.rb[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sc[j] = k < c1 ? P.rc[k] : 0.0;
     }
     __syncthreads();
 #pragma unroll UNROLL
     for (int j = 0; j < kRTS; ++j) {
       const double4 q = sa[j];
       const double4 w = sb[j];
+      const double vz = sc[j];
 #pragma unroll
       for (int t = 0; t < TPT; ++t) {
         double D = fma(-q.x, x0[t], P.one_plus_d2);
@@ -341,20 +356,23 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const AdjLaunch P) {
         D = fma(-q.z, x2[t], D);
         double r = adj_rcp_n<NEWTON>(D);
         r = (ts + j == row[t]) ? 0.0 : r;  // k == i: no self term (zero-padded sources give r*0)
-        const double sij = fma(q.x, v0[t], fma(q.y, v1[t], q.z * v2[t]));
-        const double sji = fma(x0[t], w.x, fma(x1[t], w.y, x2[t] * w.z));
-        const double c = fma(q.w, sij, gi[t] * sji) * (r * r);
-        const double w1 = q.w * r;
-        a[t][0] = fma(w1, q.x, a[t][0]);
-        a[t][1] = fma(w1, q.y, a[t][1]);
-        a[t][2] = fma(w1, q.z, a[t][2]);
-        a[t][3] = fma(c, q.x, a[t][3]);
-        a[t][4] = fma(c, q.y, a[t][4]);
-        a[t][5] = fma(c, q.z, a[t][5]);
-        a[t][6] = fma(r, w.x, a[t][6]);
-        a[t][7] = fma(r, w.y, a[t][7]);
-        a[t][8] = fma(r, w.z, a[t][8]);
-        a[t][9] = fma(sji, r, a[t][9]);
+        // (G_j x_j).v_i + (G_i x_i).v_j
+        double c = q.w * v0[t];
+        c = fma(w.x, v1[t], c);
+        c = fma(w.y, v2[t], c);
+        c = fma(g0[t], w.z, c);
+        c = fma(g1[t], w.w, c);
+        c = fma(g2[t], vz, c);
+        const double cr2 = c * (r * r);
+        a[t][0] = fma(r, q.w, a[t][0]);
+        a[t][1] = fma(r, w.x, a[t][1]);
+        a[t][2] = fma(r, w.y, a[t][2]);
+        a[t][3] = fma(cr2, q.x, a[t][3]);
+        a[t][4] = fma(cr2, q.y, a[t][4]);
+        a[t][5] = fma(cr2, q.z, a[t][5]);
+        a[t][6] = fma(r, w.z, a[t][6]);
+        a[t][7] = fma(r, w.w, a[t][7]);
+        a[t][8] = fma(r, vz, a[t][8]);
       }
     }
   }
@@ -369,9 +387,9 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const AdjLaunch P) {
   }
 }
 
-// Row-pass combination: g_x = -(S1 x ut + C + G P)/(4 pi), g_zeta = -A R/(4 pi),
+// Row-pass combination: g_x = -(S1 x ut + C + G P)/(4 pi), g_zeta = -A (x . P)/(4 pi),
 // from `chunks` partial blocks of kRowSums rows each, added in chunk order.
-__global__ void adj_combine_row_kernel(const double* __restrict__ ut,
+__global__ void adj_combine_row_kernel(const double* __restrict__ x, const double* __restrict__ ut,
                                        const double* __restrict__ zeta,
                                        const double* __restrict__ area, int n,
                                        const double* __restrict__ p, int chunks,
@@ -390,10 +408,11 @@ __global__ void adj_combine_row_kernel(const double* __restrict__ ut,
   const double g0 = (s[1] * u2 - s[2] * u1) + s[3] + G * s[6];
   const double g1 = (s[2] * u0 - s[0] * u2) + s[4] + G * s[7];
   const double g2 = (s[0] * u1 - s[1] * u0) + s[5] + G * s[8];
+  const double R = x[b] * s[6] + x[b + 1] * s[7] + x[b + 2] * s[8];
   out_x[b] = -kInv4Pi * g0;
   out_x[b + 1] = -kInv4Pi * g1;
   out_x[b + 2] = -kInv4Pi * g2;
-  out_z[i] = -kInv4Pi * area[i] * s[9];
+  out_z[i] = -kInv4Pi * area[i] * R;
 }
 
 // v_i = ut_i x x_i with ut_i = mu_x,i + (-2 Omega mu_z,i) z_hat, mu = dt * l_k.
@@ -402,7 +421,8 @@ __global__ void adj_prepare_kernel(const double* __restrict__ x, const double* _
                                    const double* __restrict__ area, int n, double dt, double m2omega,
                                    double* __restrict__ ut, double* __restrict__ v,
                                    double4* __restrict__ src1, double4* __restrict__ src2a,
-                                   double2* __restrict__ src2b, double4* __restrict__ vrow) {
+                                   double2* __restrict__ src2b, double4* __restrict__ ra,
+                                   double4* __restrict__ rb, double* __restrict__ rc) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t b = 3 * (size_t)i;
@@ -416,10 +436,13 @@ __global__ void adj_prepare_kernel(const double* __restrict__ x, const double* _
   v[b] = v0;
   v[b + 1] = v1;
   v[b + 2] = v2;
-  src1[i] = make_double4(x0, x1, x2, zeta[i] * area[i]);
+  const double G = zeta[i] * area[i];
+  src1[i] = make_double4(x0, x1, x2, G);
   src2a[i] = make_double4(x0, x1, x2, v0);
   src2b[i] = make_double2(v1, v2);
-  vrow[i] = make_double4(v0, v1, v2, 0.0);
+  ra[i] = make_double4(x0, x1, x2, G * x0);
+  rb[i] = make_double4(G * x1, G * x2, v0, v1);
+  rc[i] = v2;
 }
 
 // lY_i = J(Y)^T mu: gx (3 per row) and gz (1 per row), written to out_x/out_z.
@@ -471,7 +494,7 @@ struct AdjWork {
   DevBuf ck;        // checkpoints: ncheck x (3nA + nA)
   DevBuf ys;        // stage inputs of one segment: (steps*4) x (3nA + nA)
   DevBuf lam, lk, tmp;  // adjoint state, lk, accumulators (4nA each)
-  DevBuf ut, v, s1, s2a, s2b, vrow, p1, p2;
+  DevBuf ut, v, s1, s2a, s2b, ra, rb, rc, p1, p2;
 };
 
 int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, double dt,
@@ -485,7 +508,7 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
   tcb::adj_prepare_kernel<<<blocks, threads, 0, ctx->stream>>>(
       yx, lk, lk + 3 * (size_t)n, yz, area, n, dt, -2.0 * ctx->omega, W.ut.as<double>(),
       W.v.as<double>(), W.s1.as<double4>(), W.s2a.as<double4>(), W.s2b.as<double2>(),
-      W.vrow.as<double4>());
+      W.ra.as<double4>(), W.rb.as<double4>(), W.rc.as<double>());
   TC_CUDA_TRY(cudaGetLastError());
   int rc;
   const double d = ctx->delta[TC_ACTIVE];
@@ -526,8 +549,8 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
     chunk = (chunk + tcb::kRTS - 1) / tcb::kRTS * tcb::kRTS;
     S = (n + chunk - 1) / chunk;
     if ((rc = W.p1.ensure((size_t)S * tcb::kRowSums * n * sizeof(double)))) return rc;
-    tcb::AdjLaunch R{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), W.vrow.as<double4>(), n,
-                     chunk, 1.0 + d * d, W.p1.as<double>()};
+    tcb::RowLaunch R{W.ra.as<double4>(), W.rb.as<double4>(), W.rc.as<double>(), n, chunk,
+                     1.0 + d * d, W.p1.as<double>()};
     const dim3 grid(tiles, S);
     if (tpt == 1 && newton == 2)
       tcb::adj_row_kernel<1, 2, 2><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
@@ -539,7 +562,7 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
       tcb::adj_row_kernel<2, 1, 1><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
     TC_CUDA_TRY(cudaGetLastError());
     tcb::adj_combine_row_kernel<<<blocks, threads, 0, ctx->stream>>>(
-        W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, out, out + 3 * (size_t)n);
+        yx, W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, out, out + 3 * (size_t)n);
     TC_CUDA_TRY(cudaGetLastError());
     ctx->launches += 3;
     ctx->pair_launches += 1;
@@ -577,11 +600,11 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
     if ((rc = W.p1.ensure((size_t)S * 6 * n * sizeof(double))) ||
         (rc = W.p2.ensure((size_t)S * 7 * n * sizeof(double))))
       return rc;
-    tcb::AdjLaunch P1{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), nullptr, n, chunk,
-                      1.0 + d * d, W.p1.as<double>()};
+    tcb::AdjLaunch P1{yx, W.s1.as<double4>(), nullptr, W.v.as<double>(), n, chunk, 1.0 + d * d,
+                      W.p1.as<double>()};
     tcb::adj_target_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P1);
     TC_CUDA_TRY(cudaGetLastError());
-    tcb::AdjLaunch P2{yx, W.s2a.as<double4>(), W.s2b.as<double2>(), nullptr, nullptr, n, chunk,
+    tcb::AdjLaunch P2{yx, W.s2a.as<double4>(), W.s2b.as<double2>(), nullptr, n, chunk,
                       1.0 + d * d, W.p2.as<double>()};
     tcb::adj_source_kernel<<<dim3(tiles, S), tcb::kAdjNT, 0, ctx->stream>>>(P2);
     TC_CUDA_TRY(cudaGetLastError());
@@ -704,7 +727,9 @@ int adjoint_impl(tc_ctx* ctx, const double* xA0, const double* zetaA0, const dou
       (rc = W.s1.ensure((size_t)nA * sizeof(double4))) ||
       (rc = W.s2a.ensure((size_t)nA * sizeof(double4))) ||
       (rc = W.s2b.ensure((size_t)nA * sizeof(double2))) ||
-      (rc = W.vrow.ensure((size_t)nA * sizeof(double4))))
+      (rc = W.ra.ensure((size_t)nA * sizeof(double4))) ||
+      (rc = W.rb.ensure((size_t)nA * sizeof(double4))) ||
+      (rc = W.rc.ensure((size_t)nA * sizeof(double))))
     return rc;
   double* ck = W.ck.as<double>();
   double* ys = W.ys.as<double>();

@@ -99,7 +99,7 @@ struct tc_ctx {
   int var64 = 2, var32 = 19;  // pair-kernel variants in use (see kVariants64/32)
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
-  int adj_mode = 5;  // adjoint VJP: 3-6 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
+  int adj_mode = 6;  // adjoint VJP: 3-6 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
   tcb::DevBuf order_buf[4];             // keys, sorted keys, indices, sort scratch
   int min_chunk = 256;    // smallest source chunk a CTA walks (one shared-memory tile)
   int max_chunks = 64;
