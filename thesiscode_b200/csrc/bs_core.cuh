@@ -224,6 +224,13 @@ constexpr float kSelfBias = 1e-30f;
 // near form; the self pair never qualifies (|s_self| = |t_self| <= rho).
 // Paired reciprocal (FM bit 1): the two targets of an f32x2 lane pair share
 // one MUFU reciprocal q = 1/(D_a D_b): 1/D_a = q D_b, 1/D_b = q D_a.
+// Pre-weighted sources (FM bit 2, with bit 0): each source tile also holds
+// G_k s_k and G_k (G_k s_k from the FP64 offset, rounded once), so a far
+// pair accumulates r = 1/(D/2) directly into sum r G s_k and sum r G: the
+// weight multiply leaves the loop and a far pair costs 8 FP32 operations
+// (4 denominator, 4 accumulations) plus the MUFU reciprocal, which balances
+// the FMA pipe (2 cycles per f32x2 warp instruction) against the XU pipe
+// (8 cycles per warp MUFU): 16 cycles each per warp and source.
 constexpr float kFarRatio2 = 9.0f;  // kFarRatio = 3
 
 template <bool PR>
@@ -264,15 +271,18 @@ __device__ __forceinline__ float combine_max(const unsigned* red) {
   return __uint_as_float(m);
 }
 
-// Shared memory of one FP32C unit.
-template <int NT, int TS>
+// Shared memory of one FP32C unit. PW (pre-weighted far form) changes b to
+// (sz, sz, A_k, A_k) and adds c, d; h is then unused.
+template <int NT, int TS, bool PW = false>
 struct Fp32cSmem {
-  float4 a[TS];           // (sx, sx, sy, sy)
-  float4 b[TS];           // (sz, sz, 2G, 2G)
-  float2 e[TS];           // near form: (e_k, e_k)
-  float2 h[TS];           // far form: (A_k, A_k)
-  unsigned tmin[NT / 32]; // per-warp min of |s_k|^2 over the tile
-  unsigned rho[NT / 32];  // per-warp max of |t_i|^2 over the CTA's targets
+  float4 a[TS];              // (sx, sx, sy, sy)
+  float4 b[TS];              // (sz, sz, 2G, 2G); PW: (sz, sz, A_k, A_k)
+  float2 e[TS];              // near form: (e_k, e_k)
+  float2 h[PW ? 1 : TS];     // far form: (A_k, A_k)
+  float4 c[PW ? TS : 1];     // PW: (G sx, G sx, G sy, G sy)
+  float4 d[PW ? TS : 1];     // PW: (G sz, G sz, G, G)
+  unsigned tmin[NT / 32];    // per-warp min of |s_k|^2 over the tile
+  unsigned rho[NT / 32];     // per-warp max of |t_i|^2 over the CTA's targets
 };
 
 // One work unit (targets at visiting positions [tile0, min(tile0 + NT*2*NPAIR,
@@ -282,13 +292,16 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
                                            int tile0, int i_end, double d2,
                                            const double4* __restrict__ src, int c0, int c1,
                                            double* __restrict__ out, size_t stride,
-                                           Fp32cSmem<NT, TS>& sm) {
+                                           Fp32cSmem<NT, TS, (FM & 4) != 0>& sm) {
   static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
   static_assert(NT % 32 == 0, "whole warps");
   constexpr int TPT = 2 * NPAIR;
   constexpr int TB = NT * TPT;
   constexpr bool FAR = (FM & 1) != 0;
   constexpr bool PR = (FM & 2) != 0;
+  constexpr bool PW = FAR && (FM & 4) != 0;
+  // PW tiles hold G (not 2G): near-form sums come out halved
+  constexpr double kNearScale = PW ? 2.0 : 1.0;
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
   const int mid = perm ? perm[mid_pos] : mid_pos;
@@ -332,12 +345,19 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
     for (int j = threadIdx.x; j < TS; j += NT) {
       int k = ts + j;
       float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f, ah = 1.f;
+      float gsx = 0.f, gsy = 0.f, gsz = 0.f;
       if (k < c1) {
         const double4 q = src[k];
-        sx = (float)(q.x - cx);
-        sy = (float)(q.y - cy);
-        sz = (float)(q.z - cz);
-        g = (float)(2.0 * q.w);
+        const double dx = q.x - cx, dy = q.y - cy, dz = q.z - cz;
+        sx = (float)dx;
+        sy = (float)dy;
+        sz = (float)dz;
+        g = (float)(PW ? q.w : 2.0 * q.w);
+        if (PW) {
+          gsx = (float)(q.w * dx);
+          gsy = (float)(q.w * dy);
+          gsz = (float)(q.w * dz);
+        }
         const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
         e = (float)ek;
         if (FAR) {
@@ -347,15 +367,59 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
         }
       }
       sm.a[j] = make_float4(sx, sx, sy, sy);
-      sm.b[j] = make_float4(sz, sz, g, g);
       sm.e[j] = make_float2(e, e);
-      if (FAR) sm.h[j] = make_float2(ah, ah);
+      if (PW) {
+        sm.b[j] = make_float4(sz, sz, ah, ah);
+        sm.c[j] = make_float4(gsx, gsx, gsy, gsy);
+        sm.d[j] = make_float4(gsz, gsz, g, g);
+      } else {
+        sm.b[j] = make_float4(sz, sz, g, g);
+        if (FAR) sm.h[j] = make_float2(ah, ah);
+      }
     }
     if (FAR) warp_store_min(smin, sm.tmin);
     __syncthreads();
     // strict: with rho = 0 (one target position) no tile is far
     const bool far = FAR && combine_min<NT / 32>(sm.tmin) > kFarRatio2 * combine_max<NT / 32>(sm.rho);
-    if (far) {
+    if (PW && far) {
+      for (int jf = 0; jf < TS; jf += FLUSH) {
+#pragma unroll UNROLL
+        for (int j = jf; j < jf + FLUSH; ++j) {
+          const float4 a = sm.a[j];
+          const float4 b = sm.b[j];
+          const float4 c = sm.c[j];
+          const float4 d = sm.d[j];
+          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
+          const float2 szz = make_float2(b.x, b.y), ah = make_float2(b.z, b.w);
+          const float2 gsx = make_float2(c.x, c.y), gsy = make_float2(c.z, c.w);
+          const float2 gsz = make_float2(d.x, d.y), gg = make_float2(d.z, d.w);
+#pragma unroll
+          for (int p = 0; p < NPAIR; ++p) {
+            float2 D = __fadd2_rn(ah, bh[p]);
+            D = __ffma2_rn(sxx, ntx[p], D);
+            D = __ffma2_rn(syy, nty[p], D);
+            D = __ffma2_rn(szz, ntz[p], D);
+            const float2 r = rcp_pair<PR>(D);  // 1 / (1 - x_i.x_k + delta^2)
+            fx[p] = __ffma2_rn(r, gsx, fx[p]);
+            fy[p] = __ffma2_rn(r, gsy, fy[p]);
+            fz[p] = __ffma2_rn(r, gsz, fz[p]);
+            fw[p] = __ffma2_rn(r, gg, fw[p]);
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < NPAIR; ++p) {
+          ax[p][0] += (double)fx[p].x;
+          ax[p][1] += (double)fx[p].y;
+          ay[p][0] += (double)fy[p].x;
+          ay[p][1] += (double)fy[p].y;
+          az[p][0] += (double)fz[p].x;
+          az[p][1] += (double)fz[p].y;
+          aw[p][0] += (double)fw[p].x;
+          aw[p][1] += (double)fw[p].y;
+          fx[p] = fy[p] = fz[p] = fw[p] = make_float2(0.f, 0.f);
+        }
+      }
+    } else if (far) {
       for (int jf = 0; jf < TS; jf += FLUSH) {
 #pragma unroll UNROLL
         for (int j = jf; j < jf + FLUSH; ++j) {
@@ -398,7 +462,8 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
           const float4 b = sm.b[j];
           const float2 ee = sm.e[j];
           const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
+          const float2 szz = make_float2(b.x, b.y);
+          const float2 gg = PW ? make_float2(sm.d[j].z, sm.d[j].w) : make_float2(b.z, b.w);
 #pragma unroll
           for (int p = 0; p < NPAIR; ++p) {
             const float2 dx = __fadd2_rn(sxx, ntx[p]);
@@ -416,12 +481,12 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
         }
 #pragma unroll
         for (int p = 0; p < NPAIR; ++p) {
-          ax[p][0] += (double)fx[p].x;
-          ax[p][1] += (double)fx[p].y;
-          ay[p][0] += (double)fy[p].x;
-          ay[p][1] += (double)fy[p].y;
-          az[p][0] += (double)fz[p].x;
-          az[p][1] += (double)fz[p].y;
+          ax[p][0] = fma(kNearScale, (double)fx[p].x, ax[p][0]);
+          ax[p][1] = fma(kNearScale, (double)fx[p].y, ax[p][1]);
+          ay[p][0] = fma(kNearScale, (double)fy[p].x, ay[p][0]);
+          ay[p][1] = fma(kNearScale, (double)fy[p].y, ay[p][1]);
+          az[p][0] = fma(kNearScale, (double)fz[p].x, az[p][0]);
+          az[p][1] = fma(kNearScale, (double)fz[p].y, az[p][1]);
           fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
         }
       }
@@ -450,17 +515,290 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 }
 
 
+// ---------------------------------------------------------------------------
+// FP32C, source-paired form (FM bit 3). The f32x2 lanes of each instruction
+// carry two SOURCES (k, k+1) for one target instead of one source for two
+// targets, so a source tile sits in shared memory without duplicated values:
+// a broadcast 128-bit shared load costs two wavefronts of the SM-wide shared
+// pipe (one wavefront per clock), and the target-paired layout spent 5-8
+// wavefronts per source on duplicates; here a far source pair costs 7 (3.5
+// per source), shared by the T targets of a thread.
+//
+// Coordinates are taken in a per-CTA orthonormal frame R = (e1, e2, e3) with
+// e3 along the origin c (the CTA's middle target): s_k = R(x_k - c),
+// t_i = R(x_i - c), both from FP64 and rounded once. Distances and dot
+// products are frame-invariant, so the near form and the far denominator are
+// those of the target-paired kernel. The far numerator accumulates
+//     T' = sum_k r_ik G_k x'_k,   x'_k = R x_k,   r = 1/(1 - x_i.x_k + delta^2),
+// three sums instead of four. In this frame the first two coordinates of
+// x'_k are e1.(x_k - c) and e2.(x_k - c) (small for nearby sources) and the
+// third is e3.x_k (about 1), so the large common part of the sum (about
+// sum r G) sits in the third coordinate only; u_i = x_i x R^T T' multiplies
+// that coordinate by the target's own small offset (e1, e2 components of
+// x_i), so its rounding costs what the separate sum r G of the
+// target-paired far form costs. A far pair is then 7 FP32
+// operations (4 denominator, 3 accumulations) and one MUFU reciprocal.
+// PRF > 0: one source pair of every PRF shares a single MUFU reciprocal
+// (1/D_k = q D_k+1, 1/D_k+1 = q D_k, q = 1/(D_k D_k+1)), trading 8 XU cycles
+// for 3 FMA-pipe cycles per warp and target, so the FMA and XU pipes carry
+// equal loads. Partial sums stay in the rotated frame (near and far tiles
+// add into the same accumulators: near T'= sum w (x'_k - x'_i), far
+// sum w x'_k; they differ by multiples of x'_i, which u = x_i x T ignores)
+// and are rotated back in FP64 once per target.
+// ---------------------------------------------------------------------------
+template <int NT, int TS>
+struct SpSmem {
+  float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
+  float4 b[TS / 2];        // (sz_k, sz_k+1, A_k, A_k+1)
+  float4 c[TS / 2];        // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
+  float2 d[TS / 2];        // (G z'_k, G z'_k+1)
+  float4 n[TS / 2];        // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
+  double frame[12];        // e1, e2, e3 (rows), origin c
+  unsigned tmin[NT / 32];
+  unsigned rho[NT / 32];
+};
+
+// Orthonormal basis with e3 = c/|c| (Duff, Burgess, Christensen, Hart, Kensler,
+// Liani, Pharr, "Building an Orthonormal Basis, Revisited", JCGT 6(1), 2017).
+__device__ __forceinline__ void make_frame(double cx, double cy, double cz, double* f) {
+  const double inv = rsqrt(fma(cx, cx, fma(cy, cy, cz * cz)));
+  const double nx = cx * inv, ny = cy * inv, nz = cz * inv;
+  const double sg = copysign(1.0, nz);
+  const double a = -1.0 / (sg + nz);
+  const double b = nx * ny * a;
+  f[0] = 1.0 + sg * nx * nx * a;
+  f[1] = sg * b;
+  f[2] = -sg * nx;
+  f[3] = b;
+  f[4] = sg + ny * ny * a;
+  f[5] = -ny;
+  f[6] = nx;
+  f[7] = ny;
+  f[8] = nz;
+}
+
+// R v with explicitly fused operations, so a target and the same point as a
+// source round identically (the self pair then has d = 0 exactly).
+__device__ __forceinline__ double frame_dot(const double* e, double vx, double vy, double vz) {
+  return fma(e[0], vx, fma(e[1], vy, __dmul_rn(e[2], vz)));
+}
+
+template <bool PAIRED>
+__device__ __forceinline__ float2 rcp_sources(float2 D) {
+  if (PAIRED) {
+    const float q = rcp_approx_f32(__fmul_rn(D.x, D.y));
+    return __fmul2_rn(make_float2(q, q), make_float2(D.y, D.x));
+  }
+  return make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
+}
+
+// One far source pair against the thread's T targets.
+template <int T, bool PAIRED>
+__device__ __forceinline__ void sp_far_step(const float4 a, const float4 b, const float4 c,
+                                            const float2 d, const float2* ntx, const float2* nty,
+                                            const float2* ntz, const float2* bh, float2* fx,
+                                            float2* fy, float2* fz) {
+  const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w);
+  const float2 sz = make_float2(b.x, b.y), ah = make_float2(b.z, b.w);
+  const float2 gx = make_float2(c.x, c.y), gy = make_float2(c.z, c.w);
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    float2 D = __fadd2_rn(ah, bh[t]);
+    D = __ffma2_rn(sx, ntx[t], D);
+    D = __ffma2_rn(sy, nty[t], D);
+    D = __ffma2_rn(sz, ntz[t], D);
+    const float2 r = rcp_sources<PAIRED>(D);
+    fx[t] = __ffma2_rn(r, gx, fx[t]);
+    fy[t] = __ffma2_rn(r, gy, fy[t]);
+    fz[t] = __ffma2_rn(r, d, fz[t]);
+  }
+}
+
+template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF>
+__device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
+                                              int tile0, int i_end, double d2,
+                                              const double4* __restrict__ src, int c0, int c1,
+                                              double* __restrict__ out, size_t stride,
+                                              SpSmem<NT, TS>& sm) {
+  static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
+  static_assert(PRF == 0 || (FLUSH / 2) % PRF == 0, "paired-reciprocal period divides the flush");
+  static_assert(NT % 32 == 0, "whole warps");
+  constexpr int TB = NT * T;
+  constexpr int NP = TS / 2;
+  constexpr int FP = FLUSH / 2;
+  constexpr int GRP = PRF > 0 ? PRF : 1;  // source pairs per group; the first is paired
+
+  const int mid_pos = min(tile0 + TB / 2, i_end - 1);
+  const int mid = perm ? perm[mid_pos] : mid_pos;
+  const double cx = x[3 * (size_t)mid], cy = x[3 * (size_t)mid + 1], cz = x[3 * (size_t)mid + 2];
+  __syncthreads();  // the previous unit (persistent kernel) is done with sm.frame
+  if (threadIdx.x == 0) {
+    make_frame(cx, cy, cz, sm.frame);
+    sm.frame[9] = cx;
+    sm.frame[10] = cy;
+    sm.frame[11] = cz;
+  }
+  __syncthreads();
+  const double* fr = sm.frame;
+
+  float2 ntx[T], nty[T], ntz[T], bh[T];
+  float ei[T];  // near form only: paired on use
+  float2 fx[T], fy[T], fz[T];
+  double ax[T], ay[T], az[T];
+  float rho2 = 0.f;
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int pos = tile0 + (int)threadIdx.x + t * NT;
+    const int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
+    const double px = x[3 * (size_t)ld], py = x[3 * (size_t)ld + 1], pz = x[3 * (size_t)ld + 2];
+    const double dx = px - cx, dy = py - cy, dz = pz - cz;
+    const float tx = (float)frame_dot(fr, dx, dy, dz);
+    const float ty = (float)frame_dot(fr + 3, dx, dy, dz);
+    const float tz = (float)frame_dot(fr + 6, dx, dy, dz);
+    const double E = (1.0 - (px * px + py * py + pz * pz)) + 2.0 * d2;
+    ntx[t] = make_float2(-tx, -tx);
+    nty[t] = make_float2(-ty, -ty);
+    ntz[t] = make_float2(-tz, -tz);
+    ei[t] = (float)E + kSelfBias;
+    const float t2 = norm2_f32(tx, ty, tz);
+    const float b = (float)(0.5 * ((double)t2 + E));
+    bh[t] = make_float2(b, b);
+    rho2 = fmaxf(rho2, t2);
+    fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
+    ax[t] = ay[t] = az[t] = 0.0;
+  }
+  warp_store_max(rho2, sm.rho);
+
+  for (int ts = c0; ts < c1; ts += TS) {
+    __syncthreads();
+    float smin = __int_as_float(0x7f800000);  // +inf
+    for (int jp = threadIdx.x; jp < NP; jp += NT) {
+      float v[2][9];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = ts + 2 * jp + h;
+        // padding sources: zero weight, unit denominators
+        v[h][0] = v[h][1] = v[h][2] = 0.f;
+        v[h][3] = 1.f;
+        v[h][4] = v[h][5] = v[h][6] = 0.f;
+        v[h][7] = 1.f;
+        v[h][8] = 0.f;
+        if (k < c1) {
+          const double4 q = src[k];
+          const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
+          const float sx = (float)frame_dot(fr, dx, dy, dz);
+          const float sy = (float)frame_dot(fr + 3, dx, dy, dz);
+          const float sz = (float)frame_dot(fr + 6, dx, dy, dz);
+          const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
+          const float s2 = norm2_f32(sx, sy, sz);
+          smin = fminf(smin, s2);
+          v[h][0] = sx;
+          v[h][1] = sy;
+          v[h][2] = sz;
+          v[h][3] = (float)(0.5 * ((double)s2 + ek));
+          v[h][4] = (float)(q.w * frame_dot(fr, q.x, q.y, q.z));
+          v[h][5] = (float)(q.w * frame_dot(fr + 3, q.x, q.y, q.z));
+          v[h][6] = (float)(q.w * frame_dot(fr + 6, q.x, q.y, q.z));
+          v[h][7] = (float)ek;
+          v[h][8] = (float)(2.0 * q.w);
+        }
+      }
+      sm.a[jp] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+      sm.b[jp] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
+      sm.c[jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
+      sm.d[jp] = make_float2(v[0][6], v[1][6]);
+      sm.n[jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
+    }
+    warp_store_min(smin, sm.tmin);
+    __syncthreads();
+    const bool far = combine_min<NT / 32>(sm.tmin) > kFarRatio2 * combine_max<NT / 32>(sm.rho);
+    if (far) {
+      for (int jf = 0; jf < NP; jf += FP) {
+#pragma unroll UNROLL
+        for (int jg = jf; jg < jf + FP; jg += GRP) {
+#pragma unroll
+          for (int u = 0; u < GRP; ++u) {
+            const int j = jg + u;
+            if (PRF > 0 && u == 0)
+              sp_far_step<T, true>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
+            else
+              sp_far_step<T, false>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+          ax[t] += (double)__fadd_rn(fx[t].x, fx[t].y);
+          ay[t] += (double)__fadd_rn(fy[t].x, fy[t].y);
+          az[t] += (double)__fadd_rn(fz[t].x, fz[t].y);
+          fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
+        }
+      }
+    } else {
+      for (int jf = 0; jf < NP; jf += FP) {
+#pragma unroll 4
+        for (int j = jf; j < jf + FP; ++j) {
+          const float4 a = sm.a[j];
+          const float4 b = sm.b[j];
+          const float4 n = sm.n[j];
+          const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w);
+          const float2 sz = make_float2(b.x, b.y);
+          const float2 ee = make_float2(n.x, n.y), gg = make_float2(n.z, n.w);
+#pragma unroll
+          for (int t = 0; t < T; ++t) {
+            const float2 dx = __fadd2_rn(sx, ntx[t]);
+            const float2 dy = __fadd2_rn(sy, nty[t]);
+            const float2 dz = __fadd2_rn(sz, ntz[t]);
+            float2 D = __fadd2_rn(ee, make_float2(ei[t], ei[t]));
+            D = __ffma2_rn(dx, dx, D);
+            D = __ffma2_rn(dy, dy, D);
+            D = __ffma2_rn(dz, dz, D);
+            const float2 w = __fmul2_rn(gg, rcp_sources<false>(D));
+            fx[t] = __ffma2_rn(w, dx, fx[t]);
+            fy[t] = __ffma2_rn(w, dy, fy[t]);
+            fz[t] = __ffma2_rn(w, dz, fz[t]);
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+          ax[t] += (double)__fadd_rn(fx[t].x, fx[t].y);
+          ay[t] += (double)__fadd_rn(fy[t].x, fy[t].y);
+          az[t] += (double)__fadd_rn(fz[t].x, fz[t].y);
+          fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+  }
+  // back to the global frame: T = R^T T'
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int pos = tile0 + (int)threadIdx.x + t * NT;
+    if (pos < i_end) {
+      out[pos] = fma(fr[0], ax[t], fma(fr[3], ay[t], fr[6] * az[t]));
+      out[stride + pos] = fma(fr[1], ax[t], fma(fr[4], ay[t], fr[7] * az[t]));
+      out[2 * stride + pos] = fma(fr[2], ax[t], fma(fr[5], ay[t], fr[8] * az[t]));
+    }
+  }
+}
+
 template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
-  __shared__ Fp32cSmem<NT, TS> sm;
+  // FM bit 3: source-paired form, NPAIR = targets per thread
+  constexpr bool SP = (FM & 8) != 0;
   const TargetSeg& G = find_seg(P, blockIdx.x);
-  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * 2 * NPAIR);
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * (SP ? NPAIR : 2 * NPAIR));
   const int c0 = (int)blockIdx.y * P.chunk_len;
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-  fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
-                                               stride, sm);
+  if constexpr (SP) {
+    __shared__ SpSmem<NT, TS> sm;
+    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4)>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0,
+                                                           c1, out, stride, sm);
+  } else {
+    __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
+    fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
+                                                 stride, sm);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -505,14 +843,25 @@ __device__ __forceinline__ int next_item(int* counter, int* slot) {
 
 template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
-  __shared__ Fp32cSmem<NT, TS> sm;
   __shared__ int slot;
-  for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
-    const BatchItem I = B.items[it];
-    const BatchSeg S = B.segs[I.seg];
-    double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0,
-                                                 I.c1, out, B.stride, sm);
+  if constexpr ((FM & 8) != 0) {
+    __shared__ SpSmem<NT, TS> sm;
+    for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
+      const BatchItem I = B.items[it];
+      const BatchSeg S = B.segs[I.seg];
+      double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4)>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src,
+                                                             I.c0, I.c1, out, B.stride, sm);
+    }
+  } else {
+    __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
+    for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
+      const BatchItem I = B.items[it];
+      const BatchSeg S = B.segs[I.seg];
+      double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+      fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0,
+                                                   I.c1, out, B.stride, sm);
+    }
   }
 }
 

@@ -71,14 +71,26 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
                 launch32b<NT, NPAIR, FLUSH, MINB, UNROLL, FM>,                               \
                 (const void*)pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM>, FM }
 
+// Source-paired FP32C form: T targets per thread, UNROLL groups of PRF source
+// pairs (one paired reciprocal per group; PRF 0: none) per unrolled body.
+#define VSP(NT, T, FLUSH, MINB, UNROLL, PRF) \
+  PairVariant { TC_FP32C, NT, T, kTS, FLUSH, MINB, UNROLL, \
+                launch32<NT, T, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
+                (const void*)pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
+                launch32b<NT, T, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
+                (const void*)pair_fp32c_batch_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
+                8 | (PRF << 4) }
+
 // FP64: the `flush` field records the denominator mode (1 = fused, 0 =
 // rounded exactly like the reference).
 const PairVariant kVariants64[] = {
     V64(256, 2, 5, true),  V64(256, 4, 2, true),  V64(256, 1, 6, true), V64(128, 4, 4, true),
     V64(256, 2, 5, false), V64(256, 4, 2, false),
 };
-// FP32C: the last field selects the far-field form (1), the paired
-// reciprocal (2), or both (3).
+// FP32C: the last field is a bit set: far-field form (1), paired
+// reciprocal (2), pre-weighted far-field sources (4, with 1), source-paired
+// rotated-frame form (8, its own far/near forms; bits 4+ the period of the
+// paired reciprocal).
 const PairVariant kVariants32[] = {
     V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
     V32(256, 2, 16, 2, 4, 0), V32(128, 2, 32, 6, 4, 0), V32(256, 1, 32, 4, 8, 0),
@@ -89,6 +101,14 @@ const PairVariant kVariants32[] = {
     V32(64, 1, 32, 12, 8, 1), V32(128, 1, 64, 6, 8, 1), V32(128, 1, 32, 7, 8, 1),
     V32(256, 1, 32, 3, 8, 1), V32(128, 1, 128, 6, 8, 1), V32(128, 1, 64, 8, 8, 1),
     V32(128, 1, 64, 6, 16, 1),
+    // pre-weighted far form (bit 2): 8 FP32 operations per far pair
+    V32(128, 1, 64, 6, 8, 5), V32(128, 2, 64, 4, 8, 5), V32(128, 2, 64, 5, 4, 5),
+    V32(128, 1, 128, 6, 8, 5), V32(128, 1, 64, 8, 8, 5), V32(256, 1, 64, 3, 8, 5),
+    V32(128, 2, 128, 4, 8, 5),
+    // source-paired form (bit 3; bits 4+: paired-reciprocal period)
+    VSP(128, 2, 64, 6, 2, 4), VSP(128, 2, 64, 6, 4, 0), VSP(128, 4, 64, 4, 2, 4),
+    VSP(128, 4, 64, 4, 1, 4), VSP(128, 3, 64, 5, 2, 4), VSP(128, 2, 64, 8, 2, 4),
+    VSP(256, 2, 64, 3, 2, 4), VSP(128, 4, 64, 4, 4, 0), VSP(128, 2, 64, 6, 1, 8),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);

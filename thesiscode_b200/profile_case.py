@@ -1,7 +1,7 @@
 """One launch of the pair kernels on a workload of a chosen size, for profilers.
 
     python -m thesiscode_b200.profile_case --precision fp32c --level 6 \
-        [--what velocity|rk4|adjoint|batch|strat]
+        [--what velocity|rk4|adjoint|batch|strat] [--variant ID]
 
 `velocity` runs one TC_ACTIVE and one TC_VERTEX sum (two pair-kernel launches);
 `rk4` runs one fused RK4 step (four pair-kernel launches); `adjoint` runs the
@@ -10,6 +10,8 @@ runs one RK4 step of the 64-instance Gaussian ensemble (levels 3 to `--level`)
 without autotuning or graph (four persistent batch-kernel launches); `strat`
 runs one forced stratosphere RK4 step (parity mode). The Gaussian-vortex
 workload with delta 0.01 is used at every level for the first three.
+`--variant` selects a pair-kernel variant of the chosen precision (default:
+the library's default) for `velocity` and `rk4`.
 """
 from __future__ import annotations
 
@@ -25,6 +27,7 @@ def main() -> None:
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--level", type=int, default=6)
     ap.add_argument("--what", default="velocity", choices=["velocity", "rk4", "adjoint", "batch", "strat"])
+    ap.add_argument("--variant", type=int, default=None)
     a = ap.parse_args()
     if a.what in ("batch", "strat"):
         ctx = Context(0, a.precision)
@@ -49,6 +52,8 @@ def main() -> None:
     ctx = Context(0, a.precision)
     ctx.set_omega(w.omega)
     ctx.set_deltas(*w.deltas)
+    if a.variant is not None:
+        N.call("tc_set_pair_variant", ctx.handle, N.TC_FP64 if a.precision == "fp64" else N.TC_FP32C, a.variant)
     if a.what == "velocity":
         ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
         ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
