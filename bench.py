@@ -120,8 +120,9 @@ class ClockSampler:
 def measured_peaks(device: int) -> dict:
     from thesiscode_b200 import _native as N
 
-    out = {}
-    for key, kind, iters in (("ffma", N.TC_PROBE_FFMA, 65536), ("dfma", N.TC_PROBE_DFMA, 32768)):
+    out = {}  # ffma, dfma: FMA/s; rcp32: MUFU reciprocals/s
+    for key, kind, iters in (("ffma", N.TC_PROBE_FFMA, 65536), ("dfma", N.TC_PROBE_DFMA, 32768),
+                             ("rcp32", N.TC_PROBE_RCP32, 16384)):
         best = 0.0
         for _ in range(3):
             v = ctypes.c_double()
@@ -438,6 +439,14 @@ def run_ours(args):
                      "flops_per_interaction": FLOPS_PER_INTERACTION,
                      "pair_ms_per_launch": pair_ms_launch,
                      "peak_source": "measured live: CUDA-core FMA probe (tc_probe_peak) x 2 flops"},
+        # FP32C executes one MUFU reciprocal per interaction (the XU pipe, 16 lanes per SM) beside
+        # 7-11 FP32 operations: the hardware bound of the pair kernel, next to the 22-flop count
+        "pipe_roofline": ({"pipe": "xu (MUFU rcp.approx.f32, one per interaction)",
+                           "achieved": main["pair_interactions"] / max(main["pair_ms"] * 1e-3, 1e-30),
+                           "peak": peaks["rcp32"], "unit": "reciprocals/s",
+                           "frac": main["pair_interactions"] / max(main["pair_ms"] * 1e-3, 1e-30) / peaks["rcp32"],
+                           "peak_source": "measured live: MUFU reciprocal probe (tc_probe_peak)"}
+                          if args.precision == "fp32c" else None),
         "gpu_launches": main["launches"],
         "gpu_launches_note": "the library's own kernels (pack, Hilbert keys, pair, stage epilogue, KE finalize); "
                              "each FP32C step also runs two CUB radix sorts (6 kernels each on this "

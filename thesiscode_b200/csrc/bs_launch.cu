@@ -109,6 +109,8 @@ const PairVariant kVariants32[] = {
     VSP(128, 2, 64, 6, 2, 4), VSP(128, 2, 64, 6, 4, 0), VSP(128, 4, 64, 4, 2, 4),
     VSP(128, 4, 64, 4, 1, 4), VSP(128, 3, 64, 5, 2, 4), VSP(128, 2, 64, 8, 2, 4),
     VSP(256, 2, 64, 3, 2, 4), VSP(128, 4, 64, 4, 4, 0), VSP(128, 2, 64, 6, 1, 8),
+    VSP(128, 2, 128, 6, 4, 0), VSP(128, 2, 64, 5, 4, 0), VSP(128, 2, 64, 6, 8, 0),
+    VSP(64, 2, 64, 12, 4, 0), VSP(128, 2, 128, 6, 8, 0), VSP(128, 2, 64, 5, 8, 0),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
