@@ -310,6 +310,16 @@ int tc_icos_grid_sizes(int level, int* n_particles, int* n_edges, int* n_panels,
 int tc_icos_grid(int level, double* particles_x, double* particles_x0, double* panels_x,
                  double* panels_x0, double* panels_area, int* panels_has_children,
                  int* panels_vertices, int* panels_nest, int* panels_children);
+/* The same grid generated on the GPU of ctx (no counterpart in the
+ * reference, whose generator runs on the host): every output is a device
+ * pointer on ctx's device, written on ctx's stream; the call returns when the
+ * grid is complete. Particle positions, panel centres and all index arrays
+ * equal tc_icos_grid's bit for bit; areas agree to a few ulps (CUDA's atan2
+ * and tan). particles_x, panels_x and panels_area are required. */
+int tc_icos_grid_device(tc_ctx* ctx, int level, double* particles_x, double* particles_x0,
+                        double* panels_x, double* panels_x0, double* panels_area,
+                        int* panels_has_children, int* panels_vertices, int* panels_nest,
+                        int* panels_children);
 /* GatherPanels index maps (:1556-1619), 0-based. */
 int tc_gather_maps(int n, const int* has_children, int* active_map, int n_active,
                    int* passive_map, int n_passive);

@@ -112,6 +112,7 @@ SIGNATURES: dict[str, tuple] = {
                          POINTER(ctypes.c_longlong), dp]),
     "tc_icos_grid_sizes": (c_int, [c_int, ip, ip, ip, ip]),
     "tc_icos_grid": (c_int, [c_int, dp, dp, dp, dp, dp, ip, ip, ip, ip]),
+    "tc_icos_grid_device": (c_int, [c_void_p, c_int] + [c_void_p] * 9),
     "tc_gather_maps": (c_int, [c_int, ip, ip, c_int, ip, c_int]),
 }
 

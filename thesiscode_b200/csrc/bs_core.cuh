@@ -538,6 +538,8 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // x_i), so its rounding costs what the separate sum r G of the
 // target-paired far form costs. A far pair is then 7 FP32
 // operations (4 denominator, 3 accumulations) and one MUFU reciprocal.
+// FM bit 0 (with bit 3): the FP64 flushes widen the FP32 partials with
+// integer operations (f2d_alu) instead of F2F conversions on the XU pipe.
 // PRF > 0: one source pair of every PRF shares a single MUFU reciprocal
 // (1/D_k = q D_k+1, 1/D_k+1 = q D_k, q = 1/(D_k D_k+1)), trading 8 XU cycles
 // for 3 FMA-pipe cycles per warp and target, so the FMA and XU pipes carry
@@ -586,10 +588,35 @@ __device__ __forceinline__ double frame_dot(const double* e, double vx, double v
 template <bool PAIRED>
 __device__ __forceinline__ float2 rcp_sources(float2 D) {
   if (PAIRED) {
+    // scalar products: no register-pair shuffles around the MUFU result
     const float q = rcp_approx_f32(__fmul_rn(D.x, D.y));
-    return __fmul2_rn(make_float2(q, q), make_float2(D.y, D.x));
+    return make_float2(__fmul_rn(q, D.y), __fmul_rn(q, D.x));
   }
   return make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
+}
+
+// float -> double with integer operations (the ALU pipe) instead of an F2F
+// conversion (the XU pipe, which the MUFU reciprocals keep busy): exponent
+// rebiased by 1023 - 127, mantissa shifted into place; +-0 and FP32
+// subnormals give +-0, Inf and NaN stay Inf and NaN.
+__device__ __forceinline__ double f2d_alu(float f) {
+  const unsigned b = __float_as_uint(f);
+  const unsigned sign = b & 0x80000000u;
+  const unsigned mag = b & 0x7fffffffu;
+  unsigned hi = sign | ((mag >> 3) + (896u << 20));
+  unsigned lo = b << 29;
+  if (mag >= 0x7f800000u) hi |= 0x7ff00000u;
+  if (mag < 0x00800000u) {
+    hi = sign;
+    lo = 0u;
+  }
+  return __hiloint2double((int)hi, (int)lo);
+}
+
+template <bool ALU>
+__device__ __forceinline__ double widen(float f) {
+  if (ALU) return f2d_alu(f);
+  return (double)f;
 }
 
 // One far source pair against the thread's T targets.
@@ -614,7 +641,7 @@ __device__ __forceinline__ void sp_far_step(const float4 a, const float4 b, cons
   }
 }
 
-template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF>
+template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
@@ -727,9 +754,9 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         }
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-          ax[t] += (double)__fadd_rn(fx[t].x, fx[t].y);
-          ay[t] += (double)__fadd_rn(fy[t].x, fy[t].y);
-          az[t] += (double)__fadd_rn(fz[t].x, fz[t].y);
+          ax[t] += widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y));
+          ay[t] += widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y));
+          az[t] += widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y));
           fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
         }
       }
@@ -760,9 +787,9 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         }
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-          ax[t] += (double)__fadd_rn(fx[t].x, fx[t].y);
-          ay[t] += (double)__fadd_rn(fy[t].x, fy[t].y);
-          az[t] += (double)__fadd_rn(fz[t].x, fz[t].y);
+          ax[t] += widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y));
+          ay[t] += widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y));
+          az[t] += widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y));
           fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
         }
       }
@@ -792,7 +819,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
   if constexpr (SP) {
     __shared__ SpSmem<NT, TS> sm;
-    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4)>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0,
+    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0,
                                                            c1, out, stride, sm);
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
@@ -850,7 +877,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchL
       const BatchItem I = B.items[it];
       const BatchSeg S = B.segs[I.seg];
       double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4)>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src,
+      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src,
                                                              I.c0, I.c1, out, B.stride, sm);
     }
   } else {

@@ -73,13 +73,15 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
 
 // Source-paired FP32C form: T targets per thread, UNROLL groups of PRF source
 // pairs (one paired reciprocal per group; PRF 0: none) per unrolled body.
-#define VSP(NT, T, FLUSH, MINB, UNROLL, PRF) \
+#define VSPX(NT, T, FLUSH, MINB, UNROLL, FM) \
   PairVariant { TC_FP32C, NT, T, kTS, FLUSH, MINB, UNROLL, \
-                launch32<NT, T, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
-                (const void*)pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
-                launch32b<NT, T, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
-                (const void*)pair_fp32c_batch_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, 8 | (PRF << 4)>, \
-                8 | (PRF << 4) }
+                launch32<NT, T, FLUSH, MINB, UNROLL, FM>, \
+                (const void*)pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM>, \
+                launch32b<NT, T, FLUSH, MINB, UNROLL, FM>, \
+                (const void*)pair_fp32c_batch_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM>, FM }
+#define VSP(NT, T, FLUSH, MINB, UNROLL, PRF) VSPX(NT, T, FLUSH, MINB, UNROLL, 8 | (PRF << 4))
+// ... with the flushes widened by integer operations (form bit 0)
+#define VSPA(NT, T, FLUSH, MINB, UNROLL, PRF) VSPX(NT, T, FLUSH, MINB, UNROLL, 9 | (PRF << 4))
 
 // FP64: the `flush` field records the denominator mode (1 = fused, 0 =
 // rounded exactly like the reference).
@@ -89,7 +91,8 @@ const PairVariant kVariants64[] = {
 };
 // FP32C: the last field is a bit set: far-field form (1), paired
 // reciprocal (2), pre-weighted far-field sources (4, with 1), source-paired
-// rotated-frame form (8, its own far/near forms; bits 4+ the period of the
+// rotated-frame form (8, its own far/near forms; with it, bit 0 widens the
+// FP64 flushes by integer operations and bits 4+ give the period of the
 // paired reciprocal).
 const PairVariant kVariants32[] = {
     V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
@@ -111,6 +114,8 @@ const PairVariant kVariants32[] = {
     VSP(256, 2, 64, 3, 2, 4), VSP(128, 4, 64, 4, 4, 0), VSP(128, 2, 64, 6, 1, 8),
     VSP(128, 2, 128, 6, 4, 0), VSP(128, 2, 64, 5, 4, 0), VSP(128, 2, 64, 6, 8, 0),
     VSP(64, 2, 64, 12, 4, 0), VSP(128, 2, 128, 6, 8, 0), VSP(128, 2, 64, 5, 8, 0),
+    VSPA(128, 2, 64, 6, 4, 0), VSPA(128, 2, 64, 6, 2, 4), VSPA(128, 2, 64, 5, 4, 0),
+    VSP(256, 2, 64, 3, 4, 0),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);

@@ -286,6 +286,37 @@ struct Grid {
 
 }  // namespace
 
+// The level-0 grid (root icosahedron: 12 particles, 30 edges, 20 panels) in
+// the reference's numbering, for the device generator (icos_grid.cu), which
+// divides it level by level on the GPU.
+void tc_icos_root_tables(double px[36], double cx[60], double area[20], int pv[60], int pe[60],
+                         int ev[60], int eleft[30], int eright[30]) {
+  Grid g;
+  g.reserve(12, 30, 20);
+  g.init_icosahedron();
+  for (int j = 0; j < 12; ++j) {
+    px[3 * j] = g.px[j].x;
+    px[3 * j + 1] = g.px[j].y;
+    px[3 * j + 2] = g.px[j].z;
+  }
+  for (int p = 0; p < 20; ++p) {
+    cx[3 * p] = g.cx[p].x;
+    cx[3 * p + 1] = g.cx[p].y;
+    cx[3 * p + 2] = g.cx[p].z;
+    area[p] = g.area[p];
+    for (int s = 0; s < 3; ++s) {
+      pv[3 * p + s] = g.pv[3 * p + s];
+      pe[3 * p + s] = g.pe[3 * p + s];
+    }
+  }
+  for (int e = 0; e < 30; ++e) {
+    ev[2 * e] = g.ev[2 * e];
+    ev[2 * e + 1] = g.ev[2 * e + 1];
+    eleft[e] = g.eleft[e];
+    eright[e] = g.eright[e];
+  }
+}
+
 extern "C" int tc_icos_grid_sizes(int level, int* n_particles, int* n_edges, int* n_panels,
                                   int* n_active) {
   if (level < 0 || level > 11) {

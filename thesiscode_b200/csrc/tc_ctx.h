@@ -106,6 +106,7 @@ struct tc_ctx {
   int slots64 = 0, slots32 = 0;  // resident CTAs per GPU for each kernel
   tcb::DevBuf partial;    // pair-kernel partial sums
   tcb::DevBuf scratch[6]; // one-call buffers (velocity entry points)
+  tcb::DevBuf grid_buf[6];  // tc_icos_grid_device: edge and panel tables, prefix sums
   tcb::Rk4State rk;
   // instrumentation (tc_stats): kernels launched, and CUDA-event time of the
   // pair kernels when timing is on (events recorded on ctx->stream).

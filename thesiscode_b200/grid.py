@@ -8,6 +8,7 @@ Indices are 0-based.
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -85,6 +86,29 @@ def new_icos_grid(level: int, n_tracer: int = 0) -> tuple[Particles, Panels]:
                   children=children, absVort=np.zeros(npan), relVort=np.zeros(npan),
                   tracer=np.zeros((npan, n_tracer)))
     return parts, pans
+
+
+def new_icos_grid_device(ctx, level: int) -> dict:
+    """The grid of new_icos_grid generated on the GPU of `ctx` (tc_icos_grid_device): a dict of
+    torch CUDA tensors (particles x, x0; panels x, x0, area, hasChildren, vertices, nest,
+    children) in the host generator's numbering and shapes."""
+    import torch
+
+    from . import _native as N
+
+    s = icos_sizes(level)
+    npart, npan = s["particles"], s["panels"]
+    dev = torch.device(f"cuda:{ctx.device}")
+    f64 = dict(dtype=torch.float64, device=dev)
+    i32 = dict(dtype=torch.int32, device=dev)
+    out = dict(particles_x=torch.empty((npart, 3), **f64), particles_x0=torch.empty((npart, 3), **f64),
+               panels_x=torch.empty((npan, 3), **f64), panels_x0=torch.empty((npan, 3), **f64),
+               panels_area=torch.empty(npan, **f64), panels_has_children=torch.empty(npan, **i32),
+               panels_vertices=torch.empty((npan, 3), **i32), panels_nest=torch.empty(npan, **i32),
+               panels_children=torch.empty((npan, 4), **i32))
+    ptr = [ctypes.c_void_p(t.data_ptr()) for t in out.values()]
+    N.call("tc_icos_grid_device", ctx.handle, level, *ptr)
+    return out
 
 
 @dataclass
