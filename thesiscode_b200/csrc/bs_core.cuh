@@ -540,6 +540,8 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // operations (4 denominator, 3 accumulations) and one MUFU reciprocal.
 // FM bit 0 (with bit 3): the FP64 flushes widen the FP32 partials with
 // integer operations (f2d_alu) instead of F2F conversions on the XU pipe.
+// FM bit 1 (with bit 3): the FP64 accumulators live in shared memory (one
+// slot per thread, target and coordinate), 6 fewer registers per target.
 // PRF > 0: one source pair of every PRF shares a single MUFU reciprocal
 // (1/D_k = q D_k+1, 1/D_k+1 = q D_k, q = 1/(D_k D_k+1)), trading 8 XU cycles
 // for 3 FMA-pipe cycles per warp and target, so the FMA and XU pipes carry
@@ -548,7 +550,7 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // sum w x'_k; they differ by multiples of x'_i, which u = x_i x T ignores)
 // and are rotated back in FP64 once per target.
 // ---------------------------------------------------------------------------
-template <int NT, int TS>
+template <int NT, int TS, int T = 1, bool SMACC = false>
 struct SpSmem {
   float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
   float4 b[TS / 2];        // (sz_k, sz_k+1, A_k, A_k+1)
@@ -556,6 +558,7 @@ struct SpSmem {
   float2 d[TS / 2];        // (G z'_k, G z'_k+1)
   float4 n[TS / 2];        // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
   double frame[12];        // e1, e2, e3 (rows), origin c
+  double acc[SMACC ? 3 * T * NT : 1];  // FP64 accumulators [c][t][thread] (SMACC)
   unsigned tmin[NT / 32];
   unsigned rho[NT / 32];
 };
@@ -641,12 +644,39 @@ __device__ __forceinline__ void sp_far_step(const float4 a, const float4 b, cons
   }
 }
 
-template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT>
+// FP64 accumulator of target t, coordinate c: a register, or (SMACC) a
+// shared-memory slot of this thread (frees 6 registers per target).
+template <int NT, int T, bool SMACC>
+struct SpAcc {
+  double r[SMACC ? 1 : 3 * T];
+  double* sm;
+  __device__ __forceinline__ void init(double* base) {
+    sm = base + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 3 * T; ++k) {
+      if (SMACC)
+        sm[k * NT] = 0.0;
+      else
+        r[k] = 0.0;
+    }
+  }
+  __device__ __forceinline__ void add(int c, int t, double v) {
+    if (SMACC)
+      sm[(c * T + t) * NT] += v;
+    else
+      r[c * T + t] += v;
+  }
+  __device__ __forceinline__ double get(int c, int t) const {
+    return SMACC ? sm[(c * T + t) * NT] : r[c * T + t];
+  }
+};
+
+template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT, bool SMACC>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
-                                              SpSmem<NT, TS>& sm) {
+                                              SpSmem<NT, TS, T, SMACC>& sm) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(PRF == 0 || (FLUSH / 2) % PRF == 0, "paired-reciprocal period divides the flush");
   static_assert(NT % 32 == 0, "whole warps");
@@ -671,7 +701,8 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   float2 ntx[T], nty[T], ntz[T], bh[T];
   float ei[T];  // near form only: paired on use
   float2 fx[T], fy[T], fz[T];
-  double ax[T], ay[T], az[T];
+  SpAcc<NT, T, SMACC> acc;
+  acc.init(sm.acc);
   float rho2 = 0.f;
 #pragma unroll
   for (int t = 0; t < T; ++t) {
@@ -692,7 +723,6 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     bh[t] = make_float2(b, b);
     rho2 = fmaxf(rho2, t2);
     fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
-    ax[t] = ay[t] = az[t] = 0.0;
   }
   warp_store_max(rho2, sm.rho);
 
@@ -754,9 +784,9 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         }
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-          ax[t] += widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y));
-          ay[t] += widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y));
-          az[t] += widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y));
+          acc.add(0, t, widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y)));
+          acc.add(1, t, widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y)));
+          acc.add(2, t, widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y)));
           fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
         }
       }
@@ -787,9 +817,9 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         }
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-          ax[t] += widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y));
-          ay[t] += widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y));
-          az[t] += widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y));
+          acc.add(0, t, widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y)));
+          acc.add(1, t, widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y)));
+          acc.add(2, t, widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y)));
           fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
         }
       }
@@ -800,9 +830,10 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   for (int t = 0; t < T; ++t) {
     const int pos = tile0 + (int)threadIdx.x + t * NT;
     if (pos < i_end) {
-      out[pos] = fma(fr[0], ax[t], fma(fr[3], ay[t], fr[6] * az[t]));
-      out[stride + pos] = fma(fr[1], ax[t], fma(fr[4], ay[t], fr[7] * az[t]));
-      out[2 * stride + pos] = fma(fr[2], ax[t], fma(fr[5], ay[t], fr[8] * az[t]));
+      const double ax = acc.get(0, t), ay = acc.get(1, t), az = acc.get(2, t);
+      out[pos] = fma(fr[0], ax, fma(fr[3], ay, fr[6] * az));
+      out[stride + pos] = fma(fr[1], ax, fma(fr[4], ay, fr[7] * az));
+      out[2 * stride + pos] = fma(fr[2], ax, fma(fr[5], ay, fr[8] * az));
     }
   }
 }
@@ -818,9 +849,9 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
   if constexpr (SP) {
-    __shared__ SpSmem<NT, TS> sm;
-    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0,
-                                                           c1, out, stride, sm);
+    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0> sm;
+    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0, (FM & 2) != 0>(
+        G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
     fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
@@ -872,13 +903,13 @@ template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
   __shared__ int slot;
   if constexpr ((FM & 8) != 0) {
-    __shared__ SpSmem<NT, TS> sm;
+    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0> sm;
     for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
       const BatchItem I = B.items[it];
       const BatchSeg S = B.segs[I.seg];
       double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src,
-                                                             I.c0, I.c1, out, B.stride, sm);
+      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0, (FM & 2) != 0>(
+          S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
     }
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;

@@ -92,8 +92,8 @@ const PairVariant kVariants64[] = {
 // FP32C: the last field is a bit set: far-field form (1), paired
 // reciprocal (2), pre-weighted far-field sources (4, with 1), source-paired
 // rotated-frame form (8, its own far/near forms; with it, bit 0 widens the
-// FP64 flushes by integer operations and bits 4+ give the period of the
-// paired reciprocal).
+// FP64 flushes by integer operations, bit 1 keeps the FP64 accumulators in
+// shared memory and bits 4+ give the period of the paired reciprocal).
 const PairVariant kVariants32[] = {
     V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
     V32(256, 2, 16, 2, 4, 0), V32(128, 2, 32, 6, 4, 0), V32(256, 1, 32, 4, 8, 0),
@@ -116,6 +116,11 @@ const PairVariant kVariants32[] = {
     VSP(64, 2, 64, 12, 4, 0), VSP(128, 2, 128, 6, 8, 0), VSP(128, 2, 64, 5, 8, 0),
     VSPA(128, 2, 64, 6, 4, 0), VSPA(128, 2, 64, 6, 2, 4), VSPA(128, 2, 64, 5, 4, 0),
     VSP(256, 2, 64, 3, 4, 0),
+    // FP64 accumulators in shared memory (form bit 1 with bit 3)
+    VSPX(128, 2, 64, 7, 4, 10), VSPX(128, 2, 64, 8, 4, 10), VSPX(128, 2, 64, 6, 4, 10),
+    VSPX(128, 3, 64, 6, 4, 10),
+    VSPX(128, 3, 64, 6, 2, 10), VSPX(128, 3, 64, 5, 4, 10), VSPX(128, 4, 64, 5, 4, 10),
+    VSPX(128, 4, 64, 4, 4, 10), VSPX(128, 3, 64, 6, 8, 10), VSPX(64, 3, 64, 12, 4, 10),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
