@@ -39,7 +39,7 @@ FLOPS_PER_INTERACTION = 22  # dot 5, denominator 1, weight 1, cross 9, accumulat
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) of one FP32C pair launch on the level-7 Gaussian workload, from an
 # ncu capture of `bench.py --quick --no-cpu --steps 2` (dram__bytes_read.sum + dram__bytes_write.sum)
-PAIR_FP32C_L7_DRAM_BYTES = 27.64e6 + 53.04e6
+PAIR_FP32C_L7_DRAM_BYTES = 28.02e6 + 52.43e6
 
 
 def build_workload(name: str):

@@ -19,14 +19,15 @@ from thesiscode_b200.panel_velocity import Context
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 FP64_TOL = 1e-12
-# FP32-compensated path, stated bound: 1e-7 from level 6 up (the benchmark sizes; tiles of
-# the Hilbert target order are small against the sphere), 3e-7 at levels 4-5 and 5e-7 at
-# levels <= 3 (<= 1,280 panels), where one tile spans much of the sphere and the FP32
-# rounding of each pair term relative to the tile origin (a few ulps) is the floor; it
-# moves between 2e-7 and 4e-7 with the tile shape. Scaled to the largest value of the
+# FP32-compensated path, stated bound: 1e-7 from level 7 up (the benchmark sizes), 2e-7 at
+# level 6, 3e-7 at levels 4-5 and 5e-7 at levels <= 3 (<= 1,280 panels). The floor is the
+# rounding of each point's offset from its tile origin to FP32 (a few ulps of the tile
+# radius) in nearest-neighbour pairs, so it shrinks with the grid spacing; the hi/lo near
+# form (form bit 2) removes it and keeps 1e-7 at level 6. Scaled to the largest value of the
 # compared quantity (dVort = -2 Omega u_z scales with max |u_z|, not max |u|).
 FP32C_TOL_COARSE = 5e-7
 FP32C_TOL = 3e-7
+FP32C_TOL_L6 = 2e-7
 FP32C_TOL_FINE = 1e-7
 
 
@@ -128,7 +129,45 @@ def test_fp32c_accuracy_does_not_depend_on_target_order(ctx32):
     dX, _ = ctx32.velocity(N.TC_VERTEX, xV, w.xA, w.zetaA, w.areaA)
     rows = np.sort(rng.choice(w.nV, 768, replace=False))
     ref = O.rows(1, rows, xV, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=8)
-    assert np.abs(dX[rows] - ref).max() / np.abs(dX).max() <= FP32C_TOL_FINE
+    assert np.abs(dX[rows] - ref).max() / np.abs(dX).max() <= FP32C_TOL_L6
+
+
+def _variants_with_form(bits: int) -> list[int]:
+    import ctypes
+    cnt = ctypes.c_int()
+    N.call("tc_pair_variant_count", N.TC_FP32C, ctypes.byref(cnt))
+    out = []
+    for v in range(cnt.value):
+        info = (ctypes.c_int * 8)()
+        N.call("tc_pair_variant_info", N.TC_FP32C, v, info)
+        if info[7] & bits == bits and not info[7] & 256:
+            out.append(v)
+    return out
+
+
+def test_fp32c_level6_jet_default_and_hilo(gpu):
+    """Zonal jet, level 6, delta 0.02, 4,096 seeded rows: the default variant within the level-6
+    bound, the hi/lo near form (exact-offset near pairs) within 1e-7."""
+    import ctypes
+    w = configs.jet(level=6, delta=0.02)
+    rng = np.random.default_rng(61)
+    ra = np.sort(rng.choice(w.nA, 2048, replace=False))
+    rv = np.sort(rng.choice(w.nV, 2048, replace=False))
+    refA = O.rows(0, ra, None, w.xA, w.zetaA, w.areaA, delta=0.02, nthreads=8)
+    refV = O.rows(1, rv, w.xV, w.xA, w.zetaA, w.areaA, delta=0.02, nthreads=8)
+    scale = max(np.abs(refA).max(), np.abs(refV).max())
+    hilo = _variants_with_form(8 | 4)
+    assert hilo
+    for variant, tol in ((None, FP32C_TOL_L6), (hilo[0], FP32C_TOL_FINE), (hilo[-1], FP32C_TOL_FINE)):
+        ctx = Context(0, "fp32c")
+        setup(ctx, w.omega, w.deltas)
+        if variant is not None:
+            N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, variant)
+        dA, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+        dV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+        ctx.close()
+        err = max(np.abs(dA[ra] - refA).max(), np.abs(dV[rv] - refV).max()) / scale
+        assert err <= tol, (variant, err)
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", FP32C_TOL_COARSE)])

@@ -14,6 +14,7 @@
 #include <numeric>
 #include <vector>
 
+#include "sphere_order.cuh"
 #include "tc_ctx.h"
 
 using tcb::DevBuf;
@@ -24,51 +25,16 @@ __global__ void batch_keys_kernel(const double* __restrict__ x, const int* __res
                                   int n, unsigned long long* __restrict__ keys,
                                   int* __restrict__ idx);
 
-// Hilbert key of one point (10 bits per axis, Skilling's transform), the same
-// curve as order.cu.
-__device__ unsigned batch_hilbert(double x, double y, double z) {
-  const int kBits = 10;
-  const double scale = (double)((1u << kBits) - 1);
-  unsigned X[3];
-  const double c[3] = {x, y, z};
-  for (int i = 0; i < 3; ++i) {
-    double q = (c[i] + 1.0) * 0.5 * scale + 0.5;
-    q = q < 0.0 ? 0.0 : (q > scale ? scale : q);
-    X[i] = (unsigned)q;
-  }
-  const unsigned M = 1u << (kBits - 1);
-  for (unsigned Q = M; Q > 1; Q >>= 1) {
-    const unsigned P = Q - 1;
-    for (int i = 0; i < 3; ++i) {
-      if (X[i] & Q) {
-        X[0] ^= P;
-      } else {
-        unsigned t = (X[0] ^ X[i]) & P;
-        X[0] ^= t;
-        X[i] ^= t;
-      }
-    }
-  }
-  for (int i = 1; i < 3; ++i) X[i] ^= X[i - 1];
-  unsigned t = 0;
-  for (unsigned Q = M; Q > 1; Q >>= 1)
-    if (X[2] & Q) t ^= Q - 1;
-  for (int i = 0; i < 3; ++i) X[i] ^= t;
-  unsigned key = 0;
-  for (int b = kBits - 1; b >= 0; --b)
-    for (int i = 0; i < 3; ++i) key = (key << 1) | ((X[i] >> b) & 1u);
-  return key;
-}
-
-// key = instance << 30 | Hilbert: one stable sort orders every instance's
-// rows along the curve and keeps the instances in their ranges.
+// key = instance << 31 | sphere key (cube face, 2-D Hilbert index): one
+// stable sort orders every instance's rows along the curve and keeps the
+// instances in their ranges.
 __global__ void batch_keys_kernel(const double* __restrict__ x, const int* __restrict__ row_inst,
                                   int n, unsigned long long* __restrict__ keys,
                                   int* __restrict__ idx) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const size_t b = 3 * (size_t)j;
-  keys[j] = ((unsigned long long)row_inst[j] << 30) | batch_hilbert(x[b], x[b + 1], x[b + 2]);
+  keys[j] = ((unsigned long long)row_inst[j] << tcb::kSphereKeyBits) | tcb::sphere_key(x[b], x[b + 1], x[b + 2]);
   idx[j] = j;
 }
 
@@ -125,8 +91,8 @@ int sort_batch_rows(tc_ctx* ctx, tc_batch_plan& B, const double* x, const int* r
       x, row_inst, n, B.keys.as<unsigned long long>(), B.vals.as<int>());
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
-  int bits = 30;
-  while ((1 << (bits - 30)) < B.count + 1) ++bits;
+  int bits = tcb::kSphereKeyBits;
+  while ((1 << (bits - tcb::kSphereKeyBits)) < B.count + 1) ++bits;
   size_t temp = 0;
   TC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp, B.keys.as<unsigned long long>(),
                                               B.keys2.as<unsigned long long>(), B.vals.as<int>(),

@@ -542,6 +542,15 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // integer operations (f2d_alu) instead of F2F conversions on the XU pipe.
 // FM bit 1 (with bit 3): the FP64 accumulators live in shared memory (one
 // slot per thread, target and coordinate), 6 fewer registers per target.
+// FM bit 2 (with bit 3): near tiles take d = s - t from hi/lo FP32 splits of
+// both offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to
+// FP32 (an absolute error of ulps of the patch radius, the dominant FP32C
+// error for nearest-neighbour pairs) no longer enters, and d keeps a few
+// ulps of its own length. Far tiles are unchanged. FM bit 8 (with bits 2 and
+// 3): the source side only, d = (s_hi - t_hi) + s_lo (near sources lie up to
+// about 3 patch radii from the origin, targets within one, so the source
+// offsets carry most of the rounding), half the extra operations and no
+// per-target registers.
 // PRF > 0: one source pair of every PRF shares a single MUFU reciprocal
 // (1/D_k = q D_k+1, 1/D_k+1 = q D_k, q = 1/(D_k D_k+1)), trading 8 XU cycles
 // for 3 FMA-pipe cycles per warp and target, so the FMA and XU pipes carry
@@ -550,7 +559,7 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // sum w x'_k; they differ by multiples of x'_i, which u = x_i x T ignores)
 // and are rotated back in FP64 once per target.
 // ---------------------------------------------------------------------------
-template <int NT, int TS, int T = 1, bool SMACC = false>
+template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false>
 struct SpSmem {
   float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
   float4 b[TS / 2];        // (sz_k, sz_k+1, A_k, A_k+1)
@@ -558,7 +567,11 @@ struct SpSmem {
   float2 d[TS / 2];        // (G z'_k, G z'_k+1)
   float4 n[TS / 2];        // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
   double frame[12];        // e1, e2, e3 (rows), origin c
+  double csum[3][NT / 32]; // per-warp sums of the target positions
   double acc[SMACC ? 3 * T * NT : 1];  // FP64 accumulators [c][t][thread] (SMACC)
+  float4 lo[HILO ? TS / 2 : 1];        // HILO: low parts (slx_k, slx_k+1, sly_k, sly_k+1)
+  float2 loz[HILO ? TS / 2 : 1];       // HILO: (slz_k, slz_k+1)
+  float tlo[HILO ? 3 * T * NT : 1];    // HILO: -(target low parts) [c][t][thread]
   unsigned tmin[NT / 32];
   unsigned rho[NT / 32];
 };
@@ -671,12 +684,13 @@ struct SpAcc {
   }
 };
 
-template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT, bool SMACC>
+template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT, bool SMACC,
+          bool HILO, bool SRC_LO_ONLY = false>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
-                                              SpSmem<NT, TS, T, SMACC>& sm) {
+                                              SpSmem<NT, TS, T, SMACC, HILO>& sm) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(PRF == 0 || (FLUSH / 2) % PRF == 0, "paired-reciprocal period divides the flush");
   static_assert(NT % 32 == 0, "whole warps");
@@ -687,9 +701,53 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
   const int mid = perm ? perm[mid_pos] : mid_pos;
-  const double cx = x[3 * (size_t)mid], cy = x[3 * (size_t)mid + 1], cz = x[3 * (size_t)mid + 2];
-  __syncthreads();  // the previous unit (persistent kernel) is done with sm.frame
+  // Origin: the CTA's targets' centroid, projected to the sphere (a smaller
+  // patch radius than any one target gives: fewer near tiles, smaller FP32
+  // offsets); the middle target when the targets surround the centre.
+  double px = 0.0, py = 0.0, pz = 0.0;
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int pos = tile0 + (int)threadIdx.x + t * NT;
+    if (pos < i_end) {
+      const int ld = perm ? perm[pos] : pos;
+      px += x[3 * (size_t)ld];
+      py += x[3 * (size_t)ld + 1];
+      pz += x[3 * (size_t)ld + 2];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    px += __shfl_xor_sync(0xffffffffu, px, o);
+    py += __shfl_xor_sync(0xffffffffu, py, o);
+    pz += __shfl_xor_sync(0xffffffffu, pz, o);
+  }
+  __syncthreads();  // the previous unit (persistent kernel) is done with sm.frame, sm.csum
+  if ((threadIdx.x & 31) == 0) {
+    sm.csum[0][threadIdx.x >> 5] = px;
+    sm.csum[1][threadIdx.x >> 5] = py;
+    sm.csum[2][threadIdx.x >> 5] = pz;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int w = 0; w < NT / 32; ++w) {
+      sx += sm.csum[0][w];
+      sy += sm.csum[1][w];
+      sz += sm.csum[2][w];
+    }
+    const double count = (double)min(TB, i_end - tile0);
+    const double n2 = sx * sx + sy * sy + sz * sz;
+    double cx, cy, cz;
+    if (n2 > 0.25 * count * count) {
+      const double inv = 1.0 / sqrt(n2);
+      cx = sx * inv;
+      cy = sy * inv;
+      cz = sz * inv;
+    } else {
+      cx = x[3 * (size_t)mid];
+      cy = x[3 * (size_t)mid + 1];
+      cz = x[3 * (size_t)mid + 2];
+    }
     make_frame(cx, cy, cz, sm.frame);
     sm.frame[9] = cx;
     sm.frame[10] = cy;
@@ -697,6 +755,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   }
   __syncthreads();
   const double* fr = sm.frame;
+  const double cx = fr[9], cy = fr[10], cz = fr[11];
 
   float2 ntx[T], nty[T], ntz[T], bh[T];
   float ei[T];  // near form only: paired on use
@@ -710,9 +769,14 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     const int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
     const double px = x[3 * (size_t)ld], py = x[3 * (size_t)ld + 1], pz = x[3 * (size_t)ld + 2];
     const double dx = px - cx, dy = py - cy, dz = pz - cz;
-    const float tx = (float)frame_dot(fr, dx, dy, dz);
-    const float ty = (float)frame_dot(fr + 3, dx, dy, dz);
-    const float tz = (float)frame_dot(fr + 6, dx, dy, dz);
+    const double txd = frame_dot(fr, dx, dy, dz), tyd = frame_dot(fr + 3, dx, dy, dz),
+                 tzd = frame_dot(fr + 6, dx, dy, dz);
+    const float tx = (float)txd, ty = (float)tyd, tz = (float)tzd;
+    if (HILO && !SRC_LO_ONLY) {
+      sm.tlo[(0 * T + t) * NT + threadIdx.x] = -(float)(txd - (double)tx);
+      sm.tlo[(1 * T + t) * NT + threadIdx.x] = -(float)(tyd - (double)ty);
+      sm.tlo[(2 * T + t) * NT + threadIdx.x] = -(float)(tzd - (double)tz);
+    }
     const double E = (1.0 - (px * px + py * py + pz * pz)) + 2.0 * d2;
     ntx[t] = make_float2(-tx, -tx);
     nty[t] = make_float2(-ty, -ty);
@@ -730,7 +794,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     __syncthreads();
     float smin = __int_as_float(0x7f800000);  // +inf
     for (int jp = threadIdx.x; jp < NP; jp += NT) {
-      float v[2][9];
+      float v[2][12];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int k = ts + 2 * jp + h;
@@ -740,12 +804,18 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         v[h][4] = v[h][5] = v[h][6] = 0.f;
         v[h][7] = 1.f;
         v[h][8] = 0.f;
+        v[h][9] = v[h][10] = v[h][11] = 0.f;
         if (k < c1) {
           const double4 q = src[k];
           const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
-          const float sx = (float)frame_dot(fr, dx, dy, dz);
-          const float sy = (float)frame_dot(fr + 3, dx, dy, dz);
-          const float sz = (float)frame_dot(fr + 6, dx, dy, dz);
+          const double sxd = frame_dot(fr, dx, dy, dz), syd = frame_dot(fr + 3, dx, dy, dz),
+                       szd = frame_dot(fr + 6, dx, dy, dz);
+          const float sx = (float)sxd, sy = (float)syd, sz = (float)szd;
+          if (HILO) {
+            v[h][9] = (float)(sxd - (double)sx);
+            v[h][10] = (float)(syd - (double)sy);
+            v[h][11] = (float)(szd - (double)sz);
+          }
           const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
           const float s2 = norm2_f32(sx, sy, sz);
           smin = fminf(smin, s2);
@@ -765,6 +835,10 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
       sm.c[jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
       sm.d[jp] = make_float2(v[0][6], v[1][6]);
       sm.n[jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
+      if (HILO) {
+        sm.lo[jp] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
+        sm.loz[jp] = make_float2(v[0][11], v[1][11]);
+      }
     }
     warp_store_min(smin, sm.tmin);
     __syncthreads();
@@ -791,6 +865,12 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         }
       }
     } else {
+      // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
+      float ntl[HILO && !SRC_LO_ONLY ? 3 * T : 1];
+      if (HILO && !SRC_LO_ONLY) {
+#pragma unroll
+        for (int k = 0; k < 3 * T; ++k) ntl[k] = sm.tlo[k * NT + threadIdx.x];
+      }
       for (int jf = 0; jf < NP; jf += FP) {
 #pragma unroll 4
         for (int j = jf; j < jf + FP; ++j) {
@@ -800,11 +880,26 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
           const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w);
           const float2 sz = make_float2(b.x, b.y);
           const float2 ee = make_float2(n.x, n.y), gg = make_float2(n.z, n.w);
+          float4 lo = make_float4(0.f, 0.f, 0.f, 0.f);
+          float2 loz = make_float2(0.f, 0.f);
+          if (HILO) {
+            lo = sm.lo[j];
+            loz = sm.loz[j];
+          }
 #pragma unroll
           for (int t = 0; t < T; ++t) {
-            const float2 dx = __fadd2_rn(sx, ntx[t]);
-            const float2 dy = __fadd2_rn(sy, nty[t]);
-            const float2 dz = __fadd2_rn(sz, ntz[t]);
+            float2 dx = __fadd2_rn(sx, ntx[t]);
+            float2 dy = __fadd2_rn(sy, nty[t]);
+            float2 dz = __fadd2_rn(sz, ntz[t]);
+            if (HILO && SRC_LO_ONLY) {
+              dx = __fadd2_rn(dx, make_float2(lo.x, lo.y));
+              dy = __fadd2_rn(dy, make_float2(lo.z, lo.w));
+              dz = __fadd2_rn(dz, loz);
+            } else if (HILO) {
+              dx = __fadd2_rn(dx, __fadd2_rn(make_float2(lo.x, lo.y), make_float2(ntl[t], ntl[t])));
+              dy = __fadd2_rn(dy, __fadd2_rn(make_float2(lo.z, lo.w), make_float2(ntl[T + t], ntl[T + t])));
+              dz = __fadd2_rn(dz, __fadd2_rn(loz, make_float2(ntl[2 * T + t], ntl[2 * T + t])));
+            }
             float2 D = __fadd2_rn(ee, make_float2(ei[t], ei[t]));
             D = __ffma2_rn(dx, dx, D);
             D = __ffma2_rn(dy, dy, D);
@@ -849,9 +944,10 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
   if constexpr (SP) {
-    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0> sm;
-    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0, (FM & 2) != 0>(
-        G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
+    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0, (FM & 4) != 0> sm;
+    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
+                  (FM & 4) != 0, (FM & 256) != 0>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
+                                                  stride, sm);
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
     fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
@@ -903,13 +999,14 @@ template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
   __shared__ int slot;
   if constexpr ((FM & 8) != 0) {
-    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0> sm;
+    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0, (FM & 4) != 0> sm;
     for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
       const BatchItem I = B.items[it];
       const BatchSeg S = B.segs[I.seg];
       double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, (FM >> 4), (FM & 1) != 0, (FM & 2) != 0>(
-          S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
+      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
+                    (FM & 4) != 0, (FM & 256) != 0>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0,
+                                                    I.c1, out, B.stride, sm);
     }
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
