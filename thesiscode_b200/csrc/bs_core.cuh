@@ -842,8 +842,15 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     }
     warp_store_min(smin, sm.tmin);
     __syncthreads();
-    const bool far = combine_min<NT / 32>(sm.tmin) > kFarRatio2 * combine_max<NT / 32>(sm.rho);
-    if (far) {
+    // Far test per flush segment when every warp staged exactly one segment
+    // (NT = TS/2 source pairs, FP = 32): segment g's minimum |s|^2 is warp
+    // g's, so only the segments that hold near sources take the near form.
+    // Otherwise one test for the whole tile.
+    // A tile whose every segment is far runs one tight far loop.
+    constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
+    const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
+    const bool tile_far = combine_min<NT / 32>(sm.tmin) > lim;
+    if (tile_far) {
       for (int jf = 0; jf < NP; jf += FP) {
 #pragma unroll UNROLL
         for (int jg = jf; jg < jf + FP; jg += GRP) {
@@ -864,14 +871,29 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
           fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
         }
       }
-    } else {
-      // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
-      float ntl[HILO && !SRC_LO_ONLY ? 3 * T : 1];
-      if (HILO && !SRC_LO_ONLY) {
+      continue;
+    }
+    for (int jf = 0; jf < NP; jf += FP) {
+      const bool far = PERSEG && __uint_as_float(sm.tmin[jf / FP]) > lim;
+      if (far) {
+#pragma unroll UNROLL
+        for (int jg = jf; jg < jf + FP; jg += GRP) {
 #pragma unroll
-        for (int k = 0; k < 3 * T; ++k) ntl[k] = sm.tlo[k * NT + threadIdx.x];
-      }
-      for (int jf = 0; jf < NP; jf += FP) {
+          for (int u = 0; u < GRP; ++u) {
+            const int j = jg + u;
+            if (PRF > 0 && u == 0)
+              sp_far_step<T, true>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
+            else
+              sp_far_step<T, false>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
+          }
+        }
+      } else {
+        // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
+        float ntl[HILO && !SRC_LO_ONLY ? 3 * T : 1];
+        if (HILO && !SRC_LO_ONLY) {
+#pragma unroll
+          for (int k = 0; k < 3 * T; ++k) ntl[k] = sm.tlo[k * NT + threadIdx.x];
+        }
 #pragma unroll 4
         for (int j = jf; j < jf + FP; ++j) {
           const float4 a = sm.a[j];
@@ -910,13 +932,13 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
             fz[t] = __ffma2_rn(w, dz, fz[t]);
           }
         }
+      }
 #pragma unroll
-        for (int t = 0; t < T; ++t) {
-          acc.add(0, t, widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y)));
-          acc.add(1, t, widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y)));
-          acc.add(2, t, widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y)));
-          fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
-        }
+      for (int t = 0; t < T; ++t) {
+        acc.add(0, t, widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y)));
+        acc.add(1, t, widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y)));
+        acc.add(2, t, widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y)));
+        fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
       }
     }
   }
