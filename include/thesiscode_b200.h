@@ -236,10 +236,11 @@ int tc_rk4_vjp(tc_ctx* ctx, const double* xA0, const double* zetaA0, const doubl
 /* How each stage's vector-Jacobian product visits the pairs: 3 to 6 = one
  * row-major pass computing both sides' row sums (3: one row per thread,
  * 4: two rows per thread; 5 and 6: the same with a one-step Newton
- * reciprocal, relative error the square of the rcp.approx.f64 seed's), 0 = two
+ * reciprocal, relative error the square of the rcp.approx.f64 seed's; 7:
+ * three rows per thread, one-step Newton), 0 = two
  * passes (target side, transposed source side), 1 and 2 = one pass with
  * in-block column reductions (256 threads x 2 targets, or 128 x 4). Default 6.
- * Modes 0-4 give the same gradient to FP64 rounding; 5 and 6 differ from them
+ * Modes 0-4 give the same gradient to FP64 rounding; 5-7 differ from them
  * by the seed's squared error (below 1e-13 of the gradient's scale). */
 int tc_set_adjoint_mode(tc_ctx* ctx, int mode);
 /* Device time (ms) of the last tc_rk4_adjoint call: ms3[0] forward sweep

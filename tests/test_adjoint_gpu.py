@@ -272,15 +272,15 @@ def test_trajectory_vjp_matches_torch_autograd_fp64(gpu):
 
 
 def test_every_vjp_mode_gives_the_same_gradient(gpu):
-    """The seven ways of visiting the pairs in a stage's vector-Jacobian product (two passes,
-    fused column reductions, row passes with one or two rows per thread and one or two Newton
+    """The eight ways of visiting the pairs in a stage's vector-Jacobian product (two passes,
+    fused column reductions, row passes with one to three rows per thread and one or two Newton
     steps) agree to rounding."""
     w = configs.gaussian(level=3, delta=0.02, dt=0.01)
     ctx = Context(0, "fp64")
     ctx.set_omega(w.omega)
     ctx.set_deltas(*w.deltas)
     res = {}
-    for mode in range(7):
+    for mode in range(8):
         N.call("tc_set_adjoint_mode", ctx.handle, mode)
         res[mode] = adjoint(ctx, w.xA, w.zetaA, w.areaA, w.dt, 4, 2, N.TC_J_PROBE, 100)
     ref = res[0]
@@ -289,5 +289,5 @@ def test_every_vjp_mode_gives_the_same_gradient(gpu):
         assert J == ref[0]
         assert max(np.abs(gz - ref[1]).max(), np.abs(gx - ref[2]).max()) <= 1e-12 * scale, mode
     with pytest.raises(N.TcError):
-        N.call("tc_set_adjoint_mode", ctx.handle, 7)
+        N.call("tc_set_adjoint_mode", ctx.handle, 8)
     ctx.close()

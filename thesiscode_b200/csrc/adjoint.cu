@@ -308,6 +308,42 @@ __device__ __forceinline__ double adj_rcp_n(double d) {
   return r;
 }
 
+// One source j against the thread's TPT rows. MASK: skip j == row (the
+// self term), needed only in the source tile that holds the CTA's own rows.
+template <int TPT, int NEWTON, bool MASK>
+__device__ __forceinline__ void adj_row_source(const double4 q, const double4 w, const double vz,
+                                               int k, const int* row, double one_plus_d2,
+                                               const double* x0, const double* x1, const double* x2,
+                                               const double* g0, const double* g1, const double* g2,
+                                               const double* v0, const double* v1, const double* v2,
+                                               double (*a)[kRowSums]) {
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    double D = fma(-q.x, x0[t], one_plus_d2);
+    D = fma(-q.y, x1[t], D);
+    D = fma(-q.z, x2[t], D);
+    double r = adj_rcp_n<NEWTON>(D);
+    if (MASK) r = (k == row[t]) ? 0.0 : r;  // zero-padded sources give r * 0 anyway
+    // (G_j x_j).v_i + (G_i x_i).v_j
+    double c = q.w * v0[t];
+    c = fma(w.x, v1[t], c);
+    c = fma(w.y, v2[t], c);
+    c = fma(g0[t], w.z, c);
+    c = fma(g1[t], w.w, c);
+    c = fma(g2[t], vz, c);
+    const double cr2 = c * (r * r);
+    a[t][0] = fma(r, q.w, a[t][0]);
+    a[t][1] = fma(r, w.x, a[t][1]);
+    a[t][2] = fma(r, w.y, a[t][2]);
+    a[t][3] = fma(cr2, q.x, a[t][3]);
+    a[t][4] = fma(cr2, q.y, a[t][4]);
+    a[t][5] = fma(cr2, q.z, a[t][5]);
+    a[t][6] = fma(r, w.z, a[t][6]);
+    a[t][7] = fma(r, w.w, a[t][7]);
+    a[t][8] = fma(r, vz, a[t][8]);
+  }
+}
+
 template <int TPT, int NEWTON, int UNROLL>
 __global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
   __shared__ double4 sa[kRTS];  // {x_j, G_j x_j}
@@ -334,6 +370,8 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
 #pragma unroll
     for (int c = 0; c < kRowSums; ++c) a[t][c] = 0.0;
   }
+  // rows of this CTA: [r_lo, r_hi)
+  const int r_lo = blockIdx.x * TPT * kRNT, r_hi = r_lo + TPT * kRNT;
   const int c0 = blockIdx.y * P.chunk_len, c1 = min(P.n, c0 + P.chunk_len);
   for (int ts = c0; ts < c1; ts += kRTS) {
     __syncthreads();
@@ -344,36 +382,15 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
       sc[j] = k < c1 ? P.rc[k] : 0.0;
     }
     __syncthreads();
+    if (ts < r_hi && r_lo < ts + kRTS) {
+      for (int j = 0; j < kRTS; ++j)
+        adj_row_source<TPT, NEWTON, true>(sa[j], sb[j], sc[j], ts + j, row, P.one_plus_d2, x0, x1,
+                                          x2, g0, g1, g2, v0, v1, v2, a);
+    } else {
 #pragma unroll UNROLL
-    for (int j = 0; j < kRTS; ++j) {
-      const double4 q = sa[j];
-      const double4 w = sb[j];
-      const double vz = sc[j];
-#pragma unroll
-      for (int t = 0; t < TPT; ++t) {
-        double D = fma(-q.x, x0[t], P.one_plus_d2);
-        D = fma(-q.y, x1[t], D);
-        D = fma(-q.z, x2[t], D);
-        double r = adj_rcp_n<NEWTON>(D);
-        r = (ts + j == row[t]) ? 0.0 : r;  // k == i: no self term (zero-padded sources give r*0)
-        // (G_j x_j).v_i + (G_i x_i).v_j
-        double c = q.w * v0[t];
-        c = fma(w.x, v1[t], c);
-        c = fma(w.y, v2[t], c);
-        c = fma(g0[t], w.z, c);
-        c = fma(g1[t], w.w, c);
-        c = fma(g2[t], vz, c);
-        const double cr2 = c * (r * r);
-        a[t][0] = fma(r, q.w, a[t][0]);
-        a[t][1] = fma(r, w.x, a[t][1]);
-        a[t][2] = fma(r, w.y, a[t][2]);
-        a[t][3] = fma(cr2, q.x, a[t][3]);
-        a[t][4] = fma(cr2, q.y, a[t][4]);
-        a[t][5] = fma(cr2, q.z, a[t][5]);
-        a[t][6] = fma(r, w.z, a[t][6]);
-        a[t][7] = fma(r, w.w, a[t][7]);
-        a[t][8] = fma(r, vz, a[t][8]);
-      }
+      for (int j = 0; j < kRTS; ++j)
+        adj_row_source<TPT, NEWTON, false>(sa[j], sb[j], sc[j], ts + j, row, P.one_plus_d2, x0,
+                                           x1, x2, g0, g1, g2, v0, v1, v2, a);
     }
   }
   const size_t n = (size_t)P.n;
@@ -521,13 +538,15 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
   const double* p2ptr = nullptr;
   if (mode >= 3) {
     // row pass: mode 3 one row per thread, 4 two rows per thread (both full FP64
-    // reciprocals); 5 and 6 the same with one Newton step
-    const int tpt = (mode == 4 || mode == 6) ? 2 : 1;
+    // reciprocals); 5 and 6 the same with one Newton step; 7 three rows per
+    // thread, one Newton step
+    const int tpt = mode == 7 ? 3 : (mode == 4 || mode == 6) ? 2 : 1;
     const int newton = mode <= 4 ? 2 : 1;
-    const void* fn = tpt == 1 ? (newton == 2 ? (const void*)tcb::adj_row_kernel<1, 2, 2>
-                                             : (const void*)tcb::adj_row_kernel<1, 1, 2>)
-                              : (newton == 2 ? (const void*)tcb::adj_row_kernel<2, 2, 1>
-                                             : (const void*)tcb::adj_row_kernel<2, 1, 1>);
+    const void* fn = tpt == 3   ? (const void*)tcb::adj_row_kernel<3, 1, 1>
+                     : tpt == 1 ? (newton == 2 ? (const void*)tcb::adj_row_kernel<1, 2, 2>
+                                               : (const void*)tcb::adj_row_kernel<1, 1, 2>)
+                                : (newton == 2 ? (const void*)tcb::adj_row_kernel<2, 2, 1>
+                                               : (const void*)tcb::adj_row_kernel<2, 1, 1>);
     const int rows_per_cta = tcb::kRNT * tpt;
     const int tiles = (n + rows_per_cta - 1) / rows_per_cta;
     int per_sm = 0;
@@ -552,7 +571,9 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
     tcb::RowLaunch R{W.ra.as<double4>(), W.rb.as<double4>(), W.rc.as<double>(), n, chunk,
                      1.0 + d * d, W.p1.as<double>()};
     const dim3 grid(tiles, S);
-    if (tpt == 1 && newton == 2)
+    if (tpt == 3)
+      tcb::adj_row_kernel<3, 1, 1><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
+    else if (tpt == 1 && newton == 2)
       tcb::adj_row_kernel<1, 2, 2><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
     else if (tpt == 1)
       tcb::adj_row_kernel<1, 1, 2><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);

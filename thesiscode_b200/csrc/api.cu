@@ -195,7 +195,7 @@ extern "C" int tc_get_smooth(tc_ctx* ctx, double* smooth) {
 }
 
 extern "C" int tc_set_adjoint_mode(tc_ctx* ctx, int mode) {
-  if (!ctx || mode < 0 || mode > 6) return TC_ERR_ARG;
+  if (!ctx || mode < 0 || mode > 7) return TC_ERR_ARG;
   ctx->adj_mode = mode;
   return TC_OK;
 }
