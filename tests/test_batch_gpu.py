@@ -58,3 +58,43 @@ def test_graph_replay_equals_eager_launches(gpu):
         np.testing.assert_array_equal(wa.xA, wb.xA)
         np.testing.assert_array_equal(wa.zetaA, wb.zetaA)
         np.testing.assert_array_equal(wa.xV, wb.xV)
+
+
+def test_batch_kernel_every_form_matches_oracle(gpu):
+    """The persistent batch kernel with one variant of every FP32C form in the variant table
+    (target-paired near/far/paired-reciprocal/pre-weighted forms, source-paired forms with
+    register or shared-memory accumulators, hi/lo near offsets, paired reciprocals), autotuning
+    off: one RK4 step of each instance matches the oracle within the coarse-grid bound (5e-7
+    for the source-paired forms; 1e-6 for the target-paired forms, variants kept for comparison,
+    whose tile origin is a target rather than the tile's centroid)."""
+    import ctypes
+
+    from thesiscode_b200 import _native as N
+
+    cnt = ctypes.c_int()
+    N.call("tc_pair_variant_count", N.TC_FP32C, ctypes.byref(cnt))
+    first_of_form = {}
+    for v in range(cnt.value):
+        info = (ctypes.c_int * 8)()
+        N.call("tc_pair_variant_info", N.TC_FP32C, v, info)
+        first_of_form.setdefault(info[7], v)
+    assert len(first_of_form) >= 8
+    ref0 = small_batch(seed=9)
+    expect = []
+    for r in ref0:
+        xV, xA, zA, *_ = O.bve_rk4(r.xV, r.xA, r.zetaA, r.areaA, np.zeros((0, 3)), 0.01, r.omega, r.deltas)
+        expect.append((xA, zA, xV))
+    for form, v in sorted(first_of_form.items()):
+        ws = [w.copy() for w in ref0]
+        ctx = Context(0, "fp32c")
+        ctx.set_omega(ws[0].omega)
+        ctx.set_deltas(*ws[0].deltas)
+        N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, v)
+        batch_rk4(ctx, ws, 0.01, 1, graph=False, autotune=False)
+        assert batch_info(ctx)["variant"] == v
+        ctx.close()
+        tol = TOL["fp32c"] if form & 8 else 1e-6
+        for b, (w, r, (xA, zA, xV)) in enumerate(zip(ws, ref0, expect)):
+            scale = np.abs(xA - r.xA).max()
+            assert np.abs(w.xA - xA).max() <= tol * scale, (form, v, b)
+            assert np.abs(w.zetaA - zA).max() <= tol * np.abs(zA - r.zetaA).max(), (form, v, b)

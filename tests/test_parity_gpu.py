@@ -140,7 +140,7 @@ def _variants_with_form(bits: int) -> list[int]:
     for v in range(cnt.value):
         info = (ctypes.c_int * 8)()
         N.call("tc_pair_variant_info", N.TC_FP32C, v, info)
-        if info[7] & bits == bits and not info[7] & 256:
+        if info[7] & bits == bits:
             out.append(v)
     return out
 

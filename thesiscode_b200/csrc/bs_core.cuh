@@ -210,6 +210,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // per-pair mask is needed.
 // ---------------------------------------------------------------------------
 constexpr float kSelfBias = 1e-30f;
+constexpr float kPadDenominator = 1e30f;
 
 // Far-field form (FM bit 0). For a source tile whose every source lies
 // farther than kFarRatio times the CTA's target radius rho (the largest
@@ -327,6 +328,13 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
       tv[h][3] = (float)E + kSelfBias;
       const float t2 = norm2_f32(tx, ty, tz);
       tv[h][4] = (float)(0.5 * ((double)t2 + E));
+      if (pos >= i_end) {
+        // padding (a copy of the middle target, result discarded): huge
+        // denominators, so that a paired reciprocal (FM bit 1) with the middle
+        // target's own self pair (D = kSelfBias) in the other lane stays finite
+        tv[h][3] = kPadDenominator;
+        tv[h][4] = kPadDenominator;
+      }
       rho2 = fmaxf(rho2, t2);
       ax[p][h] = ay[p][h] = az[p][h] = aw[p][h] = 0.0;
     }
@@ -546,11 +554,10 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // both offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to
 // FP32 (an absolute error of ulps of the patch radius, the dominant FP32C
 // error for nearest-neighbour pairs) no longer enters, and d keeps a few
-// ulps of its own length. Far tiles are unchanged. FM bit 8 (with bits 2 and
-// 3): the source side only, d = (s_hi - t_hi) + s_lo (near sources lie up to
-// about 3 patch radii from the origin, targets within one, so the source
-// offsets carry most of the rounding), half the extra operations and no
-// per-target registers.
+// ulps of its own length. Far tiles are unchanged. Both low parts are needed:
+// for the self pair s and t are the same point, so (s_hi - t_hi) and
+// (s_lo - t_lo) are both exactly 0 and the pair adds w * 0; correcting one
+// side only would leave d = s_lo there, a spurious self term.
 // PRF > 0: one source pair of every PRF shares a single MUFU reciprocal
 // (1/D_k = q D_k+1, 1/D_k+1 = q D_k, q = 1/(D_k D_k+1)), trading 8 XU cycles
 // for 3 FMA-pipe cycles per warp and target, so the FMA and XU pipes carry
@@ -685,7 +692,7 @@ struct SpAcc {
 };
 
 template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT, bool SMACC,
-          bool HILO, bool SRC_LO_ONLY = false>
+          bool HILO>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
@@ -772,7 +779,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     const double txd = frame_dot(fr, dx, dy, dz), tyd = frame_dot(fr + 3, dx, dy, dz),
                  tzd = frame_dot(fr + 6, dx, dy, dz);
     const float tx = (float)txd, ty = (float)tyd, tz = (float)tzd;
-    if (HILO && !SRC_LO_ONLY) {
+    if (HILO) {
       sm.tlo[(0 * T + t) * NT + threadIdx.x] = -(float)(txd - (double)tx);
       sm.tlo[(1 * T + t) * NT + threadIdx.x] = -(float)(tyd - (double)ty);
       sm.tlo[(2 * T + t) * NT + threadIdx.x] = -(float)(tzd - (double)tz);
@@ -889,8 +896,8 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         }
       } else {
         // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
-        float ntl[HILO && !SRC_LO_ONLY ? 3 * T : 1];
-        if (HILO && !SRC_LO_ONLY) {
+        float ntl[HILO ? 3 * T : 1];
+        if (HILO) {
 #pragma unroll
           for (int k = 0; k < 3 * T; ++k) ntl[k] = sm.tlo[k * NT + threadIdx.x];
         }
@@ -913,11 +920,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
             float2 dx = __fadd2_rn(sx, ntx[t]);
             float2 dy = __fadd2_rn(sy, nty[t]);
             float2 dz = __fadd2_rn(sz, ntz[t]);
-            if (HILO && SRC_LO_ONLY) {
-              dx = __fadd2_rn(dx, make_float2(lo.x, lo.y));
-              dy = __fadd2_rn(dy, make_float2(lo.z, lo.w));
-              dz = __fadd2_rn(dz, loz);
-            } else if (HILO) {
+            if (HILO) {
               dx = __fadd2_rn(dx, __fadd2_rn(make_float2(lo.x, lo.y), make_float2(ntl[t], ntl[t])));
               dy = __fadd2_rn(dy, __fadd2_rn(make_float2(lo.z, lo.w), make_float2(ntl[T + t], ntl[T + t])));
               dz = __fadd2_rn(dz, __fadd2_rn(loz, make_float2(ntl[2 * T + t], ntl[2 * T + t])));
@@ -968,8 +971,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   if constexpr (SP) {
     __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0, (FM & 4) != 0> sm;
     fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
-                  (FM & 4) != 0, (FM & 256) != 0>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
-                                                  stride, sm);
+                  (FM & 4) != 0>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
     fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
@@ -1027,8 +1029,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchL
       const BatchSeg S = B.segs[I.seg];
       double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
       fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
-                    (FM & 4) != 0, (FM & 256) != 0>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0,
-                                                    I.c1, out, B.stride, sm);
+                    (FM & 4) != 0>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out,
+                                   B.stride, sm);
     }
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;

@@ -93,8 +93,8 @@ const PairVariant kVariants64[] = {
 // reciprocal (2), pre-weighted far-field sources (4, with 1), source-paired
 // rotated-frame form (8, its own far/near forms; with it, bit 0 widens the
 // FP64 flushes by integer operations, bit 1 keeps the FP64 accumulators in
-// shared memory, bit 2 gives near tiles hi/lo offsets (bit 8: of the sources
-// only) and bits 4-7 give the period of the paired reciprocal).
+// shared memory, bit 2 gives near tiles hi/lo offsets and bits 4-7 give the
+// period of the paired reciprocal).
 const PairVariant kVariants32[] = {
     V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
     V32(256, 2, 16, 2, 4, 0), V32(128, 2, 32, 6, 4, 0), V32(256, 1, 32, 4, 8, 0),
@@ -127,8 +127,6 @@ const PairVariant kVariants32[] = {
     // near tiles with hi/lo offsets (form bit 2 with bit 3)
     VSPX(128, 3, 64, 6, 4, 14), VSPX(128, 2, 64, 6, 4, 12), VSPX(128, 2, 64, 6, 4, 14),
     VSPX(128, 3, 64, 5, 4, 14),
-    // source-side low parts only (form bit 8)
-    VSPX(128, 3, 64, 6, 4, 270), VSPX(128, 2, 64, 6, 4, 270),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);

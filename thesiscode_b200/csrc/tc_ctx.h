@@ -42,7 +42,7 @@ struct PairVariant {
   const void* fn;
   void (*launch_batch)(int grid, cudaStream_t stream, const BatchLaunch& B);
   const void* fn_batch;
-  int form;  // FP32C: bit 0 far form, bit 1 paired reciprocal, bit 2 pre-weighted far sources, bit 3 source-paired form (bits 4+: its paired-reciprocal period); FP64: 0
+  int form;  // FP32C: bit 3 source-paired form (with it: bit 0 integer-widened flush, bit 1 shared-memory accumulators, bit 2 hi/lo near offsets, bits 4-7 paired-reciprocal period); without it: bit 0 far form, bit 1 paired reciprocal, bit 2 pre-weighted far sources. FP64: 0
 };
 
 // Target segment as the host describes it before tiles are assigned.
