@@ -132,6 +132,32 @@ def test_fp32c_accuracy_does_not_depend_on_target_order(ctx32):
     assert np.abs(dX[rows] - ref).max() / np.abs(dX).max() <= FP32C_TOL_L6
 
 
+def test_every_pair_variant_delta0_small_grid(gpu):
+    """Every FP32C variant on a level-3 Gaussian with delta = 0 (no smoothing: the self pair's
+    exact zero is what keeps it out of the sum, and one tile covers most of the sphere, with
+    partial tiles and padding): all active and vertex rows against the oracle, within the
+    coarse-grid bound (1e-6 for the target-paired forms, kept for comparison)."""
+    import ctypes
+    w = configs.gaussian(level=3, delta=0.0)
+    refA = O.rows(0, np.arange(w.nA), None, w.xA, w.zetaA, w.areaA, delta=0.0, nthreads=8)
+    refV = O.rows(1, np.arange(w.nV), w.xV, w.xA, w.zetaA, w.areaA, delta=0.0, nthreads=8)
+    scale = max(np.abs(refA).max(), np.abs(refV).max())
+    cnt = ctypes.c_int()
+    N.call("tc_pair_variant_count", N.TC_FP32C, ctypes.byref(cnt))
+    for v in range(cnt.value):
+        info = (ctypes.c_int * 8)()
+        N.call("tc_pair_variant_info", N.TC_FP32C, v, info)
+        tol = FP32C_TOL_COARSE if info[7] & 8 else 1e-6
+        ctx = Context(0, "fp32c")
+        setup(ctx, w.omega, (0.0, 0.0, 0.0))
+        N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, v)
+        dA, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+        dV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+        ctx.close()
+        err = max(np.abs(dA - refA).max(), np.abs(dV - refV).max()) / scale
+        assert err <= tol, (v, info[7], err)
+
+
 def _variants_with_form(bits: int) -> list[int]:
     import ctypes
     cnt = ctypes.c_int()
