@@ -62,15 +62,23 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     objdir = LIBDIR / "obj"
     objdir.mkdir(parents=True, exist_ok=True)
     hdrs = headers()
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = objdir / (src.name + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
-            if verbose:
-                print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
+            cmds.append([nvcc, *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)])
+    # translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(run, c) for c in cmds]:
+            f.result()
     lib = lib_path()
     if force or _stale(lib, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart"]
