@@ -1,14 +1,15 @@
 """One launch of the pair kernels on a workload of a chosen size, for profilers.
 
     python -m thesiscode_b200.profile_case --precision fp32c --level 6 \
-        [--what velocity|rk4|adjoint|batch|strat] [--variant ID]
+        [--what velocity|rk4|adjoint|batch|strat|grid] [--variant ID]
 
 `velocity` runs one TC_ACTIVE and one TC_VERTEX sum (two pair-kernel launches);
 `rk4` runs one fused RK4 step (four pair-kernel launches); `adjoint` runs the
 FP64 adjoint of two RK4 steps (eight vector-Jacobian pair launches); `batch`
 runs one RK4 step of the 64-instance Gaussian ensemble (levels 3 to `--level`)
 without autotuning or graph (four persistent batch-kernel launches); `strat`
-runs one forced stratosphere RK4 step (parity mode). The Gaussian-vortex
+runs one forced stratosphere RK4 step (parity mode); `grid` generates the
+icosahedral grid of `--level` on the GPU (tc_icos_grid_device). The Gaussian-vortex
 workload with delta 0.01 is used at every level for the first three.
 `--variant` selects a pair-kernel variant of the chosen precision (default:
 the library's default) for `velocity` and `rk4`.
@@ -26,12 +27,17 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--level", type=int, default=6)
-    ap.add_argument("--what", default="velocity", choices=["velocity", "rk4", "adjoint", "batch", "strat"])
+    ap.add_argument("--what", default="velocity",
+                    choices=["velocity", "rk4", "adjoint", "batch", "strat", "grid"])
     ap.add_argument("--variant", type=int, default=None)
     a = ap.parse_args()
-    if a.what in ("batch", "strat"):
+    if a.what in ("batch", "strat", "grid"):
         ctx = Context(0, a.precision)
-        if a.what == "batch":
+        if a.what == "grid":
+            from .grid import new_icos_grid_device
+
+            new_icos_grid_device(ctx, a.level)
+        elif a.what == "batch":
             from .batch import batch_rk4
 
             ws = configs.batched_gaussians(count=64, seed=4, levels=tuple(range(3, a.level + 1)))
