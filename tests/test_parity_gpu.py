@@ -158,6 +158,35 @@ def test_every_pair_variant_delta0_small_grid(gpu):
         assert err <= tol, (v, info[7], err)
 
 
+def test_fp32c_variant_chosen_by_size(gpu):
+    """The default FP32C variant follows the problem size (33 below 131,072 sources, 54 above);
+    selecting a variant fixes it, and -1 restores the automatic choice."""
+    import ctypes
+
+    def used(ctx):
+        v = ctypes.c_int()
+        N.call("tc_get_pair_variant", ctx.handle, N.TC_FP32C, ctypes.byref(v))
+        return v.value
+
+    small = configs.gaussian(level=4, delta=0.01)
+    large = configs.gaussian(level=7, delta=0.01)
+    ctx = Context(0, "fp32c")
+    setup(ctx, small.omega, small.deltas)
+    ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
+    assert used(ctx) == 33
+    ctx.velocity(N.TC_VERTEX, large.xV[:1024], large.xA, large.zetaA, large.areaA)
+    assert used(ctx) == 54
+    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, 54)
+    ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
+    assert used(ctx) == 54
+    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, -1)
+    dX, _ = ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
+    assert used(ctx) == 33
+    ref = O.rows(1, np.arange(small.nV), small.xV, small.xA, small.zetaA, small.areaA, delta=0.01, nthreads=8)
+    assert rel_err(dX, ref) <= FP32C_TOL
+    ctx.close()
+
+
 def _variants_with_form(bits: int) -> list[int]:
     import ctypes
     cnt = ctypes.c_int()

@@ -112,6 +112,7 @@ extern "C" int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, cons
   double* partial = reinterpret_cast<double*>(static_cast<char*>(base) + src_bytes);
 
   const bool fp64 = ctx->precision == TC_FP64;
+  if (!fp64 && (rc = tcb::use_fp32c_variant(ctx, n))) return rc;
   const tcb::PairVariant* v = tcb::variant(ctx->precision, fp64 ? ctx->var64 : ctx->var32);
   const int tb = v->nt * v->tpt;
   const int len = i1 - i0;

@@ -97,6 +97,7 @@ struct tc_ctx {
   tcb::PairCfg cfg64{256, 2, 256};
   tcb::PairCfg cfg32{256, 4, 256};
   int var64 = 2, var32 = 54;  // pair-kernel variants in use (see kVariants64/32)
+  bool auto32 = true;  // FP32C variant chosen per launch by problem size (tc_set_pair_variant turns it off)
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
   int adj_mode = 6;  // adjoint VJP: 3-6 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
@@ -156,4 +157,6 @@ __global__ void velocity_epilogue_kernel(const double* __restrict__ x, const int
                                          double* __restrict__ dVort);
 int variant_count(int precision);
 int select_variant(tc_ctx* ctx, int precision, int id);
+// With ctx->auto32, selects the FP32C variant for a launch over n sources.
+int use_fp32c_variant(tc_ctx* ctx, int n);
 }  // namespace tcb
