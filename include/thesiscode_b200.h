@@ -48,7 +48,7 @@ extern "C" {
 
 /* ---- visiting order of targets in the FP32C pair kernel --------------- */
 #define TC_ORDER_GIVEN 0   /* the caller's order                             */
-#define TC_ORDER_HILBERT 1 /* sorted along a 3-D Hilbert curve (default)     */
+#define TC_ORDER_HILBERT 1 /* along a Hilbert curve over the cube faces (default) */
 
 /* ---- target classes (the three RHS routines of the reference) ------- */
 #define TC_ACTIVE 0  /* BVEActiveRHS  PanelVelocityParallel.f90:1287-1334:
@@ -114,9 +114,10 @@ int tc_get_omega(tc_ctx* ctx, double* omega);
 int tc_set_smooth(tc_ctx* ctx, double smooth);
 int tc_get_smooth(tc_ctx* ctx, double* smooth);
 /* FP32C only: visit targets in the caller's order or along a Hilbert curve
- * (default; results are returned in the caller's order either way). The
- * compensated arithmetic is accurate when a CTA's targets are spatially
- * close; the Hilbert order guarantees that for any input order. */
+ * over the six cube faces, continuous from face to face (default; results are
+ * returned in the caller's order either way). The compensated arithmetic is
+ * accurate when a CTA's targets are spatially close; the curve order
+ * guarantees that for any input order. */
 int tc_set_target_order(tc_ctx* ctx, int order);
 /* delta of each target class (reference: 0, 0, smooth). */
 int tc_set_deltas(tc_ctx* ctx, double delta_active, double delta_vertex, double delta_passive);

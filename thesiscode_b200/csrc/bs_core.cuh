@@ -187,11 +187,12 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // ---------------------------------------------------------------------------
 // FP32-compensated pair kernel.
 //
-// Each CTA takes the position c of the middle target of its tile as origin.
+// Target-paired form (the variants without form bit 3): each CTA takes the
+// position c of the middle target of its tile as origin.
 // Sources are converted once per CTA and tile from FP64 to FP32 offsets
 // s_k = fl32(x_k - c) (their FP64 difference rounded once), targets likewise
-// t_i = fl32(x_i - c). Targets are visited in a spatially coherent order (a
-// Hilbert order computed by the library, or the caller's order), so a CTA's
+// t_i = fl32(x_i - c). Targets are visited in a spatially coherent order (the
+// library's cube-face Hilbert order, sphere_order.cuh, or the caller's), so a CTA's
 // targets form a compact patch and every nearby pair has small |s_k|, |t_i|:
 // d = s_k - t_i carries an absolute error of a few ulps of the patch size
 // instead of ulps of 1. The denominator uses the cancellation-free form
@@ -533,7 +534,8 @@ __device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const i
 // per source), shared by the T targets of a thread.
 //
 // Coordinates are taken in a per-CTA orthonormal frame R = (e1, e2, e3) with
-// e3 along the origin c (the CTA's middle target): s_k = R(x_k - c),
+// e3 along the origin c (the centroid of the CTA's targets projected to the
+// sphere): s_k = R(x_k - c),
 // t_i = R(x_i - c), both from FP64 and rounded once. Distances and dot
 // products are frame-invariant, so the near form and the far denominator are
 // those of the target-paired kernel. The far numerator accumulates

@@ -25,7 +25,7 @@ __global__ void hilbert_keys_kernel(const double* __restrict__ x, int i0, int n,
 
 }  // namespace
 
-// perm[i0 .. i1) <- the indices i0..i1-1 sorted by Hilbert key of x[i].
+// perm[i0 .. i1) <- the indices i0..i1-1 sorted by the sphere key of x[i].
 int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm) {
   const int n = i1 - i0;
   if (n <= 0) return TC_OK;

@@ -68,7 +68,7 @@ struct Rk4State {
   DevBuf ke;                            // kineticEnergy(nA), stage 1
   DevBuf keBlocks;                      // per-block partial sums of KE*A
   DevBuf totalKE;                       // one value per step
-  DevBuf permA, permV, permQ;           // FP32C visiting orders (Hilbert), per class
+  DevBuf permA, permV, permQ;           // FP32C visiting orders (cube-face Hilbert), per class
   bool ordered = false;                 // perm* hold orders of the current stage ranges
   int order_range[6] = {0, 0, 0, 0, 0, 0};
   // forced (stratosphere) model: source vorticity rebuilt each stage from absA
@@ -137,7 +137,7 @@ int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* 
 // rows are row_offset + i.
 int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int m, int i0, int i1,
                              int row_offset, int n_out, int nchunks, double* dX, double* dVort);
-// perm[i0..i1) <- i0..i1-1 sorted along a Hilbert curve through x[3*i..]
+// perm[i0..i1) <- i0..i1-1 sorted along the cube-face Hilbert curve (sphere_order.cuh)
 int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm);
 // One RK4 stage epilogue over the three classes' ranges.
 // total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
