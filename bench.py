@@ -359,9 +359,21 @@ def sample_rows(w, frac, seed=11):
     return ra, rv
 
 
+def sample_frac(w, seconds, threads, lo=1.0 / 64):
+    """Fraction of target rows (a power of two) that the CPU oracle sums in about `seconds`
+    on `threads` host threads, from a timed 1/1024 sample; at least `lo`, at most all rows."""
+    cal = cpu_baseline(w, frac=1.0 / 1024, threads=threads)["seconds"]
+    want = seconds / max(cal, 1e-6) / 1024
+    frac = lo
+    while frac * 2 <= min(want, 1.0):
+        frac *= 2
+    return frac
+
+
 def cpu_baseline(w, frac=1.0 / 64, threads=None):
-    """The CPU FP64 oracle (restated reference loops) on all host cores over a seeded 1/64
-    sample of the target rows of one RK4 stage; returns interactions/s and the sampled sums."""
+    """The CPU FP64 oracle (restated reference loops) on all host cores over a seeded
+    sample (`frac` of the target rows) of one RK4 stage; returns interactions/s and the
+    sampled sums."""
     from oracle import oracle as O
 
     threads = threads or os.cpu_count() or 1
@@ -481,7 +493,8 @@ def run_ours(args):
             line["adjoint"] = time_adjoint(device)
             line["batched"] = time_batch(device)
         if world == 1 and not args.no_cpu:
-            cb = cpu_baseline(w)
+            threads = os.cpu_count() or 1
+            cb = cpu_baseline(w, frac=sample_frac(w, 10.0, threads), threads=threads)
             line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],
                                     "kind": "port", "sample": cb["sample"], "seconds": cb["seconds"]}
             line["error_vs_fp64_oracle"] = {
@@ -499,9 +512,10 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_baseline(w, frac=1.0 / 1024, threads=threads)
+    frac = sample_frac(w, 2.0, threads, lo=1.0 / 1024)
     vals, secs = [], []
     for _ in range(args.steps):
-        cb = cpu_baseline(w, frac=1.0 / 256, threads=threads)
+        cb = cpu_baseline(w, frac=frac, threads=threads)
         vals.append(cb["value"])
         secs.append(cb["seconds"])
     v = statistics.median(vals)
