@@ -361,9 +361,9 @@ def sample_rows(w, frac, seed=11):
 
 def sample_frac(w, seconds, threads, lo=1.0 / 64):
     """Fraction of target rows (a power of two) that the CPU oracle sums in about `seconds`
-    on `threads` host threads, from a timed 1/1024 sample; at least `lo`, at most all rows."""
-    cal = cpu_baseline(w, frac=1.0 / 1024, threads=threads)["seconds"]
-    want = seconds / max(cal, 1e-6) / 1024
+    on `threads` host threads, from a timed 1/256 sample; at least `lo`, at most all rows."""
+    cal = cpu_baseline(w, frac=1.0 / 256, threads=threads)["seconds"]
+    want = seconds / max(cal, 1e-6) / 256
     frac = lo
     while frac * 2 <= min(want, 1.0):
         frac *= 2
