@@ -24,6 +24,68 @@ int check_finite_host(const double* p, size_t n, const char* what) {
   return TC_OK;
 }
 
+// Host entry points scan their inputs for NaN/Inf on the host while the GPU
+// already works on the device copies, and copy results back only once the
+// scan passed, so a refused call leaves the caller's arrays as they were.
+// Results are scanned on the device, where they already are: only the first
+// bad index of each array crosses back.
+struct HostArray {
+  const double* p;
+  size_t n;
+  const char* what;
+};
+
+int check_finite_host_all(const HostArray* a, int count) {
+  int rc = TC_OK;
+  for (int j = 0; j < count && !rc; ++j)
+    if (a[j].p) rc = check_finite_host(a[j].p, a[j].n, a[j].what);
+  return rc;
+}
+
+constexpr int kMaxScans = 4;
+
+__global__ void first_nonfinite_kernel(const double* __restrict__ p, size_t n,
+                                       unsigned long long* __restrict__ first) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    if (!isfinite(p[i])) {  // the first in this thread's stride is its smallest
+      atomicMin(first, (unsigned long long)i);
+      break;
+    }
+}
+
+// Enqueues device scans of up to kMaxScans result arrays (null or empty ones
+// are skipped) into ctx->check_buf.
+int scan_results_device(tc_ctx* ctx, const HostArray* a, int count) {
+  int rc = ctx->check_buf.ensure(kMaxScans * sizeof(unsigned long long));
+  if (rc) return rc;
+  unsigned long long* first = ctx->check_buf.as<unsigned long long>();
+  TC_CUDA_TRY(cudaMemsetAsync(first, 0xFF, kMaxScans * sizeof(unsigned long long), ctx->stream));
+  for (int j = 0; j < count; ++j) {
+    if (!a[j].p || a[j].n == 0) continue;
+    const size_t want = (a[j].n + 255) / 256, cap = (size_t)ctx->num_sms * 8;
+    first_nonfinite_kernel<<<(int)std::min(want, cap), 256, 0, ctx->stream>>>(a[j].p, a[j].n,
+                                                                               first + j);
+    TC_CUDA_TRY(cudaGetLastError());
+    ctx->launches += 1;
+  }
+  return TC_OK;
+}
+
+// Reads back what scan_results_device found (synchronises the stream).
+int scan_results_status(tc_ctx* ctx, const HostArray* a, int count) {
+  unsigned long long first[kMaxScans];
+  TC_CUDA_TRY(cudaMemcpyAsync(first, ctx->check_buf.ptr, sizeof(first), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+  TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int j = 0; j < count; ++j)
+    if (a[j].p && first[j] != ~0ull) {
+      tc_record_error("non-finite value in %s at index %llu", a[j].what, first[j]);
+      return TC_ERR_NONFINITE;
+    }
+  return TC_OK;
+}
+
 int begin(tc_ctx* ctx) {
   if (!ctx) {
     tc_record_error("null context");
@@ -126,6 +188,7 @@ extern "C" int tc_destroy(tc_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->partial.release();
+  ctx->check_buf.release();
   for (auto& b : ctx->scratch) b.release();
   tcb::Rk4State& R = ctx->rk;
   DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV, &R.xiQ,
@@ -242,11 +305,6 @@ extern "C" int tc_bs_velocity(tc_ctx* ctx, int target_class, const double* X, in
   int rc = begin(ctx);
   if (rc) return rc;
   if ((rc = check_velocity_args(target_class, X, m, src_x, vort, area, n, i0, i1, dX))) return rc;
-  if ((rc = check_finite_host(src_x, 3 * (size_t)n, "src_x")) ||
-      (rc = check_finite_host(vort, (size_t)n, "vort")) ||
-      (rc = check_finite_host(area, (size_t)n, "area")))
-    return rc;
-  if (target_class != TC_ACTIVE && (rc = check_finite_host(X, 3 * (size_t)m, "X"))) return rc;
   const size_t nb = (size_t)std::max(n, 1) * sizeof(double);
   const size_t mb = (size_t)std::max(m, 1) * sizeof(double);
   if ((rc = ctx->scratch[1].ensure(3 * nb + 2 * nb)) || (rc = ctx->scratch[2].ensure(3 * mb)) ||
@@ -267,11 +325,20 @@ extern "C" int tc_bs_velocity(tc_ctx* ctx, int target_class, const double* X, in
   rc = velocity_device(ctx, target_class, target_class == TC_ACTIVE ? nullptr : d_X, m, d_src,
                        d_vort, d_area, n, i0, i1, d_dX, d_dV);
   if (rc) return rc;
+  const HostArray in[4] = {{src_x, 3 * (size_t)n, "src_x"},
+                           {vort, (size_t)n, "vort"},
+                           {area, (size_t)n, "area"},
+                           {target_class != TC_ACTIVE ? X : nullptr, 3 * (size_t)m, "X"}};
+  if ((rc = check_finite_host_all(in, 4))) {
+    cudaStreamSynchronize(s);
+    return rc;
+  }
+  const HostArray out[1] = {{d_dX, 3 * (size_t)m, "dX (result)"}};
+  if ((rc = scan_results_device(ctx, out, 1))) return rc;
   TC_CUDA_TRY(cudaMemcpyAsync(dX, d_dX, 3 * (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
   if (target_class == TC_ACTIVE && dVort)
     TC_CUDA_TRY(cudaMemcpyAsync(dVort, d_dV, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
-  TC_CUDA_TRY(cudaStreamSynchronize(s));
-  return check_finite_host(dX, 3 * (size_t)m, "dX (result)");
+  return scan_results_status(ctx, out, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -343,11 +410,8 @@ extern "C" int tc_bs_velocity_soa(tc_ctx* ctx, const double* x, const double* y,
     tc_record_error("tc_bs_velocity_soa: bad arguments");
     return TC_ERR_ARG;
   }
-  const double* in[5] = {x, y, z, vort, area};
-  const char* names[5] = {"x", "y", "z", "vort", "area"};
-  for (int a = 0; a < 5; ++a)
-    if ((rc = check_finite_host(in[a], (size_t)n, names[a]))) return rc;
   if (n == 0) return TC_OK;
+  const double* in[5] = {x, y, z, vort, area};
   const size_t b = (size_t)n * sizeof(double);
   if ((rc = ctx->scratch[1].ensure(9 * b))) return rc;
   double* d = ctx->scratch[1].as<double>();
@@ -363,12 +427,22 @@ extern "C" int tc_bs_velocity_soa(tc_ctx* ctx, const double* x, const double* y,
   if ((rc = tc_bs_velocity_soa_device(ctx, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n,
                                       d + 4 * (size_t)n, n, i0, i1, ddx, ddy, ddz, ddv)))
     return rc;
+  const HostArray hin[5] = {{x, (size_t)n, "x"},
+                            {y, (size_t)n, "y"},
+                            {z, (size_t)n, "z"},
+                            {vort, (size_t)n, "vort"},
+                            {area, (size_t)n, "area"}};
+  if ((rc = check_finite_host_all(hin, 5))) {
+    cudaStreamSynchronize(s);
+    return rc;
+  }
+  const HostArray out[1] = {{ddx, (size_t)n, "dx (result)"}};
+  if ((rc = scan_results_device(ctx, out, 1))) return rc;
   TC_CUDA_TRY(cudaMemcpyAsync(dx, ddx, b, cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaMemcpyAsync(dy, ddy, b, cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaMemcpyAsync(dz, ddz, b, cudaMemcpyDeviceToHost, s));
   if (dVort) TC_CUDA_TRY(cudaMemcpyAsync(dVort, ddv, b, cudaMemcpyDeviceToHost, s));
-  TC_CUDA_TRY(cudaStreamSynchronize(s));
-  return check_finite_host(dx, (size_t)n, "dx (result)");
+  return scan_results_status(ctx, out, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -403,11 +477,21 @@ int check_rk4_sizes(int nA, int nV, int nQ) {
   return TC_OK;
 }
 
-}  // namespace
+// The host arrays tc_rk4_load copies, for the finite scan.
+int rk4_host_inputs(const double* xA, const double* zetaA, const double* areaA, int nA,
+                    const double* xV, int nV, const double* xQ, int nQ) {
+  const HostArray in[5] = {{xA, 3 * (size_t)nA, "xA"},
+                           {zetaA, (size_t)nA, "zetaA"},
+                           {areaA, (size_t)nA, "areaA"},
+                           {xV, 3 * (size_t)nV, "xV"},
+                           {xQ, 3 * (size_t)nQ, "xQ"}};
+  return check_finite_host_all(in, 5);
+}
 
-extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
-                           const double* areaA, int nA, const double* xV, int nV,
-                           const double* xQ, int nQ, int on_device) {
+// tc_rk4_load; with scan_host = false the caller scans the host inputs itself
+// (after it has queued the work on them).
+int rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA, const double* areaA, int nA,
+             const double* xV, int nV, const double* xQ, int nQ, int on_device, bool scan_host) {
   int rc = begin(ctx);
   if (rc) return rc;
   if ((rc = check_rk4_sizes(nA, nV, nQ))) return rc;
@@ -415,14 +499,8 @@ extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
     tc_record_error("tc_rk4_load: null array argument");
     return TC_ERR_ARG;
   }
-  if (!on_device) {
-    if ((rc = check_finite_host(xA, 3 * (size_t)nA, "xA")) ||
-        (rc = check_finite_host(zetaA, (size_t)nA, "zetaA")) ||
-        (rc = check_finite_host(areaA, (size_t)nA, "areaA")) ||
-        (rc = check_finite_host(xV, 3 * (size_t)nV, "xV")) ||
-        (rc = check_finite_host(xQ, 3 * (size_t)nQ, "xQ")))
-      return rc;
-  }
+  if (!on_device && scan_host && (rc = rk4_host_inputs(xA, zetaA, areaA, nA, xV, nV, xQ, nQ)))
+    return rc;
   if ((rc = rk4_alloc(ctx, nA, nV, nQ))) return rc;
   tcb::Rk4State& R = ctx->rk;
   cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -439,6 +517,14 @@ extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
   R.ordered = false;
   R.strat = false;
   return TC_OK;
+}
+
+}  // namespace
+
+extern "C" int tc_rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA,
+                           const double* areaA, int nA, const double* xV, int nV,
+                           const double* xQ, int nQ, int on_device) {
+  return rk4_load(ctx, xA, zetaA, areaA, nA, xV, nV, xQ, nQ, on_device, true);
 }
 
 extern "C" int tc_rk4_store(tc_ctx* ctx, double* xA, double* zetaA, double* xV, double* xQ,
@@ -698,9 +784,9 @@ int advance_graph(tc_ctx* ctx, double dt, int nsteps) {
   return TC_OK;
 }
 
-}  // namespace
-
-extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalKE) {
+// tc_rk4_advance without the read-back of totalKE: everything is queued on
+// the context's stream.
+int rk4_advance_enqueue(tc_ctx* ctx, double dt, int nsteps) {
   int rc = begin(ctx);
   if (rc) return rc;
   tcb::Rk4State& R = ctx->rk;
@@ -732,8 +818,43 @@ extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalK
   } else if ((rc = advance_steps(ctx, dt, 0, nsteps))) {
     return rc;
   }
-  if (totalKE && nsteps > 0) {
+  return TC_OK;
+}
+
+// After the steps of a host-array call: queues the device scans of the new
+// positions and (when the caller wants it) vorticity, the read-back of
+// totalKE and the state (tc_rk4_store, which synchronises). The caller then
+// reads the scans' outcome with scan_results_status(ctx, out, 2).
+int rk4_results_to_host(tc_ctx* ctx, double* xA, double* zetaA, double* xV, double* xQ,
+                        int nsteps, double* totalKE, double* kineticEnergy, HostArray out[2]) {
+  tcb::Rk4State& R = ctx->rk;
+  out[0] = HostArray{R.x0A.as<double>(), 3 * (size_t)R.nA, "xA (result)"};
+  out[1] = HostArray{zetaA ? R.z0.as<double>() : nullptr, (size_t)R.nA,
+                     R.strat ? "relVortA (result)" : "zetaA (result)"};
+  int rc = scan_results_device(ctx, out, 2);
+  if (rc) return rc;
+  if (totalKE && nsteps > 0)
     TC_CUDA_TRY(cudaMemcpyAsync(totalKE, R.totalKE.ptr, (size_t)nsteps * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  return tc_rk4_store(ctx, xA, zetaA, xV, xQ, kineticEnergy, 0);
+}
+
+// Error return of a host-array call whose work is queued: waits for it, so
+// that no copy still reads the caller's arrays, and drops the loaded state
+// when it came from rejected inputs.
+int fail_queued(tc_ctx* ctx, int rc, bool drop_state) {
+  cudaStreamSynchronize(ctx->stream);
+  if (drop_state) ctx->rk.ready = false;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalKE) {
+  int rc = rk4_advance_enqueue(ctx, dt, nsteps);
+  if (rc) return rc;
+  if (totalKE && nsteps > 0) {
+    TC_CUDA_TRY(cudaMemcpyAsync(totalKE, ctx->rk.totalKE.ptr, (size_t)nsteps * sizeof(double),
                                 cudaMemcpyDeviceToHost, ctx->stream));
     TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   }
@@ -741,16 +862,20 @@ extern "C" int tc_rk4_advance(tc_ctx* ctx, double dt, int nsteps, double* totalK
 }
 
 // The drop-in BVERK4 call on host arrays: load, nsteps fused steps on the
-// device, store back.
+// device, store back. The host scans the inputs for NaN/Inf while the steps
+// run; the results are copied back only after that scan passed.
 extern "C" int tc_rk4_step(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA, int nA,
                            double* xV, int nV, double* xQ, int nQ, double dt, int nsteps,
                            double* totalKE, double* kineticEnergy) {
-  int rc = tc_rk4_load(ctx, xA, zetaA, areaA, nA, xV, nV, xQ, nQ, 0);
+  int rc = rk4_load(ctx, xA, zetaA, areaA, nA, xV, nV, xQ, nQ, 0, false);
   if (rc) return rc;
-  if ((rc = tc_rk4_advance(ctx, dt, nsteps, totalKE))) return rc;
-  if ((rc = tc_rk4_store(ctx, xA, zetaA, xV, xQ, kineticEnergy, 0))) return rc;
-  if ((rc = check_finite_host(xA, 3 * (size_t)nA, "xA (result)"))) return rc;
-  return check_finite_host(zetaA, (size_t)nA, "zetaA (result)");
+  if ((rc = rk4_advance_enqueue(ctx, dt, nsteps))) return fail_queued(ctx, rc, false);
+  if ((rc = rk4_host_inputs(xA, zetaA, areaA, nA, xV, nV, xQ, nQ)))
+    return fail_queued(ctx, rc, true);
+  HostArray out[2];
+  if ((rc = rk4_results_to_host(ctx, xA, zetaA, xV, xQ, nsteps, totalKE, kineticEnergy, out)))
+    return rc;
+  return scan_results_status(ctx, out, 2);
 }
 
 extern "C" int tc_rk4_step_device(tc_ctx* ctx, double* xA, double* zetaA, const double* areaA,
@@ -778,9 +903,8 @@ extern "C" int tc_strat_rk4_step(tc_ctx* ctx, double* xA, const double* absVortA
     tc_record_error("tc_strat_rk4_step: bad arguments");
     return TC_ERR_ARG;
   }
-  int rc = check_finite_host(absVortA, (size_t)nA, "absVortA");
-  if (rc || (absVortV && (rc = check_finite_host(absVortV, (size_t)nV, "absVortV")))) return rc;
-  if ((rc = tc_rk4_load(ctx, xA, absVortA, areaA, nA, xV, nV, xQ, nQ, 0))) return rc;
+  int rc = rk4_load(ctx, xA, absVortA, areaA, nA, xV, nV, xQ, nQ, 0, false);
+  if (rc) return rc;
   tcb::Rk4State& R = ctx->rk;
   const size_t D = sizeof(double);
   if ((rc = R.absA.ensure((size_t)std::max(nA, 1) * D)) ||
@@ -794,19 +918,25 @@ extern "C" int tc_strat_rk4_step(tc_ctx* ctx, double* xA, const double* absVortA
   R.step = 0;
   R.strat_dt = dt;
   // (advance packs the stage-1 sources first, which also sets relVortA at t)
-  if ((rc = tc_rk4_advance(ctx, dt, nsteps, totalKE))) return rc;
-  if ((rc = tc_rk4_store(ctx, xA, relVortA, xV, xQ, kineticEnergy, 0))) return rc;
+  if ((rc = rk4_advance_enqueue(ctx, dt, nsteps))) return fail_queued(ctx, rc, false);
+  const HostArray in[2] = {{absVortA, (size_t)nA, "absVortA"},
+                           {absVortV, (size_t)nV, "absVortV"}};
+  if ((rc = check_finite_host_all(in, 2)) ||
+      (rc = rk4_host_inputs(xA, absVortA, areaA, nA, xV, nV, xQ, nQ)))
+    return fail_queued(ctx, rc, true);
+  HostArray out[2];
+  if ((rc = rk4_results_to_host(ctx, xA, relVortA, xV, xQ, nsteps, totalKE, kineticEnergy, out)))
+    return rc;
   if (relVortV && nV) {
-    tcb::DevBuf out;
-    if ((rc = out.ensure(nV * D))) return rc;
+    tcb::DevBuf rv;
+    if ((rc = rv.ensure(nV * D))) return rc;
     if ((rc = tcb::launch_strat_rel_vort(ctx, R.absV.as<double>(), R.x0V.as<double>(), nV,
-                                         R.t0 + (double)R.step * dt, out.as<double>())))
+                                         R.t0 + (double)R.step * dt, rv.as<double>())))
       return rc;
-    TC_CUDA_TRY(cudaMemcpyAsync(relVortV, out.ptr, nV * D, cudaMemcpyDeviceToHost, ctx->stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(relVortV, rv.ptr, nV * D, cudaMemcpyDeviceToHost, ctx->stream));
     TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   }
-  if ((rc = check_finite_host(xA, 3 * (size_t)nA, "xA (result)"))) return rc;
-  return relVortA ? check_finite_host(relVortA, (size_t)nA, "relVortA (result)") : TC_OK;
+  return scan_results_status(ctx, out, 2);
 }
 
 // Pair-kernel variants (the launch shapes the autotuner searches).

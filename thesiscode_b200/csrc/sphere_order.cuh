@@ -64,8 +64,9 @@ __device__ __forceinline__ unsigned sphere_key(double x, double y, double z) {
   const double inv = major != 0.0 ? 1.0 / fabs(major) : 0.0;
   const int n = 1 << kFaceBits;
   double qu = (u * inv + 1.0) * 0.5 * n, qv = (v * inv + 1.0) * 0.5 * n;
-  qu = qu < 0.0 ? 0.0 : (qu > n - 1 ? n - 1 : qu);
-  qv = qv < 0.0 ? 0.0 : (qv > n - 1 ? n - 1 : qv);
+  // fmax/fmin also send a NaN coordinate (a non-finite input) to cell 0
+  qu = fmin(fmax(qu, 0.0), (double)(n - 1));
+  qv = fmin(fmax(qv, 0.0), (double)(n - 1));
   unsigned X = (unsigned)qu, Y = (unsigned)qv, d = 0;
   for (unsigned s = (unsigned)n >> 1; s > 0; s >>= 1) {
     const unsigned rx = (X & s) ? 1u : 0u, ry = (Y & s) ? 1u : 0u;

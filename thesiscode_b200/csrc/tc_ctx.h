@@ -108,6 +108,7 @@ struct tc_ctx {
   tcb::DevBuf partial;    // pair-kernel partial sums
   tcb::DevBuf scratch[6]; // one-call buffers (velocity entry points)
   tcb::DevBuf grid_buf[6];  // tc_icos_grid_device: edge and panel tables, prefix sums
+  tcb::DevBuf check_buf;    // first non-finite index of each result array scanned on the device
   tcb::Rk4State rk;
   // instrumentation (tc_stats): kernels launched, and CUDA-event time of the
   // pair kernels when timing is on (events recorded on ctx->stream).
