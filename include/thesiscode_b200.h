@@ -290,14 +290,16 @@ int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr, int
  * lanes of each f32x2 instruction carry two sources of one target; with it
  * bit 1 = FP64 accumulators in shared memory, bit 2 = hi/lo near-pair
  * offsets (the accurate variants), bit 0 = flush widened by integer
- * operations, bits 4-7 = period of a paired reciprocal); bit 3 clear =
+ * operations, bits 4-7 = period of a paired reciprocal, bits 8-9 = log2
+ * of the flush lengths between flushes in tiles whose every source is
+ * far); bit 3 clear =
  * target-paired kernel (bit 0 far-field expansion for well-separated source
  * tiles, bit 1 one reciprocal per two targets, bit 2 pre-weighted far
  * sources). FP64 form: 0. */
 int tc_pair_variant_count(int precision, int* count);
 int tc_pair_variant_info(int precision, int id, int* info8);
 /* Select a variant. For FP32C the default is chosen per launch by problem
- * size (variant 33 below 131,072 sources, 54 above); selecting a variant turns
+ * size (variant 71 below 131,072 sources, 68 above); selecting a variant turns
  * that off, and id = -1 turns it back on. tc_get_pair_variant returns the
  * variant in use (for FP32C with the automatic choice: the one last used). */
 int tc_set_pair_variant(tc_ctx* ctx, int precision, int id);

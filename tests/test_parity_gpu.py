@@ -159,7 +159,7 @@ def test_every_pair_variant_delta0_small_grid(gpu):
 
 
 def test_fp32c_variant_chosen_by_size(gpu):
-    """The default FP32C variant follows the problem size (33 below 131,072 sources, 54 above);
+    """The default FP32C variant follows the problem size (71 below 131,072 sources, 68 above);
     selecting a variant fixes it, and -1 restores the automatic choice."""
     import ctypes
 
@@ -173,15 +173,15 @@ def test_fp32c_variant_chosen_by_size(gpu):
     ctx = Context(0, "fp32c")
     setup(ctx, small.omega, small.deltas)
     ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
-    assert used(ctx) == 33
+    assert used(ctx) == 71
     ctx.velocity(N.TC_VERTEX, large.xV[:1024], large.xA, large.zetaA, large.areaA)
-    assert used(ctx) == 54
-    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, 54)
+    assert used(ctx) == 68
+    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, 68)
     ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
-    assert used(ctx) == 54
+    assert used(ctx) == 68
     N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, -1)
     dX, _ = ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
-    assert used(ctx) == 33
+    assert used(ctx) == 71
     ref = O.rows(1, np.arange(small.nV), small.xV, small.xA, small.zetaA, small.areaA, delta=0.01, nthreads=8)
     assert rel_err(dX, ref) <= FP32C_TOL
     ctx.close()

@@ -694,7 +694,7 @@ struct SpAcc {
 };
 
 template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT, bool SMACC,
-          bool HILO>
+          bool HILO, int FARK>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
@@ -703,9 +703,11 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(PRF == 0 || (FLUSH / 2) % PRF == 0, "paired-reciprocal period divides the flush");
   static_assert(NT % 32 == 0, "whole warps");
+  static_assert(TS % (FLUSH * FARK) == 0, "far-tile flush interval divides the tile");
   constexpr int TB = NT * T;
   constexpr int NP = TS / 2;
   constexpr int FP = FLUSH / 2;
+  constexpr int FPF = FP * FARK;  // source pairs between flushes in all-far tiles
   constexpr int GRP = PRF > 0 ? PRF : 1;  // source pairs per group; the first is paired
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
@@ -855,14 +857,16 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     // (NT = TS/2 source pairs, FP = 32): segment g's minimum |s|^2 is warp
     // g's, so only the segments that hold near sources take the near form.
     // Otherwise one test for the whole tile.
-    // A tile whose every segment is far runs one tight far loop.
+    // A tile whose every segment is far runs one tight far loop, flushed
+    // every FARK segments (far terms are small and smooth: fewer F2F
+    // conversions on the XU pipe that the reciprocals also use).
     constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
     const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
     const bool tile_far = combine_min<NT / 32>(sm.tmin) > lim;
     if (tile_far) {
-      for (int jf = 0; jf < NP; jf += FP) {
+      for (int jf = 0; jf < NP; jf += FPF) {
 #pragma unroll UNROLL
-        for (int jg = jf; jg < jf + FP; jg += GRP) {
+        for (int jg = jf; jg < jf + FPF; jg += GRP) {
 #pragma unroll
           for (int u = 0; u < GRP; ++u) {
             const int j = jg + u;
@@ -973,7 +977,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   if constexpr (SP) {
     __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0, (FM & 4) != 0> sm;
     fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
-                  (FM & 4) != 0>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
+                  (FM & 4) != 0, (1 << ((FM >> 8) & 3))>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0,
+                                                         c1, out, stride, sm);
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
     fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
@@ -1031,8 +1036,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchL
       const BatchSeg S = B.segs[I.seg];
       double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
       fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
-                    (FM & 4) != 0>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out,
-                                   B.stride, sm);
+                    (FM & 4) != 0, (1 << ((FM >> 8) & 3))>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src,
+                                                           I.c0, I.c1, out, B.stride, sm);
     }
   } else {
     __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;

@@ -93,8 +93,9 @@ const PairVariant kVariants64[] = {
 // reciprocal (2), pre-weighted far-field sources (4, with 1), source-paired
 // rotated-frame form (8, its own far/near forms; with it, bit 0 widens the
 // FP64 flushes by integer operations, bit 1 keeps the FP64 accumulators in
-// shared memory, bit 2 gives near tiles hi/lo offsets and bits 4-7 give the
-// period of the paired reciprocal).
+// shared memory, bit 2 gives near tiles hi/lo offsets, bits 4-7 give the
+// period of the paired reciprocal and bits 8-9 the log2 of the number of
+// flush intervals between flushes in tiles whose every source is far).
 const PairVariant kVariants32[] = {
     V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
     V32(256, 2, 16, 2, 4, 0), V32(128, 2, 32, 6, 4, 0), V32(256, 1, 32, 4, 8, 0),
@@ -127,6 +128,10 @@ const PairVariant kVariants32[] = {
     // near tiles with hi/lo offsets (form bit 2 with bit 3)
     VSPX(128, 3, 64, 6, 4, 14), VSPX(128, 2, 64, 6, 4, 12), VSPX(128, 2, 64, 6, 4, 14),
     VSPX(128, 3, 64, 5, 4, 14),
+    // all-far tiles flushed every 128 (bit 8) or 256 (bit 9) sources
+    VSPX(128, 3, 64, 6, 4, 10 | 256), VSPX(128, 3, 64, 6, 4, 10 | 512),
+    VSPX(128, 2, 64, 6, 4, 8 | 256), VSPX(128, 2, 64, 6, 4, 8 | 512),
+    VSPX(128, 2, 64, 6, 4, 10 | 512), VSPX(128, 2, 64, 6, 4, 10 | 256),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
@@ -160,13 +165,15 @@ int select_variant(tc_ctx* ctx, int precision, int id) {
 }
 
 // Automatic FP32C variant: below kAutoSmallSources sources (icosahedral level
-// 6 and coarser) two targets per thread (variant 33: more CTAs for few
-// tiles, and smaller tile patches, hence smaller FP32 offsets: 10% faster at
-// level 5, the same speed and a lower error at level 6), above it three
-// (variant 54: 2-4% faster from level 7 on).
+// 6 and coarser) two targets per thread (variant 71: more CTAs for few
+// tiles, and smaller tile patches, hence smaller FP32 offsets), above it
+// three (variant 68: 2-4% faster from level 7 on); both flush all-far tiles
+// less often than mixed ones (68 every 128 sources, 1.8-2.0% faster than
+// every 64 at levels 7-8 with the same error; 71 every 256, 1.6% faster at
+// level 6, error 6.1e-8 against 5.2e-8 on the level-6 jet).
 constexpr int kAutoSmallSources = 131072;
-constexpr int kAutoSmallVariant = 33;
-constexpr int kAutoLargeVariant = 54;
+constexpr int kAutoSmallVariant = 71;
+constexpr int kAutoLargeVariant = 68;
 
 int use_fp32c_variant(tc_ctx* ctx, int n) {
   if (!ctx->auto32) return TC_OK;

@@ -42,7 +42,7 @@ struct PairVariant {
   const void* fn;
   void (*launch_batch)(int grid, cudaStream_t stream, const BatchLaunch& B);
   const void* fn_batch;
-  int form;  // FP32C: bit 3 source-paired form (with it: bit 0 integer-widened flush, bit 1 shared-memory accumulators, bit 2 hi/lo near offsets, bits 4-7 paired-reciprocal period); without it: bit 0 far form, bit 1 paired reciprocal, bit 2 pre-weighted far sources. FP64: 0
+  int form;  // FP32C: bit 3 source-paired form (with it: bit 0 integer-widened flush, bit 1 shared-memory accumulators, bit 2 hi/lo near offsets, bits 4-7 paired-reciprocal period, bits 8-9 log2 of flush lengths per flush in all-far tiles); without it: bit 0 far form, bit 1 paired reciprocal, bit 2 pre-weighted far sources. FP64: 0
 };
 
 // Target segment as the host describes it before tiles are assigned.
@@ -96,7 +96,7 @@ struct tc_ctx {
   double delta[3] = {0.0, 0.0, 0.05};               // ACTIVE, VERTEX, PASSIVE (smooth, :27)
   tcb::PairCfg cfg64{256, 2, 256};
   tcb::PairCfg cfg32{256, 4, 256};
-  int var64 = 2, var32 = 54;  // pair-kernel variants in use (see kVariants64/32)
+  int var64 = 2, var32 = 68;  // pair-kernel variants in use (see kVariants64/32)
   bool auto32 = true;  // FP32C variant chosen per launch by problem size (tc_set_pair_variant turns it off)
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
