@@ -22,12 +22,54 @@ dp = POINTER(c_double)
 ip = POINTER(c_int)
 
 _lib = None
+_fast: dict = {}
+
+# x86-64 ISA levels of the timing builds and the /proc/cpuinfo flags each needs
+# (the psABI's x86-64-v3 and v4 feature lists).
+_LEVELS = (
+    ("v4", {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}),
+    ("v3", {"avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "abm", "movbe", "xsave"}),
+)
 
 
 def build() -> Path:
-    """Compile the oracle with its Makefile (gcc -O2 -ffp-contract=off)."""
+    """Compile the oracle with its Makefile: the strict parity build (gcc -O2
+    -ffp-contract=off) and the timing builds."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
+
+
+def host_isa_level() -> str:
+    """The highest x86-64 level (v4, v3, else sse2) whose features the host CPU reports."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((set(line.split(":", 1)[1].split()) for line in f if line.startswith("flags")),
+                         set())
+    except OSError:
+        flags = set()
+    for name, need in _LEVELS:
+        if need <= flags:
+            return name
+    return "sse2"
+
+
+def fast_lib(level: str | None = None):
+    """(handle, ISA level) of a timing build: the same loops compiled like the reference's
+    ifort -O2 (reassociation, reciprocal division, contraction, vectorized), for `level` (default:
+    the host's highest). A level above the host's is refused: its code would not run here."""
+    order = ["sse2", "v3", "v4"]
+    host = host_isa_level()
+    level = level or host
+    if order.index(level) > order.index(host):
+        raise ValueError(f"x86-64-{level} build needs CPU features this host lacks (host: {host})")
+    if level not in _fast:
+        path = HERE / "_build" / f"liboracle_fast_{level}.so"
+        if not path.exists():
+            build()
+        h = ctypes.CDLL(str(path))
+        h.or_rows.argtypes = [c_int, ip, c_int, dp, dp, dp, dp, c_int, c_double, dp, c_int]
+        _fast[level] = h
+    return _fast[level], level
 
 
 def lib():
@@ -113,14 +155,17 @@ def voronoi_velocity(x, y, z, vort, area, i0=0, i1=None, omega=2 * np.pi, dy=Non
     return dx, dy, dz, dV
 
 
-def rows(cls, row_idx, X, x, vort, area, delta=0.0, nthreads=1):
-    """Sums for a list of target rows (cls 0 active / 1 vertex / 2 passive) -> (r,3)."""
+def rows(cls, row_idx, X, x, vort, area, delta=0.0, nthreads=1, fast=False):
+    """Sums for a list of target rows (cls 0 active / 1 vertex / 2 passive) -> (r,3).
+    fast=True (or an ISA level name) runs a timing build (fast_lib) instead of the strict
+    parity build."""
     row_idx = np.ascontiguousarray(row_idx, dtype=np.int32)
     x, vort, area = _c(x), _c(vort), _c(area)
     Xc = None if X is None else _c(X)
     out = np.zeros((row_idx.shape[0], 3))
-    lib().or_rows(int(cls), row_idx.ctypes.data_as(ip), row_idx.shape[0], _d(Xc), _d(x), _d(vort),
-                  _d(area), x.shape[0], delta, _d(out), nthreads)
+    h = fast_lib(fast if isinstance(fast, str) else None)[0] if fast else lib()
+    h.or_rows(int(cls), row_idx.ctypes.data_as(ip), row_idx.shape[0], _d(Xc), _d(x), _d(vort),
+              _d(area), x.shape[0], delta, _d(out), nthreads)
     return out
 
 

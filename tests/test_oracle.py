@@ -111,6 +111,31 @@ def test_rows_match_full_routines_and_threads_do_not_change_results():
         np.testing.assert_array_equal(u, v)
 
 
+@pytest.mark.parametrize("level", ["sse2", "v3", "v4"])
+def test_timing_builds_compute_the_parity_sums(level):
+    """The timed CPU baseline (the loops compiled with ifort -O2's floating-point freedoms) sums
+    what the strict parity build sums, to reassociation rounding."""
+    order = ["sse2", "v3", "v4"]
+    if order.index(level) > order.index(O.host_isa_level()):
+        pytest.skip(f"this host cannot run x86-64-{level} code")
+    w = configs.gaussian(level=4, delta=0.01)
+    rows = np.arange(0, w.nA, 7)
+    rv = np.arange(0, w.nV, 5)
+    for cls, r, X in ((0, rows, None), (1, rv, w.xV)):
+        ref = O.rows(cls, r, X, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=4)
+        got = O.rows(cls, r, X, w.xA, w.zetaA, w.areaA, delta=0.01, nthreads=4, fast=level)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_timing_build_above_the_host_level_is_refused():
+    order = ["sse2", "v3", "v4"]
+    host = O.host_isa_level()
+    if host == "v4":
+        pytest.skip("no level above this host's")
+    with pytest.raises(ValueError):
+        O.fast_lib(order[order.index(host) + 1])
+
+
 def test_load_balance_matches_reference_chunks():
     s, e = O.load_balance(10, 3)
     assert list(s) == [0, 3, 6] and list(e) == [3, 6, 10]
