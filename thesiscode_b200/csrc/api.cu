@@ -57,6 +57,10 @@ __global__ void first_nonfinite_kernel(const double* __restrict__ p, size_t n,
 // Enqueues device scans of up to kMaxScans result arrays (null or empty ones
 // are skipped) into ctx->check_buf.
 int scan_results_device(tc_ctx* ctx, const HostArray* a, int count) {
+  if (count < 0 || count > kMaxScans) {
+    tc_record_error("internal: %d result scans (at most %d)", count, kMaxScans);
+    return TC_ERR_ARG;
+  }
   int rc = ctx->check_buf.ensure(kMaxScans * sizeof(unsigned long long));
   if (rc) return rc;
   unsigned long long* first = ctx->check_buf.as<unsigned long long>();
@@ -74,6 +78,7 @@ int scan_results_device(tc_ctx* ctx, const HostArray* a, int count) {
 
 // Reads back what scan_results_device found (synchronises the stream).
 int scan_results_status(tc_ctx* ctx, const HostArray* a, int count) {
+  if (count < 0 || count > kMaxScans) return TC_ERR_ARG;
   unsigned long long first[kMaxScans];
   TC_CUDA_TRY(cudaMemcpyAsync(first, ctx->check_buf.ptr, sizeof(first), cudaMemcpyDeviceToHost,
                               ctx->stream));
