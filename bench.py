@@ -510,13 +510,17 @@ def run_ours(args):
             line["batched"] = time_batch(device)
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
-            cb = cpu_baseline(w, frac=sample_frac(w, 10.0, threads), threads=threads)
+            frac = sample_frac(w, 10.0, threads)
+            cb = cpu_baseline(w, frac=frac, threads=threads)
             line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],
                                     "kind": "port", "sample": cb["sample"], "seconds": cb["seconds"],
                                     "build": cb["build"]}
-            sums = oracle_sums(w, cb["rows"], threads)
+            # errors against the strict parity build on at most 1/8 of the rows
+            err_rows = sample_rows(w, min(frac, 1.0 / 8))
+            sums = oracle_sums(w, err_rows, threads)
             line["error_vs_fp64_oracle"] = {
-                p: gpu_stage1_errors(w, p, device, cb["rows"], sums) for p in ("fp32c", "fp64")}
+                p: gpu_stage1_errors(w, p, device, err_rows, sums) for p in ("fp32c", "fp64")}
+            line["error_vs_fp64_oracle"]["rows"] = int(err_rows[0].size + err_rows[1].size)
         print(json.dumps(line), flush=True)
     main["ctx"].close() if driver is None else driver.close()
 
