@@ -1,4 +1,4 @@
-"""Multi-rank driver (thesiscode_b200.dist) on CPU: world size 2, gloo.
+"""Multi-rank driver (thesiscode_b200.dist) on CPU: world sizes 2 and 3, gloo.
 
 The driver's host logic - LoadBalance ranges (PanelVelocityParallel.f90:
 167-213), one all-gather of the next stage's source rows per stage (the
@@ -179,11 +179,13 @@ def _spawn(mode, tmp_path, world=2):
     assert not alive, "a rank hung"
 
 
-def test_two_ranks_match_serial_oracle_bitwise(tmp_path, native_built):
+@pytest.mark.parametrize("world", [2, 3])
+def test_ranks_match_serial_oracle_bitwise(tmp_path, native_built, world):
+    """World size 3 gives ragged LoadBalance ranges (320 panels: 106, 106, 108 rows)."""
     from oracle import oracle as O
     from thesiscode_b200 import configs
 
-    _spawn("ok", tmp_path)
+    _spawn("ok", tmp_path, world=world)
     errs = list(tmp_path.glob("*.err"))
     assert not errs, errs[0].read_text()
     w = configs.rh4(level=2, parity=True, dt=0.01)
@@ -192,7 +194,7 @@ def test_two_ranks_match_serial_oracle_bitwise(tmp_path, native_built):
     for _ in range(2):
         xV, xA, zA, xQ, tke, ke, _ = O.bve_rk4(xV, xA, zA, w.areaA, xQ, w.dt, w.omega, w.deltas)
         tkes.append(tke)
-    for r in range(2):
+    for r in range(world):
         g = np.load(tmp_path / f"rank{r}.npz")
         np.testing.assert_array_equal(g["xA"], xA)
         np.testing.assert_array_equal(g["zetaA"], zA)
