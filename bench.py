@@ -4,21 +4,25 @@
 Metric: Biot-Savart interactions/s (one interaction = one (target, source)
 pair evaluated; one RK4 step = 4 stages x [nA(nA-1) + (nV + nQ) nA]).
 
-Default workload: Gaussian vortex exp(-16|x-x0|^2) minus its area mean,
-x0 = (22.5N, 0E), icosahedral level 7 (327,680 active panels + 163,842
-vertices), delta = 0.01 for all targets, one RK4 step per timed step, FP32-
-compensated pair arithmetic (the FP64 path is measured beside it).
+Default workload: Rossby-Haurwitz wave 4 (omega = K = Omega/14), icosahedral
+level 8 (1,310,720 active panels + 655,362 vertices, about 1.97M targets),
+delta = 0.005 for all targets, one RK4 step per timed step, FP32-compensated
+pair arithmetic (the FP64 path is measured beside it). The Gaussian vortex at
+level 7 (327,680 panels + 163,842 vertices, delta 0.01) is measured beside it
+under the key "gaussian_l7".
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config gaussian_l7|rh4_l8|rh4_l4|jet_l6] [--precision fp32c|fp64]
+                    [--config rh4_l8|gaussian_l7|rh4_l4|jet_l6] [--precision fp32c|fp64]
 
 Timing: CUDA events on the library's stream around each step, L2 flushed
 (a 256 MiB write) between timed steps, max over ranks. The reference arm
 (--impl reference) and the CPU baseline time the CPU FP64 restatement of the
 reference loops (oracle/) in its timing build (compiled with the freedoms of
 the reference's ifort -O2: vectorized, reassociated, reciprocal division) on
-all host cores over a seeded sample of target rows; errors are measured
-against the strict parity build.
+all host cores over a seeded sample of target rows, on inputs built from the
+oracle's own restatement of the icosahedral grid generator (the reference arm
+loads no part of the product library); errors are measured against the
+strict parity build.
 """
 from __future__ import annotations
 
@@ -40,23 +44,41 @@ sys.path.insert(0, str(ROOT))
 
 FLOPS_PER_INTERACTION = 22  # dot 5, denominator 1, weight 1, cross 9, accumulate 6
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) of one FP32C pair launch on the level-7 Gaussian workload, from an
-# ncu capture of `bench.py --quick --no-cpu --steps 2` (dram__bytes_read.sum + dram__bytes_write.sum)
-PAIR_FP32C_L7_DRAM_BYTES = 28.02e6 + 52.43e6
+ERROR_ROWS_MAX = 24576  # rows of the strict-oracle error sample (a seeded subset)
+# DRAM bytes (read + write) of one FP32C pair launch (the stage-1 launch of one RK4 step, every
+# target class against all sources), from ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum) summarised in profiles/
+PAIR_FP32C_DRAM_BYTES = {"gaussian_l7": 28.02e6 + 52.43e6}
 
 
-def build_workload(name: str):
+def build_workload(name: str, grid_source=None):
+    """The named workload; grid_source (a callable level -> (xV, xA, areaA, xQ)) replaces the
+    library's grid generator."""
     from thesiscode_b200 import configs
 
     if name == "gaussian_l7":
-        return configs.gaussian(level=7, delta=0.01, dt=0.01, steps=1)
+        return configs.gaussian(level=7, delta=0.01, dt=0.01, steps=1, grid_source=grid_source)
     if name == "rh4_l8":
-        return configs.rh4(level=8, delta=0.005, dt=0.01, steps=1)
+        return configs.rh4(level=8, delta=0.005, dt=0.01, steps=1, grid_source=grid_source)
     if name == "rh4_l4":
-        return configs.rh4(level=4, delta=0.0, dt=0.01, steps=10)
+        return configs.rh4(level=4, delta=0.0, dt=0.01, steps=10, grid_source=grid_source)
     if name == "jet_l6":
-        return configs.jet(level=6, delta=0.02, dt=0.005, steps=20)
+        return configs.jet(level=6, delta=0.02, dt=0.005, steps=20, grid_source=grid_source)
     raise SystemExit(f"unknown config {name}")
+
+
+def oracle_workload(name: str, check=None):
+    """The named workload on the oracle's icosahedral grid (oracle/icos_oracle.c); with `check`
+    (the same workload from the library's generator) the two must agree bit for bit."""
+    from oracle import oracle as O
+
+    w = build_workload(name, grid_source=O.gathered_grid)
+    if check is not None:
+        for a, b in ((w.xA, check.xA), (w.zetaA, check.zetaA), (w.areaA, check.areaA), (w.xV, check.xV),
+                     (w.xQ, check.xQ)):
+            if not np.array_equal(a, b):
+                raise SystemExit("the library's grid differs from the oracle's: inputs are not the same")
+    return w
 
 
 def workload_config(w, precision, scaling_note):
@@ -423,6 +445,36 @@ def gpu_stage1_errors(w, precision, device, rows, sums):
                 rms=float(np.sqrt((diff ** 2).sum(1).mean()) / scale))
 
 
+def error_sample(w, device, threads, max_rows=ERROR_ROWS_MAX):
+    """Stage-1 velocity errors of both GPU paths against the strict parity oracle on a seeded
+    sample of at most `max_rows` target rows (at most 1/8 of the rows)."""
+    frac = min(1.0 / 8, max_rows / (w.nA + w.nV))
+    err_rows = sample_rows(w, frac, seed=12)
+    sums = oracle_sums(w, err_rows, threads)
+    out = {p: gpu_stage1_errors(w, p, device, err_rows, sums) for p in ("fp32c", "fp64")}
+    out["rows"] = int(err_rows[0].size + err_rows[1].size)
+    return out
+
+
+def time_side_workload(name, device, no_cpu, steps=3):
+    """A second workload measured beside the headline: FP32C and FP64 device-resident step rates,
+    their ratio and (unless no_cpu) the errors against the strict oracle."""
+    w = build_workload(name)
+    out = {"workload": workload_config(w, "fp32c", "1 GPU")["workload"], "level": w.level,
+           "interactions_per_step": w.interactions_per_step()}
+    for prec in ("fp32c", "fp64"):
+        r = time_device_steps(w, prec, steps, 1, device)
+        r["ctx"].close()
+        out[prec] = {"value": w.interactions_per_step() * steps / (r["total_ms"] * 1e-3),
+                     "ms_per_step": r["total_ms"] / steps,
+                     "pair_ms_per_launch": r["pair_ms"] / max(r["pair_launches"], 1)}
+    out["fp32c_over_fp64"] = out["fp32c"]["value"] / out["fp64"]["value"]
+    if not no_cpu:
+        out["error_vs_fp64_oracle"] = error_sample(oracle_workload(name, check=w), device,
+                                                   os.cpu_count() or 1, max_rows=8192)
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -461,8 +513,8 @@ def run_ours(args):
         "roofline": {"bound": "fp32" if args.precision == "fp32c" else "fp64",
                      "achieved": achieved / 1e12, "peak": fp_peak / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / fp_peak,
-                     "traffic": PAIR_FP32C_L7_DRAM_BYTES if (args.precision == "fp32c" and
-                                                              args.config == "gaussian_l7") else None,
+                     "traffic": (PAIR_FP32C_DRAM_BYTES.get(args.config) if args.precision == "fp32c"
+                                 else None),
                      "kernel": f"pair_{args.precision}_kernel",
                      "flops_per_interaction": FLOPS_PER_INTERACTION,
                      "pair_ms_per_launch": pair_ms_launch,
@@ -508,21 +560,30 @@ def run_ours(args):
         if world == 1 and not args.quick:
             line["adjoint"] = time_adjoint(device)
             line["batched"] = time_batch(device)
+            if args.config != "gaussian_l7":
+                line["gaussian_l7"] = time_side_workload("gaussian_l7", device, args.no_cpu)
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
-            frac = sample_frac(w, 10.0, threads)
-            cb = cpu_baseline(w, frac=frac, threads=threads)
+            # the CPU legs run on the oracle's own grid (bit for bit the library's inputs)
+            wo = oracle_workload(args.config, check=w)
+            frac = sample_frac(wo, 10.0, threads)
+            cb = cpu_baseline(wo, frac=frac, threads=threads)
             line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],
                                     "kind": "port", "sample": cb["sample"], "seconds": cb["seconds"],
-                                    "build": cb["build"]}
-            # errors against the strict parity build on at most 1/8 of the rows
-            err_rows = sample_rows(w, min(frac, 1.0 / 8))
-            sums = oracle_sums(w, err_rows, threads)
-            line["error_vs_fp64_oracle"] = {
-                p: gpu_stage1_errors(w, p, device, err_rows, sums) for p in ("fp32c", "fp64")}
-            line["error_vs_fp64_oracle"]["rows"] = int(err_rows[0].size + err_rows[1].size)
+                                    "build": cb["build"], "inputs": "oracle grid (oracle/icos_oracle.c)"}
+            line["error_vs_fp64_oracle"] = error_sample(wo, device, threads)
         print(json.dumps(line), flush=True)
     main["ctx"].close() if driver is None else driver.close()
+
+
+def repo_libraries() -> list[str]:
+    """Shared libraries of this repository mapped into the process (from /proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so")}
+    except OSError:
+        return []
+    return sorted(os.path.relpath(q, ROOT) for q in paths if q.startswith(str(ROOT)))
 
 
 def run_reference(args):
@@ -530,7 +591,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = build_workload(args.config)
+    w = oracle_workload(args.config)  # the oracle's grid: no part of the product library is loaded
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_baseline(w, frac=1.0 / 1024, threads=threads)
@@ -554,7 +615,9 @@ def run_reference(args):
             "note": "the reference is Fortran+MPI (ifort -O2, mpif90); no Fortran compiler or MPI exists on "
                     "these machines, so the arm runs the C restatement of its loops (oracle/), compiled with "
                     "the floating-point freedoms and vectorization of ifort -O2, on all host threads with the "
-                    "reference's LoadBalance row partition"}
+                    "reference's LoadBalance row partition, on inputs from the oracle's restatement of the "
+                    "reference's icosahedral grid generator (InitIcosTriGrid/DivideTriPanel)"}
+    line["libraries_loaded"] = repo_libraries()
     print(json.dumps(line), flush=True)
 
 
@@ -564,7 +627,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="gaussian_l7", choices=["gaussian_l7", "rh4_l8", "rh4_l4", "jet_l6"])
+    ap.add_argument("--config", default="rh4_l8", choices=["rh4_l8", "gaussian_l7", "rh4_l4", "jet_l6"])
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error check")
     ap.add_argument("--quick", action="store_true", help="main measurement only")

@@ -91,6 +91,19 @@ double or_strat_rk4(double* xV, int nV, double* xA, const double* absVortA, doub
                     double* relVortV, double t, double dt, double omega, double deltaA,
                     double deltaV, double deltaQ, double* kineticEnergy, int nthreads);
 
+/* Icosahedral triangle grid, InitIcosTriGrid + DivideTriPanel + TriPanelArea,
+ * ParticlesEdgesPanels2.f90:419-645, 760-1090, 1727-1802 (icos_oracle.c).
+ * Sizes (PanelMax / ParticleMax / EdgeMax, :2614-2662) for a level in [0, 11];
+ * the grid with 0-based indices (-1 = none), x arrays (N, 3) = Fortran x(3, N).
+ * Both return 0, or -1 on a bad level or allocation failure. */
+int or_icos_sizes(int level, int* n_particles, int* n_edges, int* n_panels, int* n_active);
+int or_icos_grid(int level, double* particles_x, double* particles_x0, double* panels_x,
+                 double* panels_x0, double* panels_area, int* has_children, int* vertices,
+                 int* nest, int* children);
+/* GatherPanels maps (:1556-1619): leaf panels in index order, then divided ones. */
+int or_gather_maps(int n, const int* has_children, int* active_map, int n_active,
+                   int* passive_map, int n_passive);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,6 +98,9 @@ def lib():
         h.or_strat_rk4.argtypes = [dp, c_int, dp, dp, dp, dp, c_int, dp, c_int, dp, dp, c_double,
                                    c_double, c_double, c_double, c_double, c_double, dp, c_int]
         h.or_strat_rk4.restype = c_double
+        h.or_icos_sizes.argtypes = [c_int, ip, ip, ip, ip]
+        h.or_icos_grid.argtypes = [c_int, dp, dp, dp, dp, dp, ip, ip, ip, ip]
+        h.or_gather_maps.argtypes = [c_int, ip, ip, c_int, ip, c_int]
         _lib = h
     return _lib
 
@@ -228,3 +231,52 @@ def strat_rk4(xV, xA, absVortA, areaA, xQ, t, dt, omega=2 * np.pi, deltas=(0.0, 
                              xQ.shape[0], _d(absV), _d(relV), t, dt, omega, deltas[0], deltas[1],
                              deltas[2], _d(ke), nthreads)
     return xV, xA, relA, xQ, tke, ke, relV
+
+
+def icos_sizes(level):
+    """(particles, edges, panels, active panels) of icosahedral level `level` (PanelMax,
+    ParticleMax, EdgeMax: ParticlesEdgesPanels2.f90:2614-2662)."""
+    v = [c_int() for _ in range(4)]
+    if lib().or_icos_sizes(int(level), *[ctypes.byref(x) for x in v]) != 0:
+        raise ValueError(f"icosahedral level {level} outside [0, 11]")
+    return tuple(x.value for x in v)
+
+
+def icos_grid(level):
+    """The oracle's icosahedral grid (InitIcosTriGrid, ParticlesEdgesPanels2.f90:419-645): a dict
+    of particle positions / Lagrangian coordinates and panel centres, Lagrangian centres, areas,
+    hasChildren, vertices, nest and children, indices 0-based (-1 = none)."""
+    npart, _, npan, _ = icos_sizes(level)
+    g = dict(particles_x=np.zeros((npart, 3)), particles_x0=np.zeros((npart, 3)),
+             panels_x=np.zeros((npan, 3)), panels_x0=np.zeros((npan, 3)), panels_area=np.zeros(npan),
+             panels_has_children=np.zeros(npan, np.int32), panels_vertices=np.zeros((npan, 3), np.int32),
+             panels_nest=np.zeros(npan, np.int32), panels_children=np.zeros((npan, 4), np.int32))
+    rc = lib().or_icos_grid(int(level), *[_d(g[k]) for k in ("particles_x", "particles_x0", "panels_x",
+                                                           "panels_x0", "panels_area")],
+                            *[g[k].ctypes.data_as(ip) for k in ("panels_has_children", "panels_vertices",
+                                                                 "panels_nest", "panels_children")])
+    if rc != 0:
+        raise RuntimeError(f"or_icos_grid({level}) failed")
+    return g
+
+
+def gather_maps(has_children):
+    """GatherPanels maps (ParticlesEdgesPanels2.f90:1556-1619): (active, passive) panel indices."""
+    hc = np.ascontiguousarray(has_children, dtype=np.int32)
+    n = hc.shape[0]
+    nq = int(np.count_nonzero(hc))
+    am, pm = np.zeros(n - nq, np.int32), np.zeros(nq, np.int32)
+    if lib().or_gather_maps(n, hc.ctypes.data_as(ip), am.ctypes.data_as(ip), n - nq,
+                            pm.ctypes.data_as(ip), nq) != 0:
+        raise RuntimeError("or_gather_maps: inconsistent counts")
+    return am, pm
+
+
+def gathered_grid(level):
+    """Inputs of a workload on the oracle's grid: (particle positions (nV,3), active panel
+    centres (nA,3), their areas (nA,), divided panel centres (nQ,3)); the same arrays the product
+    builds with its own generator and GatherPanels maps."""
+    g = icos_grid(level)
+    am, pm = gather_maps(g["panels_has_children"])
+    return (g["particles_x"].copy(), np.ascontiguousarray(g["panels_x"][am]),
+            np.ascontiguousarray(g["panels_area"][am]), np.ascontiguousarray(g["panels_x"][pm]))

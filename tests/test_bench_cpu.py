@@ -1,5 +1,6 @@
 """bench.py's reference arm runs on the host alone and prints one JSON line with the keys the
-benchmark contract asks for (on the small level-4 RH4 workload, a few seconds of CPU)."""
+benchmark contract asks for (on the small level-4 RH4 workload, a few seconds of CPU), and maps
+only the oracle's libraries, none of the product's."""
 import json
 import subprocess
 import sys
@@ -23,3 +24,6 @@ def test_reference_arm_prints_one_contract_line(native_built):
     assert cb["kind"] == "port" and cb["value"] == line["value"] and cb["cores"] >= 1
     assert "x86-64-" in cb["build"] and "ifort -O2" in cb["build"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    # the arm builds its inputs on the oracle's grid: the product library is never mapped
+    libs = line["libraries_loaded"]
+    assert libs and all(lib.startswith("oracle/_build/") for lib in libs), libs

@@ -71,3 +71,49 @@ def test_bad_level_is_an_error():
 
     with pytest.raises(N.TcError):
         grid.icos_sizes(12)
+
+
+_FIELDS = ("particles_x", "particles_x0", "panels_x", "panels_x0", "panels_area", "panels_has_children",
+           "panels_vertices", "panels_nest", "panels_children")
+
+
+def _product_grid(level):
+    parts, pans = grid.new_icos_grid(level)
+    return dict(particles_x=parts.x, particles_x0=parts.x0, panels_x=pans.x, panels_x0=pans.x0,
+                panels_area=pans.area, panels_has_children=pans.hasChildren.astype(np.int32),
+                panels_vertices=pans.vertices, panels_nest=pans.nest, panels_children=pans.children)
+
+
+@pytest.mark.parametrize("level", [0, 1, 2, 3, 4, 5, 6, 7])
+def test_library_grid_equals_oracle_grid_bit_for_bit(level):
+    """tc_icos_grid against the oracle's statement-for-statement restatement of InitIcosTriGrid /
+    DivideTriPanel / TriPanelArea (oracle/icos_oracle.c): every position, Lagrangian coordinate,
+    centre, area and index table identical, bit for bit."""
+    from oracle import oracle as O
+
+    ref = O.icos_grid(level)
+    got = _product_grid(level)
+    for k in _FIELDS:
+        assert got[k].shape == ref[k].shape, k
+        assert np.array_equal(got[k], ref[k]), k
+    am, pm = O.gather_maps(ref["panels_has_children"])
+    maps = grid.gather_maps(grid.new_icos_grid(level)[1])
+    assert np.array_equal(maps.active, am) and np.array_equal(maps.passive, pm)
+
+
+def test_oracle_grid_known_answers():
+    """The oracle's grid on its own: PanelMax/ParticleMax counts, total area 4 pi, unit vectors."""
+    from oracle import oracle as O
+
+    for level in (0, 3, 6):
+        g = O.icos_grid(level)
+        npart, nedge, npan, nact = O.icos_sizes(level)
+        assert (npart, npan, nact) == (2 + 10 * 4 ** level, sum(20 * 4 ** j for j in range(level + 1)),
+                                        20 * 4 ** level)
+        assert nedge == sum(30 * 4 ** j for j in range(level + 1))
+        leaves = g["panels_has_children"] == 0
+        assert np.count_nonzero(leaves) == nact
+        assert abs(g["panels_area"][leaves].sum() - 4 * np.pi) < 1e-12
+        np.testing.assert_allclose(np.linalg.norm(g["particles_x"], axis=1), 1.0, atol=1e-15)
+    with pytest.raises(ValueError):
+        O.icos_sizes(12)
