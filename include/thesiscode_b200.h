@@ -144,11 +144,17 @@ int tc_bs_velocity_device(tc_ctx* ctx, int target_class, const double* X, int m,
  * reference), for callers that cannot let the library allocate device memory
  * during the call: applications whose device memory is owned by their own
  * pool, and stepping loops that cannot take cudaMalloc's implicit device
- * synchronisation. Same arguments and result; the scratch is a 32 MiB array
- * compiled into the library (held by every GPU that loads it), so
- * 32*n + 24*m bytes must fit in 32 MiB, else TC_ERR_ARG. The first call on a
- * device looks the array's address up (make it before any stream capture);
- * calls share the array, so calls that overlap on the GPU race. */
+ * synchronisation. Same arguments and result: FP32C keeps the library's
+ * visiting order of the targets (tc_set_target_order), so its accuracy does not
+ * depend on the order the caller stores them in, and the source chunking is
+ * tc_bs_velocity_device's, capped by the space left. The scratch is a 32 MiB
+ * array compiled into the library (held by every GPU that loads it): sources
+ * 32*n bytes, partial sums 24*m per chunk and, for FP32C in the visiting
+ * order, about 4*m + 20*(i1 - i0) for the order; a call for which one chunk
+ * does not fit returns TC_ERR_ARG. The first call on a device (and the first
+ * after its context was re-created) looks the array's address up: make it
+ * before any stream capture. Calls share the array, so calls that overlap on
+ * the GPU race. */
 int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, const double* X, int m,
                                   const double* src_x, const double* vort, const double* area,
                                   int n, int i0, int i1, double* dX, double* dVort);
@@ -286,20 +292,15 @@ int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr, int
 /* Number of compiled launch shapes for a precision, and their parameters:
  * info8 = {threads, targets/thread, sources/tile, FP32 flush length (FP64:
  * 1 fused denominator, 0 rounded like the reference), min CTAs/SM, unroll,
- * targets/CTA, form}. FP32C form: bit 3 set = source-paired kernel (the two
- * lanes of each f32x2 instruction carry two sources of one target; with it
- * bit 1 = FP64 accumulators in shared memory, bit 2 = hi/lo near-pair
- * offsets (the accurate variants), bit 0 = flush widened by integer
- * operations, bits 4-7 = period of a paired reciprocal, bits 8-9 = log2
- * of the flush lengths between flushes in tiles whose every source is
- * far); bit 3 clear =
- * target-paired kernel (bit 0 far-field expansion for well-separated source
- * tiles, bit 1 one reciprocal per two targets, bit 2 pre-weighted far
- * sources). FP64 form: 0. */
+ * targets/CTA, form}. FP32C form: bit 3 = source-paired kernel (set in every
+ * variant: the two lanes of each f32x2 instruction carry two sources of one
+ * target), bit 1 = FP64 accumulators in shared memory, bit 2 = hi/lo
+ * near-pair offsets (the accurate variants), bits 8-9 = log2 of the flush
+ * lengths between flushes in tiles whose every source is far. FP64 form: 0. */
 int tc_pair_variant_count(int precision, int* count);
 int tc_pair_variant_info(int precision, int id, int* info8);
 /* Select a variant. For FP32C the default is chosen per launch by problem
- * size (variant 71 below 131,072 sources, 68 above); selecting a variant turns
+ * size (variant 1 below 131,072 sources, 0 above); selecting a variant turns
  * that off, and id = -1 turns it back on. tc_get_pair_variant returns the
  * variant in use (for FP32C with the automatic choice: the one last used). */
 int tc_set_pair_variant(tc_ctx* ctx, int precision, int id);

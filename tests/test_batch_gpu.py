@@ -62,11 +62,9 @@ def test_graph_replay_equals_eager_launches(gpu):
 
 def test_batch_kernel_every_form_matches_oracle(gpu):
     """The persistent batch kernel with one variant of every FP32C form in the variant table
-    (target-paired near/far/paired-reciprocal/pre-weighted forms, source-paired forms with
-    register or shared-memory accumulators, hi/lo near offsets, paired reciprocals), autotuning
-    off: one RK4 step of each instance matches the oracle within the coarse-grid bound (5e-7
-    for the source-paired forms; 1e-6 for the target-paired forms, variants kept for comparison,
-    whose tile origin is a target rather than the tile's centroid)."""
+    (register or shared-memory accumulators, hi/lo near offsets, far-tile flush lengths),
+    autotuning off: one RK4 step of each instance matches the oracle within the coarse-grid
+    bound (5e-7)."""
     import ctypes
 
     from thesiscode_b200 import _native as N
@@ -78,7 +76,7 @@ def test_batch_kernel_every_form_matches_oracle(gpu):
         info = (ctypes.c_int * 8)()
         N.call("tc_pair_variant_info", N.TC_FP32C, v, info)
         first_of_form.setdefault(info[7], v)
-    assert len(first_of_form) >= 8
+    assert len(first_of_form) >= 6
     ref0 = small_batch(seed=9)
     expect = []
     for r in ref0:
@@ -93,7 +91,8 @@ def test_batch_kernel_every_form_matches_oracle(gpu):
         batch_rk4(ctx, ws, 0.01, 1, graph=False, autotune=False)
         assert batch_info(ctx)["variant"] == v
         ctx.close()
-        tol = TOL["fp32c"] if form & 8 else 1e-6
+        assert form & 8, (form, v)
+        tol = TOL["fp32c"]
         for b, (w, r, (xA, zA, xV)) in enumerate(zip(ws, ref0, expect)):
             scale = np.abs(xA - r.xA).max()
             assert np.abs(w.xA - xA).max() <= tol * scale, (form, v, b)

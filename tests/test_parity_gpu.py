@@ -136,7 +136,7 @@ def test_every_pair_variant_delta0_small_grid(gpu):
     """Every FP32C variant on a level-3 Gaussian with delta = 0 (no smoothing: the self pair's
     exact zero is what keeps it out of the sum, and one tile covers most of the sphere, with
     partial tiles and padding): all active and vertex rows against the oracle, within the
-    coarse-grid bound (1e-6 for the target-paired forms, kept for comparison)."""
+    coarse-grid bound."""
     import ctypes
     w = configs.gaussian(level=3, delta=0.0)
     refA = O.rows(0, np.arange(w.nA), None, w.xA, w.zetaA, w.areaA, delta=0.0, nthreads=8)
@@ -147,7 +147,8 @@ def test_every_pair_variant_delta0_small_grid(gpu):
     for v in range(cnt.value):
         info = (ctypes.c_int * 8)()
         N.call("tc_pair_variant_info", N.TC_FP32C, v, info)
-        tol = FP32C_TOL_COARSE if info[7] & 8 else 1e-6
+        assert info[7] & 8, (v, info[7])
+        tol = FP32C_TOL_COARSE
         ctx = Context(0, "fp32c")
         setup(ctx, w.omega, (0.0, 0.0, 0.0))
         N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, v)
@@ -159,7 +160,7 @@ def test_every_pair_variant_delta0_small_grid(gpu):
 
 
 def test_fp32c_variant_chosen_by_size(gpu):
-    """The default FP32C variant follows the problem size (71 below 131,072 sources, 68 above);
+    """The default FP32C variant follows the problem size (1 below 131,072 sources, 0 above);
     selecting a variant fixes it, and -1 restores the automatic choice."""
     import ctypes
 
@@ -173,15 +174,15 @@ def test_fp32c_variant_chosen_by_size(gpu):
     ctx = Context(0, "fp32c")
     setup(ctx, small.omega, small.deltas)
     ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
-    assert used(ctx) == 71
+    assert used(ctx) == 1
     ctx.velocity(N.TC_VERTEX, large.xV[:1024], large.xA, large.zetaA, large.areaA)
-    assert used(ctx) == 68
-    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, 68)
+    assert used(ctx) == 0
+    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, 0)
     ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
-    assert used(ctx) == 68
+    assert used(ctx) == 0
     N.call("tc_set_pair_variant", ctx.handle, N.TC_FP32C, -1)
     dX, _ = ctx.velocity(N.TC_VERTEX, small.xV, small.xA, small.zetaA, small.areaA)
-    assert used(ctx) == 71
+    assert used(ctx) == 1
     ref = O.rows(1, np.arange(small.nV), small.xV, small.xA, small.zetaA, small.areaA, delta=0.01, nthreads=8)
     assert rel_err(dX, ref) <= FP32C_TOL
     ctx.close()
@@ -343,8 +344,9 @@ def test_errors_are_reported_not_raised_on_device(ctx64):
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
 def test_every_pair_variant_matches_oracle(gpu, precision):
     """Every compiled launch shape (threads, targets per thread, flush length, register cap,
-    FP32C far-field form and paired reciprocal) gives the oracle's sums within the path's
-    tolerance, on a level-5 Gaussian (sampled rows) in its Hilbert visiting order."""
+    FP32C accumulator placement, hi/lo near form and far-tile flush length) gives the oracle's
+    sums within the path's tolerance, on a level-5 Gaussian (sampled rows) in its Hilbert
+    visiting order."""
     import ctypes
     w = configs.gaussian(level=5, delta=0.01)
     pid = N.TC_FP64 if precision == "fp64" else N.TC_FP32C

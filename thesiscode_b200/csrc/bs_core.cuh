@@ -187,62 +187,73 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // ---------------------------------------------------------------------------
 // FP32-compensated pair kernel.
 //
-// Target-paired form (the variants without form bit 3): each CTA takes the
-// position c of the middle target of its tile as origin.
-// Sources are converted once per CTA and tile from FP64 to FP32 offsets
-// s_k = fl32(x_k - c) (their FP64 difference rounded once), targets likewise
-// t_i = fl32(x_i - c). Targets are visited in a spatially coherent order (the
-// library's cube-face Hilbert order, sphere_order.cuh, or the caller's), so a CTA's
-// targets form a compact patch and every nearby pair has small |s_k|, |t_i|:
-// d = s_k - t_i carries an absolute error of a few ulps of the patch size
-// instead of ulps of 1. The denominator uses the cancellation-free form
+// Each CTA takes an origin c - the centroid of its targets projected to the
+// sphere - and an orthonormal frame R = (e1, e2, e3) with e3 along c. Sources
+// are converted once per CTA and tile from FP64 to FP32 offsets
+// s_k = fl32(R(x_k - c)) (FP64 difference and rotation, one rounding),
+// targets likewise t_i = fl32(R(x_i - c)). Targets are visited in a spatially
+// coherent order (the library's cube-face Hilbert order, sphere_order.cuh, or
+// the caller's), so a CTA's targets form a compact patch and every nearby pair
+// has small |s_k|, |t_i|: d = s_k - t_i carries an absolute error of a few
+// ulps of the patch size instead of ulps of 1. Distances and dot products are
+// frame-invariant. The denominator uses the cancellation-free form
 //     2(1 - x_i.x_k) + 2 delta^2 = |x_k - x_i|^2 + e_i + e_k,
 //     e_i = 1 - |x_i|^2 + 2 delta^2,  e_k = 1 - |x_k|^2
 // (evaluated in FP64 once per point, then rounded to FP32), so near pairs
-// keep full FP32 relative accuracy. Two targets share each f32x2 instruction
-// (FADD2/FFMA2/FMUL2 halve the issue slots; the FP32 pipe stays the bound).
-// Per-target FP32 partial sums are added into FP64 accumulators every FLUSH
-// sources.
+// keep full FP32 relative accuracy although RK4 drifts points off the sphere.
 //
-// Self pair (TC_ACTIVE, targets are sources): s_k and t_i are rounded from
-// the same double, so d = 0 exactly; e_i carries a +1e-30 bias that keeps
-// D = e_i + e_k away from 0 and from FP32 subnormals (e is either 0 or at
-// least ~1e-17 in magnitude), so w stays finite and w*d adds exactly 0. No
-// per-pair mask is needed.
+// Source pairing: the two f32x2 lanes of every FADD2/FFMA2/FMUL2 carry two
+// SOURCES (k, k+1) of one target, so a source tile sits in shared memory once
+// (no duplicated values): a warp-wide broadcast 128-bit shared load costs two
+// wavefronts of the SM-wide shared pipe, and a far source pair costs 7,
+// shared by the T targets of a thread.
+//
+// Two forms of the pair, chosen per 64-source segment (uniform over the CTA):
+// * near (11 FP32 operations): d = s_k - t_i, D = |d|^2 + e_i + e_k,
+//   T' += (2G_k / D) d;
+// * far (7 FP32 operations), for segments whose every source is farther than
+//   kFarRatio times the CTA's target radius rho (the largest |t_i|) from the
+//   origin: D/2 = A_k + B_i + s_k.(-t_i), A_k = (|s_k|^2 + e_k)/2 and
+//   B_i = (|t_i|^2 + e_i)/2 from FP64, and T' += r (G_k x'_k) with
+//   x'_k = R x_k (G x'_k from FP64, one rounding). In the rotated frame the
+//   first two coordinates of x'_k are small tangential offsets and the third
+//   is about 1, so the large common part of the sum (about sum r G) sits in
+//   the third coordinate only, and u_i = x_i x R^T T' multiplies it by the
+//   target's own small offset. With |s| > 3 rho, D >= (|s| - rho)^2 >=
+//   4|s|^2/9, so each rounding of the expansion costs at most a few ulps of D,
+//   as in the near form; the self pair never qualifies.
+// Near and far sums go into the same accumulators: near sum w (x'_k - x'_i)
+// and far sum w x'_k differ by multiples of x'_i, which u = x_i x T ignores.
+//
+// One MUFU reciprocal (rcp.approx.ftz.f32) per pair. The FP32 partials of the
+// two source lanes are added and flushed into FP64 accumulators every FLUSH
+// sources in mixed tiles (every FLUSH * FARK sources in tiles whose every
+// source is far: far terms are small and smooth, and each flush costs F2F
+// conversions on the XU pipe that the reciprocals also need), and rotated
+// back to the global frame in FP64 once per target.
+//
+// Self pair (TC_ACTIVE, targets are sources): s_k and t_i are computed by the
+// same explicitly fused FP64 operations from the same double, so d = 0
+// exactly; e_i carries a +1e-30 bias that keeps D = e_i + e_k away from 0
+// and from FP32 subnormals (e is either 0 or at least ~1e-17 in magnitude),
+// so w stays finite and w*d adds exactly 0. No per-pair mask is needed.
+//
+// Form bits (FM): bit 3 always set (the source-paired form; the bit value
+// is part of the variant-info ABI); bit 1 keeps the FP64 accumulators in
+// shared memory (one slot per thread, target and coordinate: 6 fewer
+// registers per target); bit 2 gives near tiles hi/lo offsets; bits 8-9 hold
+// log2 FARK.
+// HILO (bit 2): near tiles take d = s - t from hi/lo FP32 splits of both
+// offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to FP32
+// (an absolute error of ulps of the patch radius, the dominant FP32C error
+// for nearest-neighbour pairs) no longer enters, and d keeps a few ulps of its
+// own length. Far tiles are unchanged. Both low parts are needed: for the self
+// pair s and t are the same point, so (s_hi - t_hi) and (s_lo - t_lo) are
+// both exactly 0 and the pair adds w * 0; correcting one side only would
+// leave d = s_lo there, a spurious self term.
 // ---------------------------------------------------------------------------
 constexpr float kSelfBias = 1e-30f;
-constexpr float kPadDenominator = 1e30f;
-
-// Far-field form (FM bit 0). For a source tile whose every source lies
-// farther than kFarRatio times the CTA's target radius rho (the largest
-// |t_i| of the CTA) from the origin, the denominator is expanded as
-//     D/2 = A_k + B_i + s_k.nt_i,   A_k = (|s_k|^2 + e_k)/2,
-//     B_i = (|t_i|^2 + e_i)/2,      nt_i = -t_i
-// (A_k and B_i from FP64, rounded once), and the sum as
-//     sum w (s_k - t_i) = sum w s_k + nt_i sum w,
-// so the three offset subtractions leave the pair loop: 9 FP32 operations
-// per pair instead of 11. With |s| > 3 rho, D >= (|s| - rho)^2 >= 4|s|^2/9,
-// so each rounding of the expansion costs at most a few ulps of D, as in the
-// near form; the self pair never qualifies (|s_self| = |t_self| <= rho).
-// Paired reciprocal (FM bit 1): the two targets of an f32x2 lane pair share
-// one MUFU reciprocal q = 1/(D_a D_b): 1/D_a = q D_b, 1/D_b = q D_a.
-// Pre-weighted sources (FM bit 2, with bit 0): each source tile also holds
-// G_k s_k and G_k (G_k s_k from the FP64 offset, rounded once), so a far
-// pair accumulates r = 1/(D/2) directly into sum r G s_k and sum r G: the
-// weight multiply leaves the loop and a far pair costs 8 FP32 operations
-// (4 denominator, 4 accumulations) plus the MUFU reciprocal, which balances
-// the FMA pipe (2 cycles per f32x2 warp instruction) against the XU pipe
-// (8 cycles per warp MUFU): 16 cycles each per warp and source.
 constexpr float kFarRatio2 = 9.0f;  // kFarRatio = 3
-
-template <bool PR>
-__device__ __forceinline__ float2 rcp_pair(float2 D) {
-  if (PR) {
-    const float q = rcp_approx_f32(__fmul_rn(D.x, D.y));
-    return __fmul2_rn(make_float2(q, q), make_float2(D.y, D.x));
-  }
-  return make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
-}
 
 __device__ __forceinline__ float norm2_f32(float a, float b, float c) {
   return __fmaf_rn(c, c, __fmaf_rn(b, b, __fmul_rn(a, a)));
@@ -273,301 +284,6 @@ __device__ __forceinline__ float combine_max(const unsigned* red) {
   return __uint_as_float(m);
 }
 
-// Shared memory of one FP32C unit. PW (pre-weighted far form) changes b to
-// (sz, sz, A_k, A_k) and adds c, d; h is then unused.
-template <int NT, int TS, bool PW = false>
-struct Fp32cSmem {
-  float4 a[TS];              // (sx, sx, sy, sy)
-  float4 b[TS];              // (sz, sz, 2G, 2G); PW: (sz, sz, A_k, A_k)
-  float2 e[TS];              // near form: (e_k, e_k)
-  float2 h[PW ? 1 : TS];     // far form: (A_k, A_k)
-  float4 c[PW ? TS : 1];     // PW: (G sx, G sx, G sy, G sy)
-  float4 d[PW ? TS : 1];     // PW: (G sz, G sz, G, G)
-  unsigned tmin[NT / 32];    // per-warp min of |s_k|^2 over the tile
-  unsigned rho[NT / 32];     // per-warp max of |t_i|^2 over the CTA's targets
-};
-
-// One work unit (targets at visiting positions [tile0, min(tile0 + NT*2*NPAIR,
-// i_end)) against sources [c0, c1)).
-template <int NT, int NPAIR, int TS, int FLUSH, int UNROLL, int FM>
-__device__ __forceinline__ void fp32c_unit(const double* __restrict__ x, const int* __restrict__ perm,
-                                           int tile0, int i_end, double d2,
-                                           const double4* __restrict__ src, int c0, int c1,
-                                           double* __restrict__ out, size_t stride,
-                                           Fp32cSmem<NT, TS, (FM & 4) != 0>& sm) {
-  static_assert(TS % FLUSH == 0, "flush interval must divide the tile");
-  static_assert(NT % 32 == 0, "whole warps");
-  constexpr int TPT = 2 * NPAIR;
-  constexpr int TB = NT * TPT;
-  constexpr bool FAR = (FM & 1) != 0;
-  constexpr bool PR = (FM & 2) != 0;
-  constexpr bool PW = FAR && (FM & 4) != 0;
-  // PW tiles hold G (not 2G): near-form sums come out halved
-  constexpr double kNearScale = PW ? 2.0 : 1.0;
-
-  const int mid_pos = min(tile0 + TB / 2, i_end - 1);
-  const int mid = perm ? perm[mid_pos] : mid_pos;
-  const double cx = x[3 * (size_t)mid], cy = x[3 * (size_t)mid + 1], cz = x[3 * (size_t)mid + 2];
-
-  float2 ntx[NPAIR], nty[NPAIR], ntz[NPAIR], ei[NPAIR], bh[NPAIR];
-  float2 fx[NPAIR], fy[NPAIR], fz[NPAIR], fw[NPAIR];
-  double ax[NPAIR][2], ay[NPAIR][2], az[NPAIR][2], aw[NPAIR][2];
-  float rho2 = 0.f;
-#pragma unroll
-  for (int p = 0; p < NPAIR; ++p) {
-    float tv[2][5];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
-      int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
-      double px = x[3 * (size_t)ld], py = x[3 * (size_t)ld + 1], pz = x[3 * (size_t)ld + 2];
-      const float tx = (float)(px - cx), ty = (float)(py - cy), tz = (float)(pz - cz);
-      const double E = (1.0 - (px * px + py * py + pz * pz)) + 2.0 * d2;
-      tv[h][0] = -tx;
-      tv[h][1] = -ty;
-      tv[h][2] = -tz;
-      tv[h][3] = (float)E + kSelfBias;
-      const float t2 = norm2_f32(tx, ty, tz);
-      tv[h][4] = (float)(0.5 * ((double)t2 + E));
-      if (pos >= i_end) {
-        // padding (a copy of the middle target, result discarded): huge
-        // denominators, so that a paired reciprocal (FM bit 1) with the middle
-        // target's own self pair (D = kSelfBias) in the other lane stays finite
-        tv[h][3] = kPadDenominator;
-        tv[h][4] = kPadDenominator;
-      }
-      rho2 = fmaxf(rho2, t2);
-      ax[p][h] = ay[p][h] = az[p][h] = aw[p][h] = 0.0;
-    }
-    ntx[p] = make_float2(tv[0][0], tv[1][0]);
-    nty[p] = make_float2(tv[0][1], tv[1][1]);
-    ntz[p] = make_float2(tv[0][2], tv[1][2]);
-    ei[p] = make_float2(tv[0][3], tv[1][3]);
-    bh[p] = make_float2(tv[0][4], tv[1][4]);
-    fx[p] = fy[p] = fz[p] = fw[p] = make_float2(0.f, 0.f);
-  }
-  if (FAR) warp_store_max(rho2, sm.rho);
-
-  for (int ts = c0; ts < c1; ts += TS) {
-    __syncthreads();
-    float smin = __int_as_float(0x7f800000);  // +inf
-    for (int j = threadIdx.x; j < TS; j += NT) {
-      int k = ts + j;
-      float sx = 0.f, sy = 0.f, sz = 0.f, g = 0.f, e = 1.f, ah = 1.f;
-      float gsx = 0.f, gsy = 0.f, gsz = 0.f;
-      if (k < c1) {
-        const double4 q = src[k];
-        const double dx = q.x - cx, dy = q.y - cy, dz = q.z - cz;
-        sx = (float)dx;
-        sy = (float)dy;
-        sz = (float)dz;
-        g = (float)(PW ? q.w : 2.0 * q.w);
-        if (PW) {
-          gsx = (float)(q.w * dx);
-          gsy = (float)(q.w * dy);
-          gsz = (float)(q.w * dz);
-        }
-        const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
-        e = (float)ek;
-        if (FAR) {
-          const float s2 = norm2_f32(sx, sy, sz);
-          ah = (float)(0.5 * ((double)s2 + ek));
-          smin = fminf(smin, s2);
-        }
-      }
-      sm.a[j] = make_float4(sx, sx, sy, sy);
-      sm.e[j] = make_float2(e, e);
-      if (PW) {
-        sm.b[j] = make_float4(sz, sz, ah, ah);
-        sm.c[j] = make_float4(gsx, gsx, gsy, gsy);
-        sm.d[j] = make_float4(gsz, gsz, g, g);
-      } else {
-        sm.b[j] = make_float4(sz, sz, g, g);
-        if (FAR) sm.h[j] = make_float2(ah, ah);
-      }
-    }
-    if (FAR) warp_store_min(smin, sm.tmin);
-    __syncthreads();
-    // strict: with rho = 0 (one target position) no tile is far
-    const bool far = FAR && combine_min<NT / 32>(sm.tmin) > kFarRatio2 * combine_max<NT / 32>(sm.rho);
-    if (PW && far) {
-      for (int jf = 0; jf < TS; jf += FLUSH) {
-#pragma unroll UNROLL
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = sm.a[j];
-          const float4 b = sm.b[j];
-          const float4 c = sm.c[j];
-          const float4 d = sm.d[j];
-          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-          const float2 szz = make_float2(b.x, b.y), ah = make_float2(b.z, b.w);
-          const float2 gsx = make_float2(c.x, c.y), gsy = make_float2(c.z, c.w);
-          const float2 gsz = make_float2(d.x, d.y), gg = make_float2(d.z, d.w);
-#pragma unroll
-          for (int p = 0; p < NPAIR; ++p) {
-            float2 D = __fadd2_rn(ah, bh[p]);
-            D = __ffma2_rn(sxx, ntx[p], D);
-            D = __ffma2_rn(syy, nty[p], D);
-            D = __ffma2_rn(szz, ntz[p], D);
-            const float2 r = rcp_pair<PR>(D);  // 1 / (1 - x_i.x_k + delta^2)
-            fx[p] = __ffma2_rn(r, gsx, fx[p]);
-            fy[p] = __ffma2_rn(r, gsy, fy[p]);
-            fz[p] = __ffma2_rn(r, gsz, fz[p]);
-            fw[p] = __ffma2_rn(r, gg, fw[p]);
-          }
-        }
-#pragma unroll
-        for (int p = 0; p < NPAIR; ++p) {
-          ax[p][0] += (double)fx[p].x;
-          ax[p][1] += (double)fx[p].y;
-          ay[p][0] += (double)fy[p].x;
-          ay[p][1] += (double)fy[p].y;
-          az[p][0] += (double)fz[p].x;
-          az[p][1] += (double)fz[p].y;
-          aw[p][0] += (double)fw[p].x;
-          aw[p][1] += (double)fw[p].y;
-          fx[p] = fy[p] = fz[p] = fw[p] = make_float2(0.f, 0.f);
-        }
-      }
-    } else if (far) {
-      for (int jf = 0; jf < TS; jf += FLUSH) {
-#pragma unroll UNROLL
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = sm.a[j];
-          const float4 b = sm.b[j];
-          const float2 ah = sm.h[j];
-          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-          const float2 szz = make_float2(b.x, b.y), gg = make_float2(b.z, b.w);
-#pragma unroll
-          for (int p = 0; p < NPAIR; ++p) {
-            float2 D = __fadd2_rn(ah, bh[p]);
-            D = __ffma2_rn(sxx, ntx[p], D);
-            D = __ffma2_rn(syy, nty[p], D);
-            D = __ffma2_rn(szz, ntz[p], D);
-            const float2 w = __fmul2_rn(gg, rcp_pair<PR>(D));  // 2 w: D/2 above
-            fx[p] = __ffma2_rn(w, sxx, fx[p]);
-            fy[p] = __ffma2_rn(w, syy, fy[p]);
-            fz[p] = __ffma2_rn(w, szz, fz[p]);
-            fw[p] = __fadd2_rn(fw[p], w);
-          }
-        }
-#pragma unroll
-        for (int p = 0; p < NPAIR; ++p) {
-          ax[p][0] = fma(0.5, (double)fx[p].x, ax[p][0]);
-          ax[p][1] = fma(0.5, (double)fx[p].y, ax[p][1]);
-          ay[p][0] = fma(0.5, (double)fy[p].x, ay[p][0]);
-          ay[p][1] = fma(0.5, (double)fy[p].y, ay[p][1]);
-          az[p][0] = fma(0.5, (double)fz[p].x, az[p][0]);
-          az[p][1] = fma(0.5, (double)fz[p].y, az[p][1]);
-          aw[p][0] = fma(0.5, (double)fw[p].x, aw[p][0]);
-          aw[p][1] = fma(0.5, (double)fw[p].y, aw[p][1]);
-          fx[p] = fy[p] = fz[p] = fw[p] = make_float2(0.f, 0.f);
-        }
-      }
-    } else {
-      for (int jf = 0; jf < TS; jf += FLUSH) {
-#pragma unroll UNROLL
-        for (int j = jf; j < jf + FLUSH; ++j) {
-          const float4 a = sm.a[j];
-          const float4 b = sm.b[j];
-          const float2 ee = sm.e[j];
-          const float2 sxx = make_float2(a.x, a.y), syy = make_float2(a.z, a.w);
-          const float2 szz = make_float2(b.x, b.y);
-          const float2 gg = PW ? make_float2(sm.d[j].z, sm.d[j].w) : make_float2(b.z, b.w);
-#pragma unroll
-          for (int p = 0; p < NPAIR; ++p) {
-            const float2 dx = __fadd2_rn(sxx, ntx[p]);
-            const float2 dy = __fadd2_rn(syy, nty[p]);
-            const float2 dz = __fadd2_rn(szz, ntz[p]);
-            float2 D = __fadd2_rn(ee, ei[p]);
-            D = __ffma2_rn(dx, dx, D);
-            D = __ffma2_rn(dy, dy, D);
-            D = __ffma2_rn(dz, dz, D);
-            const float2 w = __fmul2_rn(gg, rcp_pair<PR>(D));
-            fx[p] = __ffma2_rn(w, dx, fx[p]);
-            fy[p] = __ffma2_rn(w, dy, fy[p]);
-            fz[p] = __ffma2_rn(w, dz, fz[p]);
-          }
-        }
-#pragma unroll
-        for (int p = 0; p < NPAIR; ++p) {
-          ax[p][0] = fma(kNearScale, (double)fx[p].x, ax[p][0]);
-          ax[p][1] = fma(kNearScale, (double)fx[p].y, ax[p][1]);
-          ay[p][0] = fma(kNearScale, (double)fy[p].x, ay[p][0]);
-          ay[p][1] = fma(kNearScale, (double)fy[p].y, ay[p][1]);
-          az[p][0] = fma(kNearScale, (double)fz[p].x, az[p][0]);
-          az[p][1] = fma(kNearScale, (double)fz[p].y, az[p][1]);
-          fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
-        }
-      }
-    }
-  }
-  // far tiles: + nt_i sum w; partial rows are indexed by position in the visiting order
-#pragma unroll
-  for (int p = 0; p < NPAIR; ++p) {
-    const float ntxs[2] = {ntx[p].x, ntx[p].y}, ntys[2] = {nty[p].x, nty[p].y},
-                ntzs[2] = {ntz[p].x, ntz[p].y};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int pos = tile0 + (int)threadIdx.x + (2 * p + h) * NT;
-      if (FAR) {
-        ax[p][h] = fma((double)ntxs[h], aw[p][h], ax[p][h]);
-        ay[p][h] = fma((double)ntys[h], aw[p][h], ay[p][h]);
-        az[p][h] = fma((double)ntzs[h], aw[p][h], az[p][h]);
-      }
-      if (pos < i_end) {
-        out[pos] = ax[p][h];
-        out[stride + pos] = ay[p][h];
-        out[2 * stride + pos] = az[p][h];
-      }
-    }
-  }
-}
-
-
-// ---------------------------------------------------------------------------
-// FP32C, source-paired form (FM bit 3). The f32x2 lanes of each instruction
-// carry two SOURCES (k, k+1) for one target instead of one source for two
-// targets, so a source tile sits in shared memory without duplicated values:
-// a broadcast 128-bit shared load costs two wavefronts of the SM-wide shared
-// pipe (one wavefront per clock), and the target-paired layout spent 5-8
-// wavefronts per source on duplicates; here a far source pair costs 7 (3.5
-// per source), shared by the T targets of a thread.
-//
-// Coordinates are taken in a per-CTA orthonormal frame R = (e1, e2, e3) with
-// e3 along the origin c (the centroid of the CTA's targets projected to the
-// sphere): s_k = R(x_k - c),
-// t_i = R(x_i - c), both from FP64 and rounded once. Distances and dot
-// products are frame-invariant, so the near form and the far denominator are
-// those of the target-paired kernel. The far numerator accumulates
-//     T' = sum_k r_ik G_k x'_k,   x'_k = R x_k,   r = 1/(1 - x_i.x_k + delta^2),
-// three sums instead of four. In this frame the first two coordinates of
-// x'_k are e1.(x_k - c) and e2.(x_k - c) (small for nearby sources) and the
-// third is e3.x_k (about 1), so the large common part of the sum (about
-// sum r G) sits in the third coordinate only; u_i = x_i x R^T T' multiplies
-// that coordinate by the target's own small offset (e1, e2 components of
-// x_i), so its rounding costs what the separate sum r G of the
-// target-paired far form costs. A far pair is then 7 FP32
-// operations (4 denominator, 3 accumulations) and one MUFU reciprocal.
-// FM bit 0 (with bit 3): the FP64 flushes widen the FP32 partials with
-// integer operations (f2d_alu) instead of F2F conversions on the XU pipe.
-// FM bit 1 (with bit 3): the FP64 accumulators live in shared memory (one
-// slot per thread, target and coordinate), 6 fewer registers per target.
-// FM bit 2 (with bit 3): near tiles take d = s - t from hi/lo FP32 splits of
-// both offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to
-// FP32 (an absolute error of ulps of the patch radius, the dominant FP32C
-// error for nearest-neighbour pairs) no longer enters, and d keeps a few
-// ulps of its own length. Far tiles are unchanged. Both low parts are needed:
-// for the self pair s and t are the same point, so (s_hi - t_hi) and
-// (s_lo - t_lo) are both exactly 0 and the pair adds w * 0; correcting one
-// side only would leave d = s_lo there, a spurious self term.
-// PRF > 0: one source pair of every PRF shares a single MUFU reciprocal
-// (1/D_k = q D_k+1, 1/D_k+1 = q D_k, q = 1/(D_k D_k+1)), trading 8 XU cycles
-// for 3 FMA-pipe cycles per warp and target, so the FMA and XU pipes carry
-// equal loads. Partial sums stay in the rotated frame (near and far tiles
-// add into the same accumulators: near T'= sum w (x'_k - x'_i), far
-// sum w x'_k; they differ by multiples of x'_i, which u = x_i x T ignores)
-// and are rotated back in FP64 once per target.
-// ---------------------------------------------------------------------------
 template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false>
 struct SpSmem {
   float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
@@ -610,42 +326,12 @@ __device__ __forceinline__ double frame_dot(const double* e, double vx, double v
   return fma(e[0], vx, fma(e[1], vy, __dmul_rn(e[2], vz)));
 }
 
-template <bool PAIRED>
-__device__ __forceinline__ float2 rcp_sources(float2 D) {
-  if (PAIRED) {
-    // scalar products: no register-pair shuffles around the MUFU result
-    const float q = rcp_approx_f32(__fmul_rn(D.x, D.y));
-    return make_float2(__fmul_rn(q, D.y), __fmul_rn(q, D.x));
-  }
+__device__ __forceinline__ float2 rcp2(float2 D) {
   return make_float2(rcp_approx_f32(D.x), rcp_approx_f32(D.y));
 }
 
-// float -> double with integer operations (the ALU pipe) instead of an F2F
-// conversion (the XU pipe, which the MUFU reciprocals keep busy): exponent
-// rebiased by 1023 - 127, mantissa shifted into place; +-0 and FP32
-// subnormals give +-0, Inf and NaN stay Inf and NaN.
-__device__ __forceinline__ double f2d_alu(float f) {
-  const unsigned b = __float_as_uint(f);
-  const unsigned sign = b & 0x80000000u;
-  const unsigned mag = b & 0x7fffffffu;
-  unsigned hi = sign | ((mag >> 3) + (896u << 20));
-  unsigned lo = b << 29;
-  if (mag >= 0x7f800000u) hi |= 0x7ff00000u;
-  if (mag < 0x00800000u) {
-    hi = sign;
-    lo = 0u;
-  }
-  return __hiloint2double((int)hi, (int)lo);
-}
-
-template <bool ALU>
-__device__ __forceinline__ double widen(float f) {
-  if (ALU) return f2d_alu(f);
-  return (double)f;
-}
-
 // One far source pair against the thread's T targets.
-template <int T, bool PAIRED>
+template <int T>
 __device__ __forceinline__ void sp_far_step(const float4 a, const float4 b, const float4 c,
                                             const float2 d, const float2* ntx, const float2* nty,
                                             const float2* ntz, const float2* bh, float2* fx,
@@ -659,7 +345,7 @@ __device__ __forceinline__ void sp_far_step(const float4 a, const float4 b, cons
     D = __ffma2_rn(sx, ntx[t], D);
     D = __ffma2_rn(sy, nty[t], D);
     D = __ffma2_rn(sz, ntz[t], D);
-    const float2 r = rcp_sources<PAIRED>(D);
+    const float2 r = rcp2(D);
     fx[t] = __ffma2_rn(r, gx, fx[t]);
     fy[t] = __ffma2_rn(r, gy, fy[t]);
     fz[t] = __ffma2_rn(r, d, fz[t]);
@@ -693,22 +379,22 @@ struct SpAcc {
   }
 };
 
-template <int NT, int T, int TS, int FLUSH, int UNROLL, int PRF, bool ALUCVT, bool SMACC,
-          bool HILO, int FARK>
+// One work unit: targets at visiting positions [tile0, min(tile0 + NT*T,
+// i_end)) against sources [c0, c1); FP64 sums in the global frame written to
+// out[pos], out[stride + pos], out[2*stride + pos].
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
                                               SpSmem<NT, TS, T, SMACC, HILO>& sm) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
-  static_assert(PRF == 0 || (FLUSH / 2) % PRF == 0, "paired-reciprocal period divides the flush");
   static_assert(NT % 32 == 0, "whole warps");
   static_assert(TS % (FLUSH * FARK) == 0, "far-tile flush interval divides the tile");
   constexpr int TB = NT * T;
   constexpr int NP = TS / 2;
   constexpr int FP = FLUSH / 2;
   constexpr int FPF = FP * FARK;  // source pairs between flushes in all-far tiles
-  constexpr int GRP = PRF > 0 ? PRF : 1;  // source pairs per group; the first is paired
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
   const int mid = perm ? perm[mid_pos] : mid_pos;
@@ -858,29 +544,20 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     // g's, so only the segments that hold near sources take the near form.
     // Otherwise one test for the whole tile.
     // A tile whose every segment is far runs one tight far loop, flushed
-    // every FARK segments (far terms are small and smooth: fewer F2F
-    // conversions on the XU pipe that the reciprocals also use).
+    // every FARK segments.
     constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
     const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
     const bool tile_far = combine_min<NT / 32>(sm.tmin) > lim;
     if (tile_far) {
       for (int jf = 0; jf < NP; jf += FPF) {
 #pragma unroll UNROLL
-        for (int jg = jf; jg < jf + FPF; jg += GRP) {
-#pragma unroll
-          for (int u = 0; u < GRP; ++u) {
-            const int j = jg + u;
-            if (PRF > 0 && u == 0)
-              sp_far_step<T, true>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
-            else
-              sp_far_step<T, false>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
-          }
-        }
+        for (int j = jf; j < jf + FPF; ++j)
+          sp_far_step<T>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-          acc.add(0, t, widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y)));
-          acc.add(1, t, widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y)));
-          acc.add(2, t, widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y)));
+          acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
+          acc.add(1, t, (double)__fadd_rn(fy[t].x, fy[t].y));
+          acc.add(2, t, (double)__fadd_rn(fz[t].x, fz[t].y));
           fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
         }
       }
@@ -890,16 +567,8 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
       const bool far = PERSEG && __uint_as_float(sm.tmin[jf / FP]) > lim;
       if (far) {
 #pragma unroll UNROLL
-        for (int jg = jf; jg < jf + FP; jg += GRP) {
-#pragma unroll
-          for (int u = 0; u < GRP; ++u) {
-            const int j = jg + u;
-            if (PRF > 0 && u == 0)
-              sp_far_step<T, true>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
-            else
-              sp_far_step<T, false>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
-          }
-        }
+        for (int j = jf; j < jf + FP; ++j)
+          sp_far_step<T>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
       } else {
         // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
         float ntl[HILO ? 3 * T : 1];
@@ -935,7 +604,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
             D = __ffma2_rn(dx, dx, D);
             D = __ffma2_rn(dy, dy, D);
             D = __ffma2_rn(dz, dz, D);
-            const float2 w = __fmul2_rn(gg, rcp_sources<false>(D));
+            const float2 w = __fmul2_rn(gg, rcp2(D));
             fx[t] = __ffma2_rn(w, dx, fx[t]);
             fy[t] = __ffma2_rn(w, dy, fy[t]);
             fz[t] = __ffma2_rn(w, dz, fz[t]);
@@ -944,9 +613,9 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
       }
 #pragma unroll
       for (int t = 0; t < T; ++t) {
-        acc.add(0, t, widen<ALUCVT>(__fadd_rn(fx[t].x, fx[t].y)));
-        acc.add(1, t, widen<ALUCVT>(__fadd_rn(fy[t].x, fy[t].y)));
-        acc.add(2, t, widen<ALUCVT>(__fadd_rn(fz[t].x, fz[t].y)));
+        acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
+        acc.add(1, t, (double)__fadd_rn(fy[t].x, fy[t].y));
+        acc.add(2, t, (double)__fadd_rn(fz[t].x, fz[t].y));
         fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
       }
     }
@@ -964,26 +633,27 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   }
 }
 
-template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
+// Template parameters of fp32c_sp_unit from a form bit set FM.
+template <int FM>
+struct SpForm {
+  static constexpr bool smacc = (FM & 2) != 0;
+  static constexpr bool hilo = (FM & 4) != 0;
+  static constexpr int fark = 1 << ((FM >> 8) & 3);
+};
+
+template <int NT, int T, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P) {
-  // FM bit 3: source-paired form, NPAIR = targets per thread
-  constexpr bool SP = (FM & 8) != 0;
+  using F = SpForm<FM>;
   const TargetSeg& G = find_seg(P, blockIdx.x);
-  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * (SP ? NPAIR : 2 * NPAIR));
+  const int tile0 = G.i0 + (int)(blockIdx.x - G.tile_begin) * (NT * T);
   const int c0 = (int)blockIdx.y * P.chunk_len;
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-  if constexpr (SP) {
-    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0, (FM & 4) != 0> sm;
-    fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
-                  (FM & 4) != 0, (1 << ((FM >> 8) & 3))>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0,
-                                                         c1, out, stride, sm);
-  } else {
-    __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
-    fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out,
-                                                 stride, sm);
-  }
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
+  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(G.x, G.perm, tile0, G.i1,
+                                                                      G.d2, P.src, c0, c1, out,
+                                                                      stride, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -1026,28 +696,17 @@ __device__ __forceinline__ int next_item(int* counter, int* slot) {
   return *slot;
 }
 
-template <int NT, int NPAIR, int TS, int FLUSH, int MINB, int UNROLL, int FM>
+template <int NT, int T, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
+  using F = SpForm<FM>;
   __shared__ int slot;
-  if constexpr ((FM & 8) != 0) {
-    __shared__ SpSmem<NT, TS, NPAIR, (FM & 2) != 0, (FM & 4) != 0> sm;
-    for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
-      const BatchItem I = B.items[it];
-      const BatchSeg S = B.segs[I.seg];
-      double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-      fp32c_sp_unit<NT, NPAIR, TS, FLUSH, UNROLL, ((FM >> 4) & 15), (FM & 1) != 0, (FM & 2) != 0,
-                    (FM & 4) != 0, (1 << ((FM >> 8) & 3))>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src,
-                                                           I.c0, I.c1, out, B.stride, sm);
-    }
-  } else {
-    __shared__ Fp32cSmem<NT, TS, (FM & 4) != 0> sm;
-    for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
-      const BatchItem I = B.items[it];
-      const BatchSeg S = B.segs[I.seg];
-      double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-      fp32c_unit<NT, NPAIR, TS, FLUSH, UNROLL, FM>(S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0,
-                                                   I.c1, out, B.stride, sm);
-    }
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
+  for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
+    const BatchItem I = B.items[it];
+    const BatchSeg S = B.segs[I.seg];
+    double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(
+        S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
   }
 }
 

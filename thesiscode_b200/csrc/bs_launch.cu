@@ -35,9 +35,9 @@ void DevBuf::release() {
 
 // ---------------------------------------------------------------------------
 // Kernel variants: the launch shapes the autotuner chooses from. FP32C
-// variants differ in threads per CTA, target pairs per thread, FP32 partial
-// length before the FP64 flush, minimum resident CTAs (register cap) and
-// source-loop unrolling; FP64 variants in threads and targets per thread.
+// variants differ in threads per CTA, targets per thread, FP32 partial length
+// before the FP64 flush, minimum resident CTAs (register cap), source-loop
+// unrolling and form bits; FP64 variants in threads and targets per thread.
 // ---------------------------------------------------------------------------
 constexpr int kTS = 256;
 
@@ -49,14 +49,13 @@ template <int NT, int TPT, int MINB, bool FUSED>
 void launch64b(int g, cudaStream_t s, const BatchLaunch& B) {
   pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(B);
 }
-template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL, int FM>
+template <int NT, int T, int FLUSH, int MINB, int UNROLL, int FM>
 void launch32b(int g, cudaStream_t s, const BatchLaunch& B) {
-  pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(B);
+  pair_fp32c_batch_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(B);
 }
-
-template <int NT, int NPAIR, int FLUSH, int MINB, int UNROLL, int FM>
+template <int NT, int T, int FLUSH, int MINB, int UNROLL, int FM>
 void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
-  pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(P);
+  pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(P);
 }
 
 #define V64(NT, TPT, MINB, FUSED)                                                 \
@@ -64,24 +63,13 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
                 (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED>,               \
                 launch64b<NT, TPT, MINB, FUSED>,                                         \
                 (const void*)pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED>, 0 }
-#define V32(NT, NPAIR, FLUSH, MINB, UNROLL, FM)                                             \
-  PairVariant { TC_FP32C, NT, 2 * NPAIR, kTS, FLUSH, MINB, UNROLL,                           \
-                launch32<NT, NPAIR, FLUSH, MINB, UNROLL, FM>,                                \
-                (const void*)pair_fp32c_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM>,     \
-                launch32b<NT, NPAIR, FLUSH, MINB, UNROLL, FM>,                               \
-                (const void*)pair_fp32c_batch_kernel<NT, NPAIR, kTS, FLUSH, MINB, UNROLL, FM>, FM }
-
-// Source-paired FP32C form: T targets per thread, UNROLL groups of PRF source
-// pairs (one paired reciprocal per group; PRF 0: none) per unrolled body.
-#define VSPX(NT, T, FLUSH, MINB, UNROLL, FM) \
-  PairVariant { TC_FP32C, NT, T, kTS, FLUSH, MINB, UNROLL, \
-                launch32<NT, T, FLUSH, MINB, UNROLL, FM>, \
-                (const void*)pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM>, \
-                launch32b<NT, T, FLUSH, MINB, UNROLL, FM>, \
+// FP32C: T targets per thread, FP32 flush every FLUSH sources, form bits FM
+#define V32(NT, T, FLUSH, MINB, UNROLL, FM)                                            \
+  PairVariant { TC_FP32C, NT, T, kTS, FLUSH, MINB, UNROLL,                             \
+                launch32<NT, T, FLUSH, MINB, UNROLL, FM>,                              \
+                (const void*)pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM>,   \
+                launch32b<NT, T, FLUSH, MINB, UNROLL, FM>,                             \
                 (const void*)pair_fp32c_batch_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM>, FM }
-#define VSP(NT, T, FLUSH, MINB, UNROLL, PRF) VSPX(NT, T, FLUSH, MINB, UNROLL, 8 | (PRF << 4))
-// ... with the flushes widened by integer operations (form bit 0)
-#define VSPA(NT, T, FLUSH, MINB, UNROLL, PRF) VSPX(NT, T, FLUSH, MINB, UNROLL, 9 | (PRF << 4))
 
 // FP64: the `flush` field records the denominator mode (1 = fused, 0 =
 // rounded exactly like the reference).
@@ -89,49 +77,20 @@ const PairVariant kVariants64[] = {
     V64(256, 2, 5, true),  V64(256, 4, 2, true),  V64(256, 1, 6, true), V64(128, 4, 4, true),
     V64(256, 2, 5, false), V64(256, 4, 2, false),
 };
-// FP32C: the last field is a bit set: far-field form (1), paired
-// reciprocal (2), pre-weighted far-field sources (4, with 1), source-paired
-// rotated-frame form (8, its own far/near forms; with it, bit 0 widens the
-// FP64 flushes by integer operations, bit 1 keeps the FP64 accumulators in
-// shared memory, bit 2 gives near tiles hi/lo offsets, bits 4-7 give the
-// period of the paired reciprocal and bits 8-9 the log2 of the number of
-// flush intervals between flushes in tiles whose every source is far).
+// FP32C form bits (SpForm in bs_core.cuh): 8 = source-paired form (all
+// variants), 2 = FP64 accumulators in shared memory, 4 = hi/lo near offsets,
+// 256 / 512 = tiles whose every source is far flushed every 2 / 4 flush
+// lengths.
 const PairVariant kVariants32[] = {
-    V32(256, 2, 32, 3, 4, 0), V32(256, 2, 64, 2, 4, 0), V32(128, 1, 32, 8, 8, 0),
-    V32(256, 2, 16, 2, 4, 0), V32(128, 2, 32, 6, 4, 0), V32(256, 1, 32, 4, 8, 0),
-    V32(128, 2, 32, 5, 4, 1), V32(128, 2, 32, 5, 4, 3), V32(256, 2, 32, 2, 4, 1),
-    V32(256, 2, 32, 2, 4, 3), V32(128, 1, 32, 8, 8, 1), V32(128, 1, 32, 8, 8, 3),
-    V32(128, 2, 32, 6, 4, 2), V32(128, 2, 32, 4, 4, 1), V32(128, 2, 32, 4, 4, 3),
-    V32(128, 1, 32, 6, 8, 1), V32(128, 1, 32, 8, 16, 1), V32(256, 1, 32, 4, 8, 1),
-    V32(64, 1, 32, 12, 8, 1), V32(128, 1, 64, 6, 8, 1), V32(128, 1, 32, 7, 8, 1),
-    V32(256, 1, 32, 3, 8, 1), V32(128, 1, 128, 6, 8, 1), V32(128, 1, 64, 8, 8, 1),
-    V32(128, 1, 64, 6, 16, 1),
-    // pre-weighted far form (bit 2): 8 FP32 operations per far pair
-    V32(128, 1, 64, 6, 8, 5), V32(128, 2, 64, 4, 8, 5), V32(128, 2, 64, 5, 4, 5),
-    V32(128, 1, 128, 6, 8, 5), V32(128, 1, 64, 8, 8, 5), V32(256, 1, 64, 3, 8, 5),
-    V32(128, 2, 128, 4, 8, 5),
-    // source-paired form (bit 3; bits 4+: paired-reciprocal period)
-    VSP(128, 2, 64, 6, 2, 4), VSP(128, 2, 64, 6, 4, 0), VSP(128, 4, 64, 4, 2, 4),
-    VSP(128, 4, 64, 4, 1, 4), VSP(128, 3, 64, 5, 2, 4), VSP(128, 2, 64, 8, 2, 4),
-    VSP(256, 2, 64, 3, 2, 4), VSP(128, 4, 64, 4, 4, 0), VSP(128, 2, 64, 6, 1, 8),
-    VSP(128, 2, 128, 6, 4, 0), VSP(128, 2, 64, 5, 4, 0), VSP(128, 2, 64, 6, 8, 0),
-    VSP(64, 2, 64, 12, 4, 0), VSP(128, 2, 128, 6, 8, 0), VSP(128, 2, 64, 5, 8, 0),
-    VSPA(128, 2, 64, 6, 4, 0), VSPA(128, 2, 64, 6, 2, 4), VSPA(128, 2, 64, 5, 4, 0),
-    VSP(256, 2, 64, 3, 4, 0),
-    // FP64 accumulators in shared memory (form bit 1 with bit 3)
-    VSPX(128, 2, 64, 7, 4, 10), VSPX(128, 2, 64, 8, 4, 10), VSPX(128, 2, 64, 6, 4, 10),
-    VSPX(128, 3, 64, 6, 4, 10),
-    VSPX(128, 3, 64, 6, 2, 10), VSPX(128, 3, 64, 5, 4, 10), VSPX(128, 4, 64, 5, 4, 10),
-    VSPX(128, 4, 64, 4, 4, 10), VSPX(128, 3, 64, 6, 8, 10), VSPX(64, 3, 64, 12, 4, 10),
-    // 32-source flush
-    VSPX(128, 3, 32, 6, 4, 10), VSP(128, 2, 32, 6, 4, 0), VSPX(128, 2, 32, 6, 4, 10),
-    // near tiles with hi/lo offsets (form bit 2 with bit 3)
-    VSPX(128, 3, 64, 6, 4, 14), VSPX(128, 2, 64, 6, 4, 12), VSPX(128, 2, 64, 6, 4, 14),
-    VSPX(128, 3, 64, 5, 4, 14),
-    // all-far tiles flushed every 128 (bit 8) or 256 (bit 9) sources
-    VSPX(128, 3, 64, 6, 4, 10 | 256), VSPX(128, 3, 64, 6, 4, 10 | 512),
-    VSPX(128, 2, 64, 6, 4, 8 | 256), VSPX(128, 2, 64, 6, 4, 8 | 512),
-    VSPX(128, 2, 64, 6, 4, 10 | 512), VSPX(128, 2, 64, 6, 4, 10 | 256),
+    // 0: default from 131,072 sources (3 targets per thread); 1: default below (2 per thread)
+    V32(128, 3, 64, 6, 4, 8 | 2 | 256), V32(128, 2, 64, 6, 4, 8 | 512),
+    // 2-7: the batch autotuner's other candidates (4: the 64-source far flush of 0)
+    V32(128, 2, 64, 6, 4, 8 | 2 | 512), V32(128, 2, 64, 6, 4, 8 | 2 | 256),
+    V32(128, 3, 64, 6, 4, 8 | 2), V32(128, 2, 64, 6, 4, 8), V32(128, 2, 64, 6, 4, 8 | 2),
+    V32(128, 3, 64, 6, 2, 8 | 2),
+    // 8-11: near tiles with hi/lo offsets (1e-7 at coarser grids, at a fraction of the speed)
+    V32(128, 3, 64, 6, 4, 8 | 4 | 2), V32(128, 2, 64, 6, 4, 8 | 4), V32(128, 2, 64, 6, 4, 8 | 4 | 2),
+    V32(128, 3, 64, 5, 4, 8 | 4 | 2),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
@@ -165,15 +124,15 @@ int select_variant(tc_ctx* ctx, int precision, int id) {
 }
 
 // Automatic FP32C variant: below kAutoSmallSources sources (icosahedral level
-// 6 and coarser) two targets per thread (variant 71: more CTAs for few
+// 6 and coarser) two targets per thread (variant 1: more CTAs for few
 // tiles, and smaller tile patches, hence smaller FP32 offsets), above it
-// three (variant 68: 2-4% faster from level 7 on); both flush all-far tiles
-// less often than mixed ones (68 every 128 sources, 1.8-2.0% faster than
-// every 64 at levels 7-8 with the same error; 71 every 256, 1.6% faster at
+// three (variant 0: 2-4% faster from level 7 on); both flush all-far tiles
+// less often than mixed ones (0 every 128 sources, 1.8-2.0% faster than
+// every 64 at levels 7-8 with the same error; 1 every 256, 1.6% faster at
 // level 6, error 6.1e-8 against 5.2e-8 on the level-6 jet).
 constexpr int kAutoSmallSources = 131072;
-constexpr int kAutoSmallVariant = 71;
-constexpr int kAutoLargeVariant = 68;
+constexpr int kAutoSmallVariant = 1;
+constexpr int kAutoLargeVariant = 0;
 
 int use_fp32c_variant(tc_ctx* ctx, int n) {
   if (!ctx->auto32) return TC_OK;
@@ -211,9 +170,10 @@ static int choose_chunks(int tiles, int n, int ts, int slots, int min_chunk, int
   return best;
 }
 
-int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
-                 int n_out, int* nchunks) {
-  *nchunks = 0;
+// Tiles and chunking of one pair launch: the target segments, the grid and the
+// chunk length (partial sums need S * 3 * n_out doubles).
+static int plan_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
+                      int n_out, int max_chunks, PairLaunch* P, dim3* grid) {
   const bool fp64 = ctx->precision == TC_FP64;
   if (!fp64) {
     const int rc0 = use_fp32c_variant(ctx, n);
@@ -221,12 +181,12 @@ int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src,
   }
   const PairCfg& cfg = fp64 ? ctx->cfg64 : ctx->cfg32;
   const int tb = cfg.tb();
-  PairLaunch P{};
+  *P = PairLaunch{};
   int tiles = 0, k = 0;
   for (int s = 0; s < nseg; ++s) {
     int len = segs[s].i1 - segs[s].i0;
     if (len <= 0) continue;
-    TargetSeg& g = P.seg[k++];
+    TargetSeg& g = P->seg[k++];
     g.x = segs[s].x;
     g.perm = fp64 ? nullptr : segs[s].perm;
     g.i0 = segs[s].i0;
@@ -237,21 +197,25 @@ int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src,
     g.tile_begin = tiles;
     tiles += (len + tb - 1) / tb;
   }
-  P.nseg = k;
+  P->nseg = k;
+  *grid = dim3(tiles, 0);
   if (tiles == 0 || n <= 0) return TC_OK;
   const int slots = fp64 ? ctx->slots64 : ctx->slots32;
-  int S = choose_chunks(tiles, n, cfg.ts, slots, ctx->min_chunk, ctx->max_chunks);
+  int S = choose_chunks(tiles, n, cfg.ts, slots, ctx->min_chunk, max_chunks);
   int chunk_len = (n + S - 1) / S;
   chunk_len = (chunk_len + cfg.ts - 1) / cfg.ts * cfg.ts;
   S = (n + chunk_len - 1) / chunk_len;
-  int rc = ctx->partial.ensure((size_t)S * 3 * (size_t)n_out * sizeof(double));
-  if (rc) return rc;
-  P.src = src;
-  P.n = n;
-  P.chunk_len = chunk_len;
-  P.partial = ctx->partial.as<double>();
-  P.n_out = n_out;
-  dim3 grid(tiles, S);
+  P->src = src;
+  P->n = n;
+  P->chunk_len = chunk_len;
+  P->n_out = n_out;
+  *grid = dim3(tiles, S);
+  return TC_OK;
+}
+
+// Launches a planned pair kernel (timing events and counters as tc_stats reports them).
+static int run_pairs(tc_ctx* ctx, const PairLaunch& P, dim3 grid) {
+  const bool fp64 = ctx->precision == TC_FP64;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   if (ctx->time_pairs) {
     TC_CUDA_TRY(cudaEventCreate(&ev[0]));
@@ -268,9 +232,44 @@ int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src,
   ctx->launches += 1;
   ctx->pair_launches += 1;
   for (int s = 0; s < P.nseg; ++s)
-    ctx->pair_interactions += (long long)(P.seg[s].i1 - P.seg[s].i0) * n -
+    ctx->pair_interactions += (long long)(P.seg[s].i1 - P.seg[s].i0) * P.n -
                               (P.seg[s].self_offset != kNoSelf ? (P.seg[s].i1 - P.seg[s].i0) : 0);
-  *nchunks = S;
+  return TC_OK;
+}
+
+int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
+                 int n_out, int* nchunks) {
+  *nchunks = 0;
+  PairLaunch P;
+  dim3 grid;
+  int rc = plan_pairs(ctx, segs, nseg, src, n, n_out, ctx->max_chunks, &P, &grid);
+  if (rc || grid.y == 0) return rc;
+  if ((rc = ctx->partial.ensure((size_t)grid.y * 3 * (size_t)n_out * sizeof(double)))) return rc;
+  P.partial = ctx->partial.as<double>();
+  if ((rc = run_pairs(ctx, P, grid))) return rc;
+  *nchunks = (int)grid.y;
+  return TC_OK;
+}
+
+int launch_pairs_into(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
+                      int n_out, double* partial, size_t partial_bytes, int* nchunks) {
+  *nchunks = 0;
+  const size_t per_chunk = 3 * (size_t)n_out * sizeof(double);
+  const size_t fit = per_chunk ? partial_bytes / per_chunk : (size_t)ctx->max_chunks;
+  PairLaunch P;
+  dim3 grid;
+  int rc = plan_pairs(ctx, segs, nseg, src, n, n_out,
+                      (int)std::max<size_t>(1, std::min<size_t>(fit, (size_t)ctx->max_chunks)), &P,
+                      &grid);
+  if (rc || grid.y == 0) return rc;
+  if ((size_t)grid.y * per_chunk > partial_bytes) {
+    tc_record_error("pair partial sums need %zu bytes, %zu given", (size_t)grid.y * per_chunk,
+                    partial_bytes);
+    return TC_ERR_ARG;
+  }
+  P.partial = partial;
+  if ((rc = run_pairs(ctx, P, grid))) return rc;
+  *nchunks = (int)grid.y;
   return TC_OK;
 }
 

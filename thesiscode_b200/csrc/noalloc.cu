@@ -6,25 +6,34 @@
 // time-stepping loops that overlap work on several streams, where cudaMalloc's
 // implicit device-wide synchronisation in the middle of a step is not
 // acceptable. For them, tc_bs_velocity_device_noalloc computes the same sum
-// as tc_bs_velocity_device with its scratch - the packed sources and the FP64
-// partial sums of the pair kernel - in a fixed array compiled into the
-// library, so a call allocates nothing.
+// as tc_bs_velocity_device with all of its scratch - the packed sources, the
+// FP64 partial sums of the pair kernel and, for FP32C, the targets' visiting
+// order with its sort buffers - in a fixed array compiled into the library,
+// so a call allocates nothing.
 //
 // The array is a file-scope static __device__ array of kNoAllocScratchBytes
 // (32 MiB); every GPU that loads the library holds it until the process
-// exits. A call needs 32*n (rounded up to 256) + 24*m*chunks bytes of it, so
-// the largest single-chunk problem is 32*n + 24*m <= 32 MiB (for example
-// 327,680 active panels with themselves as targets); larger calls are
-// rejected with TC_ERR_ARG. Host code cannot use the array's name as a device
-// address, so the first call on each device looks the address up with
-// cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture on the device.
+// exits. A call needs 32*n bytes for the sources (each part rounded up to 256
+// bytes), 24*m per source chunk for the partial sums and, for FP32C with the
+// library's visiting order, 4*m for the order plus about 20 bytes per target
+// in range [i0, i1) for its sort; larger calls are rejected with TC_ERR_ARG.
+// The chunk count is the allocating entry point's choice, capped by what fits,
+// so the two entry points give the same result whenever that choice fits.
+//
+// Host code cannot use the array's name as a device address: the first call
+// on each device (and the first after the device's context was destroyed and
+// created again) looks the address up with cudaGetSymbolAddress, with that
+// device current, and caches it with the context's id; make that first call
+// before any stream capture on the device.
 //
 // Every call shares the array and it keeps the previous call's contents:
-// the pair kernel writes every partial-sum row the epilogue reads, so nothing
-// has to start at zero. Calls that overlap on the GPU (on different streams
-// or from different contexts on the same device) race on the array; callers
-// must order them.
+// every buffer in it is written before it is read within a call (packed
+// sources, sort keys, the order, each partial-sum row the epilogue reads), so
+// nothing has to start at zero. Calls that overlap on the GPU (on different
+// streams or from different contexts on the same device) race on the array;
+// callers must order them.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -38,8 +47,39 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
 
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;  // id of the context the address belongs to
+  void* ptr = nullptr;
+};
+
 std::mutex g_scratch_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+ScratchSlot g_scratch[kMaxDevices];
+
+// Unique id of the current context (cuCtxGetId, reached through the runtime so
+// the library links only libcudart); 0 when the driver cannot say.
+unsigned long long current_context_id() {
+  static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f);
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c ||
+      get_id(c, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 // Device address of g_noalloc_scratch on `device` (which must be current).
 int scratch_address(int device, void** out) {
@@ -47,8 +87,11 @@ int scratch_address(int device, void** out) {
     tc_record_error("tc_bs_velocity_device_noalloc: device %d out of range", device);
     return TC_ERR_ARG;
   }
+  const unsigned long long id = current_context_id();
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[device]) {
+  ScratchSlot& s = g_scratch[device];
+  // id 0 (unknown): look the address up on every call rather than trust a cached one
+  if (!s.ptr || id == 0 || s.ctx_id != id) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -57,9 +100,10 @@ int scratch_address(int device, void** out) {
       cudaGetLastError();
       return TC_ERR_CUDA;
     }
-    g_scratch_ptr[device] = p;
+    s.ptr = p;
+    s.ctx_id = id;
   }
-  *out = g_scratch_ptr[device];
+  *out = s.ptr;
   return TC_OK;
 }
 
@@ -92,78 +136,59 @@ extern "C" int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, cons
     tc_record_error("null array argument");
     return TC_ERR_ARG;
   }
-  const size_t src_bytes = round256((size_t)n * sizeof(double4));
-  const size_t row_bytes = 3 * (size_t)m * sizeof(double);
-  if (src_bytes + row_bytes > kNoAllocScratchBytes) {
-    tc_record_error("tc_bs_velocity_device_noalloc: n=%d sources and m=%d targets need %zu bytes "
-                    "of scratch, more than the fixed %zu bytes (32*n + 24*m must fit)",
-                    n, m, src_bytes + row_bytes, kNoAllocScratchBytes);
-    return TC_ERR_ARG;
-  }
   if (cudaSetDevice(ctx->device) != cudaSuccess) {
     tc_record_error("cudaSetDevice(%d) failed", ctx->device);
     return TC_ERR_CUDA;
   }
-  void* base = nullptr;
-  int rc = scratch_address(ctx->device, &base);
-  if (rc) return rc;
-  if (target_class == TC_ACTIVE) X = src_x;
-  double4* src = static_cast<double4*>(base);
-  double* partial = reinterpret_cast<double*>(static_cast<char*>(base) + src_bytes);
-
-  const bool fp64 = ctx->precision == TC_FP64;
-  if (!fp64 && (rc = tcb::use_fp32c_variant(ctx, n))) return rc;
-  const tcb::PairVariant* v = tcb::variant(ctx->precision, fp64 ? ctx->var64 : ctx->var32);
-  const int tb = v->nt * v->tpt;
+  // layout: sources | order (perm, keys in, keys out, indices, sort temp) | partial sums
   const int len = i1 - i0;
+  const bool ordered = ctx->precision == TC_FP32C && ctx->target_order == TC_ORDER_HILBERT && len > 0;
+  size_t sort_bytes = 0;
+  int rc;
+  if (ordered && (rc = tcb::order_sort_bytes(len, &sort_bytes))) return rc;
+  const size_t src_bytes = round256((size_t)n * sizeof(double4));
+  const size_t perm_bytes = ordered ? round256((size_t)m * sizeof(int)) : 0;
+  const size_t key_bytes = ordered ? round256((size_t)len * sizeof(unsigned)) : 0;
+  const size_t order_bytes = ordered ? perm_bytes + 3 * key_bytes + round256(sort_bytes) : 0;
+  const size_t chunk_bytes = 3 * (size_t)m * sizeof(double);
+  const size_t fixed = src_bytes + order_bytes;
+  if (fixed > kNoAllocScratchBytes || (len > 0 && n > 0 && kNoAllocScratchBytes - fixed < chunk_bytes)) {
+    tc_record_error("tc_bs_velocity_device_noalloc: n=%d sources and m=%d targets need %zu bytes of "
+                    "scratch, more than its fixed 32 MiB (32*n + 24*m, plus 4*m + ~20*(i1-i0) for "
+                    "the FP32C visiting order, must fit)",
+                    n, m, fixed + chunk_bytes, kNoAllocScratchBytes);
+    return TC_ERR_ARG;
+  }
+  void* base = nullptr;
+  if ((rc = scratch_address(ctx->device, &base))) return rc;
+  char* b = static_cast<char*>(base);
+  double4* src = reinterpret_cast<double4*>(b);
+  int* perm = nullptr;
+  if (target_class == TC_ACTIVE) X = src_x;
+  if (ordered) {
+    char* o = b + src_bytes;
+    perm = reinterpret_cast<int*>(o);
+    unsigned* k_in = reinterpret_cast<unsigned*>(o + perm_bytes);
+    unsigned* k_out = reinterpret_cast<unsigned*>(o + perm_bytes + key_bytes);
+    int* v_in = reinterpret_cast<int*>(o + perm_bytes + 2 * key_bytes);
+    void* temp = o + perm_bytes + 3 * key_bytes;
+    if ((rc = tcb::compute_order_into(ctx, X, i0, i1, perm, k_in, k_out, v_in, temp, sort_bytes)))
+      return rc;
+  }
+  double* partial = reinterpret_cast<double*>(b + fixed);
+  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
+  tcb::SegDesc seg{X, perm, i0, i1, 0, target_class == TC_ACTIVE ? 0 : tcb::kNoSelf,
+                   ctx->delta[target_class] * ctx->delta[target_class]};
   int nchunks = 0;
-  if (n > 0) {
-    tcb::pack_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(src_x, vort, area, n, src);
-    TC_CUDA_TRY(cudaGetLastError());
-  }
-  if (len > 0 && n > 0) {
-    // source chunks: fill the resident CTA slots in whole waves, as far as the scratch allows
-    const int tiles = (len + tb - 1) / tb;
-    const int slots = fp64 ? ctx->slots64 : ctx->slots32;
-    const int fit = (int)std::min<size_t>((kNoAllocScratchBytes - src_bytes) / row_bytes, 64);
-    int best = 1;
-    double best_eff = 0.0;
-    for (int s = 1; s <= fit; ++s) {
-      if (s > 1 && (n + s - 1) / s < ctx->min_chunk) break;
-      long long items = (long long)tiles * s;
-      long long waves = (items + slots - 1) / slots;
-      double eff = (double)items / (double)(waves * slots);
-      if (eff > best_eff + 0.02) {
-        best_eff = eff;
-        best = s;
-      }
-    }
-    int chunk_len = (n + best - 1) / best;
-    chunk_len = (chunk_len + v->ts - 1) / v->ts * v->ts;
-    nchunks = (n + chunk_len - 1) / chunk_len;
-    tcb::PairLaunch P{};
-    P.seg[0].x = X;
-    P.seg[0].perm = nullptr;  // targets in the caller's order
-    P.seg[0].i0 = i0;
-    P.seg[0].i1 = i1;
-    P.seg[0].out_offset = 0;
-    P.seg[0].self_offset = target_class == TC_ACTIVE ? 0 : tcb::kNoSelf;
-    P.seg[0].d2 = ctx->delta[target_class] * ctx->delta[target_class];
-    P.seg[0].tile_begin = 0;
-    P.nseg = 1;
-    P.src = src;
-    P.n = n;
-    P.chunk_len = chunk_len;
-    P.partial = partial;
-    P.n_out = m;
-    v->launch(dim3(tiles, nchunks), ctx->stream, P);
-    TC_CUDA_TRY(cudaGetLastError());
-  }
+  if ((rc = tcb::launch_pairs_into(ctx, &seg, 1, src, n, m, partial, kNoAllocScratchBytes - fixed,
+                                   &nchunks)))
+    return rc;
   if (m > 0) {
     tcb::velocity_epilogue_kernel<<<(m + 255) / 256, 256, 0, ctx->stream>>>(
-        X, nullptr, m, i0, i1, 0, m, nchunks, partial, -2.0 * ctx->omega, dX,
+        X, perm, m, i0, i1, 0, m, nchunks, partial, -2.0 * ctx->omega, dX,
         target_class == TC_ACTIVE ? dVort : nullptr);
     TC_CUDA_TRY(cudaGetLastError());
+    ctx->launches += 1;
   }
   return TC_OK;
 }

@@ -42,7 +42,7 @@ struct PairVariant {
   const void* fn;
   void (*launch_batch)(int grid, cudaStream_t stream, const BatchLaunch& B);
   const void* fn_batch;
-  int form;  // FP32C: bit 3 source-paired form (with it: bit 0 integer-widened flush, bit 1 shared-memory accumulators, bit 2 hi/lo near offsets, bits 4-7 paired-reciprocal period, bits 8-9 log2 of flush lengths per flush in all-far tiles); without it: bit 0 far form, bit 1 paired reciprocal, bit 2 pre-weighted far sources. FP64: 0
+  int form;  // FP32C: bit 3 source-paired form (every variant), bit 1 shared-memory FP64 accumulators, bit 2 hi/lo near offsets, bits 8-9 log2 of flush lengths per flush in all-far tiles. FP64: 0
 };
 
 // Target segment as the host describes it before tiles are assigned.
@@ -96,7 +96,7 @@ struct tc_ctx {
   double delta[3] = {0.0, 0.0, 0.05};               // ACTIVE, VERTEX, PASSIVE (smooth, :27)
   tcb::PairCfg cfg64{256, 2, 256};
   tcb::PairCfg cfg32{256, 4, 256};
-  int var64 = 2, var32 = 68;  // pair-kernel variants in use (see kVariants64/32)
+  int var64 = 2, var32 = 0;  // pair-kernel variants in use (see kVariants64/32)
   bool auto32 = true;  // FP32C variant chosen per launch by problem size (tc_set_pair_variant turns it off)
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
@@ -128,6 +128,10 @@ namespace tcb {
 // Allocates ctx->partial and returns the number of source chunks in *nchunks.
 int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
                  int n_out, int* nchunks);
+// The same with the partial sums in caller-provided memory of partial_bytes bytes (at least one
+// chunk, 24 * n_out bytes); the chunk count is capped by what fits. Allocates nothing.
+int launch_pairs_into(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
+                      int n_out, double* partial, size_t partial_bytes, int* nchunks);
 // Pack {x, y, z, zeta*area} for n sources.
 int launch_pack_strat(tc_ctx* ctx, double t);
 int launch_strat_rel_vort(tc_ctx* ctx, const double* abs_vort, const double* x, int n, double t,
@@ -140,6 +144,11 @@ int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int 
                              int row_offset, int n_out, int nchunks, double* dX, double* dVort);
 // perm[i0..i1) <- i0..i1-1 sorted along the cube-face Hilbert curve (sphere_order.cuh)
 int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm);
+// The same in caller-provided scratch (keys in/out and indices: i1 - i0 entries each; temp:
+// order_sort_bytes(i1 - i0) bytes); allocates nothing.
+int order_sort_bytes(int n, size_t* bytes);
+int compute_order_into(tc_ctx* ctx, const double* x, int i0, int i1, int* perm, unsigned* k_in,
+                       unsigned* k_out, int* v_in, void* temp, size_t temp_bytes);
 // One RK4 stage epilogue over the three classes' ranges.
 // total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
 // stage 0; nchunks is what launch_pairs returned for this stage.
