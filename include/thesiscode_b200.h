@@ -284,9 +284,17 @@ int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int a1, int v0
                        int q1, double* total_ke_device);
 int tc_rk4_device_buffer(tc_ctx* ctx, int which, void** ptr);
 /* Copy rows [row0, row0+nrows) of an RK4 device buffer (TC_BUF_*) to
- * (to_buffer = 0) or from (to_buffer = 1) device memory at ptr, on the
- * context's stream: the exchange unit of a target-sharded run. */
+ * (to_buffer = 0) or from (to_buffer = 1) memory at ptr, device or host
+ * memory, on the context's stream (tc_synchronize before reading a host
+ * copy): the exchange unit of a target-sharded run. */
 int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr, int to_buffer);
+/* LoadBalance (PanelVelocityParallel.f90:167-213; the partition at :182-204):
+ * contiguous chunks of n / num_procs rows, the last rank takes the
+ * remainder; 0-based half-open [index_start[r], index_end[r]) per rank. */
+int tc_load_balance(int n, int num_procs, int* index_start, int* index_end);
+/* Number of visible CUDA devices (no counterpart: the reference runs on
+ * CPUs); a sharded run maps rank r to device r % count. */
+int tc_device_count(int* count);
 
 /* ---- pair-kernel variants (no counterpart in the reference) ------------ */
 /* Number of compiled launch shapes for a precision, and their parameters:

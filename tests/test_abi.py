@@ -75,3 +75,26 @@ def test_load_balance_host_mirror():
     assert list(s) == [0, 3, 6] and list(e) == [3, 6, 10]
     s, e = load_balance(2, 4)  # more ranks than rows: empty leading chunks
     assert list(e - s) == [0, 0, 0, 2]
+
+
+def test_c_load_balance_equals_oracle_partition():
+    """tc_load_balance (the C ABI a C/Fortran host shards with) against the oracle's restatement of
+    LoadBalance (PanelVelocityParallel.f90:182-204) and the Python mirror, including more ranks
+    than rows; bad arguments are refused without a GPU."""
+    from oracle import oracle as O
+    from thesiscode_b200.panel_velocity import load_balance
+
+    for n in (0, 1, 2, 7, 40962, 81920, 1310720):
+        for p in (1, 2, 3, 4, 8, 16):
+            s = (ctypes.c_int * p)()
+            e = (ctypes.c_int * p)()
+            N.call("tc_load_balance", n, p, s, e)
+            os_, oe = O.load_balance(n, p)
+            ps, pe = load_balance(n, p)
+            assert list(s) == list(os_) == list(ps) and list(e) == list(oe) == list(pe), (n, p)
+    s = (ctypes.c_int * 1)()
+    assert N.lib().tc_load_balance(5, 0, s, s) == N.TC_ERR_ARG
+    assert N.lib().tc_load_balance(-1, 1, s, s) == N.TC_ERR_ARG
+    c = ctypes.c_int(-1)
+    rc = N.lib().tc_device_count(ctypes.byref(c))
+    assert (rc == N.TC_OK and c.value >= 1) or (rc == N.TC_ERR_CUDA and c.value == 0)

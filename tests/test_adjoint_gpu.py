@@ -98,9 +98,11 @@ def jet(level):
     return configs.jet(level=level, delta=0.02, dt=0.005, steps=20)
 
 
-def test_adjoint_matches_torch_autograd_fp64(gpu):
-    # a Gaussian vortex: not zonally symmetric, so u_z != 0 and dJ/dx is not roundoff-sized
-    w = configs.gaussian(level=2, delta=0.02, dt=0.01)
+@pytest.mark.parametrize("level", [2, 3])
+def test_adjoint_matches_torch_autograd_fp64(gpu, level):
+    # a Gaussian vortex: not zonally symmetric, so u_z != 0 and dJ/dx is not roundoff-sized;
+    # level 3 (1,280 panels) is the largest the dense torch reference handles in seconds
+    w = configs.gaussian(level=level, delta=0.02, dt=0.01)
     ctx = Context(0, "fp64")
     ctx.set_omega(w.omega)
     ctx.set_deltas(*w.deltas)
@@ -143,13 +145,15 @@ def test_adjoint_probe_gradient_matches_torch_autograd_fp64(gpu):
     ctx.close()
 
 
-def test_adjoint_matches_centred_fd(gpu):
-    """32 seeded entries, eps = 1e-6, level 4 jet (delta 0.02), 20 steps, checkpoint every 5.
+@pytest.mark.parametrize("level", [4, 6])
+def test_adjoint_matches_centred_fd(gpu, level):
+    """32 seeded entries (seed 33), eps = 1e-6, jet (delta 0.02), 20 steps of dt 0.005, checkpoint
+    every 5; at level 6 (81,920 panels) this is the adjoint benchmark configuration itself.
     Error measure: |FD - adjoint| / max over all gradient entries <= 1e-6 (for J = sum zeta^2 A the
     position entries are RK4-truncation sized and FD resolves them only to ulp(J)/eps). The position
     adjoint is then checked by FD through the probe functional J = zeta_p(T), whose position
     gradient is O(1)."""
-    w = jet(4)
+    w = jet(level)
     ctx = Context(0, "fp64")
     ctx.set_omega(w.omega)
     ctx.set_deltas(*w.deltas)

@@ -1,0 +1,155 @@
+"""The benchmark configurations at their stated sizes, against the FP64 oracle.
+
+* Rossby-Haurwitz wave 4, icosahedral level 8 (1,310,720 panels + 655,362
+  vertices), delta 0.005: the velocity sums on 512 seeded rows per target
+  class, FP64 within 1e-12 and the default FP32C path within 1e-7.
+* Rossby-Haurwitz wave 4, level 4, FP64, delta 0: ten RK4 steps (dt 0.01)
+  through the fused step, against ten oracle BVERK4 steps at 1e-12.
+* The 64-instance Gaussian ensemble (seed 4, levels 3-6, beta in [4, 20]):
+  one RK4 step of the whole batch (FP32C, autotuned, CUDA graph), a seeded
+  subset of instances (one per level, the level-6 one included) against one
+  oracle BVERK4 step each, within the FP32C bound of its level.
+* The remesh cycle of the reference's drivers (RHWavePanelsMPI.f90:255-260:
+  AdaptiveRemesh changes N, then ResetRK4, PanelVelocityParallel.f90:321-429):
+  a level-5 grid stepped, the RK4 state reset, a level-6 grid loaded into the
+  same context and stepped, each against the oracle.
+
+Error measure: max |gpu - oracle| / max |oracle| for velocities, and the same
+for RK4 displacements x_new - x_old and vorticity changes.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from thesiscode_b200 import _native as N
+from thesiscode_b200 import configs
+from thesiscode_b200.batch import batch_info, batch_rk4
+from thesiscode_b200.panel_velocity import Context
+
+pytestmark = pytest.mark.gpu
+THREADS = os.cpu_count() or 1
+FP64_TOL = 1e-12
+# FP32C stated bounds by icosahedral level (the parity tests' table)
+FP32C_TOL = {3: 5e-7, 4: 3e-7, 5: 3e-7, 6: 2e-7, 7: 1e-7, 8: 1e-7}
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def rh4_l8():
+    return configs.rh4(level=8, delta=0.005, dt=0.01, steps=1)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32c", 1e-7)])
+def test_level8_velocity_sums_against_oracle(rh4_l8, prec, tol, gpu):
+    w = rh4_l8
+    rng = np.random.default_rng(85)
+    ra = np.sort(rng.choice(w.nA, 512, replace=False)).astype(np.int32)
+    rv = np.sort(rng.choice(w.nV, 512, replace=False)).astype(np.int32)
+    refA = O.rows(0, ra, None, w.xA, w.zetaA, w.areaA, delta=0.005, nthreads=THREADS)
+    refV = O.rows(1, rv, w.xV, w.xA, w.zetaA, w.areaA, delta=0.005, nthreads=THREADS)
+    ctx = Context(0, prec)
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    dA, vA = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    dV, _ = ctx.velocity(N.TC_VERTEX, w.xV, w.xA, w.zetaA, w.areaA)
+    ctx.close()
+    scale = max(np.abs(refA).max(), np.abs(refV).max())
+    err = max(np.abs(dA[ra] - refA).max(), np.abs(dV[rv] - refV).max()) / scale
+    assert err <= tol, err
+    # dVort = -2 Omega u_z on the sampled active rows
+    assert rel(vA[ra], -2.0 * w.omega * refA[:, 2]) <= tol
+
+
+def test_config1_rh4_level4_ten_fp64_steps(gpu):
+    w = configs.rh4(level=4, delta=0.0, dt=0.01, steps=10)
+    xV, xA, zA = w.xV, w.xA, w.zetaA
+    kes = []
+    for _ in range(w.steps):
+        xV, xA, zA, _, k, _, _ = O.bve_rk4(xV, xA, zA, w.areaA, np.zeros((0, 3)), w.dt, w.omega, w.deltas,
+                                          nthreads=THREADS)
+        kes.append(k)
+    ctx = Context(0, "fp64")
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    gxA, gz, gxV = w.xA.copy(), w.zetaA.copy(), w.xV.copy()
+    tke, _ = ctx.rk4_step(gxA, gz, w.areaA, gxV, np.zeros((0, 3)), w.dt, w.steps)
+    ctx.close()
+    assert rel(gxA - w.xA, xA - w.xA) <= FP64_TOL
+    assert rel(gxV - w.xV, xV - w.xV) <= FP64_TOL
+    assert rel(gz - w.zetaA, zA - w.zetaA) <= FP64_TOL
+    np.testing.assert_allclose(tke, kes, rtol=FP64_TOL)
+
+
+def test_config4_ensemble_one_step_against_oracle(gpu):
+    ws = configs.batched_gaussians(count=64, seed=4, levels=(3, 4, 5, 6))
+    ref = [w.copy() for w in ws]
+    ctx = Context(0, "fp32c")
+    ctx.set_omega(ws[0].omega)
+    ctx.set_deltas(*ws[0].deltas)
+    tke = batch_rk4(ctx, ws, ws[0].dt, 1)  # autotuned, captured in a CUDA graph
+    info = batch_info(ctx)
+    ctx.close()
+    assert info["variant"] >= 0 and info["work_items"] > 0
+    rng = np.random.default_rng(44)
+    picks = [int(rng.choice([b for b, w in enumerate(ref) if w.level == lv])) for lv in (3, 4, 5, 6)]
+    for b in picks:
+        r, w = ref[b], ws[b]
+        xV, xA, zA, _, k, _, _ = O.bve_rk4(r.xV, r.xA, r.zetaA, r.areaA, np.zeros((0, 3)), r.dt, r.omega,
+                                          r.deltas, nthreads=THREADS)
+        tol = FP32C_TOL[r.level]
+        assert rel(w.xA - r.xA, xA - r.xA) <= tol, (b, r.level)
+        assert rel(w.xV - r.xV, xV - r.xV) <= tol, (b, r.level)
+        assert rel(w.zetaA - r.zetaA, zA - r.zetaA) <= tol, (b, r.level)
+        assert abs(tke[0, b] - k) <= 2 * tol * abs(k), (b, r.level)
+
+
+def _oracle_step(w, nsteps=1):
+    xV, xA, zA, xQ = w.xV, w.xA, w.zetaA, w.xQ
+    for _ in range(nsteps):
+        xV, xA, zA, xQ, tke, _, _ = O.bve_rk4(xV, xA, zA, w.areaA, xQ, w.dt, w.omega, w.deltas,
+                                              nthreads=THREADS)
+    return xV, xA, zA, xQ, tke
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32c"])
+def test_remesh_cycle_reset_and_reload_larger_grid(prec, gpu):
+    """Level 5 (parity mode: three target classes) for two steps through load / advance / store,
+    tc_reset_rk4 (after which advancing without a new load is a state error), then level 6
+    (active panels only) loaded into the same context and stepped once."""
+    tol = FP64_TOL if prec == "fp64" else FP32C_TOL[5]
+    w5 = configs.rh4(level=5, parity=True, dt=0.01)
+    ctx = Context(0, prec)
+    ctx.set_omega(w5.omega)
+    ctx.set_deltas(*w5.deltas)
+    N.call("tc_rk4_load", ctx.handle, N.dptr(w5.xA), N.dptr(w5.zetaA), N.dptr(w5.areaA), w5.nA, N.dptr(w5.xV),
+           w5.nV, N.dptr(w5.xQ), w5.nQ, 0)
+    N.call("tc_rk4_advance", ctx.handle, w5.dt, 2, None)
+    xA, zA, xV, xQ = np.zeros_like(w5.xA), np.zeros_like(w5.zetaA), np.zeros_like(w5.xV), np.zeros_like(w5.xQ)
+    N.call("tc_rk4_store", ctx.handle, N.dptr(xA), N.dptr(zA), N.dptr(xV), N.dptr(xQ), None, 0)
+    rV, rA, rz, rQ, _ = _oracle_step(w5, 2)
+    assert rel(xA - w5.xA, rA - w5.xA) <= tol
+    assert rel(xV - w5.xV, rV - w5.xV) <= tol
+    assert rel(xQ - w5.xQ, rQ - w5.xQ) <= tol
+    assert rel(zA - w5.zetaA, rz - w5.zetaA) <= tol
+    # remesh: the particle count changes, the drivers call ResetRK4
+    ctx.reset_rk4()
+    with pytest.raises(N.TcError) as e:
+        N.call("tc_rk4_advance", ctx.handle, w5.dt, 1, None)
+    assert e.value.status == N.TC_ERR_STATE
+    w6 = configs.rh4(level=6, delta=0.0, dt=0.01)
+    w6.xV = np.zeros((0, 3))
+    tol6 = FP64_TOL if prec == "fp64" else FP32C_TOL[6]
+    N.call("tc_rk4_load", ctx.handle, N.dptr(w6.xA), N.dptr(w6.zetaA), N.dptr(w6.areaA), w6.nA, None, 0,
+           None, 0, 0)
+    N.call("tc_rk4_advance", ctx.handle, w6.dt, 1, None)
+    xA6, zA6 = np.zeros_like(w6.xA), np.zeros_like(w6.zetaA)
+    N.call("tc_rk4_store", ctx.handle, N.dptr(xA6), N.dptr(zA6), None, None, None, 0)
+    ctx.close()
+    _, rA6, rz6, _, _ = _oracle_step(w6, 1)
+    assert rel(xA6 - w6.xA, rA6 - w6.xA) <= tol6
+    assert rel(zA6 - w6.zetaA, rz6 - w6.zetaA) <= tol6

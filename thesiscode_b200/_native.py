@@ -94,6 +94,8 @@ SIGNATURES: dict[str, tuple] = {
                             c_int, c_int]),
     "tc_rk4_advance": (c_int, [c_void_p, c_double, c_int, dp]),
     "tc_rk4_store": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
+    "tc_load_balance": (c_int, [c_int, c_int, ip, ip]),
+    "tc_device_count": (c_int, [ip]),
     "tc_reset_rk4": (c_int, [c_void_p]),
     "tc_rk4_pack_sources": (c_int, [c_void_p]),
     "tc_rk4_stage_range": (c_int, [c_void_p, c_int, c_double, c_int, c_int, c_int, c_int, c_int, c_int,

@@ -635,7 +635,8 @@ extern "C" int tc_rk4_device_buffer(tc_ctx* ctx, int which, void** ptr) {
 }
 
 // Copy rows [row0, row0+nrows) of one RK4 device buffer to (to_buffer = 0)
-// or from (to_buffer = 1) device memory at `ptr`, on the context's stream.
+// or from (to_buffer = 1) memory at `ptr` - device memory or host memory
+// (unified addressing tells which) - on the context's stream.
 // Row sizes: TC_BUF_SOURCES 4 doubles, TC_BUF_XA/XV/XQ 3, TC_BUF_ZETA/KE 1.
 extern "C" int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, void* ptr,
                                 int to_buffer) {
@@ -661,8 +662,39 @@ extern "C" int tc_rk4_copy_rows(tc_ctx* ctx, int which, int row0, int nrows, voi
   if (nrows == 0) return TC_OK;
   char* b = static_cast<char*>(base) + (size_t)row0 * width * sizeof(double);
   size_t bytes = (size_t)nrows * width * sizeof(double);
-  TC_CUDA_TRY(cudaMemcpyAsync(to_buffer ? b : ptr, to_buffer ? ptr : b, bytes,
-                              cudaMemcpyDeviceToDevice, ctx->stream));
+  TC_CUDA_TRY(cudaMemcpyAsync(to_buffer ? b : ptr, to_buffer ? ptr : b, bytes, cudaMemcpyDefault,
+                              ctx->stream));
+  return TC_OK;
+}
+
+// LoadBalance (PanelVelocityParallel.f90:182-204): contiguous chunks of
+// n / num_procs rows, the last rank taking the remainder; 0-based half-open
+// [index_start[r], index_end[r]) for rank r.
+extern "C" int tc_load_balance(int n, int num_procs, int* index_start, int* index_end) {
+  if (n < 0 || num_procs < 1 || !index_start || !index_end) {
+    tc_record_error("tc_load_balance: bad arguments (n=%d, num_procs=%d)", n, num_procs);
+    return TC_ERR_ARG;
+  }
+  const int chunk = n / num_procs;
+  for (int r = 0; r < num_procs; ++r) {
+    index_start[r] = r * chunk;
+    index_end[r] = (r + 1) * chunk;
+  }
+  index_end[num_procs - 1] = n;
+  return TC_OK;
+}
+
+// Number of visible CUDA devices (ranks map to devices rank % count).
+extern "C" int tc_device_count(int* count) {
+  if (!count) return TC_ERR_ARG;
+  *count = 0;
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    *count = 0;
+    tc_record_error("cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    cudaGetLastError();
+    return TC_ERR_CUDA;
+  }
   return TC_OK;
 }
 
