@@ -241,8 +241,10 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // Form bits (FM): bit 3 always set (the source-paired form; the bit value
 // is part of the variant-info ABI); bit 1 keeps the FP64 accumulators in
 // shared memory (one slot per thread, target and coordinate: 6 fewer
-// registers per target); bit 2 gives near tiles hi/lo offsets; bits 8-9 hold
-// log2 FARK.
+// registers per target); bit 2 gives near tiles hi/lo offsets; bit 4 (PF)
+// copies the next source tile into shared memory with cp.async while the
+// current one is summed, so the per-tile conversion reads shared memory
+// instead of waiting on L2; bits 8-9 hold log2 FARK.
 // HILO (bit 2): near tiles take d = s - t from hi/lo FP32 splits of both
 // offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to FP32
 // (an absolute error of ulps of the patch radius, the dominant FP32C error
@@ -284,8 +286,9 @@ __device__ __forceinline__ float combine_max(const unsigned* red) {
   return __uint_as_float(m);
 }
 
-template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false>
+template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false, bool PF = false>
 struct SpSmem {
+  double4 raw[PF ? TS : 1];  // PF: the next tile's sources, copied in by cp.async
   float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
   float4 b[TS / 2];        // (sz_k, sz_k+1, A_k, A_k+1)
   float4 c[TS / 2];        // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
@@ -379,15 +382,44 @@ struct SpAcc {
   }
 };
 
+// Asynchronous global -> shared copies (cp.async, 16 bytes each), waited on
+// by the issuing thread (cp.async.wait_group): no barrier and no spin loop.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// PF: copy the sources of the tile at ts (those this thread converts: the
+// pairs jp = threadIdx.x + m * NT) into raw[], in flight while the current
+// tile is summed.
+template <int NT, int NP>
+__device__ __forceinline__ void prefetch_tile(const double4* __restrict__ src, int ts, int c1,
+                                              double4* raw) {
+  for (int jp = threadIdx.x; jp < NP; jp += NT) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = ts + 2 * jp + h;
+      if (k < c1) {
+        cp_async16(&raw[2 * jp + h], &src[k]);
+        cp_async16(reinterpret_cast<char*>(&raw[2 * jp + h]) + 16,
+                   reinterpret_cast<const char*>(&src[k]) + 16);
+      }
+    }
+  }
+  cp_async_commit();
+}
+
 // One work unit: targets at visiting positions [tile0, min(tile0 + NT*T,
 // i_end)) against sources [c0, c1); FP64 sums in the global frame written to
 // out[pos], out[stride + pos], out[2*stride + pos].
-template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK>
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool PF>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
-                                              SpSmem<NT, TS, T, SMACC, HILO>& sm) {
+                                              SpSmem<NT, TS, T, SMACC, HILO, PF>& sm) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(NT % 32 == 0, "whole warps");
   static_assert(TS % (FLUSH * FARK) == 0, "far-tile flush interval divides the tile");
@@ -486,9 +518,11 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
   }
   warp_store_max(rho2, sm.rho);
+  if (PF) prefetch_tile<NT, NP>(src, c0, c1, sm.raw);
 
   for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
+    if (PF) cp_async_wait_all();  // this thread's copies of the tile at ts
     float smin = __int_as_float(0x7f800000);  // +inf
     for (int jp = threadIdx.x; jp < NP; jp += NT) {
       float v[2][12];
@@ -503,7 +537,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         v[h][8] = 0.f;
         v[h][9] = v[h][10] = v[h][11] = 0.f;
         if (k < c1) {
-          const double4 q = src[k];
+          const double4 q = PF ? sm.raw[2 * jp + h] : src[k];
           const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
           const double sxd = frame_dot(fr, dx, dy, dz), syd = frame_dot(fr + 3, dx, dy, dz),
                        szd = frame_dot(fr + 6, dx, dy, dz);
@@ -537,6 +571,8 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
         sm.loz[jp] = make_float2(v[0][11], v[1][11]);
       }
     }
+    // the raw slots just read are this thread's own: refill them with the next tile
+    if (PF && ts + TS < c1) prefetch_tile<NT, NP>(src, ts + TS, c1, sm.raw);
     warp_store_min(smin, sm.tmin);
     __syncthreads();
     // Far test per flush segment when every warp staged exactly one segment
@@ -638,6 +674,7 @@ template <int FM>
 struct SpForm {
   static constexpr bool smacc = (FM & 2) != 0;
   static constexpr bool hilo = (FM & 4) != 0;
+  static constexpr bool pf = (FM & 16) != 0;
   static constexpr int fark = 1 << ((FM >> 8) & 3);
 };
 
@@ -650,10 +687,9 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
-  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(G.x, G.perm, tile0, G.i1,
-                                                                      G.d2, P.src, c0, c1, out,
-                                                                      stride, sm);
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf> sm;
+  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf>(
+      G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -700,12 +736,12 @@ template <int NT, int T, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
   using F = SpForm<FM>;
   __shared__ int slot;
-  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf> sm;
   for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
     const BatchItem I = B.items[it];
     const BatchSeg S = B.segs[I.seg];
     double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(
+    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf>(
         S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
   }
 }
