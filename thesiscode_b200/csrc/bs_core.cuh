@@ -244,7 +244,9 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // registers per target); bit 2 gives near tiles hi/lo offsets; bit 4 (PF)
 // copies the next source tile into shared memory with cp.async while the
 // current one is summed, so the per-tile conversion reads shared memory
-// instead of waiting on L2; bits 8-9 hold log2 FARK.
+// instead of waiting on L2; bit 5 (PP) keeps two converted tiles, so the
+// next tile is staged by each warp as soon as it has summed the current one
+// (one barrier per tile instead of two); bits 8-9 hold log2 FARK.
 // HILO (bit 2): near tiles take d = s - t from hi/lo FP32 splits of both
 // offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to FP32
 // (an absolute error of ulps of the patch radius, the dominant FP32C error
@@ -286,21 +288,23 @@ __device__ __forceinline__ float combine_max(const unsigned* red) {
   return __uint_as_float(m);
 }
 
-template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false, bool PF = false>
+template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false, bool PF = false,
+          bool PP = false>
 struct SpSmem {
+  static constexpr int NB = PP ? 2 : 1;  // PP: two source tiles, summed and staged in turn
   double4 raw[PF ? TS : 1];  // PF: the next tile's sources, copied in by cp.async
-  float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
-  float4 b[TS / 2];        // (sz_k, sz_k+1, A_k, A_k+1)
-  float4 c[TS / 2];        // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
-  float2 d[TS / 2];        // (G z'_k, G z'_k+1)
-  float4 n[TS / 2];        // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
-  double frame[12];        // e1, e2, e3 (rows), origin c
-  double csum[3][NT / 32]; // per-warp sums of the target positions
+  float4 a[NB][TS / 2];      // (sx_k, sx_k+1, sy_k, sy_k+1)
+  float4 b[NB][TS / 2];      // (sz_k, sz_k+1, A_k, A_k+1)
+  float4 c[NB][TS / 2];      // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
+  float2 d[NB][TS / 2];      // (G z'_k, G z'_k+1)
+  float4 n[NB][TS / 2];      // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
+  double frame[12];          // e1, e2, e3 (rows), origin c
+  double csum[3][NT / 32];   // per-warp sums of the target positions
   double acc[SMACC ? 3 * T * NT : 1];  // FP64 accumulators [c][t][thread] (SMACC)
-  float4 lo[HILO ? TS / 2 : 1];        // HILO: low parts (slx_k, slx_k+1, sly_k, sly_k+1)
-  float2 loz[HILO ? TS / 2 : 1];       // HILO: (slz_k, slz_k+1)
+  float4 lo[NB][HILO ? TS / 2 : 1];    // HILO: low parts (slx_k, slx_k+1, sly_k, sly_k+1)
+  float2 loz[NB][HILO ? TS / 2 : 1];   // HILO: (slz_k, slz_k+1)
   float tlo[HILO ? 3 * T * NT : 1];    // HILO: -(target low parts) [c][t][thread]
-  unsigned tmin[NT / 32];
+  unsigned tmin[NB][NT / 32];
   unsigned rho[NT / 32];
 };
 
@@ -411,22 +415,176 @@ __device__ __forceinline__ void prefetch_tile(const double4* __restrict__ src, i
   cp_async_commit();
 }
 
+// Converts the sources of the tile at ts into buffer `buf` of the CTA's
+// frame: offsets s_k, A_k = (|s_k|^2 + e_k)/2, G_k x'_k, e_k, 2G_k (and the
+// hi/lo low parts), padding past c1; records each warp's minimum |s_k|^2.
+template <int NT, int TS, bool HILO, bool PF, class Smem>
+__device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts, int c1,
+                                         const double* fr, Smem& sm, int buf) {
+  constexpr int NP = TS / 2;
+  if (PF) cp_async_wait_all();  // this thread's copies of the tile at ts
+  float smin = __int_as_float(0x7f800000);  // +inf
+  for (int jp = threadIdx.x; jp < NP; jp += NT) {
+    float v[2][12];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = ts + 2 * jp + h;
+      // padding sources: zero weight, unit denominators
+      v[h][0] = v[h][1] = v[h][2] = 0.f;
+      v[h][3] = 1.f;
+      v[h][4] = v[h][5] = v[h][6] = 0.f;
+      v[h][7] = 1.f;
+      v[h][8] = 0.f;
+      v[h][9] = v[h][10] = v[h][11] = 0.f;
+      if (k < c1) {
+        const double4 q = PF ? sm.raw[2 * jp + h] : src[k];
+        const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
+        const double sxd = frame_dot(fr, dx, dy, dz), syd = frame_dot(fr + 3, dx, dy, dz),
+                     szd = frame_dot(fr + 6, dx, dy, dz);
+        const float sx = (float)sxd, sy = (float)syd, sz = (float)szd;
+        if (HILO) {
+          v[h][9] = (float)(sxd - (double)sx);
+          v[h][10] = (float)(syd - (double)sy);
+          v[h][11] = (float)(szd - (double)sz);
+        }
+        const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
+        const float s2 = norm2_f32(sx, sy, sz);
+        smin = fminf(smin, s2);
+        v[h][0] = sx;
+        v[h][1] = sy;
+        v[h][2] = sz;
+        v[h][3] = (float)(0.5 * ((double)s2 + ek));
+        v[h][4] = (float)(q.w * frame_dot(fr, q.x, q.y, q.z));
+        v[h][5] = (float)(q.w * frame_dot(fr + 3, q.x, q.y, q.z));
+        v[h][6] = (float)(q.w * frame_dot(fr + 6, q.x, q.y, q.z));
+        v[h][7] = (float)ek;
+        v[h][8] = (float)(2.0 * q.w);
+      }
+    }
+    sm.a[buf][jp] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+    sm.b[buf][jp] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
+    sm.c[buf][jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
+    sm.d[buf][jp] = make_float2(v[0][6], v[1][6]);
+    sm.n[buf][jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
+    if (HILO) {
+      sm.lo[buf][jp] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
+      sm.loz[buf][jp] = make_float2(v[0][11], v[1][11]);
+    }
+  }
+  // the raw slots just read are this thread's own: refill them with the next tile
+  if (PF && ts + TS < c1) prefetch_tile<NT, NP>(src, ts + TS, c1, sm.raw);
+  warp_store_min(smin, sm.tmin[buf]);
+}
+
+// Sums one staged tile (buffer `buf`) into the thread's T targets: a tile whose
+// every source is far in one tight far loop flushed every FARK segments; else
+// per 64-source segment, far or near. With NT = TS/2 source pairs and FP = 32
+// every warp staged exactly one segment, so segment g's minimum |s|^2 is warp
+// g's and only the segments that hold near sources take the near form;
+// otherwise one far test for the whole tile.
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK,
+          class Smem>
+__device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&ntx)[T],
+                                       const float2 (&nty)[T], const float2 (&ntz)[T],
+                                       const float2 (&bh)[T], const float (&ei)[T],
+                                       float2 (&fx)[T], float2 (&fy)[T], float2 (&fz)[T],
+                                       SpAcc<NT, T, SMACC>& acc) {
+  constexpr int NP = TS / 2;
+  constexpr int FP = FLUSH / 2;
+  constexpr int FPF = FP * FARK;  // source pairs between flushes in all-far tiles
+  constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
+  const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
+  const bool tile_far = combine_min<NT / 32>(sm.tmin[buf]) > lim;
+  if (tile_far) {
+    for (int jf = 0; jf < NP; jf += FPF) {
+#pragma unroll UNROLL
+      for (int j = jf; j < jf + FPF; ++j)
+        sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], sm.d[buf][j], ntx, nty, ntz, bh,
+                       fx, fy, fz);
+#pragma unroll
+      for (int t = 0; t < T; ++t) {
+        acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
+        acc.add(1, t, (double)__fadd_rn(fy[t].x, fy[t].y));
+        acc.add(2, t, (double)__fadd_rn(fz[t].x, fz[t].y));
+        fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
+      }
+    }
+    return;
+  }
+  for (int jf = 0; jf < NP; jf += FP) {
+    const bool far = PERSEG && __uint_as_float(sm.tmin[buf][jf / FP]) > lim;
+    if (far) {
+#pragma unroll UNROLL
+      for (int j = jf; j < jf + FP; ++j)
+        sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], sm.d[buf][j], ntx, nty, ntz, bh,
+                       fx, fy, fz);
+    } else {
+      // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
+      float ntl[HILO ? 3 * T : 1];
+      if (HILO) {
+#pragma unroll
+        for (int k = 0; k < 3 * T; ++k) ntl[k] = sm.tlo[k * NT + threadIdx.x];
+      }
+#pragma unroll 4
+      for (int j = jf; j < jf + FP; ++j) {
+        const float4 a = sm.a[buf][j];
+        const float4 b = sm.b[buf][j];
+        const float4 n = sm.n[buf][j];
+        const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w);
+        const float2 sz = make_float2(b.x, b.y);
+        const float2 ee = make_float2(n.x, n.y), gg = make_float2(n.z, n.w);
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 loz = make_float2(0.f, 0.f);
+        if (HILO) {
+          lo = sm.lo[buf][j];
+          loz = sm.loz[buf][j];
+        }
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+          float2 dx = __fadd2_rn(sx, ntx[t]);
+          float2 dy = __fadd2_rn(sy, nty[t]);
+          float2 dz = __fadd2_rn(sz, ntz[t]);
+          if (HILO) {
+            dx = __fadd2_rn(dx, __fadd2_rn(make_float2(lo.x, lo.y), make_float2(ntl[t], ntl[t])));
+            dy = __fadd2_rn(dy, __fadd2_rn(make_float2(lo.z, lo.w), make_float2(ntl[T + t], ntl[T + t])));
+            dz = __fadd2_rn(dz, __fadd2_rn(loz, make_float2(ntl[2 * T + t], ntl[2 * T + t])));
+          }
+          float2 D = __fadd2_rn(ee, make_float2(ei[t], ei[t]));
+          D = __ffma2_rn(dx, dx, D);
+          D = __ffma2_rn(dy, dy, D);
+          D = __ffma2_rn(dz, dz, D);
+          const float2 w = __fmul2_rn(gg, rcp2(D));
+          fx[t] = __ffma2_rn(w, dx, fx[t]);
+          fy[t] = __ffma2_rn(w, dy, fy[t]);
+          fz[t] = __ffma2_rn(w, dz, fz[t]);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
+      acc.add(1, t, (double)__fadd_rn(fy[t].x, fy[t].y));
+      acc.add(2, t, (double)__fadd_rn(fz[t].x, fz[t].y));
+      fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
 // One work unit: targets at visiting positions [tile0, min(tile0 + NT*T,
 // i_end)) against sources [c0, c1); FP64 sums in the global frame written to
 // out[pos], out[stride + pos], out[2*stride + pos].
-template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool PF>
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool PF,
+          bool PP>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
-                                              SpSmem<NT, TS, T, SMACC, HILO, PF>& sm) {
+                                              SpSmem<NT, TS, T, SMACC, HILO, PF, PP>& sm) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(NT % 32 == 0, "whole warps");
   static_assert(TS % (FLUSH * FARK) == 0, "far-tile flush interval divides the tile");
   constexpr int TB = NT * T;
   constexpr int NP = TS / 2;
-  constexpr int FP = FLUSH / 2;
-  constexpr int FPF = FP * FARK;  // source pairs between flushes in all-far tiles
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
   const int mid = perm ? perm[mid_pos] : mid_pos;
@@ -520,140 +678,27 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   warp_store_max(rho2, sm.rho);
   if (PF) prefetch_tile<NT, NP>(src, c0, c1, sm.raw);
 
-  for (int ts = c0; ts < c1; ts += TS) {
+  if (PP) {
+    // two tile buffers: a warp that has summed tile k stages tile k+1 into the
+    // other buffer while slower warps still sum tile k; one barrier per tile
+    // (every warp has left buffer b before anyone stages into it again)
+    int buf = 0;
+    if (c0 < c1) sp_stage<NT, TS, HILO, PF>(src, c0, c1, fr, sm, 0);
     __syncthreads();
-    if (PF) cp_async_wait_all();  // this thread's copies of the tile at ts
-    float smin = __int_as_float(0x7f800000);  // +inf
-    for (int jp = threadIdx.x; jp < NP; jp += NT) {
-      float v[2][12];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int k = ts + 2 * jp + h;
-        // padding sources: zero weight, unit denominators
-        v[h][0] = v[h][1] = v[h][2] = 0.f;
-        v[h][3] = 1.f;
-        v[h][4] = v[h][5] = v[h][6] = 0.f;
-        v[h][7] = 1.f;
-        v[h][8] = 0.f;
-        v[h][9] = v[h][10] = v[h][11] = 0.f;
-        if (k < c1) {
-          const double4 q = PF ? sm.raw[2 * jp + h] : src[k];
-          const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
-          const double sxd = frame_dot(fr, dx, dy, dz), syd = frame_dot(fr + 3, dx, dy, dz),
-                       szd = frame_dot(fr + 6, dx, dy, dz);
-          const float sx = (float)sxd, sy = (float)syd, sz = (float)szd;
-          if (HILO) {
-            v[h][9] = (float)(sxd - (double)sx);
-            v[h][10] = (float)(syd - (double)sy);
-            v[h][11] = (float)(szd - (double)sz);
-          }
-          const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
-          const float s2 = norm2_f32(sx, sy, sz);
-          smin = fminf(smin, s2);
-          v[h][0] = sx;
-          v[h][1] = sy;
-          v[h][2] = sz;
-          v[h][3] = (float)(0.5 * ((double)s2 + ek));
-          v[h][4] = (float)(q.w * frame_dot(fr, q.x, q.y, q.z));
-          v[h][5] = (float)(q.w * frame_dot(fr + 3, q.x, q.y, q.z));
-          v[h][6] = (float)(q.w * frame_dot(fr + 6, q.x, q.y, q.z));
-          v[h][7] = (float)ek;
-          v[h][8] = (float)(2.0 * q.w);
-        }
-      }
-      sm.a[jp] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
-      sm.b[jp] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
-      sm.c[jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
-      sm.d[jp] = make_float2(v[0][6], v[1][6]);
-      sm.n[jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
-      if (HILO) {
-        sm.lo[jp] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
-        sm.loz[jp] = make_float2(v[0][11], v[1][11]);
-      }
+    for (int ts = c0; ts < c1; ts += TS) {
+      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, buf, ntx, nty, ntz, bh, ei, fx, fy,
+                                                          fz, acc);
+      if (ts + TS < c1) sp_stage<NT, TS, HILO, PF>(src, ts + TS, c1, fr, sm, buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
     }
-    // the raw slots just read are this thread's own: refill them with the next tile
-    if (PF && ts + TS < c1) prefetch_tile<NT, NP>(src, ts + TS, c1, sm.raw);
-    warp_store_min(smin, sm.tmin);
-    __syncthreads();
-    // Far test per flush segment when every warp staged exactly one segment
-    // (NT = TS/2 source pairs, FP = 32): segment g's minimum |s|^2 is warp
-    // g's, so only the segments that hold near sources take the near form.
-    // Otherwise one test for the whole tile.
-    // A tile whose every segment is far runs one tight far loop, flushed
-    // every FARK segments.
-    constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
-    const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
-    const bool tile_far = combine_min<NT / 32>(sm.tmin) > lim;
-    if (tile_far) {
-      for (int jf = 0; jf < NP; jf += FPF) {
-#pragma unroll UNROLL
-        for (int j = jf; j < jf + FPF; ++j)
-          sp_far_step<T>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
-#pragma unroll
-        for (int t = 0; t < T; ++t) {
-          acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
-          acc.add(1, t, (double)__fadd_rn(fy[t].x, fy[t].y));
-          acc.add(2, t, (double)__fadd_rn(fz[t].x, fz[t].y));
-          fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
-        }
-      }
-      continue;
-    }
-    for (int jf = 0; jf < NP; jf += FP) {
-      const bool far = PERSEG && __uint_as_float(sm.tmin[jf / FP]) > lim;
-      if (far) {
-#pragma unroll UNROLL
-        for (int j = jf; j < jf + FP; ++j)
-          sp_far_step<T>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
-      } else {
-        // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
-        float ntl[HILO ? 3 * T : 1];
-        if (HILO) {
-#pragma unroll
-          for (int k = 0; k < 3 * T; ++k) ntl[k] = sm.tlo[k * NT + threadIdx.x];
-        }
-#pragma unroll 4
-        for (int j = jf; j < jf + FP; ++j) {
-          const float4 a = sm.a[j];
-          const float4 b = sm.b[j];
-          const float4 n = sm.n[j];
-          const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w);
-          const float2 sz = make_float2(b.x, b.y);
-          const float2 ee = make_float2(n.x, n.y), gg = make_float2(n.z, n.w);
-          float4 lo = make_float4(0.f, 0.f, 0.f, 0.f);
-          float2 loz = make_float2(0.f, 0.f);
-          if (HILO) {
-            lo = sm.lo[j];
-            loz = sm.loz[j];
-          }
-#pragma unroll
-          for (int t = 0; t < T; ++t) {
-            float2 dx = __fadd2_rn(sx, ntx[t]);
-            float2 dy = __fadd2_rn(sy, nty[t]);
-            float2 dz = __fadd2_rn(sz, ntz[t]);
-            if (HILO) {
-              dx = __fadd2_rn(dx, __fadd2_rn(make_float2(lo.x, lo.y), make_float2(ntl[t], ntl[t])));
-              dy = __fadd2_rn(dy, __fadd2_rn(make_float2(lo.z, lo.w), make_float2(ntl[T + t], ntl[T + t])));
-              dz = __fadd2_rn(dz, __fadd2_rn(loz, make_float2(ntl[2 * T + t], ntl[2 * T + t])));
-            }
-            float2 D = __fadd2_rn(ee, make_float2(ei[t], ei[t]));
-            D = __ffma2_rn(dx, dx, D);
-            D = __ffma2_rn(dy, dy, D);
-            D = __ffma2_rn(dz, dz, D);
-            const float2 w = __fmul2_rn(gg, rcp2(D));
-            fx[t] = __ffma2_rn(w, dx, fx[t]);
-            fy[t] = __ffma2_rn(w, dy, fy[t]);
-            fz[t] = __ffma2_rn(w, dz, fz[t]);
-          }
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < T; ++t) {
-        acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
-        acc.add(1, t, (double)__fadd_rn(fy[t].x, fy[t].y));
-        acc.add(2, t, (double)__fadd_rn(fz[t].x, fz[t].y));
-        fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
-      }
+  } else {
+    for (int ts = c0; ts < c1; ts += TS) {
+      __syncthreads();
+      sp_stage<NT, TS, HILO, PF>(src, ts, c1, fr, sm, 0);
+      __syncthreads();
+      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, 0, ntx, nty, ntz, bh, ei, fx, fy, fz,
+                                                          acc);
     }
   }
   // back to the global frame: T = R^T T'
@@ -675,6 +720,7 @@ struct SpForm {
   static constexpr bool smacc = (FM & 2) != 0;
   static constexpr bool hilo = (FM & 4) != 0;
   static constexpr bool pf = (FM & 16) != 0;
+  static constexpr bool pp = (FM & 32) != 0;
   static constexpr int fark = 1 << ((FM >> 8) & 3);
 };
 
@@ -687,8 +733,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf> sm;
-  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf>(
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf, F::pp> sm;
+  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp>(
       G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
 }
 
@@ -736,12 +782,12 @@ template <int NT, int T, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
   using F = SpForm<FM>;
   __shared__ int slot;
-  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf> sm;
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf, F::pp> sm;
   for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
     const BatchItem I = B.items[it];
     const BatchSeg S = B.segs[I.seg];
     double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf>(
+    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp>(
         S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
   }
 }
