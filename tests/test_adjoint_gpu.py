@@ -7,6 +7,8 @@ step, on seeded entries: vorticities and tangent-plane position
 perturbations (renormalised to the sphere). The adjoint is wrapped in a
 torch.autograd.Function here, in the test harness only.
 """
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -150,7 +152,8 @@ def test_adjoint_matches_centred_fd(gpu, level):
     """32 seeded entries (seed 33), eps = 1e-6, jet (delta 0.02), 20 steps of dt 0.005, checkpoint
     every 5; at level 6 (81,920 panels) this is the adjoint benchmark configuration itself.
     Error measure: |FD - adjoint| / max over all gradient entries <= 1e-6 (for J = sum zeta^2 A the
-    position entries are RK4-truncation sized and FD resolves them only to ulp(J)/eps). The position
+    position entries are RK4-truncation sized; J(+) - J(-) is summed termwise with exact rounding, so
+    the FD's own rounding noise stays well below the bound). The position
     adjoint is then checked by FD through the probe functional J = zeta_p(T), whose position
     gradient is O(1)."""
     w = jet(level)
@@ -166,7 +169,13 @@ def test_adjoint_matches_centred_fd(gpu, level):
         return z
 
     def J_of(x, z):
-        return float(np.sum(final(x, z) ** 2 * w.areaA))
+        return math.fsum(final(x, z) ** 2 * w.areaA)
+
+    def J_diff(xp, zp, xm, zm):
+        # J(+) - J(-) as one exactly rounded sum of the termwise differences: rounding J ~ 12
+        # (level 6) itself would leave ulp(J) / (2 eps) ~ 1e-9 of noise, near the bound
+        fp, fm = final(xp, zp), final(xm, zm)
+        return math.fsum((fp - fm) * (fp + fm) * w.areaA)
 
     def tangent_pair(j, t):
         xp, xm = w.xA.copy(), w.xA.copy()
@@ -188,12 +197,12 @@ def test_adjoint_matches_centred_fd(gpu, level):
             zp, zm = w.zetaA.copy(), w.zetaA.copy()
             zp[j] += eps
             zm[j] -= eps
-            fd = (J_of(w.xA, zp) - J_of(w.xA, zm)) / (2 * eps)
+            fd = J_diff(w.xA, zp, w.xA, zm) / (2 * eps)
             assert abs(fd - gz[j]) <= 1e-6 * scale, (j, fd, gz[j])
         else:  # position entry along a tangent direction, renormalised
             t = tangent(rng, j)
             xp, xm = tangent_pair(j, t)
-            fd = (J_of(xp, w.zetaA) - J_of(xm, w.zetaA)) / (2 * eps)
+            fd = J_diff(xp, w.zetaA, xm, w.zetaA) / (2 * eps)
             assert abs(fd - gx[j].dot(t)) <= 1e-6 * scale, (j, fd, gx[j].dot(t))
     # position adjoint through the probe functional
     p = int(picks[0])
