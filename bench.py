@@ -475,7 +475,7 @@ def time_side_workload(name, device, no_cpu, steps=3):
     return out
 
 
-def time_config1(device, reps=5):
+def time_config1(device, check=True, reps=5):
     """Config 1: Rossby-Haurwitz wave 4, level 4 (5,120 panels + 2,562 vertices), FP64, delta 0,
     ten RK4 steps of dt 0.01 per call, device-resident (tc_rk4_load once, tc_rk4_advance(10) timed
     by CUDA events, best of `reps`), and the displacement error of the ten steps against ten
@@ -505,14 +505,17 @@ def time_config1(device, reps=5):
     xA, xV = np.zeros_like(w.xA), np.zeros_like(w.xV)
     N.call("tc_rk4_store", ctx.handle, N.dptr(xA), None, N.dptr(xV), None, None, 0)
     ctx.close()
-    rV, rA, rz = w.xV, w.xA, w.zetaA
-    for _ in range(w.steps):
-        rV, rA, rz, *_ = O.bve_rk4(rV, rA, rz, w.areaA, np.zeros((0, 3)), w.dt, w.omega, w.deltas,
-                                   nthreads=os.cpu_count() or 1)
-    err = max(np.abs(xA - rA).max() / np.abs(rA - w.xA).max(), np.abs(xV - rV).max() / np.abs(rV - w.xV).max())
-    return {"workload": f"{w.name}: {w.meta['ic']}, FP64, delta 0, {w.steps} RK4 steps of dt {w.dt}",
-            "value": w.interactions_per_step() * w.steps / (best * 1e-3), "unit": "interactions/s",
-            "ms_per_step": best / w.steps, "displacement_error_vs_fp64_oracle": float(err)}
+    out = {"workload": f"{w.name}: {w.meta['ic']}, FP64, delta 0, {w.steps} RK4 steps of dt {w.dt}",
+           "value": w.interactions_per_step() * w.steps / (best * 1e-3), "unit": "interactions/s",
+           "ms_per_step": best / w.steps}
+    if check:
+        rV, rA, rz = w.xV, w.xA, w.zetaA
+        for _ in range(w.steps):
+            rV, rA, rz, *_ = O.bve_rk4(rV, rA, rz, w.areaA, np.zeros((0, 3)), w.dt, w.omega, w.deltas,
+                                       nthreads=os.cpu_count() or 1)
+        out["displacement_error_vs_fp64_oracle"] = float(max(
+            np.abs(xA - rA).max() / np.abs(rA - w.xA).max(), np.abs(xV - rV).max() / np.abs(rV - w.xV).max()))
+    return out
 
 
 def run_ours(args):
@@ -600,7 +603,7 @@ def run_ours(args):
         if world == 1 and not args.quick:
             line["adjoint"] = time_adjoint(device)
             line["batched"] = time_batch(device)
-            line["rh4_l4_fp64"] = time_config1(device)
+            line["rh4_l4_fp64"] = time_config1(device, check=not args.no_cpu)
             if args.config != "gaussian_l7":
                 line["gaussian_l7"] = time_side_workload("gaussian_l7", device, args.no_cpu)
         if world == 1 and not args.no_cpu:
