@@ -246,7 +246,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // current one is summed, so the per-tile conversion reads shared memory
 // instead of waiting on L2; bit 5 (PP) keeps two converted tiles, so the
 // next tile is staged by each warp as soon as it has summed the current one
-// (one barrier per tile instead of two); bits 8-9 hold log2 FARK.
+// (one barrier per tile instead of two); bit 6 (MD) loads the z-weights of two
+// source pairs at once in far loops; bits 8-9 hold log2 FARK.
 // HILO (bit 2): near tiles take d = s - t from hi/lo FP32 splits of both
 // offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to FP32
 // (an absolute error of ulps of the patch radius, the dominant FP32C error
@@ -296,7 +297,7 @@ struct SpSmem {
   float4 a[NB][TS / 2];      // (sx_k, sx_k+1, sy_k, sy_k+1)
   float4 b[NB][TS / 2];      // (sz_k, sz_k+1, A_k, A_k+1)
   float4 c[NB][TS / 2];      // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
-  float2 d[NB][TS / 2];      // (G z'_k, G z'_k+1)
+  alignas(16) float2 d[NB][TS / 2];  // (G z'_k, G z'_k+1); MD reads two pairs as one float4
   float4 n[NB][TS / 2];      // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
   double frame[12];          // e1, e2, e3 (rows), origin c
   double csum[3][NT / 32];   // per-warp sums of the target positions
@@ -476,13 +477,39 @@ __device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts
   warp_store_min(smin, sm.tmin[buf]);
 }
 
+// Far source pairs [j0, j1) of buffer `buf` against the thread's targets. MD:
+// the z-weights of two consecutive pairs come from one 128-bit shared load
+// (3.5 loads per source pair instead of 4, on the MIO queue the reciprocals
+// also use); j0 and j1 are even.
+template <int T, int UNROLL, bool MD, class Smem>
+__device__ __forceinline__ void sp_far_run(const Smem& sm, int buf, int j0, int j1,
+                                           const float2 (&ntx)[T], const float2 (&nty)[T],
+                                           const float2 (&ntz)[T], const float2 (&bh)[T],
+                                           float2 (&fx)[T], float2 (&fy)[T], float2 (&fz)[T]) {
+  if (MD) {
+#pragma unroll(UNROLL > 1 ? UNROLL / 2 : 1)
+    for (int j = j0; j < j1; j += 2) {
+      const float4 dd = *reinterpret_cast<const float4*>(&sm.d[buf][j]);
+      sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], make_float2(dd.x, dd.y), ntx, nty,
+                     ntz, bh, fx, fy, fz);
+      sp_far_step<T>(sm.a[buf][j + 1], sm.b[buf][j + 1], sm.c[buf][j + 1], make_float2(dd.z, dd.w),
+                     ntx, nty, ntz, bh, fx, fy, fz);
+    }
+  } else {
+#pragma unroll UNROLL
+    for (int j = j0; j < j1; ++j)
+      sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], sm.d[buf][j], ntx, nty, ntz, bh, fx,
+                     fy, fz);
+  }
+}
+
 // Sums one staged tile (buffer `buf`) into the thread's T targets: a tile whose
 // every source is far in one tight far loop flushed every FARK segments; else
 // per 64-source segment, far or near. With NT = TS/2 source pairs and FP = 32
 // every warp staged exactly one segment, so segment g's minimum |s|^2 is warp
 // g's and only the segments that hold near sources take the near form;
 // otherwise one far test for the whole tile.
-template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK,
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool MD,
           class Smem>
 __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&ntx)[T],
                                        const float2 (&nty)[T], const float2 (&ntz)[T],
@@ -497,10 +524,7 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
   const bool tile_far = combine_min<NT / 32>(sm.tmin[buf]) > lim;
   if (tile_far) {
     for (int jf = 0; jf < NP; jf += FPF) {
-#pragma unroll UNROLL
-      for (int j = jf; j < jf + FPF; ++j)
-        sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], sm.d[buf][j], ntx, nty, ntz, bh,
-                       fx, fy, fz);
+      sp_far_run<T, UNROLL, MD>(sm, buf, jf, jf + FPF, ntx, nty, ntz, bh, fx, fy, fz);
 #pragma unroll
       for (int t = 0; t < T; ++t) {
         acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
@@ -514,10 +538,7 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
   for (int jf = 0; jf < NP; jf += FP) {
     const bool far = PERSEG && __uint_as_float(sm.tmin[buf][jf / FP]) > lim;
     if (far) {
-#pragma unroll UNROLL
-      for (int j = jf; j < jf + FP; ++j)
-        sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], sm.d[buf][j], ntx, nty, ntz, bh,
-                       fx, fy, fz);
+      sp_far_run<T, UNROLL, MD>(sm, buf, jf, jf + FP, ntx, nty, ntz, bh, fx, fy, fz);
     } else {
       // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
       float ntl[HILO ? 3 * T : 1];
@@ -574,7 +595,7 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
 // i_end)) against sources [c0, c1); FP64 sums in the global frame written to
 // out[pos], out[stride + pos], out[2*stride + pos].
 template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool PF,
-          bool PP>
+          bool PP, bool MD>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
@@ -686,8 +707,8 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     if (c0 < c1) sp_stage<NT, TS, HILO, PF>(src, c0, c1, fr, sm, 0);
     __syncthreads();
     for (int ts = c0; ts < c1; ts += TS) {
-      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, buf, ntx, nty, ntz, bh, ei, fx, fy,
-                                                          fz, acc);
+      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK, MD>(sm, buf, ntx, nty, ntz, bh, ei, fx, fy,
+                                                              fz, acc);
       if (ts + TS < c1) sp_stage<NT, TS, HILO, PF>(src, ts + TS, c1, fr, sm, buf ^ 1);
       __syncthreads();
       buf ^= 1;
@@ -697,8 +718,8 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
       __syncthreads();
       sp_stage<NT, TS, HILO, PF>(src, ts, c1, fr, sm, 0);
       __syncthreads();
-      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, 0, ntx, nty, ntz, bh, ei, fx, fy, fz,
-                                                          acc);
+      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK, MD>(sm, 0, ntx, nty, ntz, bh, ei, fx, fy,
+                                                              fz, acc);
     }
   }
   // back to the global frame: T = R^T T'
@@ -721,6 +742,7 @@ struct SpForm {
   static constexpr bool hilo = (FM & 4) != 0;
   static constexpr bool pf = (FM & 16) != 0;
   static constexpr bool pp = (FM & 32) != 0;
+  static constexpr bool md = (FM & 64) != 0;
   static constexpr int fark = 1 << ((FM >> 8) & 3);
 };
 
@@ -734,7 +756,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
   __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf, F::pp> sm;
-  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp>(
+  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp, F::md>(
       G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
 }
 
@@ -787,7 +809,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchL
     const BatchItem I = B.items[it];
     const BatchSeg S = B.segs[I.seg];
     double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp>(
+    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp, F::md>(
         S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
   }
 }
