@@ -48,7 +48,7 @@ ERROR_ROWS_MAX = 24576  # rows of the strict-oracle error sample (a seeded subse
 # DRAM bytes (read + write) of one FP32C pair launch (the stage-1 launch of one RK4 step, every
 # target class against all sources), from ncu captures (dram__bytes_read.sum +
 # dram__bytes_write.sum) summarised in profiles/
-PAIR_FP32C_DRAM_BYTES = {"gaussian_l7": 28.02e6 + 52.43e6}
+PAIR_FP32C_DRAM_BYTES = {"rh4_l8": 328.61e6 + 204.19e6, "gaussian_l7": 28.02e6 + 52.43e6}
 
 
 def build_workload(name: str, grid_source=None):
