@@ -303,11 +303,8 @@ int tc_device_count(int* count);
  * targets/CTA, form}. FP32C form: bit 3 = source-paired kernel (set in every
  * variant: the two lanes of each f32x2 instruction carry two sources of one
  * target), bit 1 = FP64 accumulators in shared memory, bit 2 = hi/lo
- * near-pair offsets (the accurate variants), bit 4 = next source tile
- * prefetched with cp.async, bit 5 = two source-tile buffers (one barrier per
- * tile), bit 6 = paired z-weight loads in far loops, bits 8-9 = log2 of the
- * flush lengths between flushes in tiles whose every source is far. FP64
- * form: 0. */
+ * near-pair offsets (the accurate variants), bits 8-9 = log2 of the flush
+ * lengths between flushes in tiles whose every source is far. FP64 form: 0. */
 int tc_pair_variant_count(int precision, int* count);
 int tc_pair_variant_info(int precision, int id, int* info8);
 /* Select a variant. For FP32C the default is chosen per launch by problem

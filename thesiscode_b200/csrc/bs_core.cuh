@@ -241,13 +241,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // Form bits (FM): bit 3 always set (the source-paired form; the bit value
 // is part of the variant-info ABI); bit 1 keeps the FP64 accumulators in
 // shared memory (one slot per thread, target and coordinate: 6 fewer
-// registers per target); bit 2 gives near tiles hi/lo offsets; bit 4 (PF)
-// copies the next source tile into shared memory with cp.async while the
-// current one is summed, so the per-tile conversion reads shared memory
-// instead of waiting on L2; bit 5 (PP) keeps two converted tiles, so the
-// next tile is staged by each warp as soon as it has summed the current one
-// (one barrier per tile instead of two); bit 6 (MD) loads the z-weights of two
-// source pairs at once in far loops; bits 8-9 hold log2 FARK.
+// registers per target); bit 2 gives near tiles hi/lo offsets; bits 8-9 hold
+// log2 FARK.
 // HILO (bit 2): near tiles take d = s - t from hi/lo FP32 splits of both
 // offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to FP32
 // (an absolute error of ulps of the patch radius, the dominant FP32C error
@@ -289,23 +284,20 @@ __device__ __forceinline__ float combine_max(const unsigned* red) {
   return __uint_as_float(m);
 }
 
-template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false, bool PF = false,
-          bool PP = false>
+template <int NT, int TS, int T = 1, bool SMACC = false, bool HILO = false>
 struct SpSmem {
-  static constexpr int NB = PP ? 2 : 1;  // PP: two source tiles, summed and staged in turn
-  double4 raw[PF ? TS : 1];  // PF: the next tile's sources, copied in by cp.async
-  float4 a[NB][TS / 2];      // (sx_k, sx_k+1, sy_k, sy_k+1)
-  float4 b[NB][TS / 2];      // (sz_k, sz_k+1, A_k, A_k+1)
-  float4 c[NB][TS / 2];      // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
-  alignas(16) float2 d[NB][TS / 2];  // (G z'_k, G z'_k+1); MD reads two pairs as one float4
-  float4 n[NB][TS / 2];      // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
-  double frame[12];          // e1, e2, e3 (rows), origin c
-  double csum[3][NT / 32];   // per-warp sums of the target positions
+  float4 a[TS / 2];        // (sx_k, sx_k+1, sy_k, sy_k+1)
+  float4 b[TS / 2];        // (sz_k, sz_k+1, A_k, A_k+1)
+  float4 c[TS / 2];        // (G x'_k, G x'_k+1, G y'_k, G y'_k+1)
+  float2 d[TS / 2];        // (G z'_k, G z'_k+1)
+  float4 n[TS / 2];        // near form: (e_k, e_k+1, 2G_k, 2G_k+1)
+  double frame[12];        // e1, e2, e3 (rows), origin c
+  double csum[3][NT / 32]; // per-warp sums of the target positions
   double acc[SMACC ? 3 * T * NT : 1];  // FP64 accumulators [c][t][thread] (SMACC)
-  float4 lo[NB][HILO ? TS / 2 : 1];    // HILO: low parts (slx_k, slx_k+1, sly_k, sly_k+1)
-  float2 loz[NB][HILO ? TS / 2 : 1];   // HILO: (slz_k, slz_k+1)
+  float4 lo[HILO ? TS / 2 : 1];        // HILO: low parts (slx_k, slx_k+1, sly_k, sly_k+1)
+  float2 loz[HILO ? TS / 2 : 1];       // HILO: (slz_k, slz_k+1)
   float tlo[HILO ? 3 * T * NT : 1];    // HILO: -(target low parts) [c][t][thread]
-  unsigned tmin[NB][NT / 32];
+  unsigned tmin[NT / 32];
   unsigned rho[NT / 32];
 };
 
@@ -387,43 +379,13 @@ struct SpAcc {
   }
 };
 
-// Asynchronous global -> shared copies (cp.async, 16 bytes each), waited on
-// by the issuing thread (cp.async.wait_group): no barrier and no spin loop.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// PF: copy the sources of the tile at ts (those this thread converts: the
-// pairs jp = threadIdx.x + m * NT) into raw[], in flight while the current
-// tile is summed.
-template <int NT, int NP>
-__device__ __forceinline__ void prefetch_tile(const double4* __restrict__ src, int ts, int c1,
-                                              double4* raw) {
-  for (int jp = threadIdx.x; jp < NP; jp += NT) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int k = ts + 2 * jp + h;
-      if (k < c1) {
-        cp_async16(&raw[2 * jp + h], &src[k]);
-        cp_async16(reinterpret_cast<char*>(&raw[2 * jp + h]) + 16,
-                   reinterpret_cast<const char*>(&src[k]) + 16);
-      }
-    }
-  }
-  cp_async_commit();
-}
-
-// Converts the sources of the tile at ts into buffer `buf` of the CTA's
-// frame: offsets s_k, A_k = (|s_k|^2 + e_k)/2, G_k x'_k, e_k, 2G_k (and the
-// hi/lo low parts), padding past c1; records each warp's minimum |s_k|^2.
-template <int NT, int TS, bool HILO, bool PF, class Smem>
+// Converts the sources of the tile at ts into the CTA's frame: offsets s_k,
+// A_k = (|s_k|^2 + e_k)/2, G_k x'_k, e_k, 2G_k (and the hi/lo low parts),
+// padding past c1; records each warp's minimum |s_k|^2.
+template <int NT, int TS, bool HILO, class Smem>
 __device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts, int c1,
-                                         const double* fr, Smem& sm, int buf) {
+                                         const double* fr, Smem& sm) {
   constexpr int NP = TS / 2;
-  if (PF) cp_async_wait_all();  // this thread's copies of the tile at ts
   float smin = __int_as_float(0x7f800000);  // +inf
   for (int jp = threadIdx.x; jp < NP; jp += NT) {
     float v[2][12];
@@ -438,7 +400,7 @@ __device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts
       v[h][8] = 0.f;
       v[h][9] = v[h][10] = v[h][11] = 0.f;
       if (k < c1) {
-        const double4 q = PF ? sm.raw[2 * jp + h] : src[k];
+        const double4 q = src[k];
         const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
         const double sxd = frame_dot(fr, dx, dy, dz), syd = frame_dot(fr + 3, dx, dy, dz),
                      szd = frame_dot(fr + 6, dx, dy, dz);
@@ -462,56 +424,38 @@ __device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts
         v[h][8] = (float)(2.0 * q.w);
       }
     }
-    sm.a[buf][jp] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
-    sm.b[buf][jp] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
-    sm.c[buf][jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
-    sm.d[buf][jp] = make_float2(v[0][6], v[1][6]);
-    sm.n[buf][jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
+    sm.a[jp] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+    sm.b[jp] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
+    sm.c[jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
+    sm.d[jp] = make_float2(v[0][6], v[1][6]);
+    sm.n[jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
     if (HILO) {
-      sm.lo[buf][jp] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
-      sm.loz[buf][jp] = make_float2(v[0][11], v[1][11]);
+      sm.lo[jp] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
+      sm.loz[jp] = make_float2(v[0][11], v[1][11]);
     }
   }
-  // the raw slots just read are this thread's own: refill them with the next tile
-  if (PF && ts + TS < c1) prefetch_tile<NT, NP>(src, ts + TS, c1, sm.raw);
-  warp_store_min(smin, sm.tmin[buf]);
+  warp_store_min(smin, sm.tmin);
 }
 
-// Far source pairs [j0, j1) of buffer `buf` against the thread's targets. MD:
-// the z-weights of two consecutive pairs come from one 128-bit shared load
-// (3.5 loads per source pair instead of 4, on the MIO queue the reciprocals
-// also use); j0 and j1 are even.
-template <int T, int UNROLL, bool MD, class Smem>
-__device__ __forceinline__ void sp_far_run(const Smem& sm, int buf, int j0, int j1,
-                                           const float2 (&ntx)[T], const float2 (&nty)[T],
-                                           const float2 (&ntz)[T], const float2 (&bh)[T],
-                                           float2 (&fx)[T], float2 (&fy)[T], float2 (&fz)[T]) {
-  if (MD) {
-#pragma unroll(UNROLL > 1 ? UNROLL / 2 : 1)
-    for (int j = j0; j < j1; j += 2) {
-      const float4 dd = *reinterpret_cast<const float4*>(&sm.d[buf][j]);
-      sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], make_float2(dd.x, dd.y), ntx, nty,
-                     ntz, bh, fx, fy, fz);
-      sp_far_step<T>(sm.a[buf][j + 1], sm.b[buf][j + 1], sm.c[buf][j + 1], make_float2(dd.z, dd.w),
-                     ntx, nty, ntz, bh, fx, fy, fz);
-    }
-  } else {
+// Far source pairs [j0, j1) of the staged tile against the thread's targets.
+template <int T, int UNROLL, class Smem>
+__device__ __forceinline__ void sp_far_run(const Smem& sm, int j0, int j1, const float2 (&ntx)[T],
+                                           const float2 (&nty)[T], const float2 (&ntz)[T],
+                                           const float2 (&bh)[T], float2 (&fx)[T], float2 (&fy)[T],
+                                           float2 (&fz)[T]) {
 #pragma unroll UNROLL
-    for (int j = j0; j < j1; ++j)
-      sp_far_step<T>(sm.a[buf][j], sm.b[buf][j], sm.c[buf][j], sm.d[buf][j], ntx, nty, ntz, bh, fx,
-                     fy, fz);
-  }
+  for (int j = j0; j < j1; ++j)
+    sp_far_step<T>(sm.a[j], sm.b[j], sm.c[j], sm.d[j], ntx, nty, ntz, bh, fx, fy, fz);
 }
 
-// Sums one staged tile (buffer `buf`) into the thread's T targets: a tile whose
+// Sums the staged tile into the thread's T targets: a tile whose
 // every source is far in one tight far loop flushed every FARK segments; else
 // per 64-source segment, far or near. With NT = TS/2 source pairs and FP = 32
 // every warp staged exactly one segment, so segment g's minimum |s|^2 is warp
 // g's and only the segments that hold near sources take the near form;
 // otherwise one far test for the whole tile.
-template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool MD,
-          class Smem>
-__device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&ntx)[T],
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, class Smem>
+__device__ __forceinline__ void sp_sum(const Smem& sm, const float2 (&ntx)[T],
                                        const float2 (&nty)[T], const float2 (&ntz)[T],
                                        const float2 (&bh)[T], const float (&ei)[T],
                                        float2 (&fx)[T], float2 (&fy)[T], float2 (&fz)[T],
@@ -521,10 +465,10 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
   constexpr int FPF = FP * FARK;  // source pairs between flushes in all-far tiles
   constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
   const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
-  const bool tile_far = combine_min<NT / 32>(sm.tmin[buf]) > lim;
+  const bool tile_far = combine_min<NT / 32>(sm.tmin) > lim;
   if (tile_far) {
     for (int jf = 0; jf < NP; jf += FPF) {
-      sp_far_run<T, UNROLL, MD>(sm, buf, jf, jf + FPF, ntx, nty, ntz, bh, fx, fy, fz);
+      sp_far_run<T, UNROLL>(sm, jf, jf + FPF, ntx, nty, ntz, bh, fx, fy, fz);
 #pragma unroll
       for (int t = 0; t < T; ++t) {
         acc.add(0, t, (double)__fadd_rn(fx[t].x, fx[t].y));
@@ -536,9 +480,9 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
     return;
   }
   for (int jf = 0; jf < NP; jf += FP) {
-    const bool far = PERSEG && __uint_as_float(sm.tmin[buf][jf / FP]) > lim;
+    const bool far = PERSEG && __uint_as_float(sm.tmin[jf / FP]) > lim;
     if (far) {
-      sp_far_run<T, UNROLL, MD>(sm, buf, jf, jf + FP, ntx, nty, ntz, bh, fx, fy, fz);
+      sp_far_run<T, UNROLL>(sm, jf, jf + FP, ntx, nty, ntz, bh, fx, fy, fz);
     } else {
       // HILO: d = (s_hi - t_hi) + (s_lo - t_lo), accurate to a few ulps of d itself
       float ntl[HILO ? 3 * T : 1];
@@ -548,17 +492,17 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
       }
 #pragma unroll 4
       for (int j = jf; j < jf + FP; ++j) {
-        const float4 a = sm.a[buf][j];
-        const float4 b = sm.b[buf][j];
-        const float4 n = sm.n[buf][j];
+        const float4 a = sm.a[j];
+        const float4 b = sm.b[j];
+        const float4 n = sm.n[j];
         const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w);
         const float2 sz = make_float2(b.x, b.y);
         const float2 ee = make_float2(n.x, n.y), gg = make_float2(n.z, n.w);
         float4 lo = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 loz = make_float2(0.f, 0.f);
         if (HILO) {
-          lo = sm.lo[buf][j];
-          loz = sm.loz[buf][j];
+          lo = sm.lo[j];
+          loz = sm.loz[j];
         }
 #pragma unroll
         for (int t = 0; t < T; ++t) {
@@ -594,13 +538,12 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int buf, const float2 (&n
 // One work unit: targets at visiting positions [tile0, min(tile0 + NT*T,
 // i_end)) against sources [c0, c1); FP64 sums in the global frame written to
 // out[pos], out[stride + pos], out[2*stride + pos].
-template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool PF,
-          bool PP, bool MD>
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
-                                              SpSmem<NT, TS, T, SMACC, HILO, PF, PP>& sm) {
+                                              SpSmem<NT, TS, T, SMACC, HILO>& sm) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(NT % 32 == 0, "whole warps");
   static_assert(TS % (FLUSH * FARK) == 0, "far-tile flush interval divides the tile");
@@ -697,30 +640,11 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     fx[t] = fy[t] = fz[t] = make_float2(0.f, 0.f);
   }
   warp_store_max(rho2, sm.rho);
-  if (PF) prefetch_tile<NT, NP>(src, c0, c1, sm.raw);
-
-  if (PP) {
-    // two tile buffers: a warp that has summed tile k stages tile k+1 into the
-    // other buffer while slower warps still sum tile k; one barrier per tile
-    // (every warp has left buffer b before anyone stages into it again)
-    int buf = 0;
-    if (c0 < c1) sp_stage<NT, TS, HILO, PF>(src, c0, c1, fr, sm, 0);
+  for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
-    for (int ts = c0; ts < c1; ts += TS) {
-      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK, MD>(sm, buf, ntx, nty, ntz, bh, ei, fx, fy,
-                                                              fz, acc);
-      if (ts + TS < c1) sp_stage<NT, TS, HILO, PF>(src, ts + TS, c1, fr, sm, buf ^ 1);
-      __syncthreads();
-      buf ^= 1;
-    }
-  } else {
-    for (int ts = c0; ts < c1; ts += TS) {
-      __syncthreads();
-      sp_stage<NT, TS, HILO, PF>(src, ts, c1, fr, sm, 0);
-      __syncthreads();
-      sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK, MD>(sm, 0, ntx, nty, ntz, bh, ei, fx, fy,
-                                                              fz, acc);
-    }
+    sp_stage<NT, TS, HILO>(src, ts, c1, fr, sm);
+    __syncthreads();
+    sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, ntx, nty, ntz, bh, ei, fx, fy, fz, acc);
   }
   // back to the global frame: T = R^T T'
 #pragma unroll
@@ -740,9 +664,6 @@ template <int FM>
 struct SpForm {
   static constexpr bool smacc = (FM & 2) != 0;
   static constexpr bool hilo = (FM & 4) != 0;
-  static constexpr bool pf = (FM & 16) != 0;
-  static constexpr bool pp = (FM & 32) != 0;
-  static constexpr bool md = (FM & 64) != 0;
   static constexpr int fark = 1 << ((FM >> 8) & 3);
 };
 
@@ -755,9 +676,10 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
-  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf, F::pp> sm;
-  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp, F::md>(
-      G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
+  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(G.x, G.perm, tile0, G.i1,
+                                                                      G.d2, P.src, c0, c1, out,
+                                                                      stride, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -804,12 +726,12 @@ template <int NT, int T, int TS, int FLUSH, int MINB, int UNROLL, int FM>
 __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchLaunch B) {
   using F = SpForm<FM>;
   __shared__ int slot;
-  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo, F::pf, F::pp> sm;
+  __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
   for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
     const BatchItem I = B.items[it];
     const BatchSeg S = B.segs[I.seg];
     double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::pf, F::pp, F::md>(
+    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(
         S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
   }
 }
