@@ -2,7 +2,8 @@
 
 * Rossby-Haurwitz wave 4, icosahedral level 8 (1,310,720 panels + 655,362
   vertices), delta 0.005: the velocity sums on 512 seeded rows per target
-  class, FP64 within 1e-12 and the default FP32C path within 1e-7.
+  class, FP64 within 1e-12 and the default FP32C path within 1e-7; over all
+  active rows, tangency and linearity in the vorticity.
 * Rossby-Haurwitz wave 4, level 4, FP64, delta 0: ten RK4 steps (dt 0.01)
   through the fused step, against ten oracle BVERK4 steps at 1e-12.
 * The 64-instance Gaussian ensemble (seed 4, levels 3-6, beta in [4, 20]):
@@ -63,6 +64,30 @@ def test_level8_velocity_sums_against_oracle(rh4_l8, prec, tol, gpu):
     assert err <= tol, err
     # dVort = -2 Omega u_z on the sampled active rows
     assert rel(vA[ra], -2.0 * w.omega * refA[:, 2]) <= tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32c", 1e-7)])
+def test_level8_every_row_tangent_and_linear_in_vorticity(rh4_l8, prec, tol, gpu):
+    """Properties of the sum over all 1,310,720 active rows at level 8, independent of the
+    oracle's size: the velocity is tangent to the sphere (x_j . sum_k (x_j x x_k) w_k = 0), and it
+    is linear in the vorticity: u(zeta) = u(zeta_a) + u(zeta - zeta_a) for a seeded random zeta_a,
+    each to the path's tolerance relative to max |u|."""
+    w = rh4_l8
+    rng = np.random.default_rng(88)
+    za = rng.standard_normal(w.nA) * np.abs(w.zetaA).max()
+    ctx = Context(0, prec)
+    ctx.set_omega(w.omega)
+    ctx.set_deltas(*w.deltas)
+    u, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    ua, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, za, w.areaA)
+    ub, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA - za, w.areaA)
+    ctx.close()
+    umax = np.abs(u).max()
+    assert np.all(np.isfinite(u))
+    # u_j = (x_j x T_j) / (-4 pi) is tangent up to the rounding of |x_j| = 1 + O(eps)
+    assert np.abs(np.einsum("ij,ij->i", u, w.xA)).max() <= 1e-12 * umax
+    scale = max(umax, np.abs(ua).max(), np.abs(ub).max())
+    assert np.abs(u - (ua + ub)).max() <= tol * scale
 
 
 def test_config1_rh4_level4_ten_fp64_steps(gpu):
