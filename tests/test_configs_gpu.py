@@ -66,12 +66,13 @@ def test_level8_velocity_sums_against_oracle(rh4_l8, prec, tol, gpu):
     assert rel(vA[ra], -2.0 * w.omega * refA[:, 2]) <= tol
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32c", 1e-7)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32c", 3e-7)])
 def test_level8_every_row_tangent_and_linear_in_vorticity(rh4_l8, prec, tol, gpu):
     """Properties of the sum over all 1,310,720 active rows at level 8, independent of the
     oracle's size: the velocity is tangent to the sphere (x_j . sum_k (x_j x x_k) w_k = 0), and it
     is linear in the vorticity: u(zeta) = u(zeta_a) + u(zeta - zeta_a) for a seeded random zeta_a,
-    each to the path's tolerance relative to max |u|."""
+    relative to the largest of the three (FP64 1e-12; FP32C 3e-7: three results, each within
+    its 1e-7 bound)."""
     w = rh4_l8
     rng = np.random.default_rng(88)
     za = rng.standard_normal(w.nA) * np.abs(w.zetaA).max()
