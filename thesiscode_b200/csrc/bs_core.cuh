@@ -398,36 +398,7 @@ __device__ __forceinline__ int sp_stage(const double4* __restrict__ src, int ts,
   float smin = __int_as_float(0x7f800000);  // +inf
   int nfar = -1;
   for (int jp = threadIdx.x; jp < NP; jp += NT) {
-    int pos = jp;
-    if (CF) {
-      // classify the pair first (only |s|^2 is live across the barrier), then convert
-      float pmin = __int_as_float(0x7f800000);  // this pair's minimum |s|^2 (real sources)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int k = ts + 2 * jp + h;
-        if (k < c1) {
-          const double4 q = src[k];
-          const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
-          pmin = fminf(pmin, norm2_f32((float)frame_dot(fr, dx, dy, dz), (float)frame_dot(fr + 3, dx, dy, dz),
-                                       (float)frame_dot(fr + 6, dx, dy, dz)));
-        }
-      }
-      const bool farp = pmin > lim;  // padding sources (zero weight) never make a pair near
-      const unsigned bal = __ballot_sync(0xffffffffu, farp);
-      const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-      if (lane == 0) sm.nfar[w] = (unsigned)__popc(bal);
-      __syncthreads();
-      int before = 0, total = 0;
-#pragma unroll
-      for (int u = 0; u < NT / 32; ++u) {
-        const int c = (int)sm.nfar[u];
-        before += u < w ? c : 0;
-        total += c;
-      }
-      const int rank = __popc(bal & ((1u << lane) - 1u));  // far pairs before this lane
-      pos = farp ? before + rank : total + (w * 32 - before) + (lane - rank);
-      nfar = total;
-    }
+    float pmin = __int_as_float(0x7f800000);  // this pair's minimum |s|^2 (real sources)
     float v[2][12];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -453,6 +424,7 @@ __device__ __forceinline__ int sp_stage(const double4* __restrict__ src, int ts,
         const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
         const float s2 = norm2_f32(sx, sy, sz);
         smin = fminf(smin, s2);
+        pmin = fminf(pmin, s2);
         v[h][0] = sx;
         v[h][1] = sy;
         v[h][2] = sz;
@@ -463,6 +435,24 @@ __device__ __forceinline__ int sp_stage(const double4* __restrict__ src, int ts,
         v[h][7] = (float)ek;
         v[h][8] = (float)(2.0 * q.w);
       }
+    }
+    int pos = jp;
+    if (CF) {
+      const bool farp = pmin > lim;  // padding sources (zero weight) never make a pair near
+      const unsigned bal = __ballot_sync(0xffffffffu, farp);
+      const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+      if (lane == 0) sm.nfar[w] = (unsigned)__popc(bal);
+      __syncthreads();
+      int before = 0, total = 0;
+#pragma unroll
+      for (int u = 0; u < NT / 32; ++u) {
+        const int c = (int)sm.nfar[u];
+        before += u < w ? c : 0;
+        total += c;
+      }
+      const int rank = __popc(bal & ((1u << lane) - 1u));  // far pairs before this lane
+      pos = farp ? before + rank : total + (w * 32 - before) + (lane - rank);
+      nfar = total;
     }
     sm.a[pos] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
     sm.b[pos] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
