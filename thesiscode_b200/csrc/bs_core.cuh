@@ -241,10 +241,8 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
 // Form bits (FM): bit 3 always set (the source-paired form; the bit value
 // is part of the variant-info ABI); bit 1 keeps the FP64 accumulators in
 // shared memory (one slot per thread, target and coordinate: 6 fewer
-// registers per target); bit 2 gives near tiles hi/lo offsets; bit 4 (CF)
-// stages each tile compacted, far source pairs first, so a segment takes the
-// near form only if it holds near pairs, not because one of its 32 pairs is
-// near; bits 8-9 hold log2 FARK.
+// registers per target); bit 2 gives near tiles hi/lo offsets; bits 8-9 hold
+// log2 FARK.
 // HILO (bit 2): near tiles take d = s - t from hi/lo FP32 splits of both
 // offsets, (s_hi - t_hi) + (s_lo - t_lo): the rounding of the offsets to FP32
 // (an absolute error of ulps of the patch radius, the dominant FP32C error
@@ -301,7 +299,6 @@ struct SpSmem {
   float tlo[HILO ? 3 * T * NT : 1];    // HILO: -(target low parts) [c][t][thread]
   unsigned tmin[NT / 32];
   unsigned rho[NT / 32];
-  unsigned nfar[NT / 32];  // CF: far source pairs staged by each warp
 };
 
 // Orthonormal basis with e3 = c/|c| (Duff, Burgess, Christensen, Hart, Kensler,
@@ -384,21 +381,13 @@ struct SpAcc {
 
 // Converts the sources of the tile at ts into the CTA's frame: offsets s_k,
 // A_k = (|s_k|^2 + e_k)/2, G_k x'_k, e_k, 2G_k (and the hi/lo low parts),
-// padding past c1; records each warp's minimum |s_k|^2. CF (one source pair
-// per thread): the pairs are stored compacted, every far pair (each real
-// source farther than the far limit, `lim` = kFarRatio^2 rho^2) before every
-// near pair, in thread order within each group; returns the number of far
-// pairs (the order within the tile is a pure function of the positions, so
-// results stay deterministic). Without CF returns -1.
-template <int NT, int TS, bool HILO, bool CF, class Smem>
-__device__ __forceinline__ int sp_stage(const double4* __restrict__ src, int ts, int c1,
-                                        const double* fr, Smem& sm, float lim) {
+// padding past c1; records each warp's minimum |s_k|^2.
+template <int NT, int TS, bool HILO, class Smem>
+__device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts, int c1,
+                                         const double* fr, Smem& sm) {
   constexpr int NP = TS / 2;
-  static_assert(!CF || NT == NP, "compaction stages one source pair per thread");
   float smin = __int_as_float(0x7f800000);  // +inf
-  int nfar = -1;
   for (int jp = threadIdx.x; jp < NP; jp += NT) {
-    float pmin = __int_as_float(0x7f800000);  // this pair's minimum |s|^2 (real sources)
     float v[2][12];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -424,7 +413,6 @@ __device__ __forceinline__ int sp_stage(const double4* __restrict__ src, int ts,
         const double ek = 1.0 - (q.x * q.x + q.y * q.y + q.z * q.z);
         const float s2 = norm2_f32(sx, sy, sz);
         smin = fminf(smin, s2);
-        pmin = fminf(pmin, s2);
         v[h][0] = sx;
         v[h][1] = sy;
         v[h][2] = sz;
@@ -436,36 +424,17 @@ __device__ __forceinline__ int sp_stage(const double4* __restrict__ src, int ts,
         v[h][8] = (float)(2.0 * q.w);
       }
     }
-    int pos = jp;
-    if (CF) {
-      const bool farp = pmin > lim;  // padding sources (zero weight) never make a pair near
-      const unsigned bal = __ballot_sync(0xffffffffu, farp);
-      const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-      if (lane == 0) sm.nfar[w] = (unsigned)__popc(bal);
-      __syncthreads();
-      int before = 0, total = 0;
-#pragma unroll
-      for (int u = 0; u < NT / 32; ++u) {
-        const int c = (int)sm.nfar[u];
-        before += u < w ? c : 0;
-        total += c;
-      }
-      const int rank = __popc(bal & ((1u << lane) - 1u));  // far pairs before this lane
-      pos = farp ? before + rank : total + (w * 32 - before) + (lane - rank);
-      nfar = total;
-    }
-    sm.a[pos] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
-    sm.b[pos] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
-    sm.c[pos] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
-    sm.d[pos] = make_float2(v[0][6], v[1][6]);
-    sm.n[pos] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
+    sm.a[jp] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+    sm.b[jp] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
+    sm.c[jp] = make_float4(v[0][4], v[1][4], v[0][5], v[1][5]);
+    sm.d[jp] = make_float2(v[0][6], v[1][6]);
+    sm.n[jp] = make_float4(v[0][7], v[1][7], v[0][8], v[1][8]);
     if (HILO) {
-      sm.lo[pos] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
-      sm.loz[pos] = make_float2(v[0][11], v[1][11]);
+      sm.lo[jp] = make_float4(v[0][9], v[1][9], v[0][10], v[1][10]);
+      sm.loz[jp] = make_float2(v[0][11], v[1][11]);
     }
   }
-  if (!CF) warp_store_min(smin, sm.tmin);
-  return nfar;
+  warp_store_min(smin, sm.tmin);
 }
 
 // Far source pairs [j0, j1) of the staged tile against the thread's targets.
@@ -486,7 +455,7 @@ __device__ __forceinline__ void sp_far_run(const Smem& sm, int j0, int j1, const
 // g's and only the segments that hold near sources take the near form;
 // otherwise one far test for the whole tile.
 template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, class Smem>
-__device__ __forceinline__ void sp_sum(const Smem& sm, int nfar, const float2 (&ntx)[T],
+__device__ __forceinline__ void sp_sum(const Smem& sm, const float2 (&ntx)[T],
                                        const float2 (&nty)[T], const float2 (&ntz)[T],
                                        const float2 (&bh)[T], const float (&ei)[T],
                                        float2 (&fx)[T], float2 (&fy)[T], float2 (&fz)[T],
@@ -495,9 +464,8 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int nfar, const float2 (&
   constexpr int FP = FLUSH / 2;
   constexpr int FPF = FP * FARK;  // source pairs between flushes in all-far tiles
   constexpr bool PERSEG = (NT == TS / 2) && (FP == 32);
-  // nfar >= 0 (compacted tile): the first nfar source pairs are far, the rest near
   const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
-  const bool tile_far = nfar >= 0 ? nfar == NP : combine_min<NT / 32>(sm.tmin) > lim;
+  const bool tile_far = combine_min<NT / 32>(sm.tmin) > lim;
   if (tile_far) {
     for (int jf = 0; jf < NP; jf += FPF) {
       sp_far_run<T, UNROLL>(sm, jf, jf + FPF, ntx, nty, ntz, bh, fx, fy, fz);
@@ -512,7 +480,7 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int nfar, const float2 (&
     return;
   }
   for (int jf = 0; jf < NP; jf += FP) {
-    const bool far = nfar >= 0 ? jf + FP <= nfar : PERSEG && __uint_as_float(sm.tmin[jf / FP]) > lim;
+    const bool far = PERSEG && __uint_as_float(sm.tmin[jf / FP]) > lim;
     if (far) {
       sp_far_run<T, UNROLL>(sm, jf, jf + FP, ntx, nty, ntz, bh, fx, fy, fz);
     } else {
@@ -570,7 +538,7 @@ __device__ __forceinline__ void sp_sum(const Smem& sm, int nfar, const float2 (&
 // One work unit: targets at visiting positions [tile0, min(tile0 + NT*T,
 // i_end)) against sources [c0, c1); FP64 sums in the global frame written to
 // out[pos], out[stride + pos], out[2*stride + pos].
-template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK, bool CF>
+template <int NT, int T, int TS, int FLUSH, int UNROLL, bool SMACC, bool HILO, int FARK>
 __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, const int* __restrict__ perm,
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
@@ -674,11 +642,9 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   warp_store_max(rho2, sm.rho);
   for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
-    const float lim = kFarRatio2 * combine_max<NT / 32>(sm.rho);
-    const int nfar = sp_stage<NT, TS, HILO, CF>(src, ts, c1, fr, sm, lim);
+    sp_stage<NT, TS, HILO>(src, ts, c1, fr, sm);
     __syncthreads();
-    sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, nfar, ntx, nty, ntz, bh, ei, fx, fy, fz,
-                                                        acc);
+    sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, ntx, nty, ntz, bh, ei, fx, fy, fz, acc);
   }
   // back to the global frame: T = R^T T'
 #pragma unroll
@@ -699,7 +665,6 @@ struct SpForm {
   static constexpr bool smacc = (FM & 2) != 0;
   static constexpr bool hilo = (FM & 4) != 0;
   static constexpr int fark = 1 << ((FM >> 8) & 3);
-  static constexpr bool cf = (FM & 16) != 0;
 };
 
 template <int NT, int T, int TS, int FLUSH, int MINB, int UNROLL, int FM>
@@ -712,8 +677,9 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const size_t stride = (size_t)P.n_out;
   double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
   __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
-  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::cf>(
-      G.x, G.perm, tile0, G.i1, G.d2, P.src, c0, c1, out, stride, sm);
+  fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(G.x, G.perm, tile0, G.i1,
+                                                                      G.d2, P.src, c0, c1, out,
+                                                                      stride, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -765,7 +731,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchL
     const BatchItem I = B.items[it];
     const BatchSeg S = B.segs[I.seg];
     double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
-    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark, F::cf>(
+    fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(
         S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
   }
 }

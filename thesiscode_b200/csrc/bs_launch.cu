@@ -79,8 +79,8 @@ const PairVariant kVariants64[] = {
 };
 // FP32C form bits (SpForm in bs_core.cuh): 8 = source-paired form (all
 // variants), 2 = FP64 accumulators in shared memory, 4 = hi/lo near offsets,
-// 16 = tiles staged far source pairs first, 256 / 512 = tiles whose every
-// source is far flushed every 2 / 4 flush lengths.
+// 256 / 512 = tiles whose every source is far flushed every 2 / 4 flush
+// lengths.
 const PairVariant kVariants32[] = {
     // 0: default from 131,072 sources (3 targets per thread); 1: default below (2 per thread)
     V32(128, 3, 64, 6, 4, 8 | 2 | 256), V32(128, 2, 64, 6, 4, 8 | 512),
@@ -91,8 +91,6 @@ const PairVariant kVariants32[] = {
     // 8-11: near tiles with hi/lo offsets (1e-7 at coarser grids, at a fraction of the speed)
     V32(128, 3, 64, 6, 4, 8 | 4 | 2), V32(128, 2, 64, 6, 4, 8 | 4), V32(128, 2, 64, 6, 4, 8 | 4 | 2),
     V32(128, 3, 64, 5, 4, 8 | 4 | 2),
-    // 12-13: the defaults with tiles staged far pairs first (form bit 4)
-    V32(128, 3, 64, 6, 4, 8 | 2 | 256 | 16), V32(128, 2, 64, 6, 4, 8 | 512 | 16),
 };
 constexpr int kN64 = sizeof(kVariants64) / sizeof(kVariants64[0]);
 constexpr int kN32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
