@@ -3,9 +3,12 @@ source counts that are not multiples of the 256-source tile (from 1 up), target 
 not multiples of a CTA's targets, target ranges starting and ending inside tiles, all three target
 classes, random subsets of a level-5 grid (sources from the panel centres, vertex and passive
 targets from the vertices, so no target sits on a source) with random vorticity. FP64 within
-1e-12; FP32C within
-1e-6 (these are index-logic checks on thinned grids; the FP32C accuracy bounds are tested on full
-grids elsewhere). Rows outside the range must be exactly zero."""
+1e-12, which checks the index logic exactly. FP32C within 1e-5: its error floor is eps * rho / h
+(rho the radius of a CTA's patch of targets, h the distance to the nearest source), and thinned
+targets make rho large against the spacing of the sources they sit among (measured 1.9e-6 for
+2,094 random vertices among level-5 panels); the FP32C bounds for grids, where targets and sources
+have the same density, are tested on full grids elsewhere, and an index error would show as an
+O(1) error. Rows outside the range must be exactly zero."""
 import numpy as np
 import pytest
 
@@ -15,7 +18,7 @@ from thesiscode_b200 import configs
 from thesiscode_b200.panel_velocity import Context
 
 pytestmark = pytest.mark.gpu
-TOL = {"fp64": 1e-12, "fp32c": 1e-6}
+TOL = {"fp64": 1e-12, "fp32c": 1e-5}
 
 
 def cases(seed=2024, count=16):
