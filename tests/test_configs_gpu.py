@@ -179,3 +179,25 @@ def test_remesh_cycle_reset_and_reload_larger_grid(prec, gpu):
     _, rA6, rz6, _, _ = _oracle_step(w6, 1)
     assert rel(xA6 - w6.xA, rA6 - w6.xA) <= tol6
     assert rel(zA6 - w6.zetaA, rz6 - w6.zetaA) <= tol6
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32c"])
+def test_rh4_wave_stays_steady_through_the_fused_step(prec, gpu):
+    """The steady Rossby-Haurwitz wave (alpha = Omega/14; RHWavePanelsMPI.f90:293-312) through
+    the library's fused RK4 step at levels 4-6: after three steps of dt 0.01 the carried panel
+    vorticity equals HaurwitzStationary4RelVort at the advected positions to the discretisation
+    error, which falls with the level; FP32C within 1e-6 of FP64's error."""
+    from thesiscode_b200 import ics
+
+    errs = []
+    for level in (4, 5, 6):
+        w = configs.rh4(level=level, parity=True, dt=0.01)
+        ctx = Context(0, prec)
+        ctx.set_omega(w.omega)
+        ctx.set_deltas(*w.deltas)
+        xA, zA, xV, xQ = w.xA.copy(), w.zetaA.copy(), w.xV.copy(), w.xQ.copy()
+        ctx.rk4_step(xA, zA, w.areaA, xV, xQ, w.dt, 3)
+        ctx.close()
+        ref = ics.rh4_reference(xA)
+        errs.append(np.abs(zA - ref).max() / np.abs(ref).max())
+    assert errs[0] > errs[1] > errs[2] and errs[0] <= 2.5e-3, errs

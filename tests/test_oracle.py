@@ -245,3 +245,26 @@ def test_stratosphere_forcing_changes_the_flow():
     assert np.abs(F).max() > 0.1
     # relVort difference at the new time is the forcing (positions differ by O(dt))
     assert np.abs((off[2] - on[2]) - F).max() < 0.05 * np.abs(F).max()
+
+
+def test_rh4_wave_is_steady_known_answer():
+    """The reference's Rossby-Haurwitz check (RHWavePanelsMPI.f90:293-312): with alpha = pi/7 =
+    Omega/14 the wave-4 field HaurwitzStationary4RelVort (PanelVelocitySerial.f90:589-598) is a
+    steady solution of the rotating barotropic vorticity equation, so after any number of BVERK4
+    steps each panel's carried vorticity equals the field at its advected position, up to the
+    discretisation error, which falls with the level. Three steps of dt 0.01, parity mode; the
+    same steps with the vorticity update left out miss by several times as much (by more than ten
+    times from level 4)."""
+    from thesiscode_b200 import ics
+
+    errs = []
+    for level in (2, 3, 4):
+        w = configs.rh4(level=level, parity=True, dt=0.01, grid_source=O.gathered_grid)
+        xV, xA, zA, xQ = w.xV, w.xA, w.zetaA, w.xQ
+        for _ in range(3):
+            xV, xA, zA, xQ, *_ = O.bve_rk4(xV, xA, zA, w.areaA, xQ, w.dt, w.omega, w.deltas, nthreads=8)
+        ref = ics.rh4_reference(xA)
+        errs.append(np.abs(zA - ref).max() / np.abs(ref).max())
+        frozen = np.abs(w.zetaA - ref).max() / np.abs(ref).max()
+        assert errs[-1] <= frozen / (10 if level >= 4 else 4), (level, errs[-1], frozen)
+    assert errs[0] > errs[1] > errs[2] and errs[2] <= 2.5e-3, errs
