@@ -184,13 +184,16 @@ def test_remesh_cycle_reset_and_reload_larger_grid(prec, gpu):
 @pytest.mark.parametrize("prec", ["fp64", "fp32c"])
 def test_rh4_wave_stays_steady_through_the_fused_step(prec, gpu):
     """The steady Rossby-Haurwitz wave (alpha = Omega/14; RHWavePanelsMPI.f90:293-312) through
-    the library's fused RK4 step at levels 4-6: after three steps of dt 0.01 the carried panel
+    the library's fused RK4 step at levels 3-5: after three steps of dt 0.01 the carried panel
     vorticity equals HaurwitzStationary4RelVort at the advected positions to the discretisation
-    error, which falls with the level; FP32C within 1e-6 of FP64's error."""
+    error, which falls with the level. (Level 6 is past this dt: stage inputs leave the unit
+    sphere by (dt |u| / 2)^2 ~ 5e-5, the squared half-spacing of nearest panels, so with
+    delta = 0 their denominator 1 - x.y nearly vanishes; the reference's loops, restated by the
+    oracle, blow up the same way.)"""
     from thesiscode_b200 import ics
 
     errs = []
-    for level in (4, 5, 6):
+    for level in (3, 4, 5):
         w = configs.rh4(level=level, parity=True, dt=0.01)
         ctx = Context(0, prec)
         ctx.set_omega(w.omega)
@@ -200,4 +203,4 @@ def test_rh4_wave_stays_steady_through_the_fused_step(prec, gpu):
         ctx.close()
         ref = ics.rh4_reference(xA)
         errs.append(np.abs(zA - ref).max() / np.abs(ref).max())
-    assert errs[0] > errs[1] > errs[2] and errs[0] <= 2.5e-3, errs
+    assert errs[0] > errs[1] > errs[2] and errs[2] <= 1.2e-3, errs
