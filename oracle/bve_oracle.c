@@ -1,8 +1,8 @@
 /*
  * bve_oracle.c - CPU FP64 restatement of the reference's Biot-Savart sums and
  * RK4 driver. TEST INFRASTRUCTURE ONLY (the parity tests' reference values and
- * the timed CPU baseline); see bve_oracle.h for the parity status ("parity unpinned"
- * against a reference binary: no Fortran compiler is available).
+ * the timed CPU baseline); see bve_oracle.h for the parity status (pinned bit for
+ * bit to the reference's own Fortran statements, run through oracle/f90).
  *
  * Every arithmetic expression keeps the reference's operand order so that a
  * strict IEEE build (gcc -O2 -ffp-contract=off, SSE2) rounds exactly as the

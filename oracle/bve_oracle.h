@@ -3,13 +3,16 @@
  * path. TEST INFRASTRUCTURE ONLY: the reference values of the CUDA library's
  * parity tests and the CPU baseline of the benchmark. Nothing in the product links or calls it.
  *
- * Parity status: the reference is Fortran (ifort/Open MPI) and no Fortran
- * compiler is available to build it, so this restatement is
- * "parity unpinned" against a reference binary. It is pinned instead by the
- * known answers the reference's own validation drivers check (solid-body
- * rotation, RK4 time-step convergence, invariants; see tests/test_oracle.py)
- * and by line-by-line correspondence of every loop and every floating-point
- * operation order with the cited Fortran lines.
+ * Parity status: pinned against the reference's own code. The reference is
+ * Fortran (ifort/Open MPI) and no Fortran compiler is available to build it,
+ * so its source is run instead through oracle/f90, a translator of the
+ * Fortran 90 subset its modules use, with strict IEEE double arithmetic; this
+ * restatement equals the outputs of those runs bit for bit (grid, initial
+ * conditions, BVERK4 and StratosphereRK4 on 1-4 ranks, the three RHS sums,
+ * the Voronoi sum: tests/test_reference_source.py, fixtures
+ * tests/golden/ref_*.npz). It is also checked against the known answers the
+ * reference's own validation drivers check (solid-body rotation, RK4
+ * time-step convergence, invariants; tests/test_oracle.py).
  *
  * Layout: a point set is x[3*k + c] (Fortran x(3,n) column-major), 0-based;
  * target ranges are half-open [i0, i1).

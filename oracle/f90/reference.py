@@ -1,0 +1,254 @@
+"""The reference's hot path run from its own Fortran source (ThesisCode, free-form .f90).
+
+TEST INFRASTRUCTURE ONLY: used by tests/ and tests/golden/make_reference_fixtures.py
+to pin the C oracle to the reference's code. Needs the reference's sources
+(REFERENCE_DIR, default the checkout this build was given); where they are
+absent, available() is False and the committed fixtures stand in for them.
+
+What runs, all of it the reference's own statements translated by
+oracle/f90 (nothing restated here):
+  * NewGrid -> InitIcosTriGrid / DivideTriPanel / TriPanelArea
+    (ParticlesEdgesPanels2.f90:362-397,419-1090,1727-1802), the grid;
+  * InitRH4WavePanels, InitGaussianVortexPanels, InitJetPanels
+    (TracerAndVorticityDistributions.f90:142-174,243-304,737-790,793-812), the initial vorticity;
+  * InitializeMPIRK4 / LoadBalance / BVERK4 / StratosphereRK4 and the three RHS sums
+    (PanelVelocityParallel.f90:126-213,435-919,1287-1412), with MPI ranks as threads and
+    MPI_BCAST as an in-process broadcast;
+  * BVEVelocity of the Voronoi solver (VoronoiVelocityParallel.f90:487-515).
+Logger and OutputWriter procedures (logging and file output) are replaced by no-ops.
+"""
+from __future__ import annotations
+
+import os
+import threading
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+from . import Runner, rt
+
+REFERENCE_DIR = Path(os.environ.get("TC_REFERENCE_DIR", "/root/reference"))
+
+FILES = ("NumberKinds.f90", "SphereGeom.f90", "OutputWriter.f90", "Logger.f90", "IntegerList.f90",
+         "ParticlesEdgesPanels2.f90", "VoronoiPanels.f90", "STRIPACK.f90",
+         "TracerAndVorticityDistributions.f90", "PanelVelocityParallel.f90",
+         "VoronoiVelocityParallel.f90")
+
+PVP = "panelvelocityparallelmodule"
+PEP = "particlesedgespanelsmodule"
+TVD = "tracerandvorticitydistributionmodule"
+VVP = "voronoivelocityparallelmodule"
+
+ENTRY = [(PVP, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4",
+                            "setsmooth", "bveactiverhs", "bvepassiverhs", "bvesmoothvelocity")] + \
+        [(PEP, "newgrid"), (TVD, "setomega"), (TVD, "initrh4wavepanels"),
+         (TVD, "initgaussianvortexpanels"), (TVD, "initjetpanels"), (TVD, "initstratosphere"),
+         (VVP, "bvevelocity")]
+
+# mpif.h stand-in: only the names the modules use; the values are handles the host procedures
+# receive and never interpret
+MPIF = {"mpi_status_size": 6, "mpi_double_precision": 17, "mpi_integer": 7, "mpi_comm_world": 0,
+        "mpi_real": 13, "mpi_sum": 1, "mpi_logical": 6, "mpi_max": 2, "mpi_min": 3}
+
+TRI_PANEL, BVE_SOLVER = 3, 61
+
+
+def available() -> bool:
+    return all((REFERENCE_DIR / f).is_file() for f in FILES)
+
+
+def _stub(mod, proc):
+    return mod == "outputwritermodule" or (mod == "loggermodule" and proc != "getlogginglevel")
+
+
+@lru_cache(maxsize=1)
+def runner() -> Runner:
+    if not available():
+        raise FileNotFoundError(f"reference sources not found under {REFERENCE_DIR}")
+    return Runner([REFERENCE_DIR / f for f in FILES], ENTRY, includes={"mpif.h": MPIF},
+                  host_procs={"mpi_bcast", "mpi_barrier"}, stubs=_stub)
+
+
+class _World:
+    """In-process MPI_COMM_WORLD for ranks run as threads."""
+
+    def __init__(self, n):
+        self.bar = threading.Barrier(n, timeout=600)
+        self.slot = None
+
+    def bcast(self, rank, buf, count, datatype, root, comm, ierr):
+        a = buf.a if isinstance(buf, rt.FArr) else None
+        if a is None or a.size != count:
+            raise ValueError(f"MPI_BCAST of {count} values on a buffer of {None if a is None else a.size}")
+        if rank == root:
+            self.slot = a.copy()
+        self.bar.wait()
+        if rank != root:
+            a[...] = self.slot
+        self.bar.wait()
+
+
+def _ranks(nprocs, body):
+    """Run body(instance, rank) on nprocs thread ranks; returns the per-rank results."""
+    r = runner()
+    world = _World(nprocs)
+    out, errs = [None] * nprocs, []
+
+    def main(rank):
+        try:
+            inst = r.instance(host={"mpi_bcast": lambda *a: world.bcast(rank, *a),
+                                    "mpi_barrier": lambda *a: world.bar.wait()})
+            out[rank] = body(inst, rank)
+        except BaseException as e:  # noqa: BLE001 - re-raised below
+            errs.append(e)
+            world.bar.abort()
+
+    threads = [threading.Thread(target=main, args=(k,)) for k in range(nprocs)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errs:
+        raise errs[0]
+    return out
+
+
+def new_grid(inst, level, n_tracer=1):
+    g = inst.proc(PEP, "newgrid")(None, None, None, TRI_PANEL, level, 0, n_tracer, BVE_SOLVER)
+    return g[0], g[1], g[2]
+
+
+def grid(level) -> dict:
+    """The reference's icosahedral grid: the arrays of oracle.icos_grid (0-based tables)."""
+    inst = runner().instance()
+    p, _, q = new_grid(inst, level)
+    n, m = p.n, q.n
+    return dict(particles_x=p.x.a[:, :n].T.copy(), particles_x0=p.x0.a[:, :n].T.copy(),
+                panels_x=q.x.a[:, :m].T.copy(), panels_x0=q.x0.a[:, :m].T.copy(),
+                panels_area=q.area.a[:m].copy(),
+                panels_has_children=q.haschildren.a[:m].astype(np.int32),
+                panels_vertices=(q.vertices.a[:, :m].T - 1).astype(np.int32),
+                panels_nest=q.nest.a[:m].astype(np.int32),
+                panels_children=(q.children.a[:, :m].T - 1).astype(np.int32))
+
+
+def _init(inst, ic, p, q):
+    if ic == "rh4":
+        inst.proc(TVD, "initrh4wavepanels")(p, q)
+    elif ic == "gauss":
+        inst.proc(TVD, "initgaussianvortexpanels")(p, q)
+    elif ic == "jet":
+        inst.proc(TVD, "initjetpanels")(p, q, np.pi / 4.0, 12.0, 0.025, 12)
+    elif ic == "strat":
+        inst.proc(TVD, "initstratosphere")(p, q)
+    else:
+        raise ValueError(ic)
+
+
+def state(p, q) -> dict:
+    """Particles and panels as arrays: the gathered classes of the RK4 step in index order."""
+    n, m = p.n, q.n
+    hc = q.haschildren.a[:m].astype(bool)
+    act, pas = np.nonzero(~hc)[0], np.nonzero(hc)[0]
+    return dict(xV=p.x.a[:, :n].T.copy(), relVortV=p.relvort.a[:n].copy(), absVortV=p.absvort.a[:n].copy(),
+                xA=q.x.a[:, act].T.copy(), zetaA=q.relvort.a[act].copy(), absVortA=q.absvort.a[act].copy(),
+                areaA=q.area.a[act].copy(), xQ=q.x.a[:, pas].T.copy())
+
+
+def initial_state(level, ic="rh4") -> dict:
+    inst = runner().instance()
+    p, _, q = new_grid(inst, level)
+    _init(inst, ic, p, q)
+    return state(p, q)
+
+
+def bve_rk4(level, steps, dt, nprocs=1, ic="rh4", smooth=0.05, omega=2 * np.pi) -> dict:
+    """BVERK4 (PanelVelocityParallel.f90:435-658) for `steps` steps on nprocs thread ranks, from
+    the reference's grid and initial condition. Returns the initial and final states, the
+    totalKE of every step and each rank's final state (all ranks must agree)."""
+    def body(inst, rank):
+        inst.proc(TVD, "setomega")(omega)
+        inst.proc(PVP, "setsmooth")(smooth)
+        p, _, q = new_grid(inst, level)
+        _init(inst, ic, p, q)
+        s0 = state(p, q)
+        inst.proc(PVP, "initializempirk4")(p, q, rank, nprocs)
+        tke = []
+        for _ in range(steps):
+            inst.proc(PVP, "bverk4")(p, q, dt, rank, nprocs)
+            tke.append(float(inst.mod(PVP).totalke))
+        ke = inst.mod(PVP).kineticenergy.a.copy()
+        inst.proc(PVP, "finalizempirk4")()
+        return s0, state(p, q), tke, ke
+
+    res = _ranks(nprocs, body)
+    s0, s1, tke, ke = res[0]
+    for _, s, t, _k in res[1:]:
+        if t != tke or any(not np.array_equal(s[k], s1[k]) for k in s1):
+            raise AssertionError("ranks disagree after BVERK4")
+    return dict(initial=s0, final=s1, totalKE=np.array(tke), kineticEnergy=ke)
+
+
+def strat_rk4(level, steps, t0, dt, nprocs=1, smooth=0.05, omega=2 * np.pi) -> dict:
+    """StratosphereRK4 (PanelVelocityParallel.f90:661-919): the forced model's step, from the
+    reference's stratosphere initial condition (InitStratosphere)."""
+    def body(inst, rank):
+        inst.proc(TVD, "setomega")(omega)
+        inst.proc(PVP, "setsmooth")(smooth)
+        p, _, q = new_grid(inst, level)
+        _init(inst, "strat", p, q)
+        s0 = state(p, q)
+        inst.proc(PVP, "initializempirk4")(p, q, rank, nprocs)
+        t = t0
+        for _ in range(steps):
+            inst.proc(PVP, "stratosphererk4")(p, q, t, dt, rank, nprocs)
+            t = t + dt
+        inst.proc(PVP, "finalizempirk4")()
+        return s0, state(p, q)
+
+    res = _ranks(nprocs, body)
+    s0, s1 = res[0]
+    for _, s in res[1:]:
+        if any(not np.array_equal(s[k], s1[k]) for k in s1):
+            raise AssertionError("ranks disagree after StratosphereRK4")
+    return dict(initial=s0, final=s1)
+
+
+def _f2(a):
+    return rt.FArr(np.asfortranarray(np.asarray(a, dtype=np.float64).T))
+
+
+def _f1(a):
+    return rt.FArr(np.array(a, dtype=np.float64))
+
+
+def rhs(cls, X, x, vort, area, i0, i1, smooth=0.05, omega=2 * np.pi):
+    """One of BVEActiveRHS (cls 0), BVEPassiveRHS (1), BVESmoothVelocity (2) over the 0-based
+    half-open row range [i0, i1) (Fortran indexStart = i0 + 1, indexEnd = i1); returns dX (m, 3)
+    and, for the active sum, dVort."""
+    inst = runner().instance()
+    inst.proc(TVD, "setomega")(omega)
+    inst.proc(PVP, "setsmooth")(smooth)
+    n = len(vort)
+    if cls == 0:
+        dx, dv = rt.FArr(np.zeros((3, n), order="F")), rt.FArr(np.zeros(n))
+        inst.proc(PVP, "bveactiverhs")(dx, dv, _f2(x), _f1(vort), _f1(area), i0 + 1, i1)
+        return dx.a.T.copy(), dv.a.copy()
+    m = len(X)
+    dx = rt.FArr(np.zeros((3, m), order="F"))
+    name = "bvepassiverhs" if cls == 1 else "bvesmoothvelocity"
+    inst.proc(PVP, name)(dx, _f2(X), _f2(x), _f1(vort), _f1(area), i0 + 1, i1)
+    return dx.a.T.copy(), None
+
+
+def voronoi_velocity(x, y, z, vort, area, i0, i1, omega=2 * np.pi, dy=None, dz=None):
+    """BVEVelocity of the Voronoi solver (VoronoiVelocityParallel.f90:487-515) over rows [i0, i1):
+    (dx, dy, dz, dVort). dy and dz start from the given arrays (the routine zeroes dx only)."""
+    inst = runner().instance()
+    inst.proc(TVD, "setomega")(omega)
+    n = len(x)
+    out = [rt.FArr(np.zeros(n)), _f1(np.zeros(n) if dy is None else dy),
+           _f1(np.zeros(n) if dz is None else dz), rt.FArr(np.zeros(n))]
+    inst.proc(VVP, "bvevelocity")(*out, _f1(x), _f1(y), _f1(z), _f1(vort), _f1(area), i0 + 1, i1)
+    return tuple(o.a.copy() for o in out)

@@ -1,0 +1,289 @@
+"""Run-time support of the Python code generated from the Fortran subset.
+
+TEST INFRASTRUCTURE ONLY (see oracle/f90/__init__.py). Fortran REAL(8)
+arithmetic is IEEE binary64 with every operation rounded once (no fused
+multiply-add), which is what Python floats and numpy's element-wise operators
+do; transcendental functions call the C library through Python's math module,
+as compiled Fortran does. Arrays are numpy arrays in column-major order with
+their lower bounds kept beside them (FArr).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+class FortranStop(Exception):
+    """A STOP statement was executed."""
+
+
+class NS:
+    """Namespace of one module's variables (or one procedure's saved locals)."""
+
+    def __repr__(self):
+        return f"NS({sorted(vars(self))})"
+
+
+class Derived:
+    """Base class of the generated derived types."""
+
+    __slots__ = ()
+
+
+class FArr:
+    """A Fortran array: numpy data (column-major) and its lower bounds."""
+
+    __slots__ = ("a", "lb")
+
+    def __init__(self, a, lb=None):
+        self.a = a
+        self.lb = tuple(lb) if lb is not None else (1,) * a.ndim
+
+    @staticmethod
+    def alloc(bounds, dtype):
+        ext = tuple(max(0, int(hi) - int(lo) + 1) for lo, hi in bounds)
+        if dtype is object:
+            a = np.empty(ext, dtype=object, order="F")
+        else:
+            a = np.zeros(ext, dtype=dtype, order="F")
+        return FArr(a, tuple(int(lo) for lo, _ in bounds))
+
+    def __repr__(self):
+        return f"FArr(shape={self.a.shape}, lb={self.lb})"
+
+
+NO = object()  # "no write-back" marker in a subroutine's returned tuple
+
+
+def assoc(x, shape):
+    """Explicit-shape dummy associated with an actual array (sequence association): the actual's
+    elements in array-element order viewed with the dummy's shape."""
+    if x is None:
+        return None
+    if not isinstance(x, FArr):
+        x = FArr(np.asarray(x))
+    if x.a.shape == tuple(shape):
+        return x if x.lb == (1,) * len(shape) else FArr(x.a)
+    n = int(np.prod(shape))
+    flat = x.a.reshape(-1, order="F")
+    if flat.size < n:
+        raise ValueError(f"actual array of {flat.size} elements for a dummy of shape {shape}")
+    v = flat[:n].reshape(shape, order="F")
+    return FArr(v)
+
+
+def as_farr(v):
+    return v if isinstance(v, FArr) else FArr(np.asarray(v))
+
+
+def section(x, sl):
+    """View of an array section (lower bounds 1)."""
+    return FArr(x.a[sl])
+
+
+def sl(lo, hi, st, lb, ext):
+    """Python slice of the Fortran triplet lo:hi:st on a dimension with lower bound lb and
+    extent ext (lo/hi None = the bound)."""
+    if lo is None:
+        lo = lb if st > 0 else lb + ext - 1
+    if hi is None:
+        hi = lb + ext - 1 if st > 0 else lb
+    a = lo - lb
+    b = hi - lb
+    if st > 0:
+        return slice(a, b + 1 if b >= a else a, st)
+    stop = b - 1
+    return slice(a, stop if stop >= 0 else None, st) if b <= a else slice(a, a, st)
+
+
+def do_range(a, b, s):
+    if s == 0:
+        raise ValueError("DO step 0")
+    return range(a, b + 1, s) if s > 0 else range(a, b - 1, s)
+
+
+def do_after(a, b, s):
+    """Value of the DO variable after the loop completed (Fortran: start + trips * step)."""
+    trips = max(0, (b - a + s) // s) if s > 0 else max(0, (a - b - s) // (-s))
+    return a + trips * s
+
+
+def idiv(a, b):
+    """Integer division truncating toward zero."""
+    a, b = int(a), int(b)
+    q = abs(a) // abs(b)
+    return q if (a >= 0) == (b >= 0) else -q
+
+
+def idiv_arr(a, b):
+    return np.trunc(np.asarray(a, dtype=np.float64) / np.asarray(b, dtype=np.float64)).astype(np.int64)
+
+
+def imod(a, p):
+    a, p = int(a), int(p)
+    return a - idiv(a, p) * p
+
+
+def fmodulo(a, p):
+    r = math.fmod(a, p)
+    if r != 0.0 and ((r < 0.0) != (p < 0.0)):
+        r += p
+    return r
+
+
+def powi(x, m):
+    """x**m for integer m as GCC computes it (__powidf2: binary powering)."""
+    m = int(m)
+    n = -m if m < 0 else m
+    y = x if n % 2 else 1.0
+    while True:
+        n >>= 1
+        if not n:
+            break
+        x = x * x
+        if n % 2:
+            y = y * x
+    return 1.0 / y if m < 0 else y
+
+
+def powi_arr(x, m):
+    return np.vectorize(lambda v: powi(float(v), m), otypes=[np.float64])(x)
+
+
+def ipow(a, b):
+    return int(a) ** int(b) if b >= 0 else idiv(1, int(a) ** (-int(b)))
+
+
+def rpow(x, y):
+    try:
+        return math.pow(x, y)
+    except (ValueError, OverflowError):
+        return float("nan")
+
+
+def _libm(fn):
+    def f(*args):
+        try:
+            return fn(*args)
+        except (ValueError, OverflowError):
+            return float("nan")
+    return f
+
+
+sqrt = _libm(math.sqrt)
+exp = _libm(math.exp)
+log = _libm(math.log)
+log10 = _libm(math.log10)
+sin, cos, tan = math.sin, math.cos, math.tan
+asin = _libm(math.asin)
+acos = _libm(math.acos)
+atan = math.atan
+atan2 = math.atan2
+sinh = _libm(math.sinh)
+cosh = _libm(math.cosh)
+tanh = math.tanh
+
+
+def vec(fn):
+    """Element-wise application of a scalar libm function to an array (same C library calls as
+    the scalar case, rather than numpy's own vectorized implementations)."""
+    def f(*args):
+        return np.vectorize(lambda *v: fn(*(float(t) for t in v)), otypes=[np.float64])(*args)
+    return f
+
+
+fmod = math.fmod
+floor = math.floor
+ceil = math.ceil
+
+
+def nint(x):
+    r = math.floor(abs(x) + 0.5)
+    return int(r) if x >= 0 else -int(r)
+
+
+def sign(a, b):
+    return abs(a) if b >= 0 else -abs(a)
+
+
+def fsum(x):
+    """SUM of an array: left-to-right in array-element order, as a compiler's strict loop."""
+    s = 0.0
+    for v in np.asarray(x).reshape(-1, order="F"):
+        s = s + v
+    return s
+
+
+def isum(x):
+    return int(np.asarray(x).sum())
+
+
+def fprod(x):
+    p = 1.0
+    for v in np.asarray(x).reshape(-1, order="F"):
+        p = p * v
+    return p
+
+
+def dot(a, b):
+    a = np.asarray(a).reshape(-1, order="F")
+    b = np.asarray(b).reshape(-1, order="F")
+    s = 0.0
+    for u, v in zip(a, b):
+        s = s + u * v
+    return s
+
+
+def maxval(x):
+    return np.asarray(x).max()
+
+
+def minval(x):
+    return np.asarray(x).min()
+
+
+def maxloc(x):
+    x = np.asarray(x)
+    return np.array([int(np.argmax(x.reshape(-1, order="F"))) + 1], dtype=np.int64)
+
+
+def minloc(x):
+    x = np.asarray(x)
+    return np.array([int(np.argmin(x.reshape(-1, order="F"))) + 1], dtype=np.int64)
+
+
+def r4(x):
+    """Rounding to a default-kind (binary32) REAL."""
+    if isinstance(x, np.ndarray):
+        return x.astype(np.float32).astype(np.float64)
+    return float(np.float32(x))
+
+
+def dcopy_into(dst, src):
+    """Intrinsic assignment of a derived-type value: every component copied (pointer components
+    keep their target)."""
+    for k in dst.__slots__:
+        v = getattr(src, k)
+        if isinstance(v, FArr) and not getattr(type(dst), "_ptr_" + k, False):
+            v = FArr(v.a.copy(order="F"), v.lb)
+        setattr(dst, k, v)
+    return dst
+
+
+def fstr(s, n=None):
+    return s if n is None else (s + " " * n)[:n]
+
+
+def streq(a, b):
+    return a.rstrip() == b.rstrip()
+
+
+def cons(parts, dtype):
+    out = []
+    for p in parts:
+        if isinstance(p, np.ndarray):
+            out.extend(p.reshape(-1, order="F").tolist())
+        else:
+            out.append(p)
+    return np.array(out, dtype=dtype)

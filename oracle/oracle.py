@@ -2,9 +2,12 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by the entry module's smoke() to
 verify one GPU step, and by bench.py's CPU-baseline leg. The product never imports
-it. Parity status: unpinned against a reference binary (the reference is
-Fortran and no Fortran compiler is available to build it); pinned
-by the reference drivers' known answers (tests/test_oracle.py).
+it. Parity status: pinned against the reference's own code. The reference is
+Fortran and no Fortran compiler is available to build it, so its source runs
+through oracle/f90 (a translator of the Fortran 90 subset its modules use,
+strict IEEE double arithmetic); this oracle equals those runs bit for bit
+(tests/test_reference_source.py), and the reference drivers' known answers
+hold for it (tests/test_oracle.py).
 """
 from __future__ import annotations
 

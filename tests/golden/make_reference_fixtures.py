@@ -1,0 +1,76 @@
+"""Generate the committed fixtures of the reference's own code (tests/golden/ref_*.npz).
+
+The reference is Fortran and no Fortran compiler is available, so its modules
+run through oracle/f90, which translates the subset of Fortran 90 they use and
+executes it with strict IEEE double arithmetic (see oracle/f90/__init__.py).
+Every array in these fixtures was computed by the reference's own statements:
+its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
+ranks run as threads, the three RHS sums and the Voronoi BVEVelocity. The
+tests compare the C oracle, the product's host code and (on a GPU) the
+product's kernels with them.
+
+Needs the reference's sources (oracle/f90/reference.py: REFERENCE_DIR). Run from
+the repository root:  python tests/golden/make_reference_fixtures.py
+(about three minutes; the level-3 step dominates).
+"""
+from __future__ import annotations
+
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle.f90 import reference as REF  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+DT = 0.01
+
+
+def _save(name, **arrays):
+    np.savez_compressed(OUT / f"{name}.npz", **arrays)
+    print(f"  {name}.npz")
+
+
+def _flat(prefix, d):
+    return {f"{prefix}_{k}": v for k, v in d.items()}
+
+
+def main():
+    t0 = time.time()
+    g = REF.grid(3)
+    _save("ref_grid_l3", **g)
+    # BVERK4, parity semantics (smooth 0.05 on the divided panels), three initial conditions
+    for ic, nprocs in (("rh4", 3), ("gauss", 2), ("jet", 1)):
+        r = REF.bve_rk4(2, 2, DT, nprocs=nprocs, ic=ic)
+        _save(f"ref_bverk4_{ic}_l2", nprocs=nprocs, dt=DT, steps=2, **_flat("initial", r["initial"]),
+              **_flat("final", r["final"]), totalKE=r["totalKE"], kineticEnergy=r["kineticEnergy"])
+    r = REF.bve_rk4(3, 1, DT, nprocs=4, ic="rh4")
+    _save("ref_bverk4_rh4_l3", nprocs=4, dt=DT, steps=1, **_flat("initial", r["initial"]),
+          **_flat("final", r["final"]), totalKE=r["totalKE"], kineticEnergy=r["kineticEnergy"])
+    # StratosphereRK4 across the forcing's ramp (t = 3.95 .. 4.05)
+    s = REF.strat_rk4(2, 2, 3.95, 0.05, nprocs=2)
+    _save("ref_strat_l2", nprocs=2, t0=3.95, dt=0.05, steps=2, **_flat("initial", s["initial"]),
+          **_flat("final", s["final"]))
+    # the three RHS sums on partial ranges (one rank's share) and the Voronoi sum
+    st = REF.initial_state(2, "rh4")
+    xA, zA, aA, xV, xQ = st["xA"], st["zetaA"], st["areaA"], st["xV"], st["xQ"]
+    dxa, dva = REF.rhs(0, None, xA, zA, aA, 37, 211)
+    dxv, _ = REF.rhs(1, xV, xA, zA, aA, 11, 150)
+    dxq, _ = REF.rhs(2, xQ, xA, zA, aA, 0, len(xQ))
+    rng = np.random.default_rng(2)
+    dy0, dz0 = rng.standard_normal(len(zA)), rng.standard_normal(len(zA))
+    vor = REF.voronoi_velocity(xA[:, 0], xA[:, 1], xA[:, 2], zA, aA, 50, 300, dy=dy0, dz=dz0)
+    _save("ref_rhs_l2", xA=xA, zetaA=zA, areaA=aA, xV=xV, xQ=xQ,
+          active_range=np.array([37, 211]), vertex_range=np.array([11, 150]),
+          active_dX=dxa, active_dVort=dva, vertex_dX=dxv, passive_dX=dxq,
+          voronoi_range=np.array([50, 300]), voronoi_dy0=dy0, voronoi_dz0=dz0,
+          voronoi_dx=vor[0], voronoi_dy=vor[1], voronoi_dz=vor[2], voronoi_dVort=vor[3])
+    print(f"done in {time.time() - t0:.0f} s")
+
+
+if __name__ == "__main__":
+    main()
