@@ -61,9 +61,38 @@ class Runner:
     def __init__(self, files, entry_points, includes=None, host_procs=(), stubs=None):
         self.prog = Program(files, includes=includes, host_procs=host_procs, stubs=stubs)
         self.source = self.prog.generate([(m.lower(), p.lower()) for m, p in entry_points])
-        ns: dict = {}
-        exec(compile(self.source, "<fortran-subset>", "exec"), ns)
-        self._build = ns["_build"]
+        self._build = _compile(self.source, "<fortran-subset>")
 
     def instance(self, host=None) -> Instance:
         return Instance(*self._build(rt, host or {}))
+
+    def save(self, path, note=""):
+        """Write the generated program (for a machine without the Fortran sources: the
+        translation is to the sources what a build is, and stays out of version control)."""
+        with open(path, "w") as f:
+            f.write("# Generated by oracle/f90 from Fortran sources; a build output, not committed.\n")
+            if note:
+                f.write(f"# {note}\n")
+            f.write(self.source)
+
+
+class Program_:
+    """A generated program loaded back from a file written by Runner.save."""
+
+    def __init__(self, path):
+        with open(path) as f:
+            self.source = f.read()
+        self._build = _compile(self.source, str(path))
+
+    def instance(self, host=None) -> Instance:
+        return Instance(*self._build(rt, host or {}))
+
+
+def load(path) -> Program_:
+    return Program_(path)
+
+
+def _compile(source, name):
+    ns: dict = {}
+    exec(compile(source, name, "exec"), ns)
+    return ns["_build"]

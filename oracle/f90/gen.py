@@ -15,7 +15,19 @@ from __future__ import annotations
 from dataclasses import dataclass
 
 from .lex import FortranSubsetError
-from .parse import BodyParser, Var, VType, read_module_file
+from .parse import BodyParser, Module, Var, VType, read_module_file
+
+# kind parameters of the intrinsic module iso_c_binding
+C_KINDS = {"c_int": 4, "c_double": 8, "c_float": 4, "c_long": 8, "c_int32_t": 4, "c_int64_t": 8,
+           "c_size_t": 8, "c_bool": 1, "c_char": 1}
+
+
+def _iso_c_binding() -> Module:
+    m = Module("iso_c_binding", "<intrinsic module>")
+    for n, k in C_KINDS.items():
+        m.vars[n] = Var(n, VType("integer", 4), None, {"parameter"}, init=("int", k))
+    m.vars["c_null_ptr"] = Var("c_null_ptr", VType("cptr", 8), None, {"parameter"})
+    return m
 
 
 @dataclass(frozen=True)
@@ -55,7 +67,7 @@ INTRINSICS = {
     "nint", "floor", "ceiling", "sum", "product", "maxval", "minval", "maxloc", "minloc", "size",
     "lbound", "ubound", "shape", "allocated", "associated", "present", "dot_product", "trim",
     "adjustl", "len_trim", "len", "huge", "tiny", "epsilon", "kind", "null", "count", "any", "all",
-    "transpose", "merge", "dfloat",
+    "transpose", "merge", "dfloat", "c_loc", "c_associated",
 }
 
 # specific (double precision) names of generic intrinsics
@@ -74,8 +86,8 @@ class Program:
     """Parsed modules and the generator state."""
 
     def __init__(self, files, includes=None, host_procs=(), stubs=None):
-        self.consts: dict = {}
-        self.mods: dict = {}
+        self.consts: dict = dict(C_KINDS)
+        self.mods: dict = {"iso_c_binding": _iso_c_binding()}
         for f in files:
             for m in read_module_file(f, self.consts):
                 self.mods[m.name] = m
@@ -107,6 +119,8 @@ class Program:
             out[n] = ("proc", mname, h)
         for n, specs in m.generics.items():
             out[n] = ("generic", [(mname, s) for s in specs])
+        for n, cp in m.cprocs.items():
+            out[n] = ("cproc", mname, cp)
         for inc in m.includes:
             if inc not in self.includes:
                 raise FortranSubsetError(f"{m.path}: include '{inc}' has no stand-in")
@@ -265,7 +279,7 @@ class Program:
         if "pointer" in v.attrs or "allocatable" in v.attrs:
             return "None"
         if v.shape:
-            if any(d in (":", "*") or d[1] == "*" for d in v.shape):
+            if any(d in (":", "*") or d[1] in ("*", ":") for d in v.shape):
                 return "None"
             g = gen or ExprGen(self, mname, {})
             bounds = ", ".join(f"({g.ex(lo)[0]}, {g.ex(hi)[0]})" for lo, hi in v.shape)
@@ -273,12 +287,13 @@ class Program:
         if v.vt.base == "type":
             tm, _ = self.typedef(v.vt.tname, mname)
             return f"T_{tm}__{v.vt.tname}()"
-        return {"real": "0.0", "integer": "0", "logical": "False", "character": "''"}[v.vt.base]
+        return {"real": "0.0", "integer": "0", "logical": "False", "character": "''",
+                "cptr": "None"}[v.vt.base]
 
     @staticmethod
     def dtype(vt: VType):
         return {"real": "_np.float64", "integer": "_np.int64", "logical": "_np.bool_",
-                "character": "object", "type": "object"}[vt.base]
+                "character": "object", "type": "object", "cptr": "object"}[vt.base]
 
     def _emit_module_inits(self):
         lines = []
@@ -349,6 +364,8 @@ class ExprGen:
             return Sym("generic", specs=e[1])
         if kind == "type":
             return Sym("type", owner=e[1], tdef=e[2])
+        if kind == "cproc":
+            return Sym("cproc", owner=e[1], tdef=e[2])
         if kind == "ambiguous":
             raise FortranSubsetError(f"'{name}' is ambiguous in module {self.mod}")
         raise FortranSubsetError(f"unknown entity kind {kind}")
@@ -358,7 +375,7 @@ class ExprGen:
             return None
         out = []
         for d in v.shape:
-            if d in (":", "*"):
+            if d in (":", "*") or d[1] == ":":
                 out.append(None)
             else:
                 lo = d[0]
@@ -570,6 +587,12 @@ class ExprGen:
             if res.shape:
                 return f"{code}.a", vt_t(res.vt, len(res.shape))
             return code, vt_t(res.vt, 0)
+        if s.cat == "cproc":
+            code, rt_, refs = self.ccall(s.tdef, args)
+            if refs:
+                raise FortranSubsetError(f"{base[1]}: by-reference scalar arguments of a C function "
+                                         "are written back only in `variable = f(...)` statements")
+            return code, rt_
         if s.cat == "host":
             return f"{s.code}({', '.join(self.obj(a)[0] if self._is_designator(a) else self.ex(a)[0] for a in args)})", T_REAL
         if s.cat in ("local", "modvar", "saved") and s.var.vt.base == "character":
@@ -652,7 +675,7 @@ class ExprGen:
         return a[0] in ("name", "comp") or (a[0] == "ref" and a[1][0] in ("name", "comp"))
 
     def _order_actuals(self, proc, args):
-        dummies = proc.header.args
+        dummies = proc.header.args if hasattr(proc, "header") else proc.args
         out = [None] * len(dummies)
         pos = 0
         for a in args:
@@ -686,6 +709,34 @@ class ExprGen:
         for dn, a in zip(proc.header.args, ordered):
             out.append(self.actual(proc.decls[dn], a))
         return ", ".join(out)
+
+    def ccall(self, cp, args):
+        """(code, result T, [actual designators of by-reference scalars]) of a call of a BIND(C)
+        procedure through the C library handed over as _host['__cdll__']."""
+        ordered = self._order_actuals(cp, args)
+        specs, refs = [], []
+        for dn, a in zip(cp.args, ordered):
+            dv = cp.decls[dn]
+            b = dv.vt.base
+            if dv.rank:
+                kind = {("real", 8): "a8", ("integer", 4): "a4"}.get((b, dv.vt.kind))
+                if kind is None:
+                    raise FortranSubsetError(f"{cp.name}: C array argument of type {b}")
+                code = self.obj(a)[0] if self._is_designator(a) else f"_rt.as_farr({self.ex(a)[0]})"
+            elif "value" in dv.attrs:
+                kind = {"integer": "i", "real": "d", "cptr": "p"}[b]
+                code = self.ex(a)[0]
+            else:
+                kind = {"integer": "ri", "real": "rd", "cptr": "rp"}[b]
+                code = self.ex(a)[0]
+                refs.append(a)
+            specs.append(f"({kind!r}, {code})")
+        res = None
+        rt_ = T_NONE
+        if cp.kind == "function":
+            res = {"integer": "i", "real": "d", "cptr": "p"}[cp.result.base]
+            rt_ = vt_t(cp.result, 0)
+        return f"_rt.ccall(_host, {cp.cname!r}, {res!r}, [{', '.join(specs)}])", rt_, refs
 
     # ---------------------------------------------------------------- operators
     def _binop(self, e):
@@ -747,6 +798,20 @@ class ExprGen:
         if name == "present":
             code, _ = self.obj(pos[0])
             return f"({code} is not None)", T_LOG
+        if name == "c_associated":
+            return f"_rt.c_associated({self.ex(pos[0])[0]})", T_LOG
+        if name == "c_loc":
+            a = pos[0]
+            if a[0] == "ref" and self._array_info(a[1]) is not None:
+                code, t = self._subscript(self._array_info(a[1]), a[2])
+                if t.rank:
+                    raise FortranSubsetError("C_LOC of an array section")
+                data, _, idx = code.partition("[")
+                return f"_rt.elem_addr({data}, ({idx[:-1]},))", T("cptr", 8)
+            code, t = self.obj(a)
+            if not t.rank:
+                raise FortranSubsetError("C_LOC of a scalar")
+            return f"_rt.arr_addr({code})", T("cptr", 8)
         if name in ("size", "lbound", "ubound", "shape"):
             dim = pos[1] if len(pos) > 1 else kw.get("dim")
             if self._is_designator(pos[0]) and (pos[0][0] != "ref" or self._array_info(pos[0][1])):
@@ -911,6 +976,9 @@ class ProcGen:
                 out.append("1" if dummy and not ({"pointer", "allocatable"} & v.attrs) else None)
             elif d == "*":
                 out.append("1")
+            elif d[1] == ":":  # assumed shape with a declared lower bound
+                lo = d[0]
+                out.append(str(lo[1]) if lo[0] == "int" else None)
             else:
                 lo = d[0]
                 out.append(str(lo[1]) if lo[0] == "int" else None)
@@ -957,7 +1025,8 @@ class ProcGen:
         for n in self.h.args:
             v = self.p.decls[n]
             s = self.g.locals[n]
-            if v.shape and all(d not in (":",) for d in v.shape) and not ({"pointer", "allocatable"} & v.attrs):
+            if v.shape and all(d != ":" and d[1] != ":" for d in v.shape) and \
+                    not ({"pointer", "allocatable"} & v.attrs):
                 if any(d == "*" or d[1] == "*" for d in v.shape):
                     if len(v.shape) != 1:
                         raise FortranSubsetError("assumed-size arrays of rank > 1")
@@ -1135,6 +1204,15 @@ class ProcGen:
 
     def assign(self, lhs, rhs):
         g = self.g
+        if rhs[0] == "ref" and rhs[1][0] == "name" and g.sym(rhs[1][1]).cat == "cproc":
+            code, rtype, refs = g.ccall(g.sym(rhs[1][1]).tdef, rhs[2])
+            if refs:
+                r = g.fresh("_c")
+                self.w(f"{r} = {code}")
+                for k, a in enumerate(refs):
+                    self.assign_code(a, f"{r}[1][{k}]")
+                self.assign_code(lhs, f"{r}[0]")
+                return
         tt = g.type_of_obj(lhs)
         rc, rt_ = g.ex(rhs)
         if lhs[0] == "ref":
@@ -1161,9 +1239,25 @@ class ProcGen:
             raise FortranSubsetError("array value assigned to a scalar")
         self.w(f"{code} = {g.convert(rc, rt_, t)}")
 
+    def assign_code(self, lhs, code):
+        """Assignment of a python value (a C result) to a scalar designator."""
+        g = self.g
+        if lhs[0] == "ref":
+            tc, _ = g._subscript(g._array_info(lhs[1]), lhs[2])
+        else:
+            tc, _ = g.obj(lhs)
+        self.w(f"{tc} = {code}")
+
     def call(self, name, args):
         g = self.g
         s = g.sym(name)
+        if s.cat == "cproc":
+            code, _, refs = g.ccall(s.tdef, args)
+            r = g.fresh("_c")
+            self.w(f"{r} = {code}")
+            for k, a in enumerate(refs):
+                self.assign_code(a, f"{r}[1][{k}]")
+            return
         if s.cat == "host":
             parts = []
             for a in args:

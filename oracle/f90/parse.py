@@ -30,6 +30,7 @@ class Toks:
         self.t = toks
         self.i = 0
         self.where = where
+        self.bind_c = None
 
     def peek(self, k=0):
         j = self.i + k
@@ -313,6 +314,7 @@ class Module:
     generics: dict = field(default_factory=dict)    # generic name -> [specific names]
     procs: dict = field(default_factory=dict)       # name -> ProcHeader
     includes: list = field(default_factory=list)
+    cprocs: dict = field(default_factory=dict)      # name -> CProc (BIND(C) interfaces)
 
 
 _TYPE_KW = ("real", "integer", "logical", "character", "complex", "double")
@@ -357,6 +359,8 @@ def parse_typespec(ts: Toks, consts) -> VType:
         ts.expect("op", "(")
         name = ts.expect("name")[1]
         ts.expect("op", ")")
+        if name == "c_ptr":  # iso_c_binding: a C address, held as an integer (None = C_NULL_PTR)
+            return VType("cptr", 8)
         return VType("type", 0, name)
     if kw == "complex":
         ts.fail("complex type outside the subset")
@@ -397,9 +401,8 @@ def parse_arrayspec(ts: Toks) -> list:
             lo = parse_expr(ts)
             if ts.accept("op", ":"):
                 if ts.at("op", ",") or ts.at("op", ")"):
-                    dims.append(":")  # assumed shape with a lower bound: not in the subset
-                    ts.fail("assumed-shape dummy with a lower bound")
-                if ts.accept("op", "*"):
+                    dims.append((lo, ":"))  # assumed shape with a lower bound
+                elif ts.accept("op", "*"):
                     dims.append((lo, "*"))
                 else:
                     dims.append((lo, parse_expr(ts)))
@@ -424,7 +427,7 @@ def parse_decl(ts: Toks, consts, where) -> list[Var]:
                 intent = "inout"
             ts.expect("op", ")")
         elif a in ("pointer", "allocatable", "save", "parameter", "optional", "target", "public",
-                   "private", "external", "intrinsic"):
+                   "private", "external", "intrinsic", "value"):
             attrs.add(a)
         else:
             ts.fail(f"attribute {a} outside the subset")
@@ -490,7 +493,64 @@ def _header(ts: Toks, consts):
         ts.expect("op", "(")
         result = ts.expect("name")[1]
         ts.expect("op", ")")
+    if ts.accept("name", "bind"):
+        ts.expect("op", "(")
+        ts.expect("name", "c")
+        cname = name
+        if ts.accept("op", ","):
+            ts.expect("name", "name")
+            ts.expect("op", "=")
+            cname = ts.expect("str")[1]
+        ts.expect("op", ")")
+        ts.bind_c = cname
     return kind, name, args, result, prefix_type
+
+
+@dataclass
+class CProc:
+    """A procedure of an interface block with BIND(C): a function of a C library."""
+    name: str
+    cname: str
+    kind: str
+    args: list
+    decls: dict
+    result: VType | None
+    where: str
+
+
+def _read_c_interfaces(path, lines, i, consts, m):
+    """Interface block without a generic name: BIND(C) procedures; returns the index of its END."""
+    while True:
+        no, text = lines[i]
+        toks = tokenize(text)
+        if toks[0] == ("name", "endinterface") or (toks[0] == ("name", "end") and len(toks) > 1
+                                                   and toks[1] == ("name", "interface")):
+            return i
+        ts = Toks(toks, f"{path}:{no}")
+        ts.bind_c = None
+        hdr = _header(ts, consts)
+        if hdr is None or ts.bind_c is None:
+            raise FortranSubsetError(f"{path}:{no}: interface bodies other than BIND(C) procedures")
+        kind, name, args, result, ptype = hdr
+        decls = {}
+        i += 1
+        while True:
+            bno, btext = lines[i]
+            bt = tokenize(btext)
+            if _is_end_of(bt, kind) or bt == [("name", "end")]:
+                break
+            if bt[0] == ("name", "import"):
+                i += 1
+                continue
+            for v in parse_decl(Toks(bt, f"{path}:{bno}"), consts, f"{path}:{bno}"):
+                decls[v.name] = v
+            i += 1
+        rtype = ptype
+        if kind == "function" and rtype is None:
+            rv = decls.get(result or name)
+            rtype = rv.vt if rv is not None else None
+        m.cprocs[name] = CProc(name, ts.bind_c, kind, args, decls, rtype, f"{path}:{no}")
+        i += 1
 
 
 def _is_end_of(text_toks, kind):
@@ -619,7 +679,8 @@ def _read_module(path, lines, i, name, consts):
             ts.next()
             gname = ts.expect("name")[1] if not ts.done() else None
             if gname is None:
-                raise FortranSubsetError(f"{where}: abstract/explicit interface blocks outside the subset")
+                i = _read_c_interfaces(path, lines, i + 1, consts, m) + 1
+                continue
             specs = []
             i += 1
             while True:

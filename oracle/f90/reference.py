@@ -16,9 +16,18 @@ oracle/f90 (nothing restated here):
     MPI_BCAST as an in-process broadcast;
   * BVEVelocity of the Voronoi solver (VoronoiVelocityParallel.f90:487-515).
 Logger and OutputWriter procedures (logging and file output) are replaced by no-ops.
+
+The same translator also runs this repository's Fortran drop-in module
+(thesiscode_b200/fortran/PanelVelocityCUDA.f90) on top of the reference's
+modules, its BIND(C) interfaces calling the library through ctypes: the module
+a Fortran driver would compile, executed against the real GPU library (no
+Fortran compiler exists on either machine). build_programs() writes both
+translations to oracle/_ref/ (a build output, git-ignored, carried to the GPU
+machine like the library), from where they load when the sources are absent.
 """
 from __future__ import annotations
 
+import ctypes
 import os
 import threading
 from functools import lru_cache
@@ -26,9 +35,12 @@ from pathlib import Path
 
 import numpy as np
 
-from . import Runner, rt
+from . import Runner, load, rt
 
 REFERENCE_DIR = Path(os.environ.get("TC_REFERENCE_DIR", "/root/reference"))
+ROOT = Path(__file__).resolve().parents[2]
+BUILD_DIR = ROOT / "oracle" / "_ref"
+SHIM = ROOT / "thesiscode_b200" / "fortran" / "PanelVelocityCUDA.f90"
 
 FILES = ("NumberKinds.f90", "SphereGeom.f90", "OutputWriter.f90", "Logger.f90", "IntegerList.f90",
          "ParticlesEdgesPanels2.f90", "VoronoiPanels.f90", "STRIPACK.f90",
@@ -39,6 +51,7 @@ PVP = "panelvelocityparallelmodule"
 PEP = "particlesedgespanelsmodule"
 TVD = "tracerandvorticitydistributionmodule"
 VVP = "voronoivelocityparallelmodule"
+PVC = "panelvelocitycudamodule"
 
 ENTRY = [(PVP, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4",
                             "setsmooth", "bveactiverhs", "bvepassiverhs", "bvesmoothvelocity")] + \
@@ -46,10 +59,17 @@ ENTRY = [(PVP, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "fi
          (TVD, "initgaussianvortexpanels"), (TVD, "initjetpanels"), (TVD, "initstratosphere"),
          (VVP, "bvevelocity")]
 
+SHIM_ENTRY = [(PVC, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4",
+                                  "setsmooth", "getsmooth", "setprecisioncuda", "resetrk4",
+                                  "loadbalance")] + \
+             [(PEP, "newgrid"), (TVD, "setomega"), (TVD, "initrh4wavepanels"),
+              (TVD, "initgaussianvortexpanels"), (TVD, "initjetpanels"), (TVD, "initstratosphere")]
+
 # mpif.h stand-in: only the names the modules use; the values are handles the host procedures
-# receive and never interpret
+# receive and never interpret (MPI_SUCCESS is 0, as in every MPI)
 MPIF = {"mpi_status_size": 6, "mpi_double_precision": 17, "mpi_integer": 7, "mpi_comm_world": 0,
-        "mpi_real": 13, "mpi_sum": 1, "mpi_logical": 6, "mpi_max": 2, "mpi_min": 3}
+        "mpi_real": 13, "mpi_sum": 1, "mpi_logical": 6, "mpi_max": 2, "mpi_min": 3, "mpi_success": 0}
+HOST_PROCS = {"mpi_bcast", "mpi_barrier", "mpi_allgatherv"}
 
 TRI_PANEL, BVE_SOLVER = 3, 61
 
@@ -62,12 +82,43 @@ def _stub(mod, proc):
     return mod == "outputwritermodule" or (mod == "loggermodule" and proc != "getlogginglevel")
 
 
+def _program(name, files, entry):
+    """The translation: generated from the sources where they are, else loaded from its build."""
+    if available():
+        return Runner(files, entry, includes={"mpif.h": MPIF}, host_procs=HOST_PROCS, stubs=_stub)
+    built = BUILD_DIR / name
+    if built.is_file():
+        return load(built)
+    raise FileNotFoundError(f"neither the reference's sources ({REFERENCE_DIR}) nor {built} exist")
+
+
 @lru_cache(maxsize=1)
-def runner() -> Runner:
+def runner():
+    """The reference's modules."""
+    return _program("f90_reference.py", [REFERENCE_DIR / f for f in FILES], ENTRY)
+
+
+@lru_cache(maxsize=1)
+def shim_runner():
+    """The Fortran drop-in module with the reference's modules it uses."""
+    return _program("f90_shim.py", [REFERENCE_DIR / f for f in FILES] + [SHIM], SHIM_ENTRY)
+
+
+def shim_built() -> bool:
+    return available() or (BUILD_DIR / "f90_shim.py").is_file()
+
+
+def build_programs() -> list:
+    """Write the translations to oracle/_ref/ (where the reference's sources are present)."""
     if not available():
-        raise FileNotFoundError(f"reference sources not found under {REFERENCE_DIR}")
-    return Runner([REFERENCE_DIR / f for f in FILES], ENTRY, includes={"mpif.h": MPIF},
-                  host_procs={"mpi_bcast", "mpi_barrier"}, stubs=_stub)
+        return []
+    BUILD_DIR.mkdir(parents=True, exist_ok=True)
+    out = []
+    for name, r in (("f90_reference.py", runner()), ("f90_shim.py", shim_runner())):
+        r.save(BUILD_DIR / name, note=f"sources: {', '.join(FILES)}" +
+               (", thesiscode_b200/fortran/PanelVelocityCUDA.f90" if "shim" in name else ""))
+        out.append(BUILD_DIR / name)
+    return out
 
 
 class _World:
@@ -88,17 +139,33 @@ class _World:
             a[...] = self.slot
         self.bar.wait()
 
+    def allgatherv(self, rank, send, scount, stype, recv, counts, displs, rtype, comm, ierr):
+        if rank == 0:
+            self.slot = {}
+        self.bar.wait()
+        self.slot[rank] = np.array(send.a.reshape(-1, order="F")[:int(scount)])
+        self.bar.wait()
+        flat = recv.a.reshape(-1, order="F")
+        for j in range(counts.a.size):
+            c, d = int(counts.a[j]), int(displs.a[j])
+            flat[d:d + c] = self.slot[j][:c]
+        if not np.shares_memory(flat, recv.a):
+            raise ValueError("MPI_ALLGATHERV receive buffer is not contiguous")
+        self.bar.wait()
 
-def _ranks(nprocs, body):
+
+def _ranks(nprocs, body, program=None, host=None):
     """Run body(instance, rank) on nprocs thread ranks; returns the per-rank results."""
-    r = runner()
+    r = program or runner()
     world = _World(nprocs)
     out, errs = [None] * nprocs, []
 
     def main(rank):
         try:
             inst = r.instance(host={"mpi_bcast": lambda *a: world.bcast(rank, *a),
-                                    "mpi_barrier": lambda *a: world.bar.wait()})
+                                    "mpi_barrier": lambda *a: world.bar.wait(),
+                                    "mpi_allgatherv": lambda *a: world.allgatherv(rank, *a),
+                                    **(host or {})})
             out[rank] = body(inst, rank)
         except BaseException as e:  # noqa: BLE001 - re-raised below
             errs.append(e)
@@ -252,3 +319,62 @@ def voronoi_velocity(x, y, z, vort, area, i0, i1, omega=2 * np.pi, dy=None, dz=N
            _f1(np.zeros(n) if dz is None else dz), rt.FArr(np.zeros(n))]
     inst.proc(VVP, "bvevelocity")(*out, _f1(x), _f1(y), _f1(z), _f1(vort), _f1(area), i0 + 1, i1)
     return tuple(o.a.copy() for o in out)
+
+
+# ----------------------------------------------------------------------------- the drop-in
+def _lib(lib_path):
+    return ctypes.CDLL(str(lib_path))
+
+
+def shim_bve_rk4(lib_path, level, steps, dt, nprocs=1, fp32c=False, ic="rh4", smooth=0.05,
+                 omega=2 * np.pi) -> dict:
+    """The drop-in module's BVERK4 (PanelVelocityCUDA.f90) on nprocs thread ranks, on the
+    reference's grid and initial condition, with the library at lib_path doing the step (one
+    context per rank; numProcs > 1 takes the sharded path with MPI_ALLGATHERV)."""
+    lib = _lib(lib_path)
+
+    def body(inst, rank):
+        inst.proc(TVD, "setomega")(omega)
+        inst.proc(PVC, "setsmooth")(smooth)
+        inst.proc(PVC, "setprecisioncuda")(bool(fp32c))
+        p, _, q = new_grid(inst, level)
+        _init(inst, ic, p, q)
+        s0 = state(p, q)
+        inst.proc(PVC, "initializempirk4")(p, q, rank, nprocs)
+        tke = []
+        for _ in range(steps):
+            inst.proc(PVC, "bverk4")(p, q, dt, rank, nprocs)
+            tke.append(float(inst.mod(PVC).totalke))
+        ke = inst.mod(PVC).kineticenergy.a.copy()
+        inst.proc(PVC, "finalizempirk4")()
+        return s0, state(p, q), tke, ke
+
+    res = _ranks(nprocs, body, shim_runner(), {"__cdll__": lib})
+    s0, s1, tke, ke = res[0]
+    return dict(initial=s0, final=s1, totalKE=np.array(tke), kineticEnergy=ke,
+                ranks=[dict(final=r[1], totalKE=np.array(r[2])) for r in res])
+
+
+def shim_strat_rk4(lib_path, level, steps, t0, dt, nprocs=1, fp32c=False, smooth=0.05,
+                   omega=2 * np.pi) -> dict:
+    """The drop-in module's StratosphereRK4 on nprocs thread ranks (every rank runs the step)."""
+    lib = _lib(lib_path)
+
+    def body(inst, rank):
+        inst.proc(TVD, "setomega")(omega)
+        inst.proc(PVC, "setsmooth")(smooth)
+        inst.proc(PVC, "setprecisioncuda")(bool(fp32c))
+        p, _, q = new_grid(inst, level)
+        _init(inst, "strat", p, q)
+        s0 = state(p, q)
+        inst.proc(PVC, "initializempirk4")(p, q, rank, nprocs)
+        t = t0
+        for _ in range(steps):
+            inst.proc(PVC, "stratosphererk4")(p, q, t, dt, rank, nprocs)
+            t = t + dt
+        inst.proc(PVC, "finalizempirk4")()
+        return s0, state(p, q)
+
+    res = _ranks(nprocs, body, shim_runner(), {"__cdll__": lib})
+    s0, s1 = res[0]
+    return dict(initial=s0, final=s1, ranks=[dict(final=r[1]) for r in res])

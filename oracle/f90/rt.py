@@ -9,6 +9,7 @@ their lower bounds kept beside them (FArr).
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
@@ -287,3 +288,58 @@ def cons(parts, dtype):
         else:
             out.append(p)
     return np.array(out, dtype=dtype)
+
+
+# --------------------------------------------------------------------------- iso_c_binding
+def c_associated(p):
+    return p is not None and p != 0
+
+
+def arr_addr(x):
+    return x.a.ctypes.data
+
+
+def elem_addr(data, idx):
+    return data.ctypes.data + sum(int(i) * st for i, st in zip(idx, data.strides))
+
+
+_CTYPES = {"i": ctypes.c_int, "d": ctypes.c_double, "p": ctypes.c_void_p}
+
+
+def ccall(host, cname, restype, args):
+    """Call a BIND(C) procedure of the C library host['__cdll__']. args: (kind, value) with kind
+    i/d/p by value, ri/rd/rp by reference (returned after the call), a8/a4 arrays of C double /
+    C int passed as the address of their first element (a temporary copy, copied back, where
+    the array is not contiguous or of another element type, as a compiler's copy-in/copy-out).
+    Returns the result, or (result, [by-reference values]) when there are any."""
+    f = getattr(host["__cdll__"], cname)
+    f.restype = _CTYPES.get(restype) if restype else None
+    cargs, refs, copies = [], [], []
+    for kind, v in args:
+        if kind in ("i", "d"):
+            cargs.append(_CTYPES[kind](v))
+        elif kind == "p":
+            cargs.append(ctypes.c_void_p(v if v else None))
+        elif kind in ("ri", "rd", "rp"):
+            c = _CTYPES[kind[1]]() if v is None else _CTYPES[kind[1]](v)
+            refs.append(c)
+            cargs.append(ctypes.byref(c))
+        elif kind in ("a8", "a4"):
+            if v is None:
+                cargs.append(ctypes.c_void_p(None))
+                continue
+            a = v.a if isinstance(v, FArr) else np.asarray(v)
+            want = np.float64 if kind == "a8" else np.int32
+            if a.dtype != want or not a.flags.f_contiguous:
+                tmp = np.asfortranarray(a, dtype=want)
+                copies.append((a, tmp))
+                a = tmp
+            cargs.append(ctypes.c_void_p(a.ctypes.data))
+        else:
+            raise ValueError(kind)
+    r = f(*cargs)
+    for a, tmp in copies:
+        a[...] = tmp
+    if not refs:
+        return r
+    return r, [c.value for c in refs]

@@ -97,3 +97,35 @@ def test_procedures_are_closed_and_public_names_match_the_reference():
     # the sharded step: one MPI_ALLGATHERV per exchange, LoadBalance rows to 0-based ranges
     assert "MPI_ALLGATHERV" in code and "tc_rk4_stage_range" in code
     assert "activePanelsIndexStart(procRank) - 1" in code
+
+
+def test_dropin_module_translates_and_runs_up_to_the_library():
+    """The module goes through the Fortran 90 subset translator (oracle/f90) together with the
+    reference's modules it uses; every public procedure exists in the translation. Without a GPU
+    its first library call (tc_device_count) fails and CheckStatus stops, as the module is
+    written to do; tests/test_fortran_shim_gpu.py runs it on the GPU."""
+    import pytest
+
+    from oracle.f90 import reference as REF
+    from oracle.f90 import rt
+
+    if not REF.shim_built():
+        pytest.skip("the drop-in's translation needs the reference's sources or its build")
+    inst = REF.shim_runner().instance(host={"__cdll__": _NoGpuLib()})
+    for name in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4", "setsmooth",
+                 "getsmooth", "resetrk4", "loadbalance"):
+        inst.proc(REF.PVC, name)
+    inst.proc(REF.PVC, "setsmooth")(0.07)
+    assert inst.proc(REF.PVC, "getsmooth")() == 0.07
+    p, _, q = REF.new_grid(inst, 1)
+    with pytest.raises(rt.FortranStop):
+        inst.proc(REF.PVC, "bverk4")(p, q, 0.01, 0, 1)
+
+
+class _NoGpuLib:
+    """A library whose every call fails, as the real one does on a machine without a GPU."""
+
+    def __getattr__(self, name):
+        def f(*args):
+            return -2
+        return f

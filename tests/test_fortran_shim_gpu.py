@@ -1,0 +1,87 @@
+"""The Fortran drop-in module itself, run against the library on the GPU.
+
+thesiscode_b200/fortran/PanelVelocityCUDA.f90 is what a reference driver
+compiles in place of PanelVelocityParallelModule. Neither machine has a
+Fortran compiler, so it runs through oracle/f90 (the translator of the
+Fortran 90 subset that also runs the reference's own modules) on top of the
+reference's ParticlesEdgesPanels / TracerAndVorticityDistributions modules,
+its BIND(C) interface calls going to libthesiscode_b200.so through ctypes
+and its MPI_ALLGATHERV to an in-process exchange between ranks run as
+threads (each rank its own library context on this GPU; no kernel of one
+rank waits for another). The reference's grid and initial condition are
+built inside the same program, exactly as a driver does before calling
+BVERK4, and the results are compared with the reference's own BVERK4 /
+StratosphereRK4 (tests/golden/ref_*.npz, PanelVelocityParallel.f90:435-919).
+
+Tolerances as in tests/test_reference_gpu.py: FP64 1e-12, FP32C 5e-7 (level
+<= 3), relative to the largest displacement (vorticity change).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.f90 import reference as REF
+from thesiscode_b200 import build
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not REF.shim_built(),
+                                 reason="the drop-in's translation is built by __graft_entry__.build() "
+                                        "where the reference's sources are present")]
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TOL = {False: 1e-12, True: 5e-7}
+
+
+def _load(name):
+    return dict(np.load(GOLDEN / f"{name}.npz"))
+
+
+def _state(f, prefix):
+    n = len(prefix) + 1
+    return {k[n:]: v for k, v in f.items() if k.startswith(prefix + "_")}
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _check(run, f, tol, keys=("xA", "xV", "xQ", "zetaA")):
+    s0, s1 = _state(f, "initial"), _state(f, "final")
+    for k, v in s0.items():  # the driver-side inputs are the reference's, bit for bit
+        assert np.array_equal(run["initial"][k], v), k
+    for k in keys:
+        assert rel_err(run["final"][k] - s0[k], s1[k] - s0[k]) <= tol, k
+    assert rel_err(run["final"]["relVortV"], s1["relVortV"]) <= tol  # :651
+
+
+@pytest.mark.parametrize("fp32c", [False, True])
+def test_dropin_bverk4_one_rank(fp32c, gpu):
+    f = _load("ref_bverk4_rh4_l2")
+    run = REF.shim_bve_rk4(build.lib_path(), 2, int(f["steps"]), float(f["dt"]), nprocs=1, fp32c=fp32c)
+    _check(run, f, TOL[fp32c])
+    assert rel_err(run["totalKE"], f["totalKE"]) <= 2 * TOL[fp32c]
+    assert rel_err(run["kineticEnergy"], f["kineticEnergy"]) <= 2 * TOL[fp32c]
+
+
+@pytest.mark.parametrize("name,level,nprocs", [("ref_bverk4_rh4_l2", 2, 3), ("ref_bverk4_rh4_l3", 3, 4)])
+def test_dropin_bverk4_sharded_ranks(name, level, nprocs, gpu):
+    """numProcs > 1: each rank steps its LoadBalance rows (ragged at level 3: 642 particles on 4
+    ranks) and exchanges source rows with MPI_ALLGATHERV after every stage; all ranks end with
+    the same state, the reference's."""
+    f = _load(name)
+    run = REF.shim_bve_rk4(build.lib_path(), level, int(f["steps"]), float(f["dt"]), nprocs=nprocs)
+    _check(run, f, TOL[False])
+    assert rel_err(run["totalKE"], f["totalKE"]) <= 2 * TOL[False]
+    for r in run["ranks"][1:]:
+        for k, v in run["final"].items():
+            assert np.array_equal(r["final"][k], v), k
+        assert np.array_equal(r["totalKE"], run["totalKE"])
+
+
+@pytest.mark.parametrize("fp32c", [False, True])
+def test_dropin_stratosphere_rk4(fp32c, gpu):
+    f = _load("ref_strat_l2")
+    run = REF.shim_strat_rk4(build.lib_path(), 2, int(f["steps"]), float(f["t0"]), float(f["dt"]),
+                             nprocs=2, fp32c=fp32c)
+    _check(run, f, TOL[fp32c], keys=("xA", "xV", "xQ"))
+    assert rel_err(run["final"]["zetaA"], _state(f, "final")["zetaA"]) <= TOL[fp32c]
