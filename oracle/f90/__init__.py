@@ -58,8 +58,9 @@ class Instance:
 class Runner:
     """Parse the given source files and generate the entry points (and all they reach)."""
 
-    def __init__(self, files, entry_points, includes=None, host_procs=(), stubs=None):
-        self.prog = Program(files, includes=includes, host_procs=host_procs, stubs=stubs)
+    def __init__(self, files, entry_points, includes=None, host_procs=(), stubs=None, use_aliases=None):
+        self.prog = Program(files, includes=includes, host_procs=host_procs, stubs=stubs,
+                            use_aliases=use_aliases)
         self.source = self.prog.generate([(m.lower(), p.lower()) for m, p in entry_points])
         self._build = _compile(self.source, "<fortran-subset>")
 

@@ -85,7 +85,8 @@ _LIBM = {"exp", "log", "log10", "sin", "cos", "tan", "asin", "acos", "atan", "si
 class Program:
     """Parsed modules and the generator state."""
 
-    def __init__(self, files, includes=None, host_procs=(), stubs=None):
+    def __init__(self, files, includes=None, host_procs=(), stubs=None, use_aliases=None):
+        self.aliases = {k.lower(): v.lower() for k, v in (use_aliases or {}).items()}
         self.consts: dict = dict(C_KINDS)
         self.mods: dict = {"iso_c_binding": _iso_c_binding()}
         for f in files:
@@ -105,7 +106,8 @@ class Program:
         key = (mod, name)
         if key not in self._parsed:
             h = self.mods[mod].procs[name]
-            self._parsed[key] = BodyParser(h, self.consts).parse()
+            # a stubbed procedure needs only its interface
+            self._parsed[key] = BodyParser(h, self.consts).parse(decls_only=bool(self.stubs(mod, name)))
         return self._parsed[key]
 
     def own_entities(self, mname):
@@ -147,6 +149,7 @@ class Program:
 
     def _use_names(self, uses, out):
         for (um, only, ren) in uses:
+            um = self.aliases.get(um, um)
             if um not in self.mods:
                 raise FortranSubsetError(f"module {um} was not read")
             ex = self.exports(um)
@@ -222,8 +225,12 @@ class Program:
         while self.queue:
             mod, name = self.queue.pop(0)
             self.done[(mod, name)] = True
-            if self.stubs(mod, name):
-                h = self.mods[mod].procs[name]
+            stub = self.stubs(mod, name)
+            if stub == "raise":
+                funcs.append(f"def P_{mod}__{name}(*args, **kw):\n"
+                             f"    raise _rt.NotTranslated({mod + '::' + name!r})\n")
+                continue
+            if stub:
                 funcs.append(f"def P_{mod}__{name}(*args, **kw):\n    return None\n")
                 continue
             funcs.append(ProcGen(self, mod, self.parsed(mod, name)).emit())
@@ -252,7 +259,7 @@ class Program:
                 return
             seen.add(mn)
             for (um, _, _) in self.mods[mn].uses:
-                visit(um)
+                visit(self.aliases.get(um, um))
             order.append(mn)
 
         for mn in self.mods:
@@ -357,7 +364,7 @@ class ExprGen:
             _, owner, inc = e
             val = self.prog.includes[inc][name]
             vt = VType("integer", 4) if isinstance(val, int) else VType("real", 8)
-            return Sym("modvar", Var(name, vt), f"M_{owner}.{name}", owner=owner)
+            return Sym("modvar", Var(name, vt, None, {"parameter"}), f"M_{owner}.{name}", owner=owner)
         if kind == "proc":
             return Sym("proc", owner=e[1], var=None, specs=[(e[1], e[2].name)])
         if kind == "generic":
@@ -1103,8 +1110,8 @@ class ProcGen:
         elif k == "do":
             _, var, a, b, st, body = s
             vs = g.sym(var)
-            if vs.cat != "local" or vs.var.rank:
-                raise FortranSubsetError(f"DO variable {var} is not a local scalar")
+            if vs.cat not in ("local", "modvar", "saved") or vs.var.rank or vs.var.vt.base != "integer":
+                raise FortranSubsetError(f"DO variable {var} is not an integer scalar variable")
             lo, hi = g.fresh("_lo"), g.fresh("_hi")
             self.w(f"{lo} = {g._int(a)}; {hi} = {g._int(b)}")
             if st is None:
@@ -1141,6 +1148,37 @@ class ProcGen:
             self.w(f"raise _rt.FortranStop({s[1]!r})")
         elif k == "nop":
             self.w("pass")
+        elif k == "nml":
+            grp = s[1]
+            names = None
+            for mn in [self.mod] + [u[0] for u in self.prog.mods[self.mod].uses]:
+                names = self.prog.mods.get(mn) and self.prog.mods[mn].namelists.get(grp)
+                if names:
+                    break
+            if not names:
+                raise FortranSubsetError(f"namelist group {grp} not declared")
+            nl = g.fresh("_nl")
+            self.w(f"{nl} = _host['__namelist__'][{grp!r}]")
+            for n in names:
+                ts = g.sym(n)
+                code = ts.code
+                conv = {"integer": "int", "real": "float", "logical": "bool", "character": "str"}[ts.var.vt.base]
+                self.w(f"if {n!r} in {nl}: {code} = {conv}({nl}[{n!r}])")
+        elif k == "write":
+            unit, items = s[1], s[2]
+            if unit[0] == "str":
+                self.w("pass")
+                return
+            uc, ut = g.ex(unit)
+            if ut.base == "character":
+                self.w("pass")  # internal write: a string for logging or a file name
+                return
+            try:
+                vals = [g.ex(it)[0] for it in items]
+            except FortranSubsetError:
+                self.w("pass")
+                return
+            self.w(f"if '__write__' in _host: _host['__write__']({uc}, [{', '.join(vals)}])")
         elif k == "alloc":
             for item in s[1]:
                 self.allocate(item)
@@ -1259,12 +1297,32 @@ class ProcGen:
                 self.assign_code(a, f"{r}[1][{k}]")
             return
         if s.cat == "host":
-            parts = []
-            for a in args:
+            parts, backs = [], []
+            for k, a in enumerate(args):
                 if a[0] == "kw":
                     raise FortranSubsetError("keyword argument to an external procedure")
-                parts.append(g.obj(a)[0] if g._is_designator(a) else g.ex(a)[0])
-            self.w(f"{s.code}({', '.join(parts)})")
+                if g._is_designator(a):
+                    code, t = g.obj(a)
+                    parts.append(code)
+                    base_sym = g.sym(a[1]) if a[0] == "name" else None
+                    constant = base_sym is not None and (base_sym.var is None or
+                                                         "parameter" in base_sym.var.attrs)
+                    if not t.rank and t.base in ("integer", "real", "logical") and not constant:
+                        backs.append((k, a))
+                else:
+                    parts.append(g.ex(a)[0])
+            r = g.fresh("_h")
+            self.w(f"{r} = {s.code}({', '.join(parts)})")
+            if backs:
+                # an external procedure may return one value per argument (_NO: unchanged)
+                self.w(f"if {r} is not None:")
+                self.ind += 1
+                for k, a in backs:
+                    self.w(f"if {r}[{k}] is not _NO:")
+                    self.ind += 1
+                    self.assign_code(a, f"{r}[{k}]")
+                    self.ind -= 1
+                self.ind -= 1
             return
         if s.cat not in ("proc", "generic"):
             raise FortranSubsetError(f"CALL of {name} ({s.cat})")

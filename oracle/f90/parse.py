@@ -315,6 +315,8 @@ class Module:
     procs: dict = field(default_factory=dict)       # name -> ProcHeader
     includes: list = field(default_factory=list)
     cprocs: dict = field(default_factory=dict)      # name -> CProc (BIND(C) interfaces)
+    namelists: dict = field(default_factory=dict)   # group -> [variable names] (programs)
+    is_program: bool = False
 
 
 _TYPE_KW = ("real", "integer", "logical", "character", "complex", "double")
@@ -575,9 +577,80 @@ def read_module_file(path, consts) -> list[Module]:
         if toks[:1] == [("name", "module")] and len(toks) == 2:
             m, i = _read_module(path, lines, i, toks[1][1], consts)
             mods.append(m)
+        elif toks[:1] == [("name", "program")] and len(toks) == 2:
+            m, i = _read_program(path, lines, i, toks[1][1], consts)
+            mods.append(m)
         else:
             i += 1
     return mods
+
+
+def _read_program(path, lines, i, name, consts):
+    """A main program as a module: its declarations become the module's variables (so a caller
+    can read them after the run), its NAMELIST groups are recorded, and its executable part is
+    the module's procedure `main`."""
+    m = Module(name, str(path))
+    m.is_program = True
+    start_no = lines[i][0]
+    i += 1
+    while i < len(lines):
+        no, text = lines[i]
+        toks = tokenize(text)
+        ts = Toks(toks, f"{path}:{no}")
+        head = toks[0]
+        if head == ("name", "use"):
+            ts.next()
+            mod = ts.expect("name")[1]
+            only = None
+            if ts.accept("op", ","):
+                ts.expect("name", "only")
+                ts.expect("op", ":")
+                only = []
+                while not ts.done():
+                    only.append(ts.expect("name")[1])
+                    ts.accept("op", ",")
+            m.uses.append((mod, only, {}))
+        elif head == ("name", "implicit"):
+            pass
+        elif head == ("name", "include"):
+            m.includes.append(toks[1][1])
+        elif head == ("name", "namelist"):
+            ts.next()
+            while not ts.done():
+                ts.expect("op", "/")
+                grp = ts.expect("name")[1]
+                ts.expect("op", "/")
+                names = []
+                while ts.at("name"):
+                    names.append(ts.next()[1])
+                    if not ts.accept("op", ","):
+                        break
+                m.namelists[grp] = names
+        elif _is_decl(ts):
+            for v in parse_decl(ts, consts, f"{path}:{no}"):
+                m.vars[v.name] = v
+                if "parameter" in v.attrs and v.vt.base == "integer" and v.init is not None:
+                    try:
+                        consts[v.name] = _const_int(v.init, consts)
+                    except FortranSubsetError:
+                        pass
+        else:
+            break
+        i += 1
+    body = []
+    while i < len(lines):
+        no, text = lines[i]
+        toks = tokenize(text)
+        if toks[0] == ("name", "endprogram") or (toks[0] == ("name", "end") and
+                                                 (len(toks) == 1 or toks[1] == ("name", "program"))):
+            m.procs["main"] = ProcHeader("main", "subroutine", [], None, None, name, body, str(path),
+                                         start_no)
+            return m, i + 1
+        if toks[0] == ("name", "contains"):
+            raise FortranSubsetError(f"{path}:{no}: internal procedures of a program outside the subset")
+        body.append((no, text))
+        i += 1
+    raise FortranSubsetError(f"{path}: program {name} not terminated")
 
 
 def _read_module(path, lines, i, name, consts):
@@ -749,7 +822,7 @@ class BodyParser:
     def where(self, no):
         return f"{self.h.path}:{no}"
 
-    def parse(self) -> Proc:
+    def parse(self, decls_only=False) -> Proc:
         global _KINDS
         _KINDS = self.consts
         decls, uses = {}, []
@@ -779,6 +852,8 @@ class BodyParser:
             else:
                 break
             self.i += 1
+        if decls_only:
+            return Proc(self.h, decls, None, uses)
         body = self.block(())
         return Proc(self.h, decls, body, uses)
 
@@ -909,9 +984,26 @@ class BodyParser:
             return ("stop", text)
         if w == "continue" and len(toks) == 1:
             return ("nop", text)
-        if w in ("print", "write", "read", "open", "close", "format", "flush") and not is_assign:
+        if w in ("print", "write", "read", "open", "close", "format", "flush", "rewind", "inquire") \
+                and not is_assign:
             if w == "read":
-                ts.fail("READ outside the subset")
+                # READ(unit, NML=group): the group's values come from the caller
+                ts.next()
+                ts.expect("op", "(")
+                depth, grp = 1, None
+                while depth and not ts.done():
+                    k, v = ts.next()
+                    if k == "name" and v == "nml" and ts.accept("op", "="):
+                        grp = ts.expect("name")[1]
+                    elif k == "op" and v == "(":
+                        depth += 1
+                    elif k == "op" and v == ")":
+                        depth -= 1
+                if grp is None or not ts.done():
+                    ts.fail("READ other than a NAMELIST read outside the subset")
+                return ("nml", grp)
+            if w == "write":
+                return self._write(ts, text)
             return ("nop", text)
         if w == "call" and not is_assign:
             ts.next()
@@ -947,6 +1039,47 @@ class BodyParser:
                 ts.fail(f"unexpected {ts.peek()[1]!r} after assignment")
             return ("assign", lhs, rhs)
         ts.fail(f"statement outside the subset: {text}")
+
+    @staticmethod
+    def _write(ts, text):
+        """WRITE(unit, fmt) items: ('write', unit, [items]); the caller may collect what is written
+        to external units. A list it cannot read (implied DO) is output only: ('nop', text)."""
+        save = ts.i
+        try:
+            ts.next()
+            ts.expect("op", "(")
+            unit = None
+            first = True
+            while True:
+                if ts.at("name") and ts.at("op", "=", 1):
+                    key = ts.next()[1]
+                    ts.next()
+                    e = ts.accept("op", "*") and ("str", "*") or parse_expr(ts)
+                    if key == "unit":
+                        unit = e
+                elif ts.accept("op", "*"):
+                    e = ("str", "*")
+                    if first:
+                        unit = e
+                else:
+                    e = parse_expr(ts)
+                    if first:
+                        unit = e
+                first = False
+                if ts.accept("op", ")"):
+                    break
+                ts.expect("op", ",")
+            items = []
+            while not ts.done():
+                items.append(parse_expr(ts))
+                if not ts.accept("op", ","):
+                    break
+            if not ts.done():
+                raise FortranSubsetError("write list")
+            return ("write", unit, items)
+        except FortranSubsetError:
+            ts.i = save
+            return ("nop", text)
 
     @staticmethod
     def _assignment_shape(toks):

@@ -30,6 +30,7 @@ from __future__ import annotations
 import ctypes
 import os
 import threading
+import time
 from functools import lru_cache
 from pathlib import Path
 
@@ -69,7 +70,14 @@ SHIM_ENTRY = [(PVC, p) for p in ("bverk4", "stratosphererk4", "initializempirk4"
 # receive and never interpret (MPI_SUCCESS is 0, as in every MPI)
 MPIF = {"mpi_status_size": 6, "mpi_double_precision": 17, "mpi_integer": 7, "mpi_comm_world": 0,
         "mpi_real": 13, "mpi_sum": 1, "mpi_logical": 6, "mpi_max": 2, "mpi_min": 3, "mpi_success": 0}
-HOST_PROCS = {"mpi_bcast", "mpi_barrier", "mpi_allgatherv"}
+HOST_PROCS = {"mpi_bcast", "mpi_barrier", "mpi_allgatherv", "mpi_init", "mpi_finalize",
+              "mpi_comm_size", "mpi_comm_rank", "mpi_wtime"}
+
+# the reference's Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) and the module it is switched
+# to by its one `use` line
+DRIVER = "RHWavePanelsMPI.f90"
+DRV = "rhwavepanelsmpi"
+DRIVER_ALIASES = {"panelvelocityparallelmodule": PVC}
 
 TRI_PANEL, BVE_SOLVER = 3, 61
 
@@ -82,10 +90,21 @@ def _stub(mod, proc):
     return mod == "outputwritermodule" or (mod == "loggermodule" and proc != "getlogginglevel")
 
 
-def _program(name, files, entry):
+def _driver_stub(mod, proc):
+    """The driver's run leaves out remeshing (out of scope; raises if reached) and VTK / statistics
+    output (no-ops)."""
+    if mod == "refineremeshmodule":
+        return "raise"
+    if mod == PEP and (proc.startswith("vtkoutput") or proc.startswith("print")):
+        return True
+    return _stub(mod, proc)
+
+
+def _program(name, files, entry, stubs=_stub, aliases=None):
     """The translation: generated from the sources where they are, else loaded from its build."""
     if available():
-        return Runner(files, entry, includes={"mpif.h": MPIF}, host_procs=HOST_PROCS, stubs=_stub)
+        return Runner(files, entry, includes={"mpif.h": MPIF}, host_procs=HOST_PROCS, stubs=stubs,
+                      use_aliases=aliases)
     built = BUILD_DIR / name
     if built.is_file():
         return load(built)
@@ -104,8 +123,23 @@ def shim_runner():
     return _program("f90_shim.py", [REFERENCE_DIR / f for f in FILES] + [SHIM], SHIM_ENTRY)
 
 
+@lru_cache(maxsize=2)
+def driver_runner(cuda: bool):
+    """The reference's RH4 driver program, with `use PanelVelocityParallelModule` as written
+    (cuda False) or switched to the drop-in module (cuda True)."""
+    files = [REFERENCE_DIR / f for f in FILES] + [REFERENCE_DIR / "RefineRemesh.f90", REFERENCE_DIR / DRIVER]
+    if cuda:
+        return _program("f90_driver_cuda.py", files + [SHIM], [(DRV, "main"), (PVC, "setprecisioncuda")],
+                        _driver_stub, DRIVER_ALIASES)
+    return _program("f90_driver.py", files, [(DRV, "main")], _driver_stub)
+
+
 def shim_built() -> bool:
     return available() or (BUILD_DIR / "f90_shim.py").is_file()
+
+
+def driver_built() -> bool:
+    return available() or (BUILD_DIR / "f90_driver_cuda.py").is_file()
 
 
 def build_programs() -> list:
@@ -114,9 +148,12 @@ def build_programs() -> list:
         return []
     BUILD_DIR.mkdir(parents=True, exist_ok=True)
     out = []
-    for name, r in (("f90_reference.py", runner()), ("f90_shim.py", shim_runner())):
-        r.save(BUILD_DIR / name, note=f"sources: {', '.join(FILES)}" +
-               (", thesiscode_b200/fortran/PanelVelocityCUDA.f90" if "shim" in name else ""))
+    for name, r, extra in (("f90_reference.py", runner(), ""),
+                           ("f90_shim.py", shim_runner(), ", thesiscode_b200/fortran/PanelVelocityCUDA.f90"),
+                           ("f90_driver_cuda.py", driver_runner(True),
+                            f", RefineRemesh.f90, {DRIVER} (use switched to the drop-in), "
+                            "thesiscode_b200/fortran/PanelVelocityCUDA.f90")):
+        r.save(BUILD_DIR / name, note=f"sources: {', '.join(FILES)}{extra}")
         out.append(BUILD_DIR / name)
     return out
 
@@ -139,6 +176,9 @@ class _World:
             a[...] = self.slot
         self.bar.wait()
 
+    def barrier(self):
+        self.bar.wait()
+
     def allgatherv(self, rank, send, scount, stype, recv, counts, displs, rtype, comm, ierr):
         if rank == 0:
             self.slot = {}
@@ -155,17 +195,24 @@ class _World:
 
 
 def _ranks(nprocs, body, program=None, host=None):
-    """Run body(instance, rank) on nprocs thread ranks; returns the per-rank results."""
+    """Run body(instance, rank) on nprocs thread ranks; returns the per-rank results. host: extra
+    host entries, or a function of the rank giving them."""
     r = program or runner()
     world = _World(nprocs)
     out, errs = [None] * nprocs, []
 
     def main(rank):
         try:
+            extra = host(rank) if callable(host) else (host or {})
             inst = r.instance(host={"mpi_bcast": lambda *a: world.bcast(rank, *a),
-                                    "mpi_barrier": lambda *a: world.bar.wait(),
+                                    "mpi_barrier": lambda *a: world.barrier(),
                                     "mpi_allgatherv": lambda *a: world.allgatherv(rank, *a),
-                                    **(host or {})})
+                                    "mpi_init": lambda *a: None,
+                                    "mpi_finalize": lambda *a: None,
+                                    "mpi_comm_size": lambda comm, n, ierr: (rt.NO, nprocs, 0),
+                                    "mpi_comm_rank": lambda comm, k, ierr: (rt.NO, rank, 0),
+                                    "mpi_wtime": time.perf_counter,
+                                    **extra})
             out[rank] = body(inst, rank)
         except BaseException as e:  # noqa: BLE001 - re-raised below
             errs.append(e)
@@ -378,3 +425,35 @@ def shim_strat_rk4(lib_path, level, steps, t0, dt, nprocs=1, fp32c=False, smooth
     res = _ranks(nprocs, body, shim_runner(), {"__cdll__": lib})
     s0, s1 = res[0]
     return dict(initial=s0, final=s1, ranks=[dict(final=r[1]) for r in res])
+
+
+# ----------------------------------------------------------------------------- the driver
+def run_driver(nprocs, namelist, cuda=False, lib_path=None, fp32c=False) -> dict:
+    """The reference's RH4 driver program (RHWavePanelsMPI.f90) on nprocs thread ranks, its
+    namelist groups (gridinit, time, fileio) given as dicts, with its own
+    PanelVelocityParallelModule (cuda False) or with its `use` line switched to the drop-in
+    module and the library at lib_path (cuda True). Returns what rank 0 writes to the data file
+    (per step: totalKE, enstrophy, relVort l1, l2, linf error against the steady wave), as an
+    array, and every rank's rows."""
+    prog = driver_runner(bool(cuda))
+    lib = _lib(lib_path) if cuda else None
+    written = [[] for _ in range(nprocs)]
+
+    def host(rank):
+        h = {"__namelist__": {k.lower(): {n.lower(): v for n, v in g.items()} for k, g in namelist.items()},
+             "__write__": lambda unit, vals: written[rank].append((int(unit), list(vals)))}
+        if lib is not None:
+            h["__cdll__"] = lib
+        return h
+
+    def body(inst, rank):
+        if cuda:
+            inst.proc(PVC, "setprecisioncuda")(bool(fp32c))
+        inst.proc(DRV, "main")()
+        return None
+
+    _ranks(nprocs, body, prog, host)
+    data_unit = 13  # writeUnit of the driver
+    rows = [[float(v) for v in vals] for unit, vals in written[0]
+            if unit == data_unit and vals and not isinstance(vals[0], str)]
+    return dict(rows=np.array(rows), written=written)

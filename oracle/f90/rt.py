@@ -19,6 +19,10 @@ class FortranStop(Exception):
     """A STOP statement was executed."""
 
 
+class NotTranslated(Exception):
+    """A procedure left out of the translation was called."""
+
+
 class NS:
     """Namespace of one module's variables (or one procedure's saved locals)."""
 

@@ -5,7 +5,9 @@ run through oracle/f90, which translates the subset of Fortran 90 they use and
 executes it with strict IEEE double arithmetic (see oracle/f90/__init__.py).
 Every array in these fixtures was computed by the reference's own statements:
 its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
-ranks run as threads, the three RHS sums and the Voronoi BVEVelocity. The
+ranks run as threads, the three RHS sums, the Voronoi BVEVelocity, and its
+Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) with the rows it writes
+to its data file. The
 tests compare the C oracle, the product's host code and (on a GPU) the
 product's kernels with them.
 
@@ -69,7 +71,19 @@ def main():
           active_dX=dxa, active_dVort=dva, vertex_dX=dxv, passive_dX=dxq,
           voronoi_range=np.array([50, 300]), voronoi_dy0=dy0, voronoi_dz0=dz0,
           voronoi_dx=vor[0], voronoi_dy=vor[1], voronoi_dz=vor[2], voronoi_dVort=vor[3])
+    # the reference's RH4 driver program (RHWavePanelsMPI.f90) on two ranks: its data-file rows
+    nl = driver_namelist()
+    d = REF.run_driver(2, nl)
+    _save("ref_driver_rh4_l2", rows=d["rows"], nprocs=2, initNest=nl["gridInit"]["initNest"],
+          dt=nl["time"]["dt"], tfinal=nl["time"]["tfinal"])
     print(f"done in {time.time() - t0:.0f} s")
+
+
+def driver_namelist():
+    """Namelist groups of the driver run (RHWavePanels.namelist's layout, level 2, three steps; no
+    remeshing within the run)."""
+    return {"gridInit": dict(panelKind=3, initNest=2, AMR=0, remeshInterval=1000, amrTol1=1.0, amrTol2=1.0),
+            "time": dict(dt=0.01, tfinal=0.03), "fileIO": dict(jobPrefix="rh4", outputDir="./")}
 
 
 if __name__ == "__main__":

@@ -85,3 +85,30 @@ def test_dropin_stratosphere_rk4(fp32c, gpu):
                              nprocs=2, fp32c=fp32c)
     _check(run, f, TOL[fp32c], keys=("xA", "xV", "xQ"))
     assert rel_err(run["final"]["zetaA"], _state(f, "final")["zetaA"]) <= TOL[fp32c]
+
+
+def _driver_namelist(f):
+    return {"gridInit": dict(panelKind=3, initNest=int(f["initNest"]), AMR=0, remeshInterval=1000,
+                             amrTol1=1.0, amrTol2=1.0),
+            "time": dict(dt=float(f["dt"]), tfinal=float(f["tfinal"])),
+            "fileIO": dict(jobPrefix="rh4", outputDir="./")}
+
+
+@pytest.mark.skipif(not REF.driver_built(), reason="the driver's translation is built by "
+                    "__graft_entry__.build() where the reference's sources are present")
+@pytest.mark.parametrize("nprocs,fp32c", [(1, False), (2, False), (1, True)])
+def test_reference_driver_with_its_use_line_switched(nprocs, fp32c, gpu):
+    """The reference's RH4 driver program (RHWavePanelsMPI.f90) unmodified except for
+    `use PanelVelocityParallelModule` -> `use PanelVelocityCUDAModule`: namelist in, grid and
+    initial condition built by the driver, BVERK4 each step on the GPU, and the rows it writes to
+    its data file (totalKE, enstrophy, relVort l1 / l2 / linf error against the steady wave) equal
+    those of the unmodified driver (tests/golden/ref_driver_rh4_l2.npz). The error norms are
+    differences of vorticities: compared to an absolute 10x the vorticity tolerance."""
+    f = _load("ref_driver_rh4_l2")
+    run = REF.run_driver(nprocs, _driver_namelist(f), cuda=True, lib_path=build.lib_path(), fp32c=fp32c)
+    rows, ref = run["rows"], f["rows"]
+    assert rows.shape == ref.shape
+    tol = TOL[fp32c]
+    assert rel_err(rows[:, 0], ref[:, 0]) <= 2 * tol      # totalKE
+    assert rel_err(rows[:, 1], ref[:, 1]) <= 2 * tol      # enstrophy
+    assert np.abs(rows[:, 2:] - ref[:, 2:]).max() <= 10 * tol
