@@ -614,10 +614,18 @@ def run_ours(args):
             cb = cpu_baseline(wo, frac=frac, threads=threads)
             line["cpu_baseline"] = {"value": cb["value"], "unit": "interactions/s", "cores": cb["cores"],
                                     "kind": "port", "sample": cb["sample"], "seconds": cb["seconds"],
-                                    "build": cb["build"], "inputs": "oracle grid (oracle/icos_oracle.c)"}
+                                    "build": cb["build"], "inputs": "oracle grid (oracle/icos_oracle.c)",
+                                    "pinned": PORT_PINNED}
             line["error_vs_fp64_oracle"] = error_sample(wo, device, threads)
         print(json.dumps(line), flush=True)
     main["ctx"].close() if driver is None else driver.close()
+
+
+# what ties the timed C port to the reference: its strict build equals, bit for bit, the
+# reference's own Fortran statements run through the Fortran 90 subset translator (oracle/f90)
+PORT_PINNED = ("strict build equal bit for bit to the reference's own Fortran source (grid, initial "
+               "conditions, BVERK4 on 1-5 MPI ranks, StratosphereRK4, the sums) run through oracle/f90; "
+               "the timed build agrees with the strict one to 1e-12")
 
 
 def repo_libraries() -> list[str]:
@@ -654,7 +662,7 @@ def run_reference(args):
             "config": workload_config(w, "fp64 (CPU)", "host cores"),
             "cpu_baseline": {"value": v, "unit": "interactions/s", "cores": threads, "kind": "port",
                              "sample": cb["sample"] + "; each step one such sample, rate extrapolated linearly",
-                             "build": cb["build"]},
+                             "build": cb["build"], "pinned": PORT_PINNED},
             "e2e": {"value": v, "unit": "interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference is Fortran+MPI (ifort -O2, mpif90); no Fortran compiler or MPI exists on "
                     "these machines, so the arm runs the C restatement of its loops (oracle/), compiled with "
