@@ -14,8 +14,10 @@ oracle/f90 (nothing restated here):
   * InitializeMPIRK4 / LoadBalance / BVERK4 / StratosphereRK4 and the three RHS sums
     (PanelVelocityParallel.f90:126-213,435-919,1287-1412), with MPI ranks as threads and
     MPI_BCAST as an in-process broadcast;
-  * BVEVelocity of the Voronoi solver (VoronoiVelocityParallel.f90:487-515).
-Logger and OutputWriter procedures (logging and file output) are replaced by no-ops.
+  * BVEVelocity and the RK4 step of BVERK4 of the Voronoi solver
+    (VoronoiVelocityParallel.f90:252-515).
+Logger and OutputWriter procedures (logging and file output) are replaced by no-ops, and so is
+the STRIPACK Delaunay / Voronoi rebuild at the end of the Voronoi BVERK4.
 
 The same translator also runs this repository's Fortran drop-in module
 (thesiscode_b200/fortran/PanelVelocityCUDA.f90) on top of the reference's
@@ -58,7 +60,8 @@ ENTRY = [(PVP, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "fi
                             "setsmooth", "bveactiverhs", "bvepassiverhs", "bvesmoothvelocity")] + \
         [(PEP, "newgrid"), (TVD, "setomega"), (TVD, "initrh4wavepanels"),
          (TVD, "initgaussianvortexpanels"), (TVD, "initjetpanels"), (TVD, "initstratosphere"),
-         (VVP, "bvevelocity")]
+         (VVP, "bvevelocity"), (VVP, "bverk4"), (VVP, "initializempirk4"), (VVP, "finalizempirk4")]
+VPM = "voronoipanelsmodule"
 
 SHIM_ENTRY = [(PVC, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4",
                                   "setsmooth", "getsmooth", "setprecisioncuda", "resetrk4",
@@ -87,6 +90,11 @@ def available() -> bool:
 
 
 def _stub(mod, proc):
+    """Logging and file output are no-ops; so is the Delaunay / Voronoi rebuild (STRIPACK) that the
+    Voronoi solver's BVERK4 calls after its step (VoronoiVelocityParallel.f90:480-482): it changes
+    the mesh for the next step, not the step's positions, vorticity or kinetic energy."""
+    if mod == "voronoipanelsmodule" and proc in ("normalizegrid", "delaunaytri", "voronoigrid"):
+        return True
     return mod == "outputwritermodule" or (mod == "loggermodule" and proc != "getlogginglevel")
 
 
@@ -366,6 +374,36 @@ def voronoi_velocity(x, y, z, vort, area, i0, i1, omega=2 * np.pi, dy=None, dz=N
            _f1(np.zeros(n) if dz is None else dz), rt.FArr(np.zeros(n))]
     inst.proc(VVP, "bvevelocity")(*out, _f1(x), _f1(y), _f1(z), _f1(vort), _f1(area), i0 + 1, i1)
     return tuple(o.a.copy() for o in out)
+
+
+def voronoi_rk4(x, y, z, relvort, area, n, dt, steps, nprocs=1, omega=2 * np.pi) -> dict:
+    """BVERK4 of the Voronoi solver (VoronoiVelocityParallel.f90:300-483) on nprocs thread ranks:
+    generators 1..n of arrays of length N_Max = len(x) (the sums run over all N_Max slots, the
+    unused ones carrying zero vorticity and area). Returns the first n positions and relVort after
+    `steps` steps and totalKE of each step."""
+    def body(inst, rank):
+        inst.proc(TVD, "setomega")(omega)
+        vp = inst.new(VPM, "vorpanels")
+        nmax = len(x)
+        vp.x, vp.y, vp.z = _f1(x), _f1(y), _f1(z)
+        vp.x0, vp.y0, vp.z0 = _f1(x), _f1(y), _f1(z)
+        vp.relvort, vp.area = _f1(relvort), _f1(area)
+        vp.absvort = _f1(np.asarray(relvort) + 2.0 * omega * np.asarray(z))
+        vp.n, vp.n_max = int(n), int(nmax)
+        inst.proc(VVP, "initializempirk4")(int(n), rank, nprocs)
+        tke = []
+        for _ in range(steps):
+            inst.proc(VVP, "bverk4")(vp, dt, rank, nprocs)
+            tke.append(float(inst.mod(VVP).totalke))
+        inst.proc(VVP, "finalizempirk4")()
+        return dict(x=vp.x.a[:n].copy(), y=vp.y.a[:n].copy(), z=vp.z.a[:n].copy(),
+                    relVort=vp.relvort.a[:n].copy(), totalKE=np.array(tke))
+
+    res = _ranks(nprocs, body)
+    for r in res[1:]:
+        if any(not np.array_equal(r[k], res[0][k]) for k in res[0]):
+            raise AssertionError("ranks disagree after the Voronoi BVERK4")
+    return res[0]
 
 
 # ----------------------------------------------------------------------------- the drop-in

@@ -5,7 +5,8 @@ run through oracle/f90, which translates the subset of Fortran 90 they use and
 executes it with strict IEEE double arithmetic (see oracle/f90/__init__.py).
 Every array in these fixtures was computed by the reference's own statements:
 its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
-ranks run as threads, the three RHS sums, the Voronoi BVEVelocity, and its
+ranks run as threads, the three RHS sums, the Voronoi BVEVelocity and
+BVERK4, and its
 Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) with the rows it writes
 to its data file. The
 tests compare the C oracle, the product's host code and (on a GPU) the
@@ -71,6 +72,12 @@ def main():
           active_dX=dxa, active_dVort=dva, vertex_dX=dxv, passive_dX=dxq,
           voronoi_range=np.array([50, 300]), voronoi_dy0=dy0, voronoi_dz0=dz0,
           voronoi_dx=vor[0], voronoi_dy=vor[1], voronoi_dz=vor[2], voronoi_dVort=vor[3])
+    # the Voronoi solver's BVERK4 on the same generators, N_Max 10 above N, two ranks
+    n, pad = len(zA), 10
+    vin = {k: np.concatenate([v, np.zeros(pad)]) for k, v in
+           (("x", xA[:, 0]), ("y", xA[:, 1]), ("z", xA[:, 2]), ("relVort", zA), ("area", aA))}
+    vr = REF.voronoi_rk4(vin["x"], vin["y"], vin["z"], vin["relVort"], vin["area"], n, DT, 2, nprocs=2)
+    _save("ref_voronoi_rk4_l2", n=n, dt=DT, steps=2, **_flat("initial", vin), **_flat("final", vr))
     # the reference's RH4 driver program (RHWavePanelsMPI.f90) on two ranks: its data-file rows
     nl = driver_namelist()
     d = REF.run_driver(2, nl)

@@ -3,8 +3,8 @@
 tests/golden/ref_*.npz hold what the reference's Fortran statements computed,
 run through oracle/f90 (tests/golden/make_reference_fixtures.py): its grid and
 initial conditions, BVERK4 and StratosphereRK4 on several MPI ranks, the
-three RHS sums on partial index ranges and the Voronoi BVEVelocity
-(PanelVelocityParallel.f90:435-919,1287-1412; VoronoiVelocityParallel.f90:487-515).
+three RHS sums on partial index ranges, and the Voronoi BVEVelocity and BVERK4
+(PanelVelocityParallel.f90:435-919,1287-1412; VoronoiVelocityParallel.f90:300-515).
 Here the library computes the same steps and sums through the C ABI, and
 through the drop-in host mirror of the reference's interface (BVERK4 on
 Particles/Panels), and is compared with them.
@@ -137,3 +137,23 @@ def test_sums_equal_reference_rhs(prec, gpu):
     for got, key in zip(out, ("voronoi_dx", "voronoi_dy", "voronoi_dz", "voronoi_dVort")):
         assert rel_err(got, f[key]) <= tol, key
     ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32c"])
+def test_voronoi_rk4_equals_reference(prec, gpu):
+    """BVERK4 of the Voronoi solver (VoronoiVelocityParallel.f90:300-483; its STRIPACK rebuild after
+    the step is the caller's) on generators 1..N of arrays of N_Max > N slots, two steps."""
+    from thesiscode_b200.voronoi_velocity import BVERK4, VorPanels
+
+    f = _load("ref_voronoi_rk4_l2")
+    s0, s1 = _state(f, "initial"), _state(f, "final")
+    n = int(f["n"])
+    vp = VorPanels(x=s0["x"].copy(), y=s0["y"].copy(), z=s0["z"].copy(), relVort=s0["relVort"].copy(),
+                   absVort=s0["relVort"] + 2 * OMEGA * s0["z"], area=s0["area"].copy(), N=n)
+    ctx = _ctx(prec)
+    tke, _ = BVERK4(ctx, vp, float(f["dt"]), int(f["steps"]))
+    ctx.close()
+    tol = TOL[prec]
+    for k in ("x", "y", "z", "relVort"):
+        assert rel_err(getattr(vp, k)[:n] - s0[k][:n], s1[k] - s0[k][:n]) <= tol, k
+    assert rel_err(tke, s1["totalKE"]) <= 2 * tol
