@@ -55,6 +55,7 @@ PEP = "particlesedgespanelsmodule"
 TVD = "tracerandvorticitydistributionmodule"
 VVP = "voronoivelocityparallelmodule"
 PVC = "panelvelocitycudamodule"
+PVS = "panelvelocityserialmodule"
 
 ENTRY = [(PVP, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4",
                             "setsmooth", "bveactiverhs", "bvepassiverhs", "bvesmoothvelocity")] + \
@@ -140,6 +141,30 @@ def driver_runner(cuda: bool):
         return _program("f90_driver_cuda.py", files + [SHIM], [(DRV, "main"), (PVC, "setprecisioncuda")],
                         _driver_stub, DRIVER_ALIASES)
     return _program("f90_driver.py", files, [(DRV, "main")], _driver_stub)
+
+
+@lru_cache(maxsize=1)
+def serial_runner():
+    """The reference's serial twin of the RK4 module (PanelVelocitySerial.f90)."""
+    return _program("f90_serial.py", [REFERENCE_DIR / f for f in FILES] +
+                    [REFERENCE_DIR / "PanelVelocitySerial.f90"],
+                    [(PVS, "bverk4"), (PVS, "resetrk4"), (PEP, "newgrid"), (TVD, "initrh4wavepanels"),
+                     (TVD, "initgaussianvortexpanels"), (TVD, "initjetpanels")])
+
+
+def serial_bve_rk4(level, steps, dt, ic="rh4") -> dict:
+    """BVERK4 of PanelVelocitySerial.f90:272-425 (one process, smooth 0.05, Omega 2 pi) from the
+    reference's grid and initial condition."""
+    inst = serial_runner().instance()
+    p, _, q = new_grid(inst, level)
+    _init(inst, ic, p, q)
+    s0 = state(p, q)
+    tke = []
+    for _ in range(steps):
+        inst.proc(PVS, "bverk4")(p, q, dt)
+        tke.append(float(inst.mod(PVS).totalke))
+    return dict(initial=s0, final=state(p, q), totalKE=np.array(tke),
+                kineticEnergy=inst.mod(PVS).kineticenergy.a.copy())
 
 
 def shim_built() -> bool:

@@ -329,3 +329,23 @@ def test_translator_refuses_constructs_outside_the_subset(tmp_path):
                    "10 x = 1\nend subroutine\nend module BadM\n")
     with pytest.raises(FortranSubsetError):
         Runner([src], [("badm", "s")])
+
+
+@needs_source
+@pytest.mark.parametrize("ic", ["rh4", "jet"])
+def test_oracle_equals_the_reference_serial_module(ic):
+    """The serial twin PanelVelocitySerial.f90:272-557 (its own copies of the three sums): the same
+    step as the parallel module, bit for bit, except that it leaves the particles' relVort as it
+    was (the parallel module's :651 update is missing from it)."""
+    r = REF.serial_bve_rk4(1, 2, 0.01, ic=ic)
+    s0, s1 = r["initial"], r["final"]
+    xV, xA, zA, xQ = s0["xV"], s0["xA"], s0["zetaA"], s0["xQ"]
+    tke = []
+    for _ in range(2):
+        xV, xA, zA, xQ, t, ke, _ = O.bve_rk4(xV, xA, zA, s0["areaA"], xQ, 0.01, 2 * np.pi, DELTAS)
+        tke.append(t)
+    for got, key in ((xV, "xV"), (xA, "xA"), (zA, "zetaA"), (xQ, "xQ")):
+        assert np.array_equal(got, s1[key]), key
+    assert np.array_equal(np.array(tke), r["totalKE"])
+    assert np.array_equal(ke, r["kineticEnergy"])
+    assert np.array_equal(s1["relVortV"], s0["relVortV"])
