@@ -6,8 +6,10 @@ modules use, with strict IEEE double arithmetic. tests/golden/ref_*.npz hold
 what the reference's statements computed (tests/golden/make_reference_fixtures.py):
 its grid generator (NewGrid, ParticlesEdgesPanels2.f90:362-397), its initial
 conditions, BVERK4 and StratosphereRK4 on 1-4 MPI ranks run as threads
-(PanelVelocityParallel.f90:435-919), the three RHS sums (:1287-1412) and the
-Voronoi BVEVelocity (VoronoiVelocityParallel.f90:487-515).
+(PanelVelocityParallel.f90:435-919), the three RHS sums (:1287-1412), the
+Voronoi BVEVelocity and BVERK4 (VoronoiVelocityParallel.f90:300-515) and the
+RH4 driver program's output; the serial twin (PanelVelocitySerial.f90) is run
+live where the sources are.
 
 Checked here, bit for bit: the C oracle (the checker of every GPU test) and
 the library's host grid generator against those fixtures; the library's
