@@ -337,6 +337,27 @@ def bve_rk4(level, steps, dt, nprocs=1, ic="rh4", smooth=0.05, omega=2 * np.pi) 
     return dict(initial=s0, final=s1, totalKE=np.array(tke), kineticEnergy=ke)
 
 
+def final_active_vorticity(level, steps, dt, xA, zetaA, ic="rh4", omega=2 * np.pi) -> np.ndarray:
+    """BVERK4 (one rank) from the reference's grid and initial condition with the active panels'
+    positions and vorticity replaced by xA, zetaA (the inputs of a finite difference); returns the
+    active panels' vorticity after `steps` steps."""
+    def body(inst, rank):
+        inst.proc(TVD, "setomega")(omega)
+        p, _, q = new_grid(inst, level)
+        _init(inst, ic, p, q)
+        act = np.nonzero(~q.haschildren.a[:q.n].astype(bool))[0]
+        q.x.a[:, act] = np.asarray(xA).T
+        q.relvort.a[act] = zetaA
+        inst.proc(PVP, "initializempirk4")(p, q, rank, 1)
+        for _ in range(steps):
+            inst.proc(PVP, "bverk4")(p, q, dt, rank, 1)
+        out = q.relvort.a[act].copy()
+        inst.proc(PVP, "finalizempirk4")()
+        return out
+
+    return _ranks(1, body)[0]
+
+
 def strat_rk4(level, steps, t0, dt, nprocs=1, smooth=0.05, omega=2 * np.pi) -> dict:
     """StratosphereRK4 (PanelVelocityParallel.f90:661-919): the forced model's step, from the
     reference's stratosphere initial condition (InitStratosphere)."""

@@ -6,7 +6,7 @@ executes it with strict IEEE double arithmetic (see oracle/f90/__init__.py).
 Every array in these fixtures was computed by the reference's own statements:
 its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
 ranks run as threads, the three RHS sums, the Voronoi BVEVelocity and
-BVERK4, and its
+BVERK4, finite differences of the enstrophy through its BVERK4, and its
 Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) with the rows it writes
 to its data file. The
 tests compare the C oracle, the product's host code and (on a GPU) the
@@ -78,12 +78,43 @@ def main():
            (("x", xA[:, 0]), ("y", xA[:, 1]), ("z", xA[:, 2]), ("relVort", zA), ("area", aA))}
     vr = REF.voronoi_rk4(vin["x"], vin["y"], vin["z"], vin["relVort"], vin["area"], n, DT, 2, nprocs=2)
     _save("ref_voronoi_rk4_l2", n=n, dt=DT, steps=2, **_flat("initial", vin), **_flat("final", vr))
+    # centred finite differences of J = sum zeta(T)^2 A through the reference's BVERK4 (level 1,
+    # three steps): the final active vorticity for each +/- perturbation of 16 seeded entries
+    _save("ref_fd_rh4_l1", **fd_inputs())
     # the reference's RH4 driver program (RHWavePanelsMPI.f90) on two ranks: its data-file rows
     nl = driver_namelist()
     d = REF.run_driver(2, nl)
     _save("ref_driver_rh4_l2", rows=d["rows"], nprocs=2, initNest=nl["gridInit"]["initNest"],
           dt=nl["time"]["dt"], tfinal=nl["time"]["tfinal"])
     print(f"done in {time.time() - t0:.0f} s")
+
+
+def fd_inputs(level=1, steps=3, dt=0.01, eps=1e-6, entries=16, seed=33):
+    """Perturbed initial states: even entries move one panel's vorticity by +/- eps, odd entries one
+    panel's position along a seeded tangent direction, renormalised to the sphere."""
+    st = REF.initial_state(level, "rh4")
+    xA, zA = st["xA"], st["zetaA"]
+    rng = np.random.default_rng(seed)
+    picks = rng.choice(len(zA), entries, replace=False)
+    tangents = np.zeros((entries, 3))
+    fp, fm = [], []
+    for m, j in enumerate(picks):
+        xp, xm, zp, zm = xA.copy(), xA.copy(), zA.copy(), zA.copy()
+        if m % 2 == 0:
+            zp[j] += eps
+            zm[j] -= eps
+        else:
+            t = rng.standard_normal(3)
+            t -= t.dot(xA[j]) * xA[j]
+            t /= np.linalg.norm(t)
+            tangents[m] = t
+            xp[j] = (xA[j] + eps * t) / np.linalg.norm(xA[j] + eps * t)
+            xm[j] = (xA[j] - eps * t) / np.linalg.norm(xA[j] - eps * t)
+        fp.append(REF.final_active_vorticity(level, steps, dt, xp, zp))
+        fm.append(REF.final_active_vorticity(level, steps, dt, xm, zm))
+    return dict(xA=xA, zetaA=zA, areaA=st["areaA"], picks=picks, tangents=tangents, eps=eps,
+                dt=dt, steps=steps, zeta_plus=np.array(fp), zeta_minus=np.array(fm),
+                zeta_final=REF.final_active_vorticity(level, steps, dt, xA, zA))
 
 
 def driver_namelist():
