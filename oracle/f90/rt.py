@@ -82,11 +82,6 @@ def as_farr(v):
     return v if isinstance(v, FArr) else FArr(np.asarray(v))
 
 
-def section(x, sl):
-    """View of an array section (lower bounds 1)."""
-    return FArr(x.a[sl])
-
-
 def sl(lo, hi, st, lb, ext):
     """Python slice of the Fortran triplet lo:hi:st on a dimension with lower bound lb and
     extent ext (lo/hi None = the bound)."""
@@ -274,10 +269,6 @@ def dcopy_into(dst, src):
             v = FArr(v.a.copy(order="F"), v.lb)
         setattr(dst, k, v)
     return dst
-
-
-def fstr(s, n=None):
-    return s if n is None else (s + " " * n)[:n]
 
 
 def streq(a, b):
