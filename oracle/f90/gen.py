@@ -1032,7 +1032,7 @@ class ProcGen:
         for n in self.h.args:
             v = self.p.decls[n]
             s = self.g.locals[n]
-            if v.shape and all(d != ":" and d[1] != ":" for d in v.shape) and \
+            if v.shape and all(d != ":" and (d == "*" or d[1] != ":") for d in v.shape) and \
                     not ({"pointer", "allocatable"} & v.attrs):
                 if any(d == "*" or d[1] == "*" for d in v.shape):
                     if len(v.shape) != 1:
