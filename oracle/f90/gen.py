@@ -1165,20 +1165,44 @@ class ProcGen:
                 conv = {"integer": "int", "real": "float", "logical": "bool", "character": "str"}[ts.var.vt.base]
                 self.w(f"if {n!r} in {nl}: {code} = {conv}({nl}[{n!r}])")
         elif k == "write":
-            unit, items = s[1], s[2]
-            if unit[0] == "str":
-                self.w("pass")
-                return
-            uc, ut = g.ex(unit)
-            if ut.base == "character":
-                self.w("pass")  # internal write: a string for logging or a file name
-                return
+            unit, fmt, items = s[1], s[2], s[3]
+            if fmt[0] == "star":
+                fcode = "None"
+            elif fmt[0] == "label":
+                if fmt[1] not in self.p.formats:
+                    raise FortranSubsetError(f"{self.h.path}: FORMAT {fmt[1]} not found in {self.h.name}")
+                fcode = repr(self.p.formats[fmt[1]])
+            elif fmt[0] == "str":
+                fcode = repr(fmt[1])
+            else:
+                fcode = g.ex(fmt[1])[0]
             try:
                 vals = [g.ex(it)[0] for it in items]
             except FortranSubsetError:
                 self.w("pass")
                 return
-            self.w(f"if '__write__' in _host: _host['__write__']({uc}, [{', '.join(vals)}])")
+            if unit[0] == "star":
+                self.w(f"_rt.fwrite(_host, '*', {fcode}, [{', '.join(vals)}])")
+                return
+            uc, ut = g.ex(unit)
+            if ut.base == "character":
+                # internal write: the record becomes the variable's value; such strings only name
+                # files and label log lines, so a format outside the formatter's subset leaves it
+                r = g.fresh("_w")
+                self.w(f"{r} = _rt.fformat_or_none({fcode}, [{', '.join(vals)}])")
+                self.w(f"if {r} is not None:")
+                self.ind += 1
+                self.assign_code(unit, f"{r}[0]")
+                self.ind -= 1
+                return
+            self.w(f"_rt.fwrite(_host, {uc}, {fcode}, [{', '.join(vals)}])")
+        elif k in ("open", "close"):
+            uc = g.ex(s[1])[0] if s[1] is not None else "None"
+            if k == "open":
+                fc = g.ex(s[2])[0] if s[2] is not None else "None"
+                self.w(f"if '__open__' in _host: _host['__open__']({uc}, {fc})")
+            else:
+                self.w(f"if '__close__' in _host: _host['__close__']({uc})")
         elif k == "alloc":
             for item in s[1]:
                 self.allocate(item)

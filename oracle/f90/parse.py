@@ -802,6 +802,7 @@ class Proc:
     decls: dict          # name -> Var (dummies, locals, result)
     body: list           # statements
     uses: list
+    formats: dict = field(default_factory=dict)   # FORMAT statements by label
 
 
 class BodyParser:
@@ -818,6 +819,7 @@ class BodyParser:
         self.consts = consts
         self.lines = header.lines
         self.i = 0
+        self.formats = {}
 
     def where(self, no):
         return f"{self.h.path}:{no}"
@@ -855,7 +857,7 @@ class BodyParser:
         if decls_only:
             return Proc(self.h, decls, None, uses)
         body = self.block(())
-        return Proc(self.h, decls, body, uses)
+        return Proc(self.h, decls, body, uses, self.formats)
 
     @staticmethod
     def _looks_like_assignment(toks):
@@ -867,6 +869,17 @@ class BodyParser:
         while self.i < len(self.lines):
             no, text = self.lines[self.i]
             toks = tokenize(text)
+            if toks and toks[0][0] == "int":
+                # a statement label: FORMAT statements are kept by label, other labels are dropped
+                # (no GO TO is in the subset, so nothing can jump to them)
+                label = int(toks[0][1])
+                text = text.lstrip()[len(str(toks[0][1])):].lstrip()
+                toks = toks[1:]
+                if toks and toks[0] == ("name", "format"):
+                    self.formats[label] = text[text.index("("):]
+                    self.i += 1
+                    out.append(("nop", text))
+                    continue
             key = self._keyword(toks)
             if key in terminators:
                 return out
@@ -1004,6 +1017,8 @@ class BodyParser:
                 return ("nml", grp)
             if w == "write":
                 return self._write(ts, text)
+            if w in ("open", "close"):
+                return self._open_close(w, ts, text)
             return ("nop", text)
         if w == "call" and not is_assign:
             ts.next()
@@ -1042,30 +1057,31 @@ class BodyParser:
 
     @staticmethod
     def _write(ts, text):
-        """WRITE(unit, fmt) items: ('write', unit, [items]); the caller may collect what is written
-        to external units. A list it cannot read (implied DO) is output only: ('nop', text)."""
+        """WRITE(unit, fmt) items: ('write', unit, fmt, [items]) with fmt ('label', n), ('str', text),
+        ('star',) for list-directed, or ('expr', e). A list it cannot read (implied DO) is output
+        only: ('nop', text)."""
         save = ts.i
         try:
             ts.next()
             ts.expect("op", "(")
-            unit = None
-            first = True
+            unit, fmt = None, None
+            pos = 0
             while True:
+                key = None
                 if ts.at("name") and ts.at("op", "=", 1):
                     key = ts.next()[1]
                     ts.next()
-                    e = ts.accept("op", "*") and ("str", "*") or parse_expr(ts)
-                    if key == "unit":
-                        unit = e
-                elif ts.accept("op", "*"):
-                    e = ("str", "*")
-                    if first:
-                        unit = e
+                if ts.accept("op", "*"):
+                    e = ("star",)
+                elif ts.at("int") and (key == "fmt" or (key is None and pos == 1)):
+                    e = ("label", int(str(ts.next()[1]).partition("_")[0]))
                 else:
                     e = parse_expr(ts)
-                    if first:
-                        unit = e
-                first = False
+                if key == "unit" or (key is None and pos == 0):
+                    unit = e
+                elif key == "fmt" or (key is None and pos == 1):
+                    fmt = e if e[0] in ("star", "label") else (("str", e[1]) if e[0] == "str" else ("expr", e))
+                pos += 1
                 if ts.accept("op", ")"):
                     break
                 ts.expect("op", ",")
@@ -1074,11 +1090,38 @@ class BodyParser:
                 items.append(parse_expr(ts))
                 if not ts.accept("op", ","):
                     break
-            if not ts.done():
+            if not ts.done() or unit is None:
                 raise FortranSubsetError("write list")
-            return ("write", unit, items)
+            return ("write", unit, fmt or ("star",), items)
         except FortranSubsetError:
             ts.i = save
+            return ("nop", text)
+
+    @staticmethod
+    def _open_close(w, ts, text):
+        """OPEN(unit=, file=, ...) -> ('open', unit, file); CLOSE(unit) -> ('close', unit): the
+        caller may attach files to units; other specifiers (status, action, iostat) are ignored."""
+        try:
+            ts.next()
+            ts.expect("op", "(")
+            unit = file = None
+            pos = 0
+            while True:
+                key = None
+                if ts.at("name") and ts.at("op", "=", 1):
+                    key = ts.next()[1]
+                    ts.next()
+                e = parse_expr(ts)
+                if key == "unit" or (key is None and pos == 0):
+                    unit = e
+                elif key == "file":
+                    file = e
+                pos += 1
+                if ts.accept("op", ")"):
+                    break
+                ts.expect("op", ",")
+            return (w, unit, file) if w == "open" else ("close", unit)
+        except FortranSubsetError:
             return ("nop", text)
 
     @staticmethod

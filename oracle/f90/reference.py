@@ -15,7 +15,9 @@ oracle/f90 (nothing restated here):
     (PanelVelocityParallel.f90:126-213,435-919,1287-1412), with MPI ranks as threads and
     MPI_BCAST as an in-process broadcast;
   * BVEVelocity and the RK4 step of BVERK4 of the Voronoi solver
-    (VoronoiVelocityParallel.f90:252-515).
+    (VoronoiVelocityParallel.f90:252-515);
+  * the legacy-VTK writer vtkOutputUnif (ParticlesEdgesPanels2.f90:2116-2237), its formatted
+    WRITEs collected as text.
 Logger and OutputWriter procedures (logging and file output) are replaced by no-ops, and so is
 the STRIPACK Delaunay / Voronoi rebuild at the end of the Voronoi BVERK4.
 
@@ -61,7 +63,8 @@ ENTRY = [(PVP, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "fi
                             "setsmooth", "bveactiverhs", "bvepassiverhs", "bvesmoothvelocity")] + \
         [(PEP, "newgrid"), (TVD, "setomega"), (TVD, "initrh4wavepanels"),
          (TVD, "initgaussianvortexpanels"), (TVD, "initjetpanels"), (TVD, "initstratosphere"),
-         (VVP, "bvevelocity"), (VVP, "bverk4"), (VVP, "initializempirk4"), (VVP, "finalizempirk4")]
+         (VVP, "bvevelocity"), (VVP, "bverk4"), (VVP, "initializempirk4"), (VVP, "finalizempirk4"),
+         (PEP, "vtkoutputunif")]
 VPM = "voronoipanelsmodule"
 
 SHIM_ENTRY = [(PVC, p) for p in ("bverk4", "stratosphererk4", "initializempirk4", "finalizempirk4",
@@ -450,6 +453,29 @@ def voronoi_rk4(x, y, z, relvort, area, n, dt, steps, nprocs=1, omega=2 * np.pi)
         if any(not np.array_equal(r[k], res[0][k]) for k in res[0]):
             raise AssertionError("ranks disagree after the Voronoi BVERK4")
     return res[0]
+
+
+def vtk_output(level, ic="rh4", n_tracer=2) -> dict:
+    """vtkOutputUnif (ParticlesEdgesPanels2.f90:2116-2237) on the reference's grid with its
+    initial condition and seeded tracer values: the text of the file it writes, and the arrays it
+    was written from (particles then panels, every panel)."""
+    files, records = {}, {}
+    host = {"__open__": lambda unit, name: files.__setitem__(int(unit), name),
+            "__record__": lambda unit, recs: records.setdefault(int(unit), []).extend(recs),
+            "__close__": lambda unit: None}
+    inst = runner().instance(host=host)
+    p, _, q = new_grid(inst, level, n_tracer)
+    _init(inst, ic, p, q)
+    rng = np.random.default_rng(level)
+    n, m = p.n, q.n
+    p.tracer.a[:n, :] = rng.standard_normal((n, n_tracer))
+    q.tracer.a[:m, :] = rng.standard_normal((m, n_tracer))
+    inst.proc(PEP, "vtkoutputunif")(p, q, "grid.vtk")
+    (unit,) = [u for u, name in files.items() if name == "grid.vtk"]
+    return dict(text="\n".join(records[unit]) + "\n",
+                particles_relVort=p.relvort.a[:n].copy(), particles_absVort=p.absvort.a[:n].copy(),
+                particles_tracer=p.tracer.a[:n, :].copy(), panels_relVort=q.relvort.a[:m].copy(),
+                panels_absVort=q.absvort.a[:m].copy(), panels_tracer=q.tracer.a[:m, :].copy())
 
 
 # ----------------------------------------------------------------------------- the drop-in

@@ -338,3 +338,185 @@ def ccall(host, cname, restype, args):
     if not refs:
         return r
     return r, [c.value for c in refs]
+
+
+# --------------------------------------------------------------------------- formatted output
+def _parse_format(fmt: str):
+    """A format specification '(...)' as nested nodes: ('lit', text), ('nl',), ('x', n),
+    ('ed', repeat, letter, w, d), ('grp', repeat, [nodes])."""
+    s = fmt.strip()
+    if not (s.startswith("(") and s.endswith(")")):
+        raise ValueError(f"format {fmt!r}")
+    pos = 0
+
+    def digits():
+        nonlocal pos
+        j = pos
+        while pos < len(s) and s[pos].isdigit():
+            pos += 1
+        return int(s[j:pos]) if pos > j else None
+
+    def group():
+        nonlocal pos
+        pos += 1
+        out = []
+        while True:
+            while pos < len(s) and s[pos] in " ,:":
+                pos += 1
+            ch = s[pos]
+            if ch == ")":
+                pos += 1
+                return out
+            if ch in "'\"":
+                j, text = pos + 1, []
+                while True:
+                    if s[j] == ch:
+                        if j + 1 < len(s) and s[j + 1] == ch:
+                            text.append(ch)
+                            j += 2
+                            continue
+                        break
+                    text.append(s[j])
+                    j += 1
+                out.append(("lit", "".join(text)))
+                pos = j + 1
+                continue
+            if ch == "/":
+                out.append(("nl",))
+                pos += 1
+                continue
+            rep = digits()
+            if s[pos] == "(":
+                out.append(("grp", rep or 1, group()))
+                continue
+            j = pos
+            while pos < len(s) and s[pos].isalpha():
+                pos += 1
+            letter = s[j:pos].upper()
+            if letter == "X":
+                out.append(("x", rep or 1))
+                continue
+            w = digits()
+            d = None
+            if pos < len(s) and s[pos] == ".":
+                pos += 1
+                d = digits()
+            if letter not in ("A", "I", "F", "L"):
+                raise NotImplementedError(f"edit descriptor {letter} outside the subset")
+            out.append(("ed", rep or 1, letter, w, d))
+
+    return group()
+
+
+def _edit(letter, w, d, v):
+    if letter == "A":
+        t = str(v)
+        if w is None:
+            return t
+        return t[:w] if len(t) >= w else " " * (w - len(t)) + t
+    if letter == "L":
+        t = "T" if v else "F"
+        return t if w is None else t.rjust(w)
+    if letter == "I":
+        k = int(v)
+        t = str(abs(k))
+        if d is not None:
+            t = t.zfill(d)
+        if k < 0:
+            t = "-" + t
+        if not w:
+            return t
+        return t.rjust(w) if len(t) <= w else "*" * w
+    if letter == "F":
+        t = f"{float(v):.{d}f}"
+        if not w:
+            return t
+        if len(t) > w and t.lstrip("-").startswith("0."):
+            t = t.replace("0.", ".", 1)  # the optional leading zero goes first
+        return t.rjust(w) if len(t) <= w else "*" * w
+    raise NotImplementedError(letter)
+
+
+def _flatten_items(items):
+    out = []
+    for v in items:
+        if isinstance(v, np.ndarray):
+            out.extend(v.reshape(-1, order="F").tolist())
+        else:
+            out.append(v)
+    return out
+
+
+def fformat(fmt, items):
+    """Records written by a WRITE with format `fmt` (None: list-directed) of `items`. Formats use
+    A, I, F, L, X, literals, '/' and repeated groups, with reversion to the last top-level group
+    (the whole format when there is none); list-directed records are gfortran's layout for
+    character and integer items (a leading blank, characters as they are, integers in 12
+    columns)."""
+    vals = _flatten_items(items)
+    if fmt is None:
+        parts = [" "]
+        for v in vals:
+            if isinstance(v, str):
+                parts.append(v)
+            elif isinstance(v, (int, np.integer)) and not isinstance(v, bool):
+                parts.append(f"{int(v):12d}")
+            else:
+                raise NotImplementedError("list-directed output of non-character, non-integer items")
+        return ["".join(parts)]
+    nodes = _parse_format(fmt)
+    records, cur = [], []
+    k = 0
+
+    def run(seq):
+        nonlocal k
+        for node in seq:
+            kind = node[0]
+            if kind == "lit":
+                cur.append(node[1])
+            elif kind == "x":
+                cur.append(" " * node[1])
+            elif kind == "nl":
+                records.append("".join(cur))
+                cur.clear()
+            elif kind == "grp":
+                for _ in range(node[1]):
+                    if not run(node[2]):
+                        return False
+            else:
+                _, rep, letter, w, d = node
+                for _ in range(rep):
+                    if k >= len(vals):
+                        return False
+                    cur.append(_edit(letter, w, d, vals[k]))
+                    k += 1
+        return True
+
+    run(nodes)
+    last_group = next((i for i in range(len(nodes) - 1, -1, -1) if nodes[i][0] == "grp"), None)
+    restart = nodes[last_group:] if last_group is not None else nodes
+    while k < len(vals):
+        records.append("".join(cur))
+        cur.clear()
+        before = k
+        run(restart)
+        if k == before:
+            raise ValueError(f"format {fmt!r} has no data edit descriptor for the remaining items")
+    records.append("".join(cur))
+    return records
+
+
+def fformat_or_none(fmt, items):
+    try:
+        return fformat(fmt, items)
+    except NotImplementedError:
+        return None
+
+
+def fwrite(host, unit, fmt, items):
+    """WRITE to an external unit: the caller may collect the raw values (host['__write__']) and
+    the formatted records (host['__record__'])."""
+    if "__write__" in host:
+        host["__write__"](unit, list(items))
+    if "__record__" in host:
+        host["__record__"](unit, fformat(fmt, items))

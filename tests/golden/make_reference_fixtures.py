@@ -6,7 +6,8 @@ executes it with strict IEEE double arithmetic (see oracle/f90/__init__.py).
 Every array in these fixtures was computed by the reference's own statements:
 its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
 ranks run as threads, the three RHS sums, the Voronoi BVEVelocity and
-BVERK4, finite differences of the enstrophy through its BVERK4, and its
+BVERK4, finite differences of the enstrophy through its BVERK4, the file its
+legacy-VTK writer writes, and its
 Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) with the rows it writes
 to its data file. The
 tests compare the C oracle, the product's host code and (on a GPU) the
@@ -81,6 +82,9 @@ def main():
     # centred finite differences of J = sum zeta(T)^2 A through the reference's BVERK4 (level 1,
     # three steps): the final active vorticity for each +/- perturbation of 16 seeded entries
     _save("ref_fd_rh4_l1", **fd_inputs())
+    # the file the reference's legacy-VTK writer writes (level 1, two tracers)
+    v = REF.vtk_output(1)
+    _save("ref_vtk_l1", **{k: (np.array(val) if k == "text" else val) for k, val in v.items()})
     # the reference's RH4 driver program (RHWavePanelsMPI.f90) on two ranks: its data-file rows
     nl = driver_namelist()
     d = REF.run_driver(2, nl)

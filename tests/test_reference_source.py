@@ -351,3 +351,29 @@ def test_oracle_equals_the_reference_serial_module(ic):
     assert np.array_equal(np.array(tke), r["totalKE"])
     assert np.array_equal(ke, r["kineticEnergy"])
     assert np.array_equal(s1["relVortV"], s0["relVortV"])
+
+
+@needs_source
+def test_vtk_fixture_regenerates_from_the_reference_source():
+    f = _load("ref_vtk_l1")
+    v = REF.vtk_output(1)
+    assert v["text"] == str(f["text"])
+    for k, val in v.items():
+        if k != "text":
+            assert np.array_equal(val, f[k]), k
+
+
+def test_translator_formatted_output():
+    """The formatter behind WRITE: edit descriptors, groups, format reversion, the optional
+    leading zero of F, overflow asterisks and gfortran's list-directed layout."""
+    assert rt.fformat("(A,I0.2,A)", ["K", 7, ":"]) == ["K07:"]
+    assert rt.fformat("(2(I3,1X),A4)", [1, -2, "abcdef"]) == ["  1  -2 abcd"]
+    assert rt.fformat("(F5.3)", [0.5]) == ["0.500"]
+    assert rt.fformat("(F4.3)", [0.5]) == [".500"]
+    assert rt.fformat("(F4.1)", [-123.0]) == ["****"]
+    assert rt.fformat("(I2)", [123]) == ["**"]
+    assert rt.fformat("(F6.2)", [1.0, 2.0]) == ["  1.00", "  2.00"]  # reversion: one record each
+    assert rt.fformat("('x=',F4.1,/,'y')", [1.0]) == ["x= 1.0", "y"]
+    assert rt.fformat(None, ["a", "b", 5]) == [" ab           5"]
+    with pytest.raises(NotImplementedError):
+        rt.fformat("(E12.4)", [1.0])
