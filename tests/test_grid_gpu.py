@@ -40,3 +40,21 @@ def test_device_grid_rejects_bad_level(gpu):
         assert e.value.status == N.TC_ERR_ARG
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_device_grid_equals_the_reference_grid(gpu):
+    """The same at level 3 against the reference's own NewGrid, run from its Fortran source by
+    oracle/f90 (tests/golden/ref_grid_l3.npz)."""
+    from pathlib import Path
+
+    ref = np.load(Path(__file__).resolve().parent / "golden" / "ref_grid_l3.npz")
+    ctx = Context(0, "fp64")
+    try:
+        d = {k: v.cpu().numpy() for k, v in grid.new_icos_grid_device(ctx, 3).items()}
+    finally:
+        ctx.close()
+    for k in ("particles_x", "particles_x0", "panels_x", "panels_x0", "panels_has_children",
+              "panels_vertices", "panels_nest", "panels_children"):
+        assert np.array_equal(d[k], ref[k]), k
+    assert np.abs(d["panels_area"] - ref["panels_area"]).max() <= 1e-14 * ref["panels_area"].max()
