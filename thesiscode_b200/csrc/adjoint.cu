@@ -886,6 +886,7 @@ extern "C" int tc_rk4_adjoint(tc_ctx* ctx, const double* xA0, const double* zeta
     tc_record_error("tc_rk4_adjoint: bad arguments");
     return TC_ERR_ARG;
   }
+  TcNvtxRange nvtx_adjoint("tc rk4 adjoint");
   return adjoint_impl(ctx, xA0, zetaA0, areaA, nA, dt, nsteps, ckpt_every, functional, probe,
                       nullptr, nullptr, J, g_zeta0, g_x0);
 }

@@ -572,6 +572,9 @@ extern "C" int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int
     tc_record_error("tc_rk4_stage_range: bad stage or range");
     return TC_ERR_ARG;
   }
+  static const char* const kStageNames[4] = {"tc rk4 stage 1", "tc rk4 stage 2", "tc rk4 stage 3",
+                                              "tc rk4 stage 4"};
+  TcNvtxRange nvtx_stage(kStageNames[stage]);
   const bool first = stage == 0;
   const double* tx[3] = {first ? R.x0A.as<double>() : R.xiA.as<double>(),
                          first ? R.x0V.as<double>() : R.xiV.as<double>(),
@@ -813,6 +816,7 @@ int advance_graph(tc_ctx* ctx, double dt, int nsteps) {
     ctx->pair_launches += G.pair_launches;
     ctx->pair_interactions += G.pair_interactions;
   }
+  TcNvtxRange nvtx_replay("tc rk4 graph replay");
   TC_CUDA_TRY(cudaEventRecord(G.ev[0], ctx->stream));
   TC_CUDA_TRY(cudaStreamWaitEvent(G.stream, G.ev[0], 0));
   TC_CUDA_TRY(cudaGraphLaunch(G.exec, G.stream));
@@ -824,6 +828,7 @@ int advance_graph(tc_ctx* ctx, double dt, int nsteps) {
 // tc_rk4_advance without the read-back of totalKE: everything is queued on
 // the context's stream.
 int rk4_advance_enqueue(tc_ctx* ctx, double dt, int nsteps) {
+  TcNvtxRange nvtx_advance("tc rk4 advance");
   int rc = begin(ctx);
   if (rc) return rc;
   tcb::Rk4State& R = ctx->rk;

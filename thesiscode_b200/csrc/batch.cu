@@ -429,6 +429,7 @@ extern "C" int tc_batch_rk4(tc_ctx* ctx, int count, const int* nA, const int* nV
     tc_record_error("tc_batch_rk4: bad arguments");
     return TC_ERR_ARG;
   }
+  TcNvtxRange nvtx_batch("tc batch rk4");
   if (cudaSetDevice(ctx->device) != cudaSuccess) return TC_ERR_CUDA;
   if (!ctx->batch) ctx->batch = new tc_batch_plan();
   tc_batch_plan& B = *ctx->batch;

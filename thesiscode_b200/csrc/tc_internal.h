@@ -1,7 +1,18 @@
 // Internal helpers shared by the CUDA translation units of libthesiscode_b200.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include "thesiscode_b200.h"
+
+// A named NVTX range over a scope, for tracing tools (Nsight Systems, ncu --nvtx): the RK4
+// stages, the step loops, the graph replays, the adjoint and the batch calls each open one.
+// Without a tool attached each push/pop is a call that returns at once.
+struct TcNvtxRange {
+  explicit TcNvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~TcNvtxRange() { nvtxRangePop(); }
+  TcNvtxRange(const TcNvtxRange&) = delete;
+  TcNvtxRange& operator=(const TcNvtxRange&) = delete;
+};
 
 // Make `device` current, failing with TC_ERR_ARG for an index that does not
 // exist and TC_ERR_CUDA when the runtime cannot be reached.
