@@ -80,10 +80,11 @@ MPIF = {"mpi_status_size": 6, "mpi_double_precision": 17, "mpi_integer": 7, "mpi
 HOST_PROCS = {"mpi_bcast", "mpi_barrier", "mpi_allgatherv", "mpi_init", "mpi_finalize",
               "mpi_comm_size", "mpi_comm_rank", "mpi_wtime"}
 
-# the reference's Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) and the module it is switched
-# to by its one `use` line
-DRIVER = "RHWavePanelsMPI.f90"
-DRV = "rhwavepanelsmpi"
+# the reference's driver programs run here: (source file, program name); each is switched to the
+# drop-in module by its one `use PanelVelocityParallelModule` line
+DRIVERS = {"rh4": ("RHWavePanelsMPI.f90", "rhwavepanelsmpi"),
+           "strat": ("StratospherePanels.f90", "stratospherepanels")}
+DRIVER, DRV = DRIVERS["rh4"]
 DRIVER_ALIASES = {"panelvelocityparallelmodule": PVC}
 
 TRI_PANEL, BVE_SOLVER = 3, 61
@@ -135,15 +136,20 @@ def shim_runner():
     return _program("f90_shim.py", [REFERENCE_DIR / f for f in FILES] + [SHIM], SHIM_ENTRY)
 
 
-@lru_cache(maxsize=2)
-def driver_runner(cuda: bool):
-    """The reference's RH4 driver program, with `use PanelVelocityParallelModule` as written
-    (cuda False) or switched to the drop-in module (cuda True)."""
-    files = [REFERENCE_DIR / f for f in FILES] + [REFERENCE_DIR / "RefineRemesh.f90", REFERENCE_DIR / DRIVER]
+def _driver_file(which, cuda):
+    return f"f90_driver{'' if which == 'rh4' else '_' + which}{'_cuda' if cuda else ''}.py"
+
+
+@lru_cache(maxsize=4)
+def driver_runner(cuda: bool, which: str = "rh4"):
+    """A driver program of the reference (DRIVERS), with `use PanelVelocityParallelModule` as
+    written (cuda False) or switched to the drop-in module (cuda True)."""
+    src, prog = DRIVERS[which]
+    files = [REFERENCE_DIR / f for f in FILES] + [REFERENCE_DIR / "RefineRemesh.f90", REFERENCE_DIR / src]
     if cuda:
-        return _program("f90_driver_cuda.py", files + [SHIM], [(DRV, "main"), (PVC, "setprecisioncuda")],
+        return _program(_driver_file(which, True), files + [SHIM], [(prog, "main"), (PVC, "setprecisioncuda")],
                         _driver_stub, DRIVER_ALIASES)
-    return _program("f90_driver.py", files, [(DRV, "main")], _driver_stub)
+    return _program(_driver_file(which, False), files, [(prog, "main")], _driver_stub)
 
 
 @lru_cache(maxsize=1)
@@ -174,8 +180,8 @@ def shim_built() -> bool:
     return available() or (BUILD_DIR / "f90_shim.py").is_file()
 
 
-def driver_built() -> bool:
-    return available() or (BUILD_DIR / "f90_driver_cuda.py").is_file()
+def driver_built(which: str = "rh4") -> bool:
+    return available() or (BUILD_DIR / _driver_file(which, True)).is_file()
 
 
 def build_programs() -> list:
@@ -186,9 +192,9 @@ def build_programs() -> list:
     out = []
     for name, r, extra in (("f90_reference.py", runner(), ""),
                            ("f90_shim.py", shim_runner(), ", thesiscode_b200/fortran/PanelVelocityCUDA.f90"),
-                           ("f90_driver_cuda.py", driver_runner(True),
-                            f", RefineRemesh.f90, {DRIVER} (use switched to the drop-in), "
-                            "thesiscode_b200/fortran/PanelVelocityCUDA.f90")):
+                           *((_driver_file(w, True), driver_runner(True, w),
+                              f", RefineRemesh.f90, {DRIVERS[w][0]} (use switched to the drop-in), "
+                              "thesiscode_b200/fortran/PanelVelocityCUDA.f90") for w in DRIVERS)):
         r.save(BUILD_DIR / name, note=f"sources: {', '.join(FILES)}{extra}")
         out.append(BUILD_DIR / name)
     return out
@@ -538,14 +544,15 @@ def shim_strat_rk4(lib_path, level, steps, t0, dt, nprocs=1, fp32c=False, smooth
 
 
 # ----------------------------------------------------------------------------- the driver
-def run_driver(nprocs, namelist, cuda=False, lib_path=None, fp32c=False) -> dict:
-    """The reference's RH4 driver program (RHWavePanelsMPI.f90) on nprocs thread ranks, its
-    namelist groups (gridinit, time, fileio) given as dicts, with its own
-    PanelVelocityParallelModule (cuda False) or with its `use` line switched to the drop-in
-    module and the library at lib_path (cuda True). Returns what rank 0 writes to the data file
-    (per step: totalKE, enstrophy, relVort l1, l2, linf error against the steady wave), as an
-    array, and every rank's rows."""
-    prog = driver_runner(bool(cuda))
+def run_driver(nprocs, namelist, cuda=False, lib_path=None, fp32c=False, which="rh4") -> dict:
+    """A driver program of the reference on nprocs thread ranks: RHWavePanelsMPI.f90 ("rh4") or
+    StratospherePanels.f90 ("strat"), its namelist groups (gridinit, time, fileio) given as dicts,
+    with its own PanelVelocityParallelModule (cuda False) or with its `use` line switched to the
+    drop-in module and the library at lib_path (cuda True). Returns what rank 0 writes to the
+    data file as an array (per step; rh4: totalKE, enstrophy, relVort l1, l2, linf error against
+    the steady wave; strat: totalKE, enstrophy), and everything every rank wrote."""
+    prog = driver_runner(bool(cuda), which)
+    DRV = DRIVERS[which][1]
     lib = _lib(lib_path) if cuda else None
     written = [[] for _ in range(nprocs)]
 

@@ -8,8 +8,8 @@ its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
 ranks run as threads, the three RHS sums, the Voronoi BVEVelocity and
 BVERK4, finite differences of the enstrophy through its BVERK4, the file its
 legacy-VTK writer writes, and its
-Rossby-Haurwitz driver program (RHWavePanelsMPI.f90) with the rows it writes
-to its data file. The
+Rossby-Haurwitz and stratosphere driver programs (RHWavePanelsMPI.f90,
+StratospherePanels.f90) with the rows they write to their data files. The
 tests compare the C oracle, the product's host code and (on a GPU) the
 product's kernels with them.
 
@@ -90,6 +90,11 @@ def main():
     d = REF.run_driver(2, nl)
     _save("ref_driver_rh4_l2", rows=d["rows"], nprocs=2, initNest=nl["gridInit"]["initNest"],
           dt=nl["time"]["dt"], tfinal=nl["time"]["tfinal"])
+    # the reference's stratosphere driver program (StratospherePanels.f90) on two ranks
+    nl = driver_namelist("strat")
+    d = REF.run_driver(2, nl, which="strat")
+    _save("ref_driver_strat_l2", rows=d["rows"], nprocs=2, initNest=nl["gridInit"]["initNest"],
+          dt=nl["time"]["dt"], tfinal=nl["time"]["tfinal"])
     print(f"done in {time.time() - t0:.0f} s")
 
 
@@ -121,9 +126,14 @@ def fd_inputs(level=1, steps=3, dt=0.01, eps=1e-6, entries=16, seed=33):
                 zeta_final=REF.final_active_vorticity(level, steps, dt, xA, zA))
 
 
-def driver_namelist():
-    """Namelist groups of the driver run (RHWavePanels.namelist's layout, level 2, three steps; no
-    remeshing within the run)."""
+def driver_namelist(which="rh4"):
+    """Namelist groups of a driver run (the layout of the driver's .namelist file, level 2, a few
+    steps, no remeshing within the run). The stratosphere run's tfinal / dt is 2.9999... in binary,
+    so its floor(tfinal/dt) takes two steps, as the reference's driver does."""
+    if which == "strat":
+        return {"gridInit": dict(panelKind=3, initNest=2, AMR=0, remeshInterval=1000, amrTol1=1.0,
+                                 amrTol2=1.0, useRelativeTol=0, maxRefine=0),
+                "time": dict(dt=0.05, tfinal=0.15), "fileIO": dict(jobPrefix="strat")}
     return {"gridInit": dict(panelKind=3, initNest=2, AMR=0, remeshInterval=1000, amrTol1=1.0, amrTol2=1.0),
             "time": dict(dt=0.01, tfinal=0.03), "fileIO": dict(jobPrefix="rh4", outputDir="./")}
 

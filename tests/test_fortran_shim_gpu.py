@@ -112,3 +112,22 @@ def test_reference_driver_with_its_use_line_switched(nprocs, fp32c, gpu):
     assert rel_err(rows[:, 0], ref[:, 0]) <= 2 * tol      # totalKE
     assert rel_err(rows[:, 1], ref[:, 1]) <= 2 * tol      # enstrophy
     assert np.abs(rows[:, 2:] - ref[:, 2:]).max() <= 10 * tol
+
+
+@pytest.mark.skipif(not REF.driver_built("strat"), reason="the driver's translation is built by "
+                    "__graft_entry__.build() where the reference's sources are present")
+@pytest.mark.parametrize("nprocs,fp32c", [(1, False), (2, False), (1, True)])
+def test_reference_stratosphere_driver_with_its_use_line_switched(nprocs, fp32c, gpu):
+    """The reference's forced-model driver (StratospherePanels.f90) with only its `use` line
+    switched to the drop-in module: StratosphereRK4 each step on the GPU; its data-file rows
+    (totalKE, enstrophy per step) equal the unmodified driver's (tests/golden/ref_driver_strat_l2.npz)."""
+    f = _load("ref_driver_strat_l2")
+    nl = {"gridInit": dict(panelKind=3, initNest=int(f["initNest"]), AMR=0, remeshInterval=1000,
+                           amrTol1=1.0, amrTol2=1.0, useRelativeTol=0, maxRefine=0),
+          "time": dict(dt=float(f["dt"]), tfinal=float(f["tfinal"])), "fileIO": dict(jobPrefix="strat")}
+    run = REF.run_driver(nprocs, nl, cuda=True, lib_path=build.lib_path(), fp32c=fp32c, which="strat")
+    rows, ref = run["rows"], f["rows"]
+    assert rows.shape == ref.shape
+    tol = TOL[fp32c]
+    assert rel_err(rows[1:, 0], ref[1:, 0]) <= 2 * tol     # totalKE (row 0 is the unset initial 0)
+    assert rel_err(rows[:, 1], ref[:, 1]) <= 2 * tol       # enstrophy
