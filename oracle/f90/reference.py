@@ -83,7 +83,23 @@ HOST_PROCS = {"mpi_bcast", "mpi_barrier", "mpi_allgatherv", "mpi_init", "mpi_fin
 # the reference's driver programs run here: (source file, program name); each is switched to the
 # drop-in module by its one `use PanelVelocityParallelModule` line
 DRIVERS = {"rh4": ("RHWavePanelsMPI.f90", "rhwavepanelsmpi"),
-           "strat": ("StratospherePanels.f90", "stratospherepanels")}
+           "strat": ("StratospherePanels.f90", "stratospherepanels"),
+           "gauss": ("GaussVort.f90", "gaussianvortex"),
+           "jet": ("JetPanels.f90", "jetpanels"),
+           "twovorts": ("TwoVortsPanels.f90", "twovortices"),
+           "manyvorts": ("ManyVortsPanels.f90", "manyvortspanels"),
+           "rh2": ("RH2Panels.f90", "rh2wavepanels"),
+           "solidbody": ("solidBody.f90", "solidbody"),
+           "dtconv": ("BVEDeltaTConv.f90", "bvedeltatconv"),
+           "directrh4": ("DirectRH4Panels.f90", "directrhwave"),
+           "zonalmean": ("ZonalMeanPanels.f90", "zonalmean")}
+# the namelist file each driver opens
+DRIVER_NAMELISTS = {"rh4": "RHWavePanels.namelist", "strat": "StratospherePanels.namelist",
+                    "gauss": "GaussVortPanels.namelist", "jet": "JetPanels.namelist",
+                    "twovorts": "TwoVorts.namelist", "manyvorts": "ManyVortsPanels.namelist",
+                    "rh2": "RH2Panels.namelist", "solidbody": "SolidBody.namelist",
+                    "dtconv": "BVEDTConv.namelist", "directrh4": "RHWavePanels.namelist",
+                    "zonalmean": "ZonalMeanPanels.namelist"}
 DRIVER, DRV = DRIVERS["rh4"]
 DRIVER_ALIASES = {"panelvelocityparallelmodule": PVC}
 
@@ -544,6 +560,41 @@ def shim_strat_rk4(lib_path, level, steps, t0, dt, nprocs=1, fp32c=False, smooth
 
 
 # ----------------------------------------------------------------------------- the driver
+def read_namelist(path) -> dict:
+    """The groups of a namelist file (&group key = value ... /) as {group: {key: value}}: integers,
+    reals (d exponents too), logicals and quoted strings; text outside a group is ignored."""
+    groups, cur = {}, None
+    with open(path, encoding="latin-1") as f:
+        for raw in f:
+            line = raw.split("!")[0].strip()
+            if not line:
+                continue
+            if line.startswith("&"):
+                cur = groups.setdefault(line[1:].split()[0].lower(), {})
+                continue
+            if line.startswith("/"):
+                cur = None
+                continue
+            if cur is None or "=" not in line:
+                continue
+            for item in line.split(","):
+                if "=" not in item:
+                    continue
+                k, v = (t.strip() for t in item.split("=", 1))
+                if v[:1] in "'\"":
+                    val = v.strip("'\"")
+                elif v.lower() in (".true.", "t", ".false.", "f"):
+                    val = v.lower() in (".true.", "t")
+                else:
+                    try:
+                        val = int(v)
+                    except ValueError:
+                        val = float(v.lower().replace("d", "e"))
+                cur[k.lower()] = val
+    return groups
+
+
+
 def run_driver(nprocs, namelist, cuda=False, lib_path=None, fp32c=False, which="rh4") -> dict:
     """A driver program of the reference on nprocs thread ranks: RHWavePanelsMPI.f90 ("rh4") or
     StratospherePanels.f90 ("strat"), its namelist groups (gridinit, time, fileio) given as dicts,

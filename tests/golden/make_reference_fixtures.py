@@ -8,16 +8,18 @@ its grid generator, its initial conditions, BVERK4 / StratosphereRK4 with MPI
 ranks run as threads, the three RHS sums, the Voronoi BVEVelocity and
 BVERK4, finite differences of the enstrophy through its BVERK4, the file its
 legacy-VTK writer writes, and its
-Rossby-Haurwitz and stratosphere driver programs (RHWavePanelsMPI.f90,
-StratospherePanels.f90) with the rows they write to their data files. The
+driver programs (RHWavePanelsMPI.f90, StratospherePanels.f90 and the nine
+other BVE drivers) with the rows they write to their data files. The
 tests compare the C oracle, the product's host code and (on a GPU) the
 product's kernels with them.
 
 Needs the reference's sources (oracle/f90/reference.py: REFERENCE_DIR). Run from
 the repository root:  python tests/golden/make_reference_fixtures.py
-(about three minutes; the level-3 step dominates).
+(about five minutes).
 """
 from __future__ import annotations
+
+import json
 
 import sys
 import time
@@ -95,6 +97,15 @@ def main():
     d = REF.run_driver(2, nl, which="strat")
     _save("ref_driver_strat_l2", rows=d["rows"], nprocs=2, initNest=nl["gridInit"]["initNest"],
           dt=nl["time"]["dt"], tfinal=nl["time"]["tfinal"])
+    # the reference's other BVE driver programs, each from its own namelist file with the overrides
+    # of other_driver_namelist, on two ranks: their data-file rows
+    out = {}
+    for which in OTHER_DRIVERS:
+        nl = other_driver_namelist(which)
+        d = REF.run_driver(2, nl, which=which)
+        out[f"{which}_rows"] = d["rows"]
+        out[f"{which}_namelist"] = np.array(json.dumps(nl))
+    _save("ref_drivers_l2", **out)
     print(f"done in {time.time() - t0:.0f} s")
 
 
@@ -124,6 +135,22 @@ def fd_inputs(level=1, steps=3, dt=0.01, eps=1e-6, entries=16, seed=33):
     return dict(xA=xA, zetaA=zA, areaA=st["areaA"], picks=picks, tangents=tangents, eps=eps,
                 dt=dt, steps=steps, zeta_plus=np.array(fp), zeta_minus=np.array(fm),
                 zeta_final=REF.final_active_vorticity(level, steps, dt, xA, zA))
+
+
+OTHER_DRIVERS = ("gauss", "jet", "twovorts", "manyvorts", "rh2", "solidbody", "dtconv", "directrh4",
+                 "zonalmean")
+
+
+def other_driver_namelist(which):
+    """A driver's own namelist file with the run kept small: triangular panels at level 2 (level 1
+    for the dt-convergence driver, which runs five step sizes), no adaptive refinement and no
+    remeshing within the run, two steps of the file's dt."""
+    g = REF.read_namelist(REF.REFERENCE_DIR / REF.DRIVER_NAMELISTS[which])
+    g.setdefault("gridinit", {}).update(panelkind=3, initnest=1 if which == "dtconv" else 2, amr=0,
+                                        remeshinterval=1000, userelativetol=0, maxrefine=0)
+    t = g.setdefault("time", {})
+    t["tfinal"] = 2.5 * t["dt"]
+    return g
 
 
 def driver_namelist(which="rh4"):

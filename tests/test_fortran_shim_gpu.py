@@ -131,3 +131,29 @@ def test_reference_stratosphere_driver_with_its_use_line_switched(nprocs, fp32c,
     tol = TOL[fp32c]
     assert rel_err(rows[1:, 0], ref[1:, 0]) <= 2 * tol     # totalKE (row 0 is the unset initial 0)
     assert rel_err(rows[:, 1], ref[:, 1]) <= 2 * tol       # enstrophy
+
+
+OTHER_DRIVERS = ("gauss", "jet", "twovorts", "manyvorts", "rh2", "solidbody", "dtconv", "directrh4",
+                 "zonalmean")
+
+
+@pytest.mark.parametrize("which", OTHER_DRIVERS)
+def test_other_reference_drivers_with_their_use_line_switched(which, gpu):
+    """Every other BVE driver of the reference (Gaussian vortex, jet, two and many vortices,
+    Rossby-Haurwitz 2, solid body, the dt-convergence study that resets the RK4 state for each of
+    its step sizes, the direct RH4 run, the zonal mean), each from its own namelist file kept
+    small (tests/golden/make_reference_fixtures.py), with only its `use` line switched to the
+    drop-in module, on 2 ranks in FP64: the rows it writes to its data file equal those the
+    unmodified driver writes (tests/golden/ref_drivers_l2.npz), to 1e-10 relative or 1e-12
+    absolute (some columns are error norms of a few 1e-10, differences of two runs)."""
+    import json
+
+    if not REF.driver_built(which):
+        pytest.skip("the driver's translation is built by __graft_entry__.build() where the "
+                    "reference's sources are present")
+    f = _load("ref_drivers_l2")
+    nl = json.loads(str(f[f"{which}_namelist"]))
+    run = REF.run_driver(2, nl, cuda=True, lib_path=build.lib_path(), which=which)
+    ref = f[f"{which}_rows"]
+    assert run["rows"].shape == ref.shape
+    assert np.allclose(run["rows"], ref, rtol=1e-10, atol=1e-12), np.abs(run["rows"] - ref).max()
