@@ -323,6 +323,50 @@ int tc_stats_enable_timing(tc_ctx* ctx, int on);
 int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* pair_launches,
              long long* pair_interactions, double* pair_ms);
 
+/* ---- index checks (checked build; the reference's commented-out ifort
+ * flags -check bounds -check pointers, Makefile:7) ---------------------- */
+/* The same sources compiled with -DTC_BOUNDS_CHECK=1 give
+ * libthesiscode_b200_checked.so (`python -m thesiscode_b200.build --checked`).
+ * In it the pair kernels (single and batched), source packing and the
+ * velocity and RK4 stage epilogues check every global-memory index against
+ * its array's extent. That extent is the library's own allocation, or the
+ * size the caller declared. An index outside it is not accessed: a load
+ * reads 0 and a store is skipped. The first such index goes into the
+ * device's record. Other kernels (adjoint, grid, Voronoi adapters) are not
+ * checked. */
+#define TC_BC_PAIR_X 1        /* pair kernels: target positions (points)       */
+#define TC_BC_PAIR_PERM 2     /* pair kernels: target visiting order           */
+#define TC_BC_PAIR_SRC 3      /* pair kernels: packed sources                  */
+#define TC_BC_PAIR_OUT 4      /* pair kernels: partial-sum stores (doubles)    */
+#define TC_BC_BATCH_SEG 5     /* batched pair kernels: segment table           */
+#define TC_BC_PACK_IN 6       /* packing: positions, vorticity, area (points)  */
+#define TC_BC_PACK_OUT 7      /* packing: packed-source stores                 */
+#define TC_BC_EPI_PERM 8      /* velocity epilogue: visiting order             */
+#define TC_BC_EPI_X 9         /* velocity epilogue: target positions (points)  */
+#define TC_BC_EPI_PARTIAL 10  /* velocity epilogue: partial sums (doubles)     */
+#define TC_BC_EPI_OUT 11      /* velocity epilogue: dX / dVort stores (points) */
+#define TC_BC_STAGE_PERM 12   /* stage epilogue: visiting orders               */
+#define TC_BC_STAGE_STATE 13  /* stage epilogue: a class's state arrays        */
+#define TC_BC_STAGE_PARTIAL 14 /* stage epilogue: partial sums (doubles)       */
+#define TC_BC_STAGE_CHUNKS 15 /* stage epilogue: per-row chunk counts (batch)  */
+#define TC_BC_STAGE_ACTIVE 16 /* stage epilogue: active-only arrays            */
+#define TC_BC_STAGE_KEBLOCK 17 /* stage epilogue: per-block KE sums            */
+/* 1 in the checked library, 0 in the release library. */
+int tc_bounds_checked(void);
+/* Waits for the device, then reads its record: rec[0] = violations since the
+ * last reset, rec[1] = TC_BC_* site of the first one, rec[2] = its index,
+ * rec[3] = the extent it was checked against. reset != 0 clears the record.
+ * Every context on the device shares the one record. The release library
+ * gives all zeros. */
+int tc_bounds_status(int device, long long rec[4], int reset);
+/* Checked library only; the release library returns TC_ERR_STATE. Launches made
+ * after the call declare at most `cap` elements for `site` (0: every site),
+ * while the arrays keep their size. So the checks can be seen firing on
+ * accesses that still lie inside the real allocation. cap < 0 removes the
+ * cap. A CUDA graph captured earlier keeps the extents it was captured
+ * with. */
+int tc_bounds_cap(tc_ctx* ctx, int site, long long cap);
+
 /* ---- icosahedral grid (input generator) ------------------------------- */
 /* PanelMax / ParticleMax / EdgeMax (ParticlesEdgesPanels2.f90:2614-2662)
  * and the number of leaf panels, 20*4^level. level in [0, 11]. */

@@ -14,13 +14,32 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def native_built():
-    """Build the library and the oracle once per session (seconds when up to date)."""
+    """Build the library (and, with TC_LIBRARY=checked, its index-checked build) and the
+    oracle once per session (seconds when up to date)."""
+    from thesiscode_b200 import _native as N
     from thesiscode_b200 import build as b
     from oracle import oracle
 
     b.build()
+    if N.CHECKED:
+        b.build(checked=True)
     oracle.build()
     return True
+
+
+@pytest.fixture(autouse=True)
+def _index_checks_clean(request):
+    """With the index-checked library loaded (TC_LIBRARY=checked), a GPU test fails when any
+    kernel it launched indexed outside an array (the device's record is read and cleared)."""
+    yield
+    if request.node.get_closest_marker("gpu") is None:
+        return
+    from thesiscode_b200 import _native as N
+
+    if not N.CHECKED or N._lib is None:
+        return
+    rec = N.bounds_status(0, reset=True)
+    assert rec["count"] == 0, f"index check fired: {rec}"
 
 
 @pytest.fixture(scope="session")

@@ -22,7 +22,7 @@ import numpy as np
 import pytest
 
 from oracle.f90 import reference as REF
-from thesiscode_b200 import build
+from thesiscode_b200 import _native as N
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not REF.shim_built(),
@@ -57,7 +57,7 @@ def _check(run, f, tol, keys=("xA", "xV", "xQ", "zetaA")):
 @pytest.mark.parametrize("fp32c", [False, True])
 def test_dropin_bverk4_one_rank(fp32c, gpu):
     f = _load("ref_bverk4_rh4_l2")
-    run = REF.shim_bve_rk4(build.lib_path(), 2, int(f["steps"]), float(f["dt"]), nprocs=1, fp32c=fp32c)
+    run = REF.shim_bve_rk4(N.LIB_PATH, 2, int(f["steps"]), float(f["dt"]), nprocs=1, fp32c=fp32c)
     _check(run, f, TOL[fp32c])
     assert rel_err(run["totalKE"], f["totalKE"]) <= 2 * TOL[fp32c]
     assert rel_err(run["kineticEnergy"], f["kineticEnergy"]) <= 2 * TOL[fp32c]
@@ -69,7 +69,7 @@ def test_dropin_bverk4_sharded_ranks(name, level, nprocs, gpu):
     ranks) and exchanges source rows with MPI_ALLGATHERV after every stage; all ranks end with
     the same state, the reference's."""
     f = _load(name)
-    run = REF.shim_bve_rk4(build.lib_path(), level, int(f["steps"]), float(f["dt"]), nprocs=nprocs)
+    run = REF.shim_bve_rk4(N.LIB_PATH, level, int(f["steps"]), float(f["dt"]), nprocs=nprocs)
     _check(run, f, TOL[False])
     assert rel_err(run["totalKE"], f["totalKE"]) <= 2 * TOL[False]
     for r in run["ranks"][1:]:
@@ -81,7 +81,7 @@ def test_dropin_bverk4_sharded_ranks(name, level, nprocs, gpu):
 @pytest.mark.parametrize("fp32c", [False, True])
 def test_dropin_stratosphere_rk4(fp32c, gpu):
     f = _load("ref_strat_l2")
-    run = REF.shim_strat_rk4(build.lib_path(), 2, int(f["steps"]), float(f["t0"]), float(f["dt"]),
+    run = REF.shim_strat_rk4(N.LIB_PATH, 2, int(f["steps"]), float(f["t0"]), float(f["dt"]),
                              nprocs=2, fp32c=fp32c)
     _check(run, f, TOL[fp32c], keys=("xA", "xV", "xQ"))
     assert rel_err(run["final"]["zetaA"], _state(f, "final")["zetaA"]) <= TOL[fp32c]
@@ -105,7 +105,7 @@ def test_reference_driver_with_its_use_line_switched(nprocs, fp32c, gpu):
     those of the unmodified driver (tests/golden/ref_driver_rh4_l2.npz). The error norms are
     differences of vorticities: compared to an absolute 10x the vorticity tolerance."""
     f = _load("ref_driver_rh4_l2")
-    run = REF.run_driver(nprocs, _driver_namelist(f), cuda=True, lib_path=build.lib_path(), fp32c=fp32c)
+    run = REF.run_driver(nprocs, _driver_namelist(f), cuda=True, lib_path=N.LIB_PATH, fp32c=fp32c)
     rows, ref = run["rows"], f["rows"]
     assert rows.shape == ref.shape
     tol = TOL[fp32c]
@@ -125,7 +125,7 @@ def test_reference_stratosphere_driver_with_its_use_line_switched(nprocs, fp32c,
     nl = {"gridInit": dict(panelKind=3, initNest=int(f["initNest"]), AMR=0, remeshInterval=1000,
                            amrTol1=1.0, amrTol2=1.0, useRelativeTol=0, maxRefine=0),
           "time": dict(dt=float(f["dt"]), tfinal=float(f["tfinal"])), "fileIO": dict(jobPrefix="strat")}
-    run = REF.run_driver(nprocs, nl, cuda=True, lib_path=build.lib_path(), fp32c=fp32c, which="strat")
+    run = REF.run_driver(nprocs, nl, cuda=True, lib_path=N.LIB_PATH, fp32c=fp32c, which="strat")
     rows, ref = run["rows"], f["rows"]
     assert rows.shape == ref.shape
     tol = TOL[fp32c]
@@ -153,7 +153,7 @@ def test_other_reference_drivers_with_their_use_line_switched(which, gpu):
                     "reference's sources are present")
     f = _load("ref_drivers_l2")
     nl = json.loads(str(f[f"{which}_namelist"]))
-    run = REF.run_driver(2, nl, cuda=True, lib_path=build.lib_path(), which=which)
+    run = REF.run_driver(2, nl, cuda=True, lib_path=N.LIB_PATH, which=which)
     ref = f[f"{which}_rows"]
     assert run["rows"].shape == ref.shape
     assert np.allclose(run["rows"], ref, rtol=1e-10, atol=1e-12), np.abs(run["rows"] - ref).max()

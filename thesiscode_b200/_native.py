@@ -8,10 +8,15 @@ the library's CUDA status, which is raised as ``TcError``.
 from __future__ import annotations
 
 import ctypes
+import os
 from ctypes import POINTER, c_char_p, c_double, c_int, c_void_p
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libthesiscode_b200.so"
+LIB_DIR = Path(__file__).resolve().parent / "_lib"
+# TC_LIBRARY=checked loads the build whose hot-path kernels check every
+# global-memory index (tc_bounds_*); anything else loads the release build.
+CHECKED = os.environ.get("TC_LIBRARY", "") == "checked"
+LIB_PATH = LIB_DIR / ("libthesiscode_b200_checked.so" if CHECKED else "libthesiscode_b200.so")
 
 # status codes
 TC_OK = 0
@@ -42,6 +47,17 @@ TC_J_ENSTROPHY = 0
 TC_J_PROBE = 1
 # RK4 device buffers
 TC_BUF_SOURCES, TC_BUF_XA, TC_BUF_ZETA, TC_BUF_XV, TC_BUF_XQ, TC_BUF_KE = range(6)
+# index-check sites of the checked build (TC_BC_*), by id
+BC_SITES = {
+    1: "pair target positions", 2: "pair visiting order", 3: "pair packed sources",
+    4: "pair partial-sum stores", 5: "batch segment table", 6: "packing inputs",
+    7: "packing stores", 8: "velocity epilogue visiting order",
+    9: "velocity epilogue target positions", 10: "velocity epilogue partial sums",
+    11: "velocity epilogue stores", 12: "stage epilogue visiting orders",
+    13: "stage epilogue state arrays", 14: "stage epilogue partial sums",
+    15: "stage epilogue chunk counts", 16: "stage epilogue active-only arrays",
+    17: "stage epilogue KE block sums",
+}
 
 _STATUS = {
     TC_ERR_ARG: "bad argument",
@@ -116,6 +132,9 @@ SIGNATURES: dict[str, tuple] = {
     "tc_icos_grid": (c_int, [c_int, dp, dp, dp, dp, dp, ip, ip, ip, ip]),
     "tc_icos_grid_device": (c_int, [c_void_p, c_int] + [c_void_p] * 9),
     "tc_gather_maps": (c_int, [c_int, ip, ip, c_int, ip, c_int]),
+    "tc_bounds_checked": (c_int, []),
+    "tc_bounds_status": (c_int, [c_int, POINTER(ctypes.c_longlong), c_int]),
+    "tc_bounds_cap": (c_int, [c_void_p, c_int, ctypes.c_longlong]),
 }
 
 
@@ -137,7 +156,8 @@ def lib() -> ctypes.CDLL:
         if not LIB_PATH.exists():
             raise ImportError(
                 f"{LIB_PATH} is missing: build the sm_100a library with "
-                "`python -m thesiscode_b200.build` (no CPU fallback exists)")
+                f"`python -m thesiscode_b200.build{' --checked' if CHECKED else ''}` "
+                "(no CPU fallback exists)")
         handle = ctypes.CDLL(str(LIB_PATH))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(handle, name)
@@ -169,3 +189,12 @@ def iptr(a) -> ctypes._Pointer:
     if a is None:
         return None
     return a.ctypes.data_as(ip)
+
+
+def bounds_status(device: int = 0, reset: bool = False) -> dict:
+    """The device's index-check record (checked build; zeros in the release
+    build): violations, and site, index and extent of the first."""
+    rec = (ctypes.c_longlong * 4)()
+    call("tc_bounds_status", device, rec, 1 if reset else 0)
+    return {"count": rec[0], "site": rec[1], "site_name": BC_SITES.get(rec[1], ""),
+            "index": rec[2], "extent": rec[3]}

@@ -6,6 +6,12 @@ Every CUDA and C++ source under ``csrc/`` is compiled by nvcc for
 types in its ABI and links only the CUDA runtime, so a C, C++ or Fortran
 caller can load it directly. Objects are rebuilt only when a source or
 header is newer than the library.
+
+``--checked`` builds the same sources with ``-DTC_BOUNDS_CHECK=1`` into
+``libthesiscode_b200_checked.so``: its hot-path kernels check every
+global-memory index against its array's extent and record violations
+(tc_bounds_status) instead of accessing out of range. ``TC_LIBRARY=checked``
+makes the Python package load it.
 """
 from __future__ import annotations
 
@@ -45,8 +51,11 @@ def headers() -> list[Path]:
     return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
 
 
-def lib_path() -> Path:
-    return LIBDIR / LIBNAME
+CHECKED_LIBNAME = "libthesiscode_b200_checked.so"
+
+
+def lib_path(checked: bool = False) -> Path:
+    return LIBDIR / (CHECKED_LIBNAME if checked else LIBNAME)
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -56,10 +65,12 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    """Compile csrc/ into _lib/libthesiscode_b200.so; returns the library path."""
+def build(verbose: bool = False, force: bool = False, checked: bool = False) -> Path:
+    """Compile csrc/ into _lib/libthesiscode_b200.so (checked: the index-checked
+    libthesiscode_b200_checked.so); returns the library path."""
     nvcc = nvcc_path()
-    objdir = LIBDIR / "obj"
+    objdir = LIBDIR / ("obj_checked" if checked else "obj")
+    defines = ["-DTC_BOUNDS_CHECK=1"] if checked else []
     objdir.mkdir(parents=True, exist_ok=True)
     hdrs = headers()
     objs, cmds = [], []
@@ -67,7 +78,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         obj = objdir / (src.name + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
-            cmds.append([nvcc, *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)])
+            cmds.append([nvcc, *ARCH, *NVCC_FLAGS, *defines, f"-I{INCLUDE}", f"-I{CSRC}", "-c",
+                         str(src), "-o", str(obj)])
     # translation units are independent: compile them side by side
     from concurrent.futures import ThreadPoolExecutor
 
@@ -79,7 +91,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
         for f in [pool.submit(run, c) for c in cmds]:
             f.result()
-    lib = lib_path()
+    lib = lib_path(checked)
     if force or _stale(lib, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart"]
         if verbose:
@@ -89,4 +101,4 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, checked="--checked" in sys.argv))

@@ -150,11 +150,13 @@ int velocity_device(tc_ctx* ctx, int cls, const double* X, int m, const double* 
     perm = ctx->scratch[4].as<int>();
     if ((rc = tcb::compute_order(ctx, X, i0, i1, perm))) return rc;
   }
-  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
+  const long long src_len = (long long)(ctx->scratch[0].bytes / sizeof(double4));
+  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src, src_len))) return rc;
   SegDesc seg{X, perm, i0, i1, 0, cls == TC_ACTIVE ? 0 : tcb::kNoSelf,
-              ctx->delta[cls] * ctx->delta[cls]};
+              ctx->delta[cls] * ctx->delta[cls], m,
+              perm ? (long long)(ctx->scratch[4].bytes / sizeof(int)) : 0};
   int nch = 0;
-  if ((rc = tcb::launch_pairs(ctx, &seg, 1, src, n, m, &nch))) return rc;
+  if ((rc = tcb::launch_pairs(ctx, &seg, 1, src, n, src_len, m, &nch))) return rc;
   return tcb::launch_velocity_epilogue(ctx, X, perm, m, i0, i1, 0, m, nch, dX,
                                        cls == TC_ACTIVE ? dVort : nullptr);
 }
@@ -180,7 +182,7 @@ extern "C" int tc_create(int device, int precision, tc_ctx** out) {
   if (!ctx) return TC_ERR_NOMEM;
   ctx->device = device;
   ctx->precision = precision;
-  if ((rc = tcb::resolve_slots(ctx))) {
+  if ((rc = tcb::resolve_slots(ctx)) || (rc = tcb::bounds_attach(ctx))) {
     delete ctx;
     return rc;
   }
@@ -597,15 +599,27 @@ extern "C" int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int
     R.ordered = true;
   }
   const bool ord = want_order && R.ordered;
+  // extents (checked build): the class's stage-input buffer and visiting order
+  const tcb::DevBuf* xb[3] = {first ? &R.x0A : &R.xiA, first ? &R.x0V : &R.xiV,
+                              first ? &R.x0Q : &R.xiQ};
+  const tcb::DevBuf* pbuf[3] = {&R.permA, &R.permV, &R.permQ};
+  long long xl[3], pl[3];
+  for (int c = 0; c < 3; ++c) {
+    xl[c] = (long long)(xb[c]->bytes / (3 * sizeof(double)));
+    pl[c] = ord ? (long long)(pbuf[c]->bytes / sizeof(int)) : 0;
+  }
   SegDesc segs[3] = {
-      {tx[0], ord ? R.permA.as<int>() : nullptr, a0, a1, 0, 0, ctx->delta[0] * ctx->delta[0]},
+      {tx[0], ord ? R.permA.as<int>() : nullptr, a0, a1, 0, 0, ctx->delta[0] * ctx->delta[0],
+       xl[0], pl[0]},
       {tx[1], ord ? R.permV.as<int>() : nullptr, v0, v1, R.nA, tcb::kNoSelf,
-       ctx->delta[1] * ctx->delta[1]},
+       ctx->delta[1] * ctx->delta[1], xl[1], pl[1]},
       {tx[2], ord ? R.permQ.as<int>() : nullptr, q0, q1, R.nA + R.nV, tcb::kNoSelf,
-       ctx->delta[2] * ctx->delta[2]}};
+       ctx->delta[2] * ctx->delta[2], xl[2], pl[2]}};
   int nch = 0;
   const int n_out = R.nA + R.nV + R.nQ;
-  if ((rc = tcb::launch_pairs(ctx, segs, 3, R.src.as<double4>(), R.nA, n_out, &nch))) return rc;
+  if ((rc = tcb::launch_pairs(ctx, segs, 3, R.src.as<double4>(), R.nA,
+                              (long long)(R.src.bytes / sizeof(double4)), n_out, &nch)))
+    return rc;
   if ((rc = tcb::launch_stage_epilogue(ctx, stage, dt, range, nch, total_ke_device))) return rc;
   if (stage == 3 && R.strat) ++R.step;
   return TC_OK;
@@ -619,7 +633,7 @@ extern "C" int tc_rk4_pack_sources(tc_ctx* ctx) {
   if (!R.ready) return TC_ERR_STATE;
   if (R.strat) return tcb::launch_pack_strat(ctx, R.t0 + (double)R.step * R.strat_dt);
   return tcb::launch_pack(ctx, R.x0A.as<double>(), R.z0.as<double>(), R.areaA.as<double>(), R.nA,
-                          R.src.as<double4>());
+                          R.src.as<double4>(), (long long)(R.src.bytes / sizeof(double4)));
 }
 
 extern "C" int tc_rk4_device_buffer(tc_ctx* ctx, int which, void** ptr) {

@@ -175,9 +175,12 @@ int upload_segments(tc_ctx* ctx, tc_batch_plan& B) {
       g.out_offset = cls == 0 ? 0 : B.nA_tot;
       g.self_offset = cls == 0 ? 0 : tcb::kNoSelf;
       g.d2 = ctx->delta[cls] * ctx->delta[cls];
+      g.perm_len = g.perm ? (long long)((cls == 0 ? R.permA : R.permV).bytes / sizeof(int)) : 0;
       g.x = cls == 0 ? R.x0A.as<double>() : R.x0V.as<double>();
+      g.x_len = (long long)((cls == 0 ? R.x0A : R.x0V).bytes / (3 * sizeof(double)));
       s0.push_back(g);
       g.x = cls == 0 ? R.xiA.as<double>() : R.xiV.as<double>();
+      g.x_len = (long long)((cls == 0 ? R.xiA : R.xiV).bytes / (3 * sizeof(double)));
       s1.push_back(g);
     }
   int rc;
@@ -201,6 +204,12 @@ int launch_batch_pairs(tc_ctx* ctx, tc_batch_plan& B, int stage) {
   L.src = ctx->rk.src.as<double4>();
   L.partial = B.partial.as<double>();
   L.stride = (size_t)(B.nA_tot + B.nV_tot);
+  L.bc = ctx->bc_rec;
+  L.n_segs = (int)tcb::bc_extent(ctx, tcb::BC_BATCH_SEG, 2 * B.count);
+  L.src_len =
+      tcb::bc_extent(ctx, tcb::BC_PAIR_SRC, (long long)(ctx->rk.src.bytes / sizeof(double4)));
+  L.partial_len =
+      tcb::bc_extent(ctx, tcb::BC_PAIR_OUT, (long long)(B.partial.bytes / sizeof(double)));
   v->launch_batch(B.slots, ctx->stream, L);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
@@ -216,8 +225,10 @@ int enqueue_steps(tc_ctx* ctx, tc_batch_plan& B, double dt, int nsteps) {
   for (int step = 0; step < nsteps; ++step)
     for (int s = 0; s < 4; ++s) {
       if ((rc = launch_batch_pairs(ctx, B, s))) return rc;
-      if ((rc = tcb::launch_stage_epilogue(ctx, s, dt, range, 0, nullptr, B.row_nchunks.as<int>(),
-                                           B.partial.as<double>())))
+      if ((rc = tcb::launch_stage_epilogue(
+               ctx, s, dt, range, 0, nullptr, B.row_nchunks.as<int>(), B.partial.as<double>(),
+               (long long)(B.row_nchunks.bytes / sizeof(int)),
+               (long long)(B.partial.bytes / sizeof(double)))))
         return rc;
       if (s == 0) {
         ke_segments_kernel<<<B.count, 256, 0, ctx->stream>>>(

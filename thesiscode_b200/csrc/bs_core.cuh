@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "bounds.cuh"
+
 namespace tcb {
 
 constexpr int kNoSelf = INT32_MIN;
@@ -28,6 +30,8 @@ struct TargetSeg {
   int self_offset;  // source index of target i is i + self_offset (ACTIVE), else kNoSelf
   double d2;        // delta^2 for this class
   int tile_begin;   // first blockIdx.x of this segment
+  long long x_len;     // checked build: points in x
+  long long perm_len;  // checked build: entries in perm
 };
 
 struct PairLaunch {
@@ -38,6 +42,17 @@ struct PairLaunch {
   int chunk_len;        // sources per blockIdx.y chunk (multiple of the tile)
   double* partial;      // partial[(chunk*3 + c)*n_out + row]
   int n_out;
+  BoundsRec* bc;        // checked build: violation record (null: release build)
+  long long src_len;    // checked build: packed sources in src
+  long long partial_len;  // checked build: doubles in partial
+};
+
+// Extents a work unit checks its global indices against (checked build).
+struct UnitBounds {
+  BoundsRec* rec;
+  long long x_len, perm_len, src_len;
+  long long out_base;  // offset of the unit's out pointer within the partial sums
+  long long out_len;   // doubles in the partial sums
 };
 
 // ---------------------------------------------------------------------------
@@ -103,7 +118,8 @@ template <int NT, int TPT, int TS, bool FUSED>
 __device__ __forceinline__ void fp64_unit(const double* __restrict__ x, int tile0, int i_end,
                                           int self_offset, double d2,
                                           const double4* __restrict__ src, int c0, int c1,
-                                          double* __restrict__ out, size_t stride, double4* sm) {
+                                          double* __restrict__ out, size_t stride, double4* sm,
+                                          const UnitBounds& ub) {
   constexpr int TB = NT * TPT;
   const double one_plus_d2 = 1.0 + d2;
   const bool has_self = self_offset != kNoSelf;
@@ -114,9 +130,10 @@ __device__ __forceinline__ void fp64_unit(const double* __restrict__ x, int tile
   for (int t = 0; t < TPT; ++t) {
     int i = tile0 + (int)threadIdx.x + t * NT;
     int ld = i < i_end ? i : tile0;
-    xi[t][0] = x[3 * (size_t)ld];
-    xi[t][1] = x[3 * (size_t)ld + 1];
-    xi[t][2] = x[3 * (size_t)ld + 2];
+    const bool okx = TC_BC(ub.rec, BC_PAIR_X, ld, ub.x_len);
+    xi[t][0] = okx ? x[3 * (size_t)ld] : 0.0;
+    xi[t][1] = okx ? x[3 * (size_t)ld + 1] : 0.0;
+    xi[t][2] = okx ? x[3 * (size_t)ld + 2] : 0.0;
     acc[t][0] = acc[t][1] = acc[t][2] = 0.0;
     self_k[t] = has_self ? i + self_offset : -1;
   }
@@ -127,7 +144,9 @@ __device__ __forceinline__ void fp64_unit(const double* __restrict__ x, int tile
     __syncthreads();
     for (int j = threadIdx.x; j < TS; j += NT) {
       int k = ts + j;
-      sm[j] = k < c1 ? src[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sm[j] = (k < c1 && TC_BC(ub.rec, BC_PAIR_SRC, k, ub.src_len))
+                  ? src[k]
+                  : make_double4(0.0, 0.0, 0.0, 0.0);
     }
     __syncthreads();
     const bool diag = has_self && ts < self_hi && self_lo < ts + TS;
@@ -164,9 +183,11 @@ __device__ __forceinline__ void fp64_unit(const double* __restrict__ x, int tile
   for (int t = 0; t < TPT; ++t) {
     int i = tile0 + (int)threadIdx.x + t * NT;
     if (i < i_end) {
-      out[i] = acc[t][0];
-      out[stride + i] = acc[t][1];
-      out[2 * stride + i] = acc[t][2];
+      if (TC_BC(ub.rec, BC_PAIR_OUT, ub.out_base + i, ub.out_len)) out[i] = acc[t][0];
+      if (TC_BC(ub.rec, BC_PAIR_OUT, ub.out_base + (long long)stride + i, ub.out_len))
+        out[stride + i] = acc[t][1];
+      if (TC_BC(ub.rec, BC_PAIR_OUT, ub.out_base + 2 * (long long)stride + i, ub.out_len))
+        out[2 * stride + i] = acc[t][2];
     }
   }
 }
@@ -179,9 +200,11 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_kernel(const PairLaunch P)
   const int c0 = (int)blockIdx.y * P.chunk_len;
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
-  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+  const long long base = (long long)blockIdx.y * 3 * (long long)stride + G.out_offset;
+  double* out = P.partial + base;
+  const UnitBounds ub{P.bc, G.x_len, G.perm_len, P.src_len, base, P.partial_len};
   fp64_unit<NT, TPT, TS, FUSED>(G.x, tile0, G.i1, G.self_offset, G.d2, P.src, c0, c1, out, stride,
-                                sm);
+                                sm, ub);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,7 +407,7 @@ struct SpAcc {
 // padding past c1; records each warp's minimum |s_k|^2.
 template <int NT, int TS, bool HILO, class Smem>
 __device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts, int c1,
-                                         const double* fr, Smem& sm) {
+                                         const double* fr, Smem& sm, const UnitBounds& ub) {
   constexpr int NP = TS / 2;
   float smin = __int_as_float(0x7f800000);  // +inf
   for (int jp = threadIdx.x; jp < NP; jp += NT) {
@@ -399,7 +422,7 @@ __device__ __forceinline__ void sp_stage(const double4* __restrict__ src, int ts
       v[h][7] = 1.f;
       v[h][8] = 0.f;
       v[h][9] = v[h][10] = v[h][11] = 0.f;
-      if (k < c1) {
+      if (k < c1 && TC_BC(ub.rec, BC_PAIR_SRC, k, ub.src_len)) {
         const double4 q = src[k];
         const double dx = q.x - fr[9], dy = q.y - fr[10], dz = q.z - fr[11];
         const double sxd = frame_dot(fr, dx, dy, dz), syd = frame_dot(fr + 3, dx, dy, dz),
@@ -543,15 +566,22 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
                                               int tile0, int i_end, double d2,
                                               const double4* __restrict__ src, int c0, int c1,
                                               double* __restrict__ out, size_t stride,
-                                              SpSmem<NT, TS, T, SMACC, HILO>& sm) {
+                                              SpSmem<NT, TS, T, SMACC, HILO>& sm,
+                                              const UnitBounds& ub) {
   static_assert(TS % FLUSH == 0 && FLUSH % 2 == 0, "flush interval: even, divides the tile");
   static_assert(NT % 32 == 0, "whole warps");
   static_assert(TS % (FLUSH * FARK) == 0, "far-tile flush interval divides the tile");
   constexpr int TB = NT * T;
-  constexpr int NP = TS / 2;
 
   const int mid_pos = min(tile0 + TB / 2, i_end - 1);
-  const int mid = perm ? perm[mid_pos] : mid_pos;
+  int mid = mid_pos;
+  if (perm) mid = TC_BC(ub.rec, BC_PAIR_PERM, mid_pos, ub.perm_len) ? perm[mid_pos] : 0;
+  // checked build: an out-of-range target index reads point 0 instead (and is recorded)
+  auto target = [&](int p) -> int {
+    int ld = p;
+    if (perm) ld = TC_BC(ub.rec, BC_PAIR_PERM, p, ub.perm_len) ? perm[p] : 0;
+    return TC_BC(ub.rec, BC_PAIR_X, ld, ub.x_len) ? ld : 0;
+  };
   // Origin: the CTA's targets' centroid, projected to the sphere (a smaller
   // patch radius than any one target gives: fewer near tiles, smaller FP32
   // offsets); the middle target when the targets surround the centre.
@@ -560,7 +590,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   for (int t = 0; t < T; ++t) {
     const int pos = tile0 + (int)threadIdx.x + t * NT;
     if (pos < i_end) {
-      const int ld = perm ? perm[pos] : pos;
+      const int ld = target(pos);
       px += x[3 * (size_t)ld];
       py += x[3 * (size_t)ld + 1];
       pz += x[3 * (size_t)ld + 2];
@@ -595,9 +625,10 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
       cy = sy * inv;
       cz = sz * inv;
     } else {
-      cx = x[3 * (size_t)mid];
-      cy = x[3 * (size_t)mid + 1];
-      cz = x[3 * (size_t)mid + 2];
+      const int c = TC_BC(ub.rec, BC_PAIR_X, mid, ub.x_len) ? mid : 0;
+      cx = x[3 * (size_t)c];
+      cy = x[3 * (size_t)c + 1];
+      cz = x[3 * (size_t)c + 2];
     }
     make_frame(cx, cy, cz, sm.frame);
     sm.frame[9] = cx;
@@ -617,7 +648,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
 #pragma unroll
   for (int t = 0; t < T; ++t) {
     const int pos = tile0 + (int)threadIdx.x + t * NT;
-    const int ld = pos < i_end ? (perm ? perm[pos] : pos) : mid;
+    const int ld = pos < i_end ? target(pos) : (TC_BC(ub.rec, BC_PAIR_X, mid, ub.x_len) ? mid : 0);
     const double px = x[3 * (size_t)ld], py = x[3 * (size_t)ld + 1], pz = x[3 * (size_t)ld + 2];
     const double dx = px - cx, dy = py - cy, dz = pz - cz;
     const double txd = frame_dot(fr, dx, dy, dz), tyd = frame_dot(fr + 3, dx, dy, dz),
@@ -642,7 +673,7 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
   warp_store_max(rho2, sm.rho);
   for (int ts = c0; ts < c1; ts += TS) {
     __syncthreads();
-    sp_stage<NT, TS, HILO>(src, ts, c1, fr, sm);
+    sp_stage<NT, TS, HILO>(src, ts, c1, fr, sm, ub);
     __syncthreads();
     sp_sum<NT, T, TS, FLUSH, UNROLL, SMACC, HILO, FARK>(sm, ntx, nty, ntz, bh, ei, fx, fy, fz, acc);
   }
@@ -652,9 +683,12 @@ __device__ __forceinline__ void fp32c_sp_unit(const double* __restrict__ x, cons
     const int pos = tile0 + (int)threadIdx.x + t * NT;
     if (pos < i_end) {
       const double ax = acc.get(0, t), ay = acc.get(1, t), az = acc.get(2, t);
-      out[pos] = fma(fr[0], ax, fma(fr[3], ay, fr[6] * az));
-      out[stride + pos] = fma(fr[1], ax, fma(fr[4], ay, fr[7] * az));
-      out[2 * stride + pos] = fma(fr[2], ax, fma(fr[5], ay, fr[8] * az));
+      if (TC_BC(ub.rec, BC_PAIR_OUT, ub.out_base + pos, ub.out_len))
+        out[pos] = fma(fr[0], ax, fma(fr[3], ay, fr[6] * az));
+      if (TC_BC(ub.rec, BC_PAIR_OUT, ub.out_base + (long long)stride + pos, ub.out_len))
+        out[stride + pos] = fma(fr[1], ax, fma(fr[4], ay, fr[7] * az));
+      if (TC_BC(ub.rec, BC_PAIR_OUT, ub.out_base + 2 * (long long)stride + pos, ub.out_len))
+        out[2 * stride + pos] = fma(fr[2], ax, fma(fr[5], ay, fr[8] * az));
     }
   }
 }
@@ -675,11 +709,13 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_kernel(const PairLaunch P
   const int c0 = (int)blockIdx.y * P.chunk_len;
   const int c1 = min(P.n, c0 + P.chunk_len);
   const size_t stride = (size_t)P.n_out;
-  double* out = P.partial + (size_t)blockIdx.y * 3 * stride + G.out_offset;
+  const long long base = (long long)blockIdx.y * 3 * (long long)stride + G.out_offset;
+  double* out = P.partial + base;
+  const UnitBounds ub{P.bc, G.x_len, G.perm_len, P.src_len, base, P.partial_len};
   __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
   fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(G.x, G.perm, tile0, G.i1,
                                                                       G.d2, P.src, c0, c1, out,
-                                                                      stride, sm);
+                                                                      stride, sm, ub);
 }
 
 // ---------------------------------------------------------------------------
@@ -696,6 +732,8 @@ struct BatchSeg {
   int out_offset;    // partial row of target position p is out_offset + p
   int self_offset;   // TC_ACTIVE: source index of target i is i + self_offset
   double d2;
+  long long x_len;     // checked build: points in x
+  long long perm_len;  // checked build: entries in perm
 };
 
 struct BatchItem {
@@ -713,6 +751,10 @@ struct BatchLaunch {
   const double4* src;
   double* partial;   // partial[(chunk*3 + c)*stride + row]
   size_t stride;
+  BoundsRec* bc;          // checked build: violation record (null: release build)
+  int n_segs;             // checked build: entries in segs
+  long long src_len;      // checked build: packed sources in src
+  long long partial_len;  // checked build: doubles in partial
 };
 
 __device__ __forceinline__ int next_item(int* counter, int* slot) {
@@ -729,10 +771,13 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp32c_batch_kernel(const BatchL
   __shared__ SpSmem<NT, TS, T, F::smacc, F::hilo> sm;
   for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
     const BatchItem I = B.items[it];
+    if (!TC_BC(B.bc, BC_BATCH_SEG, I.seg, B.n_segs)) continue;
     const BatchSeg S = B.segs[I.seg];
-    double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+    const long long base = (long long)I.chunk * 3 * (long long)B.stride + S.out_offset;
+    double* out = B.partial + base;
+    const UnitBounds ub{B.bc, S.x_len, S.perm_len, B.src_len, base, B.partial_len};
     fp32c_sp_unit<NT, T, TS, FLUSH, UNROLL, F::smacc, F::hilo, F::fark>(
-        S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm);
+        S.x, S.perm, I.tile0, I.i1, S.d2, B.src, I.c0, I.c1, out, B.stride, sm, ub);
   }
 }
 
@@ -742,10 +787,13 @@ __global__ void __launch_bounds__(NT, MINB) pair_fp64_batch_kernel(const BatchLa
   __shared__ int slot;
   for (int it = next_item(B.counter, &slot); it < B.n_items; it = next_item(B.counter, &slot)) {
     const BatchItem I = B.items[it];
+    if (!TC_BC(B.bc, BC_BATCH_SEG, I.seg, B.n_segs)) continue;
     const BatchSeg S = B.segs[I.seg];
-    double* out = B.partial + (size_t)I.chunk * 3 * B.stride + S.out_offset;
+    const long long base = (long long)I.chunk * 3 * (long long)B.stride + S.out_offset;
+    double* out = B.partial + base;
+    const UnitBounds ub{B.bc, S.x_len, S.perm_len, B.src_len, base, B.partial_len};
     fp64_unit<NT, TPT, TS, FUSED>(S.x, I.tile0, I.i1, S.self_offset, S.d2, B.src, I.c0, I.c1, out,
-                                  B.stride, sm);
+                                  B.stride, sm, ub);
   }
 }
 

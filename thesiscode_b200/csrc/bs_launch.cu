@@ -173,7 +173,7 @@ static int choose_chunks(int tiles, int n, int ts, int slots, int min_chunk, int
 // Tiles and chunking of one pair launch: the target segments, the grid and the
 // chunk length (partial sums need S * 3 * n_out doubles).
 static int plan_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
-                      int n_out, int max_chunks, PairLaunch* P, dim3* grid) {
+                      long long src_len, int n_out, int max_chunks, PairLaunch* P, dim3* grid) {
   const bool fp64 = ctx->precision == TC_FP64;
   if (!fp64) {
     const int rc0 = use_fp32c_variant(ctx, n);
@@ -194,6 +194,8 @@ static int plan_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4*
     g.out_offset = segs[s].out_offset;
     g.self_offset = segs[s].self_offset;
     g.d2 = segs[s].d2;
+    g.x_len = bc_extent(ctx, BC_PAIR_X, segs[s].x_len);
+    g.perm_len = bc_extent(ctx, BC_PAIR_PERM, segs[s].perm_len);
     g.tile_begin = tiles;
     tiles += (len + tb - 1) / tb;
   }
@@ -209,6 +211,8 @@ static int plan_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4*
   P->n = n;
   P->chunk_len = chunk_len;
   P->n_out = n_out;
+  P->bc = ctx->bc_rec;
+  P->src_len = bc_extent(ctx, BC_PAIR_SRC, src_len);
   *grid = dim3(tiles, S);
   return TC_OK;
 }
@@ -238,27 +242,29 @@ static int run_pairs(tc_ctx* ctx, const PairLaunch& P, dim3 grid) {
 }
 
 int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
-                 int n_out, int* nchunks) {
+                 long long src_len, int n_out, int* nchunks) {
   *nchunks = 0;
   PairLaunch P;
   dim3 grid;
-  int rc = plan_pairs(ctx, segs, nseg, src, n, n_out, ctx->max_chunks, &P, &grid);
+  int rc = plan_pairs(ctx, segs, nseg, src, n, src_len, n_out, ctx->max_chunks, &P, &grid);
   if (rc || grid.y == 0) return rc;
   if ((rc = ctx->partial.ensure((size_t)grid.y * 3 * (size_t)n_out * sizeof(double)))) return rc;
   P.partial = ctx->partial.as<double>();
+  P.partial_len = bc_extent(ctx, BC_PAIR_OUT, (long long)(ctx->partial.bytes / sizeof(double)));
   if ((rc = run_pairs(ctx, P, grid))) return rc;
   *nchunks = (int)grid.y;
   return TC_OK;
 }
 
 int launch_pairs_into(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
-                      int n_out, double* partial, size_t partial_bytes, int* nchunks) {
+                      long long src_len, int n_out, double* partial, size_t partial_bytes,
+                      int* nchunks) {
   *nchunks = 0;
   const size_t per_chunk = 3 * (size_t)n_out * sizeof(double);
   const size_t fit = per_chunk ? partial_bytes / per_chunk : (size_t)ctx->max_chunks;
   PairLaunch P;
   dim3 grid;
-  int rc = plan_pairs(ctx, segs, nseg, src, n, n_out,
+  int rc = plan_pairs(ctx, segs, nseg, src, n, src_len, n_out,
                       (int)std::max<size_t>(1, std::min<size_t>(fit, (size_t)ctx->max_chunks)), &P,
                       &grid);
   if (rc || grid.y == 0) return rc;
@@ -268,6 +274,7 @@ int launch_pairs_into(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4*
     return TC_ERR_ARG;
   }
   P.partial = partial;
+  P.partial_len = bc_extent(ctx, BC_PAIR_OUT, (long long)(partial_bytes / sizeof(double)));
   if ((rc = run_pairs(ctx, P, grid))) return rc;
   *nchunks = (int)grid.y;
   return TC_OK;
@@ -276,10 +283,19 @@ int launch_pairs_into(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4*
 // ---------------------------------------------------------------------------
 // Packing: {x, y, z, zeta*area} per source.
 // ---------------------------------------------------------------------------
+// Checked build: extents of the packing's inputs (points) and output.
+struct PackBounds {
+  BoundsRec* rec;
+  long long in_len, out_len;
+};
+
 __global__ void pack_kernel(const double* __restrict__ x, const double* __restrict__ zeta,
-                            const double* __restrict__ area, int n, double4* __restrict__ out) {
+                            const double* __restrict__ area, int n, double4* __restrict__ out,
+                            const PackBounds pb) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
+  if (!TC_BC(pb.rec, BC_PACK_IN, k, pb.in_len)) return;
+  if (!TC_BC(pb.rec, BC_PACK_OUT, k, pb.out_len)) return;
   out[k] = make_double4(x[3 * (size_t)k], x[3 * (size_t)k + 1], x[3 * (size_t)k + 2],
                         __dmul_rn(zeta[k], area[k]));
 }
@@ -328,9 +344,11 @@ int launch_strat_rel_vort(tc_ctx* ctx, const double* abs_vort, const double* x, 
 }
 
 int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* area, int n,
-                double4* out) {
+                double4* out, long long out_len) {
   if (n <= 0) return TC_OK;
-  pack_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(x, zeta, area, n, out);
+  const PackBounds pb{ctx->bc_rec, bc_extent(ctx, BC_PACK_IN, n),
+                      bc_extent(ctx, BC_PACK_OUT, out_len)};
+  pack_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(x, zeta, area, n, out, pb);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
   return TC_OK;
@@ -339,14 +357,19 @@ int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* 
 // ---------------------------------------------------------------------------
 // Shared epilogue math.
 // ---------------------------------------------------------------------------
+// Sum of a partial row over the chunks; the checked build checks each read
+// against partial_len doubles (site: BC_EPI_PARTIAL or BC_STAGE_PARTIAL).
 __device__ __forceinline__ void reduce_row(const double* __restrict__ partial, int nchunks,
-                                           size_t n_out, size_t row, double T[3]) {
+                                           size_t n_out, size_t row, double T[3],
+                                           BoundsRec* rec, int site, long long partial_len) {
   T[0] = T[1] = T[2] = 0.0;
   for (int c = 0; c < nchunks; ++c) {
-    const double* p = partial + (size_t)c * 3 * n_out + row;
-    T[0] += p[0];
-    T[1] += p[n_out];
-    T[2] += p[2 * n_out];
+    const size_t o = (size_t)c * 3 * n_out + row;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const size_t j = o + (size_t)k * n_out;
+      if (TC_BC(rec, site, j, partial_len)) T[k] += partial[j];
+    }
   }
 }
 
@@ -360,22 +383,35 @@ __device__ __forceinline__ void velocity_from_sum(const double x[3], const doubl
 
 // Thread p handles partial row p; with a visiting order perm (a permutation
 // of [i0, i1)) that row belongs to target perm[p].
+// Checked build: extents of the velocity epilogue's arrays.
+struct EpiBounds {
+  BoundsRec* rec;
+  long long x_len, perm_len, partial_len, out_len;
+};
+
 __global__ void velocity_epilogue_kernel(const double* __restrict__ x, const int* __restrict__ perm,
                                          int m, int i0, int i1, int row_offset, int n_out,
                                          int nchunks, const double* __restrict__ partial,
                                          double m2omega, double* __restrict__ dX,
-                                         double* __restrict__ dVort) {
+                                         double* __restrict__ dVort, const EpiBounds eb) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= m) return;
   const bool in_range = p >= i0 && p < i1;
-  const int i = (in_range && perm) ? perm[p] : p;
+  int i = p;
+  if (in_range && perm) {
+    if (!TC_BC(eb.rec, BC_EPI_PERM, p, eb.perm_len)) return;
+    i = perm[p];
+  }
   double u[3] = {0.0, 0.0, 0.0};
   if (in_range) {
+    if (!TC_BC(eb.rec, BC_EPI_X, i, eb.x_len)) return;
     double xi[3] = {x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2]};
     double T[3];
-    reduce_row(partial, nchunks, (size_t)n_out, (size_t)(row_offset + p), T);
+    reduce_row(partial, nchunks, (size_t)n_out, (size_t)(row_offset + p), T, eb.rec,
+               BC_EPI_PARTIAL, eb.partial_len);
     velocity_from_sum(xi, T, u);
   }
+  if (!TC_BC(eb.rec, BC_EPI_OUT, i, eb.out_len)) return;
   dX[3 * (size_t)i] = u[0];
   dX[3 * (size_t)i + 1] = u[1];
   dX[3 * (size_t)i + 2] = u[2];
@@ -383,11 +419,18 @@ __global__ void velocity_epilogue_kernel(const double* __restrict__ x, const int
 }
 
 int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int m, int i0, int i1,
-                             int row_offset, int n_out, int nchunks, double* dX, double* dVort) {
+                             int row_offset, int n_out, int nchunks, double* dX, double* dVort,
+                             const double* partial, long long partial_len) {
   if (m <= 0) return TC_OK;
+  if (!partial) {
+    partial = ctx->partial.as<double>();
+    partial_len = (long long)(ctx->partial.bytes / sizeof(double));
+  }
+  if (ctx->precision == TC_FP64) perm = nullptr;
+  const EpiBounds eb{ctx->bc_rec, bc_extent(ctx, BC_EPI_X, m), bc_extent(ctx, BC_EPI_PERM, m),
+                     bc_extent(ctx, BC_EPI_PARTIAL, partial_len), bc_extent(ctx, BC_EPI_OUT, m)};
   velocity_epilogue_kernel<<<(m + 255) / 256, 256, 0, ctx->stream>>>(
-      x, ctx->precision == TC_FP64 ? nullptr : perm, m, i0, i1, row_offset, n_out, nchunks,
-      ctx->partial.as<double>(), -2.0 * ctx->omega, dX, dVort);
+      x, perm, m, i0, i1, row_offset, n_out, nchunks, partial, -2.0 * ctx->omega, dX, dVort, eb);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
   return TC_OK;
@@ -421,6 +464,12 @@ struct StageEpi {
   const int* row_nchunks;            // batched runs: chunks of each partial row (null: nchunks)
   const double* absA;                // forced model: absolute vorticity (null: BVE)
   double two_omega, t_next;          // forced model: 2 Omega, time of the next stage input
+  // checked build: violation record and extents
+  BoundsRec* rec;
+  long long state_len[3];            // points in every state/stage array of each class
+  long long active_len;              // entries in every active-only array
+  long long perm_len[3];
+  long long partial_len, chunks_len, keblock_len;
 };
 
 constexpr int kEpiThreads = 256;
@@ -443,64 +492,76 @@ __global__ void __launch_bounds__(kEpiThreads) stage_epilogue_kernel(const Stage
       pos = E.q0 + (r - lenA - lenV);
     }
     const int* perm = cls == 0 ? E.permA : cls == 1 ? E.permV : E.permQ;
-    const int i = perm ? perm[pos] : pos;
-    const int row = (cls == 0 ? 0 : cls == 1 ? E.nA : E.nA + E.nV) + pos;
-    double* x0 = cls == 0 ? E.x0A : cls == 1 ? E.x0V : E.x0Q;
-    double* xi = cls == 0 ? E.xiA : cls == 1 ? E.xiV : E.xiQ;
-    double* nw = cls == 0 ? E.newA : cls == 1 ? E.newV : E.newQ;
-    const double* xin = E.stage == 0 ? x0 : xi;
-    const size_t b = 3 * (size_t)i;
-    double xs[3] = {xin[b], xin[b + 1], xin[b + 2]};
-    double T[3], u[3];
-    reduce_row(E.partial, E.row_nchunks ? E.row_nchunks[row] : E.nchunks, (size_t)E.n_out,
-               (size_t)row, T);
-    velocity_from_sum(xs, T, u);
-    if (cls == 0 && E.stage == 0) {
-      double k2 = __dadd_rn(__dadd_rn(__dmul_rn(u[0], u[0]), __dmul_rn(u[1], u[1])),
-                            __dmul_rn(u[2], u[2]));
-      E.ke[i] = k2;
-      ke_area = k2 * E.areaA[i];
+    int i = pos;
+    bool ok = true;
+    if (perm) {
+      ok = TC_BC(E.rec, BC_STAGE_PERM, pos, E.perm_len[cls]);
+      i = ok ? perm[pos] : 0;
     }
-    const double div = (E.stage == 0 || E.stage == 3) ? 6.0 : 3.0;
-    const double cnext = E.stage == 2 ? 1.0 : 0.5;
-    double xnext[3];
-    for (int c = 0; c < 3; ++c) {
-      double kc = __dmul_rn(E.dt, u[c]);  // rounded like the reference's dt*stage
-      double base = E.stage == 0 ? x0[b + c] : nw[b + c];
-      double nv = base + kc / div;
-      if (E.stage < 3) {
-        nw[b + c] = nv;
-        xnext[c] = x0[b + c] + (E.stage == 2 ? kc : cnext * kc);
-        xi[b + c] = xnext[c];
-      } else {
-        x0[b + c] = nv;
-        xnext[c] = nv;
+    ok = ok && TC_BC(E.rec, BC_STAGE_STATE, i, E.state_len[cls]);
+    if (cls == 0) ok = ok && TC_BC(E.rec, BC_STAGE_ACTIVE, i, E.active_len);
+    if (ok) {
+      const int row = (cls == 0 ? 0 : cls == 1 ? E.nA : E.nA + E.nV) + pos;
+      double* x0 = cls == 0 ? E.x0A : cls == 1 ? E.x0V : E.x0Q;
+      double* xi = cls == 0 ? E.xiA : cls == 1 ? E.xiV : E.xiQ;
+      double* nw = cls == 0 ? E.newA : cls == 1 ? E.newV : E.newQ;
+      const double* xin = E.stage == 0 ? x0 : xi;
+      const size_t b = 3 * (size_t)i;
+      double xs[3] = {xin[b], xin[b + 1], xin[b + 2]};
+      double T[3], u[3];
+      int nch = E.nchunks;
+      if (E.row_nchunks)
+        nch = TC_BC(E.rec, BC_STAGE_CHUNKS, row, E.chunks_len) ? E.row_nchunks[row] : 0;
+      reduce_row(E.partial, nch, (size_t)E.n_out, (size_t)row, T, E.rec, BC_STAGE_PARTIAL,
+                 E.partial_len);
+      velocity_from_sum(xs, T, u);
+      if (cls == 0 && E.stage == 0) {
+        double k2 = __dadd_rn(__dadd_rn(__dmul_rn(u[0], u[0]), __dmul_rn(u[1], u[1])),
+                              __dmul_rn(u[2], u[2]));
+        E.ke[i] = k2;
+        ke_area = k2 * E.areaA[i];
       }
-    }
-    if (cls == 0 && E.absA) {
-      // forced model (PanelVelocityParallel.f90:752-755, :800-803, :847-850, :908-911): the
-      // vorticity is not integrated; the next input is rebuilt from absVort at t_next
-      const double znext =
-          strat_rel_vort(E.absA[i], E.two_omega, xnext[0], xnext[1], xnext[2], E.t_next);
-      if (E.stage < 3)
-        E.ziA[i] = znext;
-      else
-        E.z0[i] = znext;
-      E.src[i] = make_double4(xnext[0], xnext[1], xnext[2], znext * E.areaA[i]);
-    } else if (cls == 0) {
-      double kz = __dmul_rn(E.dt, __dmul_rn(E.m2omega, u[2]));
-      double zbase = E.stage == 0 ? E.z0[i] : E.newZ[i];
-      double zn = zbase + kz / div;
-      double znext;
-      if (E.stage < 3) {
-        E.newZ[i] = zn;
-        znext = E.z0[i] + (E.stage == 2 ? kz : cnext * kz);
-        E.ziA[i] = znext;
-      } else {
-        E.z0[i] = zn;
-        znext = zn;
+      const double div = (E.stage == 0 || E.stage == 3) ? 6.0 : 3.0;
+      const double cnext = E.stage == 2 ? 1.0 : 0.5;
+      double xnext[3];
+      for (int c = 0; c < 3; ++c) {
+        double kc = __dmul_rn(E.dt, u[c]);  // rounded like the reference's dt*stage
+        double base = E.stage == 0 ? x0[b + c] : nw[b + c];
+        double nv = base + kc / div;
+        if (E.stage < 3) {
+          nw[b + c] = nv;
+          xnext[c] = x0[b + c] + (E.stage == 2 ? kc : cnext * kc);
+          xi[b + c] = xnext[c];
+        } else {
+          x0[b + c] = nv;
+          xnext[c] = nv;
+        }
       }
-      E.src[i] = make_double4(xnext[0], xnext[1], xnext[2], znext * E.areaA[i]);
+      if (cls == 0 && E.absA) {
+        // forced model (PanelVelocityParallel.f90:752-755, :800-803, :847-850, :908-911): the
+        // vorticity is not integrated; the next input is rebuilt from absVort at t_next
+        const double znext =
+            strat_rel_vort(E.absA[i], E.two_omega, xnext[0], xnext[1], xnext[2], E.t_next);
+        if (E.stage < 3)
+          E.ziA[i] = znext;
+        else
+          E.z0[i] = znext;
+        E.src[i] = make_double4(xnext[0], xnext[1], xnext[2], znext * E.areaA[i]);
+      } else if (cls == 0) {
+        double kz = __dmul_rn(E.dt, __dmul_rn(E.m2omega, u[2]));
+        double zbase = E.stage == 0 ? E.z0[i] : E.newZ[i];
+        double zn = zbase + kz / div;
+        double znext;
+        if (E.stage < 3) {
+          E.newZ[i] = zn;
+          znext = E.z0[i] + (E.stage == 2 ? kz : cnext * kz);
+          E.ziA[i] = znext;
+        } else {
+          E.z0[i] = zn;
+          znext = zn;
+        }
+        E.src[i] = make_double4(xnext[0], xnext[1], xnext[2], znext * E.areaA[i]);
+      }
     }
   }
   if (E.stage == 0) {
@@ -510,7 +571,8 @@ __global__ void __launch_bounds__(kEpiThreads) stage_epilogue_kernel(const Stage
       if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
       __syncthreads();
     }
-    if (threadIdx.x == 0) E.keBlocks[blockIdx.x] = red[0];
+    if (threadIdx.x == 0 && TC_BC(E.rec, BC_STAGE_KEBLOCK, blockIdx.x, E.keblock_len))
+      E.keBlocks[blockIdx.x] = red[0];
   }
 }
 
@@ -528,8 +590,15 @@ __global__ void ke_finalize_kernel(const double* __restrict__ blocks, int nblock
   if (threadIdx.x == 0) *out = 0.5 * red[0];
 }
 
+// Capacity of a context buffer in elements of T.
+template <class T>
+static long long cap_of(const DevBuf& b) {
+  return (long long)(b.bytes / sizeof(T));
+}
+
 int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
-                          double* total_ke, const int* row_nchunks, const double* partial) {
+                          double* total_ke, const int* row_nchunks, const double* partial,
+                          long long row_nchunks_len, long long partial_len) {
   Rk4State& R = ctx->rk;
   StageEpi E;
   E.row_nchunks = row_nchunks;
@@ -570,6 +639,23 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
   E.permQ = ordered ? R.permQ.as<int>() : nullptr;
   E.absA = R.strat ? R.absA.as<double>() : nullptr;
   E.two_omega = 2.0 * ctx->omega;
+  E.rec = ctx->bc_rec;
+  const DevBuf* cls_bufs[3][3] = {
+      {&R.x0A, &R.xiA, &R.newA}, {&R.x0V, &R.xiV, &R.newV}, {&R.x0Q, &R.xiQ, &R.newQ}};
+  const DevBuf* perm_bufs[3] = {&R.permA, &R.permV, &R.permQ};
+  for (int c = 0; c < 3; ++c) {
+    long long len = cap_of<double>(*cls_bufs[c][0]) / 3;
+    for (int b = 1; b < 3; ++b) len = std::min(len, cap_of<double>(*cls_bufs[c][b]) / 3);
+    E.state_len[c] = bc_extent(ctx, BC_STAGE_STATE, len);
+    E.perm_len[c] = bc_extent(ctx, BC_STAGE_PERM, cap_of<int>(*perm_bufs[c]));
+  }
+  long long alen = cap_of<double4>(R.src);
+  for (const DevBuf* b : {&R.z0, &R.ziA, &R.newZ, &R.areaA, &R.ke})
+    alen = std::min(alen, cap_of<double>(*b));
+  if (R.strat) alen = std::min(alen, cap_of<double>(R.absA));
+  E.active_len = bc_extent(ctx, BC_STAGE_ACTIVE, alen);
+  E.partial_len = bc_extent(ctx, BC_STAGE_PARTIAL, partial ? partial_len : cap_of<double>(ctx->partial));
+  E.chunks_len = bc_extent(ctx, BC_STAGE_CHUNKS, row_nchunks_len);
   // stage inputs at t, t + dt/2, t + dt/2, t + dt; after stage 4 the next step's t
   const double t_step = R.t0 + (double)R.step * dt;
   E.t_next = stage < 2 ? t_step + 0.5 * dt
@@ -581,6 +667,7 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
     if (rc) return rc;
     E.keBlocks = R.keBlocks.as<double>();
   }
+  E.keblock_len = bc_extent(ctx, BC_STAGE_KEBLOCK, cap_of<double>(R.keBlocks));
   stage_epilogue_kernel<<<blocks, kEpiThreads, 0, ctx->stream>>>(E);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;

@@ -176,19 +176,17 @@ extern "C" int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, cons
       return rc;
   }
   double* partial = reinterpret_cast<double*>(b + fixed);
-  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src))) return rc;
+  const long long src_len = (long long)(src_bytes / sizeof(double4));
+  if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src, src_len))) return rc;
   tcb::SegDesc seg{X, perm, i0, i1, 0, target_class == TC_ACTIVE ? 0 : tcb::kNoSelf,
-                   ctx->delta[target_class] * ctx->delta[target_class]};
+                   ctx->delta[target_class] * ctx->delta[target_class], m,
+                   perm ? (long long)(perm_bytes / sizeof(int)) : 0};
   int nchunks = 0;
-  if ((rc = tcb::launch_pairs_into(ctx, &seg, 1, src, n, m, partial, kNoAllocScratchBytes - fixed,
+  const size_t partial_bytes = kNoAllocScratchBytes - fixed;
+  if ((rc = tcb::launch_pairs_into(ctx, &seg, 1, src, n, src_len, m, partial, partial_bytes,
                                    &nchunks)))
     return rc;
-  if (m > 0) {
-    tcb::velocity_epilogue_kernel<<<(m + 255) / 256, 256, 0, ctx->stream>>>(
-        X, perm, m, i0, i1, 0, m, nchunks, partial, -2.0 * ctx->omega, dX,
-        target_class == TC_ACTIVE ? dVort : nullptr);
-    TC_CUDA_TRY(cudaGetLastError());
-    ctx->launches += 1;
-  }
-  return TC_OK;
+  return tcb::launch_velocity_epilogue(ctx, X, perm, m, i0, i1, 0, m, nchunks, dX,
+                                       target_class == TC_ACTIVE ? dVort : nullptr, partial,
+                                       (long long)(partial_bytes / sizeof(double)));
 }

@@ -53,6 +53,8 @@ struct SegDesc {
   int out_offset;
   int self_offset;
   double d2;
+  long long x_len;     // points in x (its allocation or the caller's declared size)
+  long long perm_len;  // entries in perm
 };
 
 // RK4 state and scratch kept on the device between calls (the reference's
@@ -121,27 +123,42 @@ struct tc_ctx {
   tc_batch_plan* batch = nullptr;
   tc_advance_graph* agraph = nullptr;
   int rk4_graphs = 1;  // tc_rk4_advance graph replay: 0 never, 1 small problems, 2 always
+  // checked build: the device's violation record, and per-site caps on the declared
+  // extents (tc_bounds_cap)
+  tcb::BoundsRec* bc_rec = nullptr;
+  bool bc_capped[tcb::BC_SITE_END] = {};
+  long long bc_cap[tcb::BC_SITE_END] = {};
 };
 
 namespace tcb {
-// Launch the pair kernel of ctx->precision over up to three target segments.
+// Checked build: the extent the kernels check `site`'s indices against, n or the
+// cap tc_bounds_cap set (the smaller).
+inline long long bc_extent(const tc_ctx* ctx, int site, long long n) {
+  return (ctx->bc_capped[site] && ctx->bc_cap[site] < n) ? ctx->bc_cap[site] : n;
+}
+// Launch the pair kernel of ctx->precision over up to three target segments
+// (src_len: packed sources the src allocation holds, at least n).
 // Allocates ctx->partial and returns the number of source chunks in *nchunks.
 int launch_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
-                 int n_out, int* nchunks);
+                 long long src_len, int n_out, int* nchunks);
 // The same with the partial sums in caller-provided memory of partial_bytes bytes (at least one
 // chunk, 24 * n_out bytes); the chunk count is capped by what fits. Allocates nothing.
 int launch_pairs_into(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4* src, int n,
-                      int n_out, double* partial, size_t partial_bytes, int* nchunks);
+                      long long src_len, int n_out, double* partial, size_t partial_bytes,
+                      int* nchunks);
 // Pack {x, y, z, zeta*area} for n sources.
 int launch_pack_strat(tc_ctx* ctx, double t);
 int launch_strat_rel_vort(tc_ctx* ctx, const double* abs_vort, const double* x, int n, double t,
                           double* out);
+// out_len: packed sources the out allocation holds (at least n).
 int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* area, int n,
-                double4* out);
+                double4* out, long long out_len);
 // dX (3*m) and dVort (m, nullable) for rows [i0, i1), zero elsewhere; partial
-// rows are row_offset + i.
+// rows are row_offset + i. The partial sums are ctx->partial, or `partial`
+// (partial_len doubles) when that is given.
 int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int m, int i0, int i1,
-                             int row_offset, int n_out, int nchunks, double* dX, double* dVort);
+                             int row_offset, int n_out, int nchunks, double* dX, double* dVort,
+                             const double* partial = nullptr, long long partial_len = 0);
 // perm[i0..i1) <- i0..i1-1 sorted along the cube-face Hilbert curve (sphere_order.cuh)
 int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm);
 // The same in caller-provided scratch (keys in/out and indices: i1 - i0 entries each; temp:
@@ -152,19 +169,16 @@ int compute_order_into(tc_ctx* ctx, const double* x, int i0, int i1, int* perm, 
 // One RK4 stage epilogue over the three classes' ranges.
 // total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
 // stage 0; nchunks is what launch_pairs returned for this stage.
+// Batched runs pass row_nchunks (row_nchunks_len entries) and their own partial sums
+// (partial_len doubles).
 int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6], int nchunks,
                           double* total_ke, const int* row_nchunks = nullptr,
-                          const double* partial = nullptr);
+                          const double* partial = nullptr, long long row_nchunks_len = 0,
+                          long long partial_len = 0);
 int resolve_slots(tc_ctx* ctx);
+// Checked build: points ctx->bc_rec at the device's violation record (allocated on first use).
+int bounds_attach(tc_ctx* ctx);
 const PairVariant* variant(int precision, int id);
-// Kernels defined in bs_launch.cu and also launched from other files.
-__global__ void pack_kernel(const double* __restrict__ x, const double* __restrict__ zeta,
-                            const double* __restrict__ area, int n, double4* __restrict__ out);
-__global__ void velocity_epilogue_kernel(const double* __restrict__ x, const int* __restrict__ perm,
-                                         int m, int i0, int i1, int row_offset, int n_out,
-                                         int nchunks, const double* __restrict__ partial,
-                                         double m2omega, double* __restrict__ dX,
-                                         double* __restrict__ dVort);
 int variant_count(int precision);
 int select_variant(tc_ctx* ctx, int precision, int id);
 // With ctx->auto32, selects the FP32C variant for a launch over n sources.
