@@ -220,6 +220,24 @@ int tc_rk4_store(tc_ctx* ctx, double* xA, double* zetaA, double* xV, double* xQ,
                  double* kineticEnergy, int on_device);
 /* ResetRK4 (:321-372): frees the state; call after a remesh changes N. */
 int tc_reset_rk4(tc_ctx* ctx);
+/* Checkpoint and restart (no counterpart in the reference, whose drivers keep
+ * no restart files). tc_rk4_save writes the loaded state to `path`: the
+ * positions of the three classes, zetaA, areaA, Omega, the deltas, the step
+ * count and, for a forced run, absVortA/absVortV and its clock. It writes
+ * `path`.tmp and renames it, so an interrupted save leaves any earlier file
+ * whole. The format is a fixed header, the arrays, and an FNV-1a checksum
+ * (csrc/checkpoint.cu).
+ * tc_rk4_restore loads such a file into ctx as tc_rk4_load would, and also
+ * sets Omega, the deltas, the step count and the forced run's clock.
+ * tc_rk4_advance then continues bit for bit as the run that wrote the file
+ * would have, given the same precision, which is the context's own and is
+ * not changed. A missing, truncated or corrupted file (bad magic, sizes or
+ * checksum) returns TC_ERR_ARG and leaves the context's state as it was. */
+int tc_rk4_save(tc_ctx* ctx, const char* path);
+int tc_rk4_restore(tc_ctx* ctx, const char* path);
+/* Steps advanced since the state was loaded (tc_rk4_advance / tc_rk4_step),
+ * counting those recorded in a restored checkpoint. */
+int tc_rk4_steps_done(tc_ctx* ctx, long long* steps);
 
 /* ---- adjoint (no counterpart in the reference) ------------------------- */
 /* Gradient of J(T), T = nsteps*dt, with respect to the initial state of the

@@ -132,6 +132,9 @@ SIGNATURES: dict[str, tuple] = {
     "tc_icos_grid": (c_int, [c_int, dp, dp, dp, dp, dp, ip, ip, ip, ip]),
     "tc_icos_grid_device": (c_int, [c_void_p, c_int] + [c_void_p] * 9),
     "tc_gather_maps": (c_int, [c_int, ip, ip, c_int, ip, c_int]),
+    "tc_rk4_save": (c_int, [c_void_p, c_char_p]),
+    "tc_rk4_restore": (c_int, [c_void_p, c_char_p]),
+    "tc_rk4_steps_done": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
     "tc_bounds_checked": (c_int, []),
     "tc_bounds_status": (c_int, [c_int, POINTER(ctypes.c_longlong), c_int]),
     "tc_bounds_cap": (c_int, [c_void_p, c_int, ctypes.c_longlong]),

@@ -523,6 +523,7 @@ int rk4_load(tc_ctx* ctx, const double* xA, const double* zetaA, const double* a
   R.ready = true;
   R.ordered = false;
   R.strat = false;
+  R.steps_total = 0;
   return TC_OK;
 }
 
@@ -874,6 +875,7 @@ int rk4_advance_enqueue(tc_ctx* ctx, double dt, int nsteps) {
   } else if ((rc = advance_steps(ctx, dt, 0, nsteps))) {
     return rc;
   }
+  R.steps_total += nsteps;
   return TC_OK;
 }
 

@@ -79,6 +79,7 @@ struct Rk4State {
   double t0 = 0.0;                      // time at the start of step 0
   double strat_dt = 0.0;                // step length of the forced run
   long long step = 0;                   // steps completed since t0
+  long long steps_total = 0;            // steps advanced since the state was loaded (checkpoints)
 };
 
 }  // namespace tcb

@@ -144,6 +144,40 @@ class Context:
     def reset_rk4(self) -> None:
         N.call("tc_reset_rk4", self.handle)
 
+    # device-resident state, checkpoints ------------------------------------------
+    def rk4_load(self, xA, zetaA, areaA, xV, xQ) -> None:
+        """Copy a state (host arrays) to the device (tc_rk4_load)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xA, zetaA, areaA, xV, xQ)]
+        N.call("tc_rk4_load", self.handle, N.dptr(arrs[0]), N.dptr(arrs[1]), N.dptr(arrs[2]),
+               arrs[0].shape[0], N.dptr(arrs[3]), arrs[3].shape[0], N.dptr(arrs[4]),
+               arrs[4].shape[0], 0)
+
+    def rk4_advance(self, dt: float, nsteps: int) -> np.ndarray:
+        """nsteps RK4 steps of the device-resident state; returns totalKE per step."""
+        tke = np.zeros(max(nsteps, 1))
+        N.call("tc_rk4_advance", self.handle, float(dt), int(nsteps), N.dptr(tke))
+        return tke[:nsteps]
+
+    def rk4_store(self, nA: int, nV: int, nQ: int) -> tuple:
+        """The device-resident state as host arrays (xA, zetaA, xV, xQ)."""
+        xA, zA, xV, xQ = np.zeros((nA, 3)), np.zeros(nA), np.zeros((nV, 3)), np.zeros((nQ, 3))
+        N.call("tc_rk4_store", self.handle, N.dptr(xA), N.dptr(zA), N.dptr(xV), N.dptr(xQ), None, 0)
+        return xA, zA, xV, xQ
+
+    def save_state(self, path) -> None:
+        """Checkpoint the device-resident state to `path` (tc_rk4_save)."""
+        N.call("tc_rk4_save", self.handle, str(path).encode())
+
+    def restore_state(self, path) -> None:
+        """Load a checkpoint written by save_state (tc_rk4_restore)."""
+        N.call("tc_rk4_restore", self.handle, str(path).encode())
+
+    def steps_done(self) -> int:
+        """Steps advanced since the state was loaded, counting a restored checkpoint's."""
+        v = ctypes.c_longlong()
+        N.call("tc_rk4_steps_done", self.handle, ctypes.byref(v))
+        return v.value
+
 
 class PanelVelocity:
     """The `save` state of PanelVelocityParallelModule for one rank."""
