@@ -325,10 +325,14 @@ int tc_device_count(int* count);
  * lengths between flushes in tiles whose every source is far. FP64 form: 0. */
 int tc_pair_variant_count(int precision, int* count);
 int tc_pair_variant_info(int precision, int id, int* info8);
-/* Select a variant. For FP32C the default is chosen per launch by problem
- * size (variant 1 below 131,072 sources, 0 above); selecting a variant turns
- * that off, and id = -1 turns it back on. tc_get_pair_variant returns the
- * variant in use (for FP32C with the automatic choice: the one last used). */
+/* Select a variant. By default the variant is chosen per launch by problem
+ * size. For FP32C: variant 1 below 131,072 sources, 0 above. For FP64:
+ * variant 2, or variant 6 (the same shape with 32-source tiles and chunks of
+ * any multiple of 32 sources) for launches that would fill less than 90% of
+ * one wave of CTAs with whole 256-source chunks. Selecting a variant turns
+ * the automatic choice off; id = -1 turns it back on. tc_get_pair_variant
+ * returns the variant in use (with the automatic choice: the one last
+ * used). */
 int tc_set_pair_variant(tc_ctx* ctx, int precision, int id);
 int tc_get_pair_variant(tc_ctx* ctx, int precision, int* id);
 

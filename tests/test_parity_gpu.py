@@ -188,6 +188,39 @@ def test_fp32c_variant_chosen_by_size(gpu):
     ctx.close()
 
 
+def test_fp64_small_launches_take_the_small_tile_variant(gpu):
+    """FP64 launches that would fill less than 90% of one wave with whole 256-source chunks run
+    variant 6 (32-source tiles, finer chunks). Larger ones run variant 2. Both match the oracle.
+    Selecting a variant fixes it, and -1 restores the automatic choice."""
+    import ctypes
+
+    def used(ctx):
+        v = ctypes.c_int()
+        N.call("tc_get_pair_variant", ctx.handle, N.TC_FP64, ctypes.byref(v))
+        return v.value
+
+    ctx = Context(0, "fp64")
+    for level, want in ((2, 6), (4, 6), (6, 2), (4, 6)):
+        w = configs.rh4(level=level, parity=True)
+        setup(ctx, w.omega, w.deltas)
+        dA, _ = ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+        dQ, _ = ctx.velocity(N.TC_PASSIVE, w.xQ, w.xA, w.zetaA, w.areaA)
+        assert used(ctx) == want, level
+        rows = np.sort(np.random.default_rng(level).choice(w.nA, min(w.nA, 512), replace=False))
+        refA = O.rows(0, rows, None, w.xA, w.zetaA, w.areaA, delta=0.0, nthreads=8)
+        qrows = np.arange(min(w.nQ, 512))
+        refQ = O.rows(2, qrows, w.xQ, w.xA, w.zetaA, w.areaA, delta=0.05, nthreads=8)
+        assert rel_err(dA[rows], refA) <= FP64_TOL, level
+        assert rel_err(dQ[qrows], refQ) <= FP64_TOL, level
+    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP64, 2)
+    ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    assert used(ctx) == 2
+    N.call("tc_set_pair_variant", ctx.handle, N.TC_FP64, -1)
+    ctx.velocity(N.TC_ACTIVE, None, w.xA, w.zetaA, w.areaA)
+    assert used(ctx) == 6
+    ctx.close()
+
+
 def _variants_with_form(bits: int) -> list[int]:
     import ctypes
     cnt = ctypes.c_int()

@@ -772,7 +772,8 @@ std::vector<uint64_t> graph_key(tc_ctx* ctx, double dt, int nsteps) {
   tcb::Rk4State& R = ctx->rk;
   std::vector<uint64_t> k = {(uint64_t)R.nA, (uint64_t)R.nV, (uint64_t)R.nQ, bits(dt),
                              (uint64_t)nsteps, (uint64_t)ctx->precision, (uint64_t)ctx->var64,
-                             (uint64_t)ctx->var32, (uint64_t)ctx->auto32, (uint64_t)ctx->target_order,
+                             (uint64_t)ctx->var32, (uint64_t)ctx->auto32, (uint64_t)ctx->auto64,
+                             (uint64_t)ctx->target_order,
                              bits(ctx->omega),
                              bits(ctx->delta[0]), bits(ctx->delta[1]), bits(ctx->delta[2])};
   const tcb::DevBuf* bufs[] = {&R.x0A, &R.z0, &R.areaA, &R.x0V, &R.x0Q, &R.xiA, &R.ziA, &R.xiV,
@@ -1015,12 +1016,15 @@ extern "C" int tc_pair_variant_info(int precision, int id, int* info8) {
 extern "C" int tc_set_pair_variant(tc_ctx* ctx, int precision, int id) {
   int rc = begin(ctx);
   if (rc) return rc;
-  if (precision == TC_FP32C && id == -1) {  // back to the per-size automatic choice
-    ctx->auto32 = true;
+  if (id == -1 && (precision == TC_FP32C || precision == TC_FP64)) {
+    // back to the per-size automatic choice
+    if (precision == TC_FP32C) ctx->auto32 = true;
+    if (precision == TC_FP64) ctx->auto64 = true;
     return TC_OK;
   }
   if ((rc = tcb::select_variant(ctx, precision, id))) return rc;
   if (precision == TC_FP32C) ctx->auto32 = false;
+  if (precision == TC_FP64) ctx->auto64 = false;
   return TC_OK;
 }
 

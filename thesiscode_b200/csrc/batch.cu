@@ -389,7 +389,8 @@ static int batch_rk4_impl(tc_ctx* ctx, int count, const int* nA, const int* nV, 
     if (flags & TC_BATCH_AUTOTUNE) {
       if ((rc = autotune(ctx, B))) return rc;
     } else {
-      const int v = ctx->precision == TC_FP64 ? ctx->var64 : ctx->var32;
+      const int v = ctx->precision == TC_FP64 ? (ctx->auto64 ? tcb::kAuto64Default : ctx->var64)
+                                              : ctx->var32;
       if ((rc = build_items(ctx, B, v, 4096))) return rc;
     }
     if ((rc = tc_rk4_pack_sources(ctx))) return rc;  // autotuning ran stage-0 launches only

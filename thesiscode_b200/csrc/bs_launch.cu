@@ -41,13 +41,13 @@ void DevBuf::release() {
 // ---------------------------------------------------------------------------
 constexpr int kTS = 256;
 
-template <int NT, int TPT, int MINB, bool FUSED>
+template <int NT, int TPT, int MINB, bool FUSED, int TS>
 void launch64(dim3 g, cudaStream_t s, const PairLaunch& P) {
-  pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(P);
+  pair_fp64_kernel<NT, TPT, TS, MINB, FUSED><<<g, NT, 0, s>>>(P);
 }
-template <int NT, int TPT, int MINB, bool FUSED>
+template <int NT, int TPT, int MINB, bool FUSED, int TS>
 void launch64b(int g, cudaStream_t s, const BatchLaunch& B) {
-  pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED><<<g, NT, 0, s>>>(B);
+  pair_fp64_batch_kernel<NT, TPT, TS, MINB, FUSED><<<g, NT, 0, s>>>(B);
 }
 template <int NT, int T, int FLUSH, int MINB, int UNROLL, int FM>
 void launch32b(int g, cudaStream_t s, const BatchLaunch& B) {
@@ -58,11 +58,12 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
   pair_fp32c_kernel<NT, T, kTS, FLUSH, MINB, UNROLL, FM><<<g, NT, 0, s>>>(P);
 }
 
-#define V64(NT, TPT, MINB, FUSED)                                                 \
-  PairVariant { TC_FP64, NT, TPT, kTS, FUSED, MINB, 0, launch64<NT, TPT, MINB, FUSED>, \
-                (const void*)pair_fp64_kernel<NT, TPT, kTS, MINB, FUSED>,               \
-                launch64b<NT, TPT, MINB, FUSED>,                                         \
-                (const void*)pair_fp64_batch_kernel<NT, TPT, kTS, MINB, FUSED>, 0 }
+#define V64T(NT, TPT, MINB, FUSED, TS)                                              \
+  PairVariant { TC_FP64, NT, TPT, TS, FUSED, MINB, 0, launch64<NT, TPT, MINB, FUSED, TS>, \
+                (const void*)pair_fp64_kernel<NT, TPT, TS, MINB, FUSED>,                  \
+                launch64b<NT, TPT, MINB, FUSED, TS>,                                        \
+                (const void*)pair_fp64_batch_kernel<NT, TPT, TS, MINB, FUSED>, 0 }
+#define V64(NT, TPT, MINB, FUSED) V64T(NT, TPT, MINB, FUSED, kTS)
 // FP32C: T targets per thread, FP32 flush every FLUSH sources, form bits FM
 #define V32(NT, T, FLUSH, MINB, UNROLL, FM)                                            \
   PairVariant { TC_FP32C, NT, T, kTS, FLUSH, MINB, UNROLL,                             \
@@ -73,10 +74,13 @@ void launch32(dim3 g, cudaStream_t s, const PairLaunch& P) {
 
 // FP64: the `flush` field records the denominator mode (1 = fused, 0 =
 // rounded exactly like the reference).
+// Variant 6 is variant 2 with 32-source tiles, for launches too small to fill
+// one wave of whole 256-source chunks (chosen automatically, fp64_small).
 const PairVariant kVariants64[] = {
     V64(256, 2, 5, true),  V64(256, 4, 2, true),  V64(256, 1, 6, true), V64(128, 4, 4, true),
-    V64(256, 2, 5, false), V64(256, 4, 2, false),
+    V64(256, 2, 5, false), V64(256, 4, 2, false), V64T(256, 1, 6, true, 32),
 };
+static_assert(kAuto64Default == 2 && kAuto64Small == 6, "automatic FP64 variants");
 // FP32C form bits (SpForm in bs_core.cuh): 8 = source-paired form (all
 // variants), 2 = FP64 accumulators in shared memory, 4 = hi/lo near offsets,
 // 256 / 512 = tiles whose every source is far flushed every 2 / 4 flush
@@ -144,6 +148,10 @@ int resolve_slots(tc_ctx* ctx) {
   cudaDeviceProp prop;
   TC_CUDA_TRY(cudaGetDeviceProperties(&prop, ctx->device));
   ctx->num_sms = prop.multiProcessorCount;
+  int blocks = 0;
+  TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &blocks, kVariants64[kAuto64Default].fn, kVariants64[kAuto64Default].nt, 0));
+  ctx->slots64_default = std::max(1, blocks) * ctx->num_sms;
   int rc = select_variant(ctx, TC_FP64, ctx->var64);
   if (rc) return rc;
   return select_variant(ctx, TC_FP32C, ctx->var32);
@@ -168,6 +176,48 @@ static int choose_chunks(int tiles, int n, int ts, int slots, int min_chunk, int
   }
   (void)ts;
   return best;
+}
+
+// Source chunk length of an FP64 launch too small to fill the GPU with
+// whole 256-source chunks (run with kAuto64Small's 32-source tiles, so that
+// chunks may be any multiple of 32 sources without padding). The work items run
+// in one or two waves, and each SM works through its CTAs at its FP64 pipe's
+// rate. The length minimised is therefore ceil(items / SMs) x chunk length.
+// Example: 5,120 sources and 31 tiles on 148 SMs. Whole-tile chunks allow at
+// most 20 chunks: 620 items, 5 per SM, of 256 sources each (1,280). Chunks of
+// 224 give 23 chunks: 713 items, 5 per SM, 1,120 (-12.5%).
+static int fine_chunk_len(int tiles, int n, int num_sms, int slots, int max_chunks, int gran) {
+  long long best_cost = -1;
+  int best_len = n;
+  for (int s = 1; s <= max_chunks; ++s) {
+    int len = (n + s - 1) / s;
+    len = (len + gran - 1) / gran * gran;
+    const int chunks = (n + len - 1) / len;
+    const long long items = (long long)tiles * chunks;
+    if (items > 2LL * slots) break;
+    const long long cost = (items + num_sms - 1) / num_sms * (long long)len;
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best_len = len;
+    }
+  }
+  return best_len;
+}
+
+// Chunk length of whole-tile chunks (tiles of ts sources).
+static int whole_chunk_len(int tiles, int n, int ts, int slots, int min_chunk, int max_chunks) {
+  const int S = choose_chunks(tiles, n, ts, slots, min_chunk, max_chunks);
+  const int len = (n + S - 1) / S;
+  return (len + ts - 1) / ts * ts;
+}
+
+// With the default FP64 variant's whole-tile chunks, does this launch fill
+// less than 90% of one wave's CTA slots?
+static bool fp64_small(const tc_ctx* ctx, int tiles, int n, int max_chunks) {
+  const int slots = ctx->slots64_default;
+  const int len = whole_chunk_len(tiles, n, kTS, slots, ctx->min_chunk, max_chunks);
+  const long long items = (long long)tiles * ((n + len - 1) / len);
+  return items * 10 < 9LL * slots;
 }
 
 // Tiles and chunking of one pair launch: the target segments, the grid and the
@@ -202,11 +252,21 @@ static int plan_pairs(tc_ctx* ctx, const SegDesc* segs, int nseg, const double4*
   P->nseg = k;
   *grid = dim3(tiles, 0);
   if (tiles == 0 || n <= 0) return TC_OK;
+  // automatic FP64 variant: the same target tiles either way, only the source tiles differ
+  if (fp64 && ctx->auto64) {
+    const int want = fp64_small(ctx, tiles, n, max_chunks) ? kAuto64Small : kAuto64Default;
+    if (want != ctx->var64) {
+      const int rc = select_variant(ctx, TC_FP64, want);
+      if (rc) return rc;
+    }
+  }
+  const PairCfg& cur = fp64 ? ctx->cfg64 : ctx->cfg32;
   const int slots = fp64 ? ctx->slots64 : ctx->slots32;
-  int S = choose_chunks(tiles, n, cfg.ts, slots, ctx->min_chunk, max_chunks);
-  int chunk_len = (n + S - 1) / S;
-  chunk_len = (chunk_len + cfg.ts - 1) / cfg.ts * cfg.ts;
-  S = (n + chunk_len - 1) / chunk_len;
+  const int chunk_len =
+      (fp64 && ctx->auto64 && ctx->var64 == kAuto64Small)
+          ? fine_chunk_len(tiles, n, ctx->num_sms, slots, max_chunks, cur.ts)
+          : whole_chunk_len(tiles, n, cur.ts, slots, ctx->min_chunk, max_chunks);
+  const int S = (n + chunk_len - 1) / chunk_len;
   P->src = src;
   P->n = n;
   P->chunk_len = chunk_len;

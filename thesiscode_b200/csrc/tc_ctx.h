@@ -101,6 +101,8 @@ struct tc_ctx {
   tcb::PairCfg cfg32{256, 4, 256};
   int var64 = 2, var32 = 0;  // pair-kernel variants in use (see kVariants64/32)
   bool auto32 = true;  // FP32C variant chosen per launch by problem size (tc_set_pair_variant turns it off)
+  bool auto64 = true;  // FP64: 32-source tiles for launches too small to fill a wave (likewise)
+  int slots64_default = 0;  // resident CTAs per GPU of the default FP64 variant
   int target_order = TC_ORDER_HILBERT;  // FP32C visiting order of targets
   double adj_ms[3] = {0.0, 0.0, 0.0};  // last adjoint: forward sweep, recompute, backward
   int adj_mode = 6;  // adjoint VJP: 3-6 row pass, 0 two passes, 1 and 2 fused (tc_set_adjoint_mode)
@@ -132,6 +134,10 @@ struct tc_ctx {
 };
 
 namespace tcb {
+// The automatic FP64 variants: the default, and the same shape with 32-source
+// tiles for launches that leave most of one wave's CTA slots empty.
+constexpr int kAuto64Default = 2;
+constexpr int kAuto64Small = 6;
 // Checked build: the extent the kernels check `site`'s indices against, n or the
 // cap tc_bounds_cap set (the smaller).
 inline long long bc_extent(const tc_ctx* ctx, int site, long long n) {
