@@ -80,6 +80,13 @@ def noalloc(ctx, w):
     return u.cpu().numpy()
 
 
+def adjoint(ctx, w, steps=3):
+    J, gz, gx = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
+    N.call("tc_rk4_adjoint", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, 0.01,
+           steps, 2, N.TC_J_ENSTROPHY, 0, N.dptr(J), N.dptr(gz), N.dptr(gx))
+    return np.concatenate([J, gz, gx.ravel()])
+
+
 def results(out_path):
     w, ws = _rh4(), _batch()
     st = configs.stratosphere(level=3)
@@ -92,6 +99,8 @@ def results(out_path):
         out[f"{prec}_passive_u"] = ctx.velocity(N.TC_PASSIVE, w.xQ, w.xA, w.zetaA, w.areaA)[0]
         out[f"{prec}_rk4"] = rk4_step(ctx, w, nsteps=3)  # steps 2-3 replay a CUDA graph
         out[f"{prec}_noalloc"] = noalloc(ctx, w)
+        if prec == "fp64":
+            out["fp64_adjoint"] = adjoint(ctx, w)
         ctx.close()
         ctx = _ctx(prec, st)
         s = st.copy()
@@ -123,17 +132,21 @@ CAP_CASES = [
     ("STAGE_KEBLOCK", "fp32c", "rk4"), ("STAGE_STATE", "fp64", "rk4"),
     ("BATCH_SEG", "fp32c", "batch"), ("BATCH_SEG", "fp64", "batch"),
     ("STAGE_CHUNKS", "fp32c", "batch"),
+    ("ADJ_ROW_IN", "fp64", "adjoint"), ("ADJ_ROW_OUT", "fp64", "adjoint"),
+    ("ADJ_COMBINE", "fp64", "adjoint"),
 ]
 SITE_IDS = {name: i for i, name in enumerate(
     ["", "PAIR_X", "PAIR_PERM", "PAIR_SRC", "PAIR_OUT", "BATCH_SEG", "PACK_IN", "PACK_OUT",
      "EPI_PERM", "EPI_X", "EPI_PARTIAL", "EPI_OUT", "STAGE_PERM", "STAGE_STATE",
-     "STAGE_PARTIAL", "STAGE_CHUNKS", "STAGE_ACTIVE", "STAGE_KEBLOCK"])}
+     "STAGE_PARTIAL", "STAGE_CHUNKS", "STAGE_ACTIVE", "STAGE_KEBLOCK", "ADJ_ROW_IN",
+     "ADJ_ROW_OUT", "ADJ_COMBINE"])}
 
 
 def caps(out_path):
     w, ws = _rh4(), _batch()
     runs = {"velocity": lambda c: velocity_vertex(c, w), "rk4": lambda c: rk4_step(c, w),
-            "batch": lambda c: batch(c, ws), "noalloc": lambda c: noalloc(c, w)}
+            "batch": lambda c: batch(c, ws), "noalloc": lambda c: noalloc(c, w),
+            "adjoint": lambda c: adjoint(c, w)}
     report = []
     for site, prec, case in CAP_CASES:
         ctx = _ctx(prec, ws[0] if case == "batch" else w)

@@ -3,13 +3,15 @@
 compute-sanitizer cannot be run on these machines. Its stand-in is a build of
 the same sources in which the hot-path kernels check every global-memory index
 against its array's extent. Those kernels are the pair kernels (single and
-batched), packing, and the velocity and stage epilogues. An out-of-range
+batched), packing, the velocity and stage epilogues, and the adjoint's row
+pass. An out-of-range
 access is skipped and recorded, never performed. This file checks four things:
 
 * The checks change no arithmetic. A fixed set of calls gives bit for bit the
   release build's results: velocity of every target class, RK4 steps with
-  graph replay, the forced model, the allocation-free entry point and a
-  batched ensemble, in both precisions. The record stays empty.
+  graph replay, the forced model, the allocation-free entry point, a
+  batched ensemble and the adjoint, in both precisions. The record stays
+  empty.
 * The checks fire. For each site, the declared extent is capped below what
   the call touches, while the real arrays keep their size. The device's record
   then names that site, with an index at or past the cap. Once the cap is
@@ -41,7 +43,7 @@ CASES = Path(__file__).resolve().parent / "bounds_cases.py"
 SUITE = ["test_parity_gpu.py", "test_random_sizes_gpu.py", "test_graph_gpu.py", "test_batch_gpu.py",
          "test_strat_gpu.py", "test_voronoi_gpu.py", "test_dist_gpu.py", "test_finite_checks_gpu.py",
          "test_reference_gpu.py", "test_fortran_shim_gpu.py", "test_configs_gpu.py",
-         "test_zz_no_alloc.py"]
+         "test_adjoint_gpu.py", "test_zz_no_alloc.py"]
 
 
 def _child(args, checked, timeout):

@@ -56,7 +56,8 @@ BC_SITES = {
     11: "velocity epilogue stores", 12: "stage epilogue visiting orders",
     13: "stage epilogue state arrays", 14: "stage epilogue partial sums",
     15: "stage epilogue chunk counts", 16: "stage epilogue active-only arrays",
-    17: "stage epilogue KE block sums",
+    17: "stage epilogue KE block sums", 18: "adjoint row-pass inputs",
+    19: "adjoint row-pass partial stores", 20: "adjoint combination partial reads",
 }
 
 _STATUS = {

@@ -27,6 +27,7 @@
 // The state is checkpointed every `ckpt_every` steps on the forward sweep;
 // the backward sweep recomputes each segment's stage inputs from its
 // checkpoint (one extra forward pass in total).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -297,6 +298,9 @@ struct RowLaunch {
   int chunk_len;
   double one_plus_d2;
   double* partial;    // [chunk][kRowSums][n]
+  BoundsRec* bc;          // checked build: violation record (null: release build)
+  long long src_len;      // checked build: entries of ra, rb and rc
+  long long partial_len;  // checked build: doubles in partial
 };
 
 template <int NEWTON>
@@ -355,7 +359,8 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
 #pragma unroll
   for (int t = 0; t < TPT; ++t) {
     row[t] = (blockIdx.x * TPT + t) * kRNT + threadIdx.x;
-    const int ld = row[t] < P.n ? row[t] : P.n - 1;
+    int ld = row[t] < P.n ? row[t] : P.n - 1;
+    if (!TC_BC(P.bc, BC_ADJ_ROW_IN, ld, P.src_len)) ld = 0;
     const double4 q = P.ra[ld];
     const double4 w = P.rb[ld];
     x0[t] = q.x;
@@ -377,9 +382,10 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
     __syncthreads();
     for (int j = threadIdx.x; j < kRTS; j += kRNT) {
       const int k = ts + j;
-      sa[j] = k < c1 ? P.ra[k] : make_double4(0.0, 0.0, 0.0, 0.0);
-      sb[j] = k < c1 ? P.rb[k] : make_double4(0.0, 0.0, 0.0, 0.0);
-      sc[j] = k < c1 ? P.rc[k] : 0.0;
+      const bool in = k < c1 && TC_BC(P.bc, BC_ADJ_ROW_IN, k, P.src_len);
+      sa[j] = in ? P.ra[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sb[j] = in ? P.rb[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+      sc[j] = in ? P.rc[k] : 0.0;
     }
     __syncthreads();
     if (ts < r_hi && r_lo < ts + kRTS) {
@@ -397,9 +403,11 @@ __global__ void __launch_bounds__(kRNT) adj_row_kernel(const RowLaunch P) {
 #pragma unroll
   for (int t = 0; t < TPT; ++t) {
     if (row[t] < P.n) {
-      double* out = P.partial + (size_t)blockIdx.y * kRowSums * n + row[t];
+      const size_t base = (size_t)blockIdx.y * kRowSums * n + row[t];
+      double* out = P.partial + base;
 #pragma unroll
-      for (int c = 0; c < kRowSums; ++c) out[c * n] = a[t][c];
+      for (int c = 0; c < kRowSums; ++c)
+        if (TC_BC(P.bc, BC_ADJ_ROW_OUT, base + c * n, P.partial_len)) out[c * n] = a[t][c];
     }
   }
 }
@@ -410,7 +418,8 @@ __global__ void adj_combine_row_kernel(const double* __restrict__ x, const doubl
                                        const double* __restrict__ zeta,
                                        const double* __restrict__ area, int n,
                                        const double* __restrict__ p, int chunks,
-                                       double* __restrict__ out_x, double* __restrict__ out_z) {
+                                       double* __restrict__ out_x, double* __restrict__ out_z,
+                                       BoundsRec* bc, long long p_len) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t N = (size_t)n, b = 3 * (size_t)i;
@@ -419,7 +428,10 @@ __global__ void adj_combine_row_kernel(const double* __restrict__ x, const doubl
   for (int w = 0; w < kRowSums; ++w) s[w] = 0.0;
   for (int c = 0; c < chunks; ++c)
 #pragma unroll
-    for (int w = 0; w < kRowSums; ++w) s[w] += p[((size_t)c * kRowSums + w) * N + i];
+    for (int w = 0; w < kRowSums; ++w) {
+      const size_t j = ((size_t)c * kRowSums + w) * N + i;
+      if (TC_BC(bc, BC_ADJ_COMBINE, j, p_len)) s[w] += p[j];
+    }
   const double u0 = ut[b], u1 = ut[b + 1], u2 = ut[b + 2];
   const double G = zeta[i] * area[i];
   const double g0 = (s[1] * u2 - s[2] * u1) + s[3] + G * s[6];
@@ -568,8 +580,19 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
     chunk = (chunk + tcb::kRTS - 1) / tcb::kRTS * tcb::kRTS;
     S = (n + chunk - 1) / chunk;
     if ((rc = W.p1.ensure((size_t)S * tcb::kRowSums * n * sizeof(double)))) return rc;
-    tcb::RowLaunch R{W.ra.as<double4>(), W.rb.as<double4>(), W.rc.as<double>(), n, chunk,
-                     1.0 + d * d, W.p1.as<double>()};
+    const long long src_len = (long long)std::min(
+        {W.ra.bytes / sizeof(double4), W.rb.bytes / sizeof(double4), W.rc.bytes / sizeof(double)});
+    const long long p1_len = (long long)(W.p1.bytes / sizeof(double));
+    tcb::RowLaunch R{W.ra.as<double4>(),
+                     W.rb.as<double4>(),
+                     W.rc.as<double>(),
+                     n,
+                     chunk,
+                     1.0 + d * d,
+                     W.p1.as<double>(),
+                     ctx->bc_rec,
+                     tcb::bc_extent(ctx, tcb::BC_ADJ_ROW_IN, src_len),
+                     tcb::bc_extent(ctx, tcb::BC_ADJ_ROW_OUT, p1_len)};
     const dim3 grid(tiles, S);
     if (tpt == 3)
       tcb::adj_row_kernel<3, 1, 1><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
@@ -583,7 +606,8 @@ int adj_stage_vjp(tc_ctx* ctx, AdjWork& W, const double* y, const double* lk, do
       tcb::adj_row_kernel<2, 1, 1><<<grid, tcb::kRNT, 0, ctx->stream>>>(R);
     TC_CUDA_TRY(cudaGetLastError());
     tcb::adj_combine_row_kernel<<<blocks, threads, 0, ctx->stream>>>(
-        yx, W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, out, out + 3 * (size_t)n);
+        yx, W.ut.as<double>(), yz, area, n, W.p1.as<double>(), S, out, out + 3 * (size_t)n,
+        ctx->bc_rec, tcb::bc_extent(ctx, tcb::BC_ADJ_COMBINE, p1_len));
     TC_CUDA_TRY(cudaGetLastError());
     ctx->launches += 3;
     ctx->pair_launches += 1;

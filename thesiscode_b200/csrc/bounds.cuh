@@ -4,9 +4,9 @@
 // `python -m thesiscode_b200.build --checked`), the hot-path kernels check
 // every global-memory index against the extent of the array it addresses.
 // Those kernels are the pair kernels (single and batched), source packing,
-// and the velocity and RK4 stage epilogues. The extent is the size of the
-// allocation the library made, or the size the caller declared for its own
-// array.
+// the velocity and RK4 stage epilogues, and the adjoint's row pass and its
+// combination. The extent is the size of the allocation the library made, or
+// the size the caller declared for its own array.
 //
 // An index outside [0, extent) is not accessed: a load gives zero and a store
 // is skipped. The first such index is recorded in a per-device record that
@@ -52,6 +52,9 @@ enum BoundsSite : int {
   BC_STAGE_CHUNKS,   // stage epilogue: per-row chunk counts (batched runs)
   BC_STAGE_ACTIVE,   // stage epilogue: active-only arrays (vorticity, area, KE, sources)
   BC_STAGE_KEBLOCK,  // stage epilogue: per-block KE sums
+  BC_ADJ_ROW_IN,     // adjoint row pass: per-panel inputs (ra, rb, rc)
+  BC_ADJ_ROW_OUT,    // adjoint row pass: partial-sum stores (doubles)
+  BC_ADJ_COMBINE,    // adjoint row combination: partial-sum reads (doubles)
   BC_SITE_END
 };
 
