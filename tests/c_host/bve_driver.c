@@ -4,14 +4,18 @@
  * library, GatherPanels maps, Rossby-Haurwitz wave-4 vorticity at the
  * active panels, nsteps fused RK4 steps, and checks that hold for the exact
  * flow (velocity tangent to the sphere, kinetic energy positive and nearly
- * conserved). Exit status 0 = pass, 1 = check failed, 2 = library error,
- * 3 = no GPU (the library reports a CUDA error from tc_create).
+ * conserved). With a CHECKPOINT path it also stops a device-resident run
+ * halfway, saves it (tc_rk4_save), restores it into a new context
+ * (tc_rk4_restore) and checks that the continued run ends bit for bit where
+ * the uninterrupted one does. Exit status 0 = pass, 1 = check failed, 2 =
+ * library error, 3 = no GPU (the library reports a CUDA error from tc_create).
  *
- * usage: bve_driver LEVEL NSTEPS PRECISION(0 = FP64, 1 = FP32C) */
+ * usage: bve_driver LEVEL NSTEPS PRECISION(0 = FP64, 1 = FP32C) [CHECKPOINT] */
 #define _DEFAULT_SOURCE /* M_PI */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include "thesiscode_b200.h"
 
@@ -84,6 +88,35 @@ int main(int argc, char** argv) {
   if (!(umax > 0.0) || dotmax > tang_tol * umax) {
     fprintf(stderr, "tangency: max |u.x| = %g, max |u| = %g\n", dotmax, umax);
     return 1;
+  }
+  /* checkpoint round trip of the device-resident state */
+  if (argc > 4 && nsteps >= 2) {
+    const char* path = argv[4];
+    const size_t bA = sizeof(double) * 3 * nact, bz = sizeof(double) * nact,
+                 bV = sizeof(double) * 3 * np, bQ = sizeof(double) * 3 * (npas > 0 ? npas : 1);
+    double *sA = malloc(bA), *sz = malloc(bz), *sV = malloc(bV), *sQ = malloc(bQ);
+    double *rA = malloc(bA), *rz = malloc(bz), *rV = malloc(bV), *rQ = malloc(bQ);
+    CHECK(tc_rk4_load(ctx, xA, zA, aA, nact, px, np, xQ, npas, 0));
+    CHECK(tc_rk4_advance(ctx, 0.01, nsteps, NULL));
+    CHECK(tc_rk4_store(ctx, sA, sz, sV, sQ, NULL, 0));
+    CHECK(tc_rk4_load(ctx, xA, zA, aA, nact, px, np, xQ, npas, 0));
+    CHECK(tc_rk4_advance(ctx, 0.01, nsteps / 2, NULL));
+    CHECK(tc_rk4_save(ctx, path));
+    tc_ctx* ctx2 = NULL;
+    CHECK(tc_create(0, precision, &ctx2));
+    CHECK(tc_rk4_restore(ctx2, path));
+    CHECK(tc_rk4_advance(ctx2, 0.01, nsteps - nsteps / 2, NULL));
+    CHECK(tc_rk4_store(ctx2, rA, rz, rV, rQ, NULL, 0));
+    long long done = 0;
+    CHECK(tc_rk4_steps_done(ctx2, &done));
+    CHECK(tc_destroy(ctx2));
+    if (done != nsteps || memcmp(sA, rA, bA) || memcmp(sz, rz, bz) || memcmp(sV, rV, bV) ||
+        (npas > 0 && memcmp(sQ, rQ, sizeof(double) * 3 * npas))) {
+      fprintf(stderr, "checkpoint: the restored run differs from the uninterrupted one\n");
+      return 1;
+    }
+    printf("checkpoint round trip after %d of %d steps: identical\n", nsteps / 2, nsteps);
+    free(sA), free(sz), free(sV), free(sQ), free(rA), free(rz), free(rV), free(rQ);
   }
   /* BVERK4 steps, fused on the device */
   double* tke = malloc(sizeof(double) * nsteps);

@@ -1,7 +1,8 @@
 """The C ABI from compiled C host programs: tests/c_host/bve_driver.c (one rank, the way a
 Fortran BVE driver calls BVERK4) and tests/c_host/bve_sharded.c (ranks as threads, each computing
 its LoadBalance rows of every RK4 stage and exchanging the packed source rows through host memory,
-the sequence an MPI host runs with MPI_Allgatherv). Both build with gcc against
+the sequence an MPI host runs with MPI_Allgatherv). The first also round-trips a checkpoint
+(tc_rk4_save / tc_rk4_restore). Both build with gcc against
 include/thesiscode_b200.h and link libthesiscode_b200.so like a Fortran or C driver would; on a
 machine without a GPU they fail cleanly with the library's CUDA status. On the GPU the sharded
 run matches the serial oracle."""
@@ -60,9 +61,11 @@ def test_c_driver_builds_and_fails_cleanly_without_gpu(tmp_path, native_built):
 @pytest.mark.parametrize("precision", [0, 1])
 def test_c_driver_runs_bve_steps(tmp_path, native_built, gpu, precision):
     exe = build_driver(tmp_path, native_built)
-    r = subprocess.run([str(exe), "4", "5", str(precision)], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([str(exe), "4", "5", str(precision), str(tmp_path / "run.tcb")],
+                       capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
     assert "5120 active panels" in r.stdout
+    assert "checkpoint round trip after 2 of 5 steps: identical" in r.stdout
 
 
 def test_sharded_c_driver_builds_and_fails_cleanly_without_gpu(tmp_path, native_built):
