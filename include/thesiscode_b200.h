@@ -350,9 +350,9 @@ int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* pair_launch
 /* The same sources compiled with -DTC_BOUNDS_CHECK=1 give
  * libthesiscode_b200_checked.so (`python -m thesiscode_b200.build --checked`).
  * In it the pair kernels (single and batched), source packing, the
- * velocity and RK4 stage epilogues and the adjoint's row pass (the default
- * adjoint mode) check every global-memory index against its array's
- * extent. That extent is the library's own allocation, or the size the
+ * velocity and RK4 stage epilogues, the FP32C visiting-order keys and the
+ * adjoint's row pass (the default adjoint mode) check every global-memory
+ * index against its array's extent. That extent is the library's own allocation, or the size the
  * caller declared. An index outside it is not accessed: a load reads 0 and
  * a store is skipped. The first such index goes into the device's record.
  * Other kernels (the adjoint's other modes, grid, Voronoi adapters) are not
@@ -377,6 +377,8 @@ int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* pair_launch
 #define TC_BC_ADJ_ROW_IN 18   /* adjoint row pass: per-panel inputs            */
 #define TC_BC_ADJ_ROW_OUT 19  /* adjoint row pass: partial-sum stores          */
 #define TC_BC_ADJ_COMBINE 20  /* adjoint row combination: partial-sum reads    */
+#define TC_BC_ORDER_X 21      /* visiting-order keys: target positions (points) */
+#define TC_BC_ORDER_KEYS 22   /* visiting-order keys: key and index stores     */
 /* 1 in the checked library, 0 in the release library. */
 int tc_bounds_checked(void);
 /* Waits for the device, then reads its record: rec[0] = violations since the

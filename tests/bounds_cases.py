@@ -134,12 +134,14 @@ CAP_CASES = [
     ("STAGE_CHUNKS", "fp32c", "batch"),
     ("ADJ_ROW_IN", "fp64", "adjoint"), ("ADJ_ROW_OUT", "fp64", "adjoint"),
     ("ADJ_COMBINE", "fp64", "adjoint"),
+    ("ORDER_X", "fp32c", "velocity"), ("ORDER_KEYS", "fp32c", "velocity"),
+    ("ORDER_X", "fp32c", "rk4"), ("ORDER_KEYS", "fp32c", "noalloc"),
 ]
 SITE_IDS = {name: i for i, name in enumerate(
     ["", "PAIR_X", "PAIR_PERM", "PAIR_SRC", "PAIR_OUT", "BATCH_SEG", "PACK_IN", "PACK_OUT",
      "EPI_PERM", "EPI_X", "EPI_PARTIAL", "EPI_OUT", "STAGE_PERM", "STAGE_STATE",
      "STAGE_PARTIAL", "STAGE_CHUNKS", "STAGE_ACTIVE", "STAGE_KEBLOCK", "ADJ_ROW_IN",
-     "ADJ_ROW_OUT", "ADJ_COMBINE"])}
+     "ADJ_ROW_OUT", "ADJ_COMBINE", "ORDER_X", "ORDER_KEYS"])}
 
 
 def caps(out_path):

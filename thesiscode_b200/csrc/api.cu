@@ -148,7 +148,7 @@ int velocity_device(tc_ctx* ctx, int cls, const double* X, int m, const double* 
   if (ctx->precision == TC_FP32C && ctx->target_order == TC_ORDER_HILBERT && i1 > i0) {
     if ((rc = ctx->scratch[4].ensure((size_t)m * sizeof(int)))) return rc;
     perm = ctx->scratch[4].as<int>();
-    if ((rc = tcb::compute_order(ctx, X, i0, i1, perm))) return rc;
+    if ((rc = tcb::compute_order(ctx, X, i0, i1, perm, m, m))) return rc;
   }
   const long long src_len = (long long)(ctx->scratch[0].bytes / sizeof(double4));
   if ((rc = tcb::launch_pack(ctx, src_x, vort, area, n, src, src_len))) return rc;
@@ -593,7 +593,8 @@ extern "C" int tc_rk4_stage_range(tc_ctx* ctx, int stage, double dt, int a0, int
     const int nn[3] = {R.nA, R.nV, R.nQ};
     for (int c = 0; c < 3; ++c) {
       if ((rc = pb[c]->ensure((size_t)std::max(nn[c], 1) * sizeof(int)))) return rc;
-      if ((rc = tcb::compute_order(ctx, tx[c], range[2 * c], range[2 * c + 1], pb[c]->as<int>())))
+      if ((rc = tcb::compute_order(ctx, tx[c], range[2 * c], range[2 * c + 1], pb[c]->as<int>(),
+                                   nn[c], nn[c])))
         return rc;
     }
     memcpy(R.order_range, range, sizeof(range));

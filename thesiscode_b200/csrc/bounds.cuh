@@ -4,8 +4,8 @@
 // `python -m thesiscode_b200.build --checked`), the hot-path kernels check
 // every global-memory index against the extent of the array it addresses.
 // Those kernels are the pair kernels (single and batched), source packing,
-// the velocity and RK4 stage epilogues, and the adjoint's row pass and its
-// combination. The extent is the size of the allocation the library made, or
+// the velocity and RK4 stage epilogues, the visiting-order keys, and the
+// adjoint's row pass and its combination. The extent is the size of the allocation the library made, or
 // the size the caller declared for its own array.
 //
 // An index outside [0, extent) is not accessed: a load gives zero and a store
@@ -55,6 +55,8 @@ enum BoundsSite : int {
   BC_ADJ_ROW_IN,     // adjoint row pass: per-panel inputs (ra, rb, rc)
   BC_ADJ_ROW_OUT,    // adjoint row pass: partial-sum stores (doubles)
   BC_ADJ_COMBINE,    // adjoint row combination: partial-sum reads (doubles)
+  BC_ORDER_X,        // visiting-order keys: target positions (points)
+  BC_ORDER_KEYS,     // visiting-order keys: key and index stores
   BC_SITE_END
 };
 

@@ -172,7 +172,10 @@ extern "C" int tc_bs_velocity_device_noalloc(tc_ctx* ctx, int target_class, cons
     unsigned* k_out = reinterpret_cast<unsigned*>(o + perm_bytes + key_bytes);
     int* v_in = reinterpret_cast<int*>(o + perm_bytes + 2 * key_bytes);
     void* temp = o + perm_bytes + 3 * key_bytes;
-    if ((rc = tcb::compute_order_into(ctx, X, i0, i1, perm, k_in, k_out, v_in, temp, sort_bytes)))
+    const tcb::OrderExtents ext{m, (long long)(perm_bytes / sizeof(int)),
+                                (long long)(key_bytes / sizeof(unsigned))};
+    if ((rc = tcb::compute_order_into(ctx, X, i0, i1, perm, k_in, k_out, v_in, temp, sort_bytes,
+                                      ext)))
       return rc;
   }
   double* partial = reinterpret_cast<double*>(b + fixed);

@@ -166,13 +166,21 @@ int launch_pack(tc_ctx* ctx, const double* x, const double* zeta, const double* 
 int launch_velocity_epilogue(tc_ctx* ctx, const double* x, const int* perm, int m, int i0, int i1,
                              int row_offset, int n_out, int nchunks, double* dX, double* dVort,
                              const double* partial = nullptr, long long partial_len = 0);
-// perm[i0..i1) <- i0..i1-1 sorted along the cube-face Hilbert curve (sphere_order.cuh)
-int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm);
+// perm[i0..i1) <- i0..i1-1 sorted along the cube-face Hilbert curve (sphere_order.cuh);
+// x holds x_len points, perm perm_len entries (a range past either is an error)
+int compute_order(tc_ctx* ctx, const double* x, int i0, int i1, int* perm, long long x_len,
+                  long long perm_len);
+// Extents of an order computation: points in x, entries in perm, entries in each key and
+// index buffer.
+struct OrderExtents {
+  long long x_len, perm_len, key_len;
+};
 // The same in caller-provided scratch (keys in/out and indices: i1 - i0 entries each; temp:
 // order_sort_bytes(i1 - i0) bytes); allocates nothing.
 int order_sort_bytes(int n, size_t* bytes);
 int compute_order_into(tc_ctx* ctx, const double* x, int i0, int i1, int* perm, unsigned* k_in,
-                       unsigned* k_out, int* v_in, void* temp, size_t temp_bytes);
+                       unsigned* k_out, int* v_in, void* temp, size_t temp_bytes,
+                       const OrderExtents& ext);
 // One RK4 stage epilogue over the three classes' ranges.
 // total_ke (device, nullable) receives 0.5*sum(KE*A) of the rows in range at
 // stage 0; nchunks is what launch_pairs returned for this stage.
