@@ -377,8 +377,9 @@ int tc_stats(tc_ctx* ctx, int reset, long long* launches, long long* pair_launch
 #define TC_BC_ADJ_ROW_IN 18   /* adjoint row pass: per-panel inputs            */
 #define TC_BC_ADJ_ROW_OUT 19  /* adjoint row pass: partial-sum stores          */
 #define TC_BC_ADJ_COMBINE 20  /* adjoint row combination: partial-sum reads    */
-#define TC_BC_ORDER_X 21      /* visiting-order keys: target positions (points) */
+#define TC_BC_ORDER_X 21      /* visiting-order keys: per-target inputs        */
 #define TC_BC_ORDER_KEYS 22   /* visiting-order keys: key and index stores     */
+#define TC_BC_BATCH_KE 23     /* batched runs: per-instance KE sums' reads     */
 /* 1 in the checked library, 0 in the release library. */
 int tc_bounds_checked(void);
 /* Waits for the device, then reads its record: rec[0] = violations since the

@@ -136,12 +136,13 @@ CAP_CASES = [
     ("ADJ_COMBINE", "fp64", "adjoint"),
     ("ORDER_X", "fp32c", "velocity"), ("ORDER_KEYS", "fp32c", "velocity"),
     ("ORDER_X", "fp32c", "rk4"), ("ORDER_KEYS", "fp32c", "noalloc"),
+    ("ORDER_X", "fp32c", "batch"), ("ORDER_KEYS", "fp32c", "batch"), ("BATCH_KE", "fp64", "batch"),
 ]
 SITE_IDS = {name: i for i, name in enumerate(
     ["", "PAIR_X", "PAIR_PERM", "PAIR_SRC", "PAIR_OUT", "BATCH_SEG", "PACK_IN", "PACK_OUT",
      "EPI_PERM", "EPI_X", "EPI_PARTIAL", "EPI_OUT", "STAGE_PERM", "STAGE_STATE",
      "STAGE_PARTIAL", "STAGE_CHUNKS", "STAGE_ACTIVE", "STAGE_KEBLOCK", "ADJ_ROW_IN",
-     "ADJ_ROW_OUT", "ADJ_COMBINE", "ORDER_X", "ORDER_KEYS"])}
+     "ADJ_ROW_OUT", "ADJ_COMBINE", "ORDER_X", "ORDER_KEYS", "BATCH_KE"])}
 
 
 def caps(out_path):

@@ -58,7 +58,8 @@ BC_SITES = {
     15: "stage epilogue chunk counts", 16: "stage epilogue active-only arrays",
     17: "stage epilogue KE block sums", 18: "adjoint row-pass inputs",
     19: "adjoint row-pass partial stores", 20: "adjoint combination partial reads",
-    21: "visiting-order key positions", 22: "visiting-order key stores",
+    21: "visiting-order key inputs", 22: "visiting-order key stores",
+    23: "batch KE sums' reads",
 }
 
 _STATUS = {

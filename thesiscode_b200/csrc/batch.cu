@@ -21,31 +21,41 @@ using tcb::DevBuf;
 
 namespace {
 
-__global__ void batch_keys_kernel(const double* __restrict__ x, const int* __restrict__ row_inst,
-                                  int n, unsigned long long* __restrict__ keys,
-                                  int* __restrict__ idx);
+// Checked build: extents of the batch kernels' per-row arrays.
+struct RowBounds {
+  tcb::BoundsRec* rec;
+  long long in_len;   // rows of the inputs (positions and instance ids; KE and areas)
+  long long out_len;  // rows of the key and index outputs
+};
 
 // key = instance << 31 | sphere key (cube face, 2-D Hilbert index): one
 // stable sort orders every instance's rows along the curve and keeps the
 // instances in their ranges.
 __global__ void batch_keys_kernel(const double* __restrict__ x, const int* __restrict__ row_inst,
                                   int n, unsigned long long* __restrict__ keys,
-                                  int* __restrict__ idx) {
+                                  int* __restrict__ idx, const RowBounds rb) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
+  if (!TC_BC(rb.rec, tcb::BC_ORDER_KEYS, j, rb.out_len)) return;
   const size_t b = 3 * (size_t)j;
-  keys[j] = ((unsigned long long)row_inst[j] << tcb::kSphereKeyBits) | tcb::sphere_key(x[b], x[b + 1], x[b + 2]);
+  keys[j] = TC_BC(rb.rec, tcb::BC_ORDER_X, j, rb.in_len)
+                ? ((unsigned long long)row_inst[j] << tcb::kSphereKeyBits) |
+                      tcb::sphere_key(x[b], x[b + 1], x[b + 2])
+                : 0ull;
   idx[j] = j;
 }
 
 // Kinetic energy of each instance: 0.5 * sum over its active rows of KE * A.
 __global__ void ke_segments_kernel(const double* __restrict__ ke, const double* __restrict__ area,
                                    const int* __restrict__ off, const int* __restrict__ cnt,
-                                   double* __restrict__ out) {
+                                   double* __restrict__ out, const RowBounds rb) {
   __shared__ double red[256];
   const int b = blockIdx.x;
   double s = 0.0;
-  for (int j = threadIdx.x; j < cnt[b]; j += 256) s += ke[off[b] + j] * area[off[b] + j];
+  for (int j = threadIdx.x; j < cnt[b]; j += 256) {
+    const int r = off[b] + j;
+    if (TC_BC(rb.rec, tcb::BC_BATCH_KE, r, rb.in_len)) s += ke[r] * area[r];
+  }
   red[threadIdx.x] = s;
   __syncthreads();
   for (int w = 128; w > 0; w >>= 1) {
@@ -80,15 +90,19 @@ namespace {
 
 std::map<std::vector<int>, std::pair<int, int>> g_tuned;  // batch shape -> (variant, chunk)
 
-int sort_batch_rows(tc_ctx* ctx, tc_batch_plan& B, const double* x, const int* row_inst, int n,
-                    int* perm) {
+int sort_batch_rows(tc_ctx* ctx, tc_batch_plan& B, const double* x, long long x_len,
+                    const int* row_inst, int n, int* perm) {
   if (n <= 0) return TC_OK;
   int rc;
   if ((rc = B.keys.ensure((size_t)n * 8)) || (rc = B.keys2.ensure((size_t)n * 8)) ||
       (rc = B.vals.ensure((size_t)n * 4)))
     return rc;
+  const long long in_len = std::min(x_len, (long long)(B.row_inst.bytes / sizeof(int)));
+  const long long out_len = (long long)std::min(B.keys.bytes / 8, B.vals.bytes / 4);
+  const RowBounds rb{ctx->bc_rec, tcb::bc_extent(ctx, tcb::BC_ORDER_X, in_len),
+                     tcb::bc_extent(ctx, tcb::BC_ORDER_KEYS, out_len)};
   batch_keys_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(
-      x, row_inst, n, B.keys.as<unsigned long long>(), B.vals.as<int>());
+      x, row_inst, n, B.keys.as<unsigned long long>(), B.vals.as<int>(), rb);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
   int bits = tcb::kSphereKeyBits;
@@ -231,9 +245,12 @@ int enqueue_steps(tc_ctx* ctx, tc_batch_plan& B, double dt, int nsteps) {
                (long long)(B.partial.bytes / sizeof(double)))))
         return rc;
       if (s == 0) {
+        const long long ke_len = (long long)std::min(ctx->rk.ke.bytes, ctx->rk.areaA.bytes) /
+                                 (long long)sizeof(double);
+        const RowBounds rb{ctx->bc_rec, tcb::bc_extent(ctx, tcb::BC_BATCH_KE, ke_len), 0};
         ke_segments_kernel<<<B.count, 256, 0, ctx->stream>>>(
             ctx->rk.ke.as<double>(), ctx->rk.areaA.as<double>(), B.off_d.as<int>(),
-            B.cnt_d.as<int>(), B.ke_out.as<double>() + (size_t)step * B.count);
+            B.cnt_d.as<int>(), B.ke_out.as<double>() + (size_t)step * B.count, rb);
         TC_CUDA_TRY(cudaGetLastError());
         ctx->launches += 1;
       }
@@ -374,9 +391,14 @@ static int batch_rk4_impl(tc_ctx* ctx, int count, const int* nA, const int* nV, 
       }
       TC_CUDA_TRY(cudaMemcpyAsync(ri, inst.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice,
                                   ctx->stream));
-      if ((rc = sort_batch_rows(ctx, B, cls == 0 ? R.x0A.as<double>() : R.x0V.as<double>(), ri, n,
-                                cls == 0 ? R.permA.as<int>() : R.permV.as<int>())))
-        return rc;
+      const tcb::DevBuf& xb = cls == 0 ? R.x0A : R.x0V;
+      const tcb::DevBuf& pbuf = cls == 0 ? R.permA : R.permV;
+      if ((long long)(pbuf.bytes / sizeof(int)) < n) {
+        tc_record_error("batch visiting order: %d rows, room for %zu", n, pbuf.bytes / sizeof(int));
+        return TC_ERR_ARG;
+      }
+      const long long x_len = (long long)(xb.bytes / (3 * sizeof(double)));
+      if ((rc = sort_batch_rows(ctx, B, xb.as<double>(), x_len, ri, n, pbuf.as<int>()))) return rc;
       TC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // `inst` is reused for the next class
     }
     R.ordered = true;

@@ -55,8 +55,9 @@ enum BoundsSite : int {
   BC_ADJ_ROW_IN,     // adjoint row pass: per-panel inputs (ra, rb, rc)
   BC_ADJ_ROW_OUT,    // adjoint row pass: partial-sum stores (doubles)
   BC_ADJ_COMBINE,    // adjoint row combination: partial-sum reads (doubles)
-  BC_ORDER_X,        // visiting-order keys: target positions (points)
+  BC_ORDER_X,        // visiting-order keys: per-target inputs (positions, instance ids)
   BC_ORDER_KEYS,     // visiting-order keys: key and index stores
+  BC_BATCH_KE,       // batched runs: per-instance KE sums' reads (KE, areas)
   BC_SITE_END
 };
 
