@@ -80,6 +80,13 @@ def noalloc(ctx, w):
     return u.cpu().numpy()
 
 
+def strat(ctx, w):
+    s = w.copy()
+    relA, _, tke, ke = ctx.strat_rk4_step(s.xA, w.meta["absVortA"], s.areaA, s.xV, s.xQ,
+                                          w.meta["t0"], w.dt, 1)
+    return np.concatenate([s.xA.ravel(), relA, s.xV.ravel(), tke, ke])
+
+
 def adjoint(ctx, w, steps=3):
     J, gz, gx = np.zeros(1), np.zeros(w.nA), np.zeros((w.nA, 3))
     N.call("tc_rk4_adjoint", ctx.handle, N.dptr(w.xA), N.dptr(w.zetaA), N.dptr(w.areaA), w.nA, 0.01,
@@ -137,6 +144,7 @@ CAP_CASES = [
     ("ORDER_X", "fp32c", "velocity"), ("ORDER_KEYS", "fp32c", "velocity"),
     ("ORDER_X", "fp32c", "rk4"), ("ORDER_KEYS", "fp32c", "noalloc"),
     ("ORDER_X", "fp32c", "batch"), ("ORDER_KEYS", "fp32c", "batch"), ("BATCH_KE", "fp64", "batch"),
+    ("PACK_IN", "fp64", "strat"), ("PACK_OUT", "fp64", "strat"),
 ]
 SITE_IDS = {name: i for i, name in enumerate(
     ["", "PAIR_X", "PAIR_PERM", "PAIR_SRC", "PAIR_OUT", "BATCH_SEG", "PACK_IN", "PACK_OUT",
@@ -147,12 +155,13 @@ SITE_IDS = {name: i for i, name in enumerate(
 
 def caps(out_path):
     w, ws = _rh4(), _batch()
-    runs = {"velocity": lambda c: velocity_vertex(c, w), "rk4": lambda c: rk4_step(c, w),
+    st = configs.stratosphere(level=3)
+    runs = {"strat": lambda c: strat(c, st),"velocity": lambda c: velocity_vertex(c, w), "rk4": lambda c: rk4_step(c, w),
             "batch": lambda c: batch(c, ws), "noalloc": lambda c: noalloc(c, w),
             "adjoint": lambda c: adjoint(c, w)}
     report = []
     for site, prec, case in CAP_CASES:
-        ctx = _ctx(prec, ws[0] if case == "batch" else w)
+        ctx = _ctx(prec, ws[0] if case == "batch" else st if case == "strat" else w)
         run = runs[case]
         base = run(ctx)
         clean_before = N.bounds_status(0, reset=True)["count"]

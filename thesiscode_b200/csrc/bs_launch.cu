@@ -364,9 +364,12 @@ __global__ void pack_kernel(const double* __restrict__ x, const double* __restri
 // relative vorticity is also written to z0 (it is the state's zeta at t).
 __global__ void pack_strat_kernel(const double* __restrict__ x, const double* __restrict__ absv,
                                   const double* __restrict__ area, int n, double two_omega,
-                                  double t, double* __restrict__ zeta, double4* __restrict__ out) {
+                                  double t, double* __restrict__ zeta, double4* __restrict__ out,
+                                  const PackBounds pb) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
+  if (!TC_BC(pb.rec, BC_PACK_IN, k, pb.in_len)) return;
+  if (!TC_BC(pb.rec, BC_PACK_OUT, k, pb.out_len)) return;
   const double px = x[3 * (size_t)k], py = x[3 * (size_t)k + 1], pz = x[3 * (size_t)k + 2];
   const double z = strat_rel_vort(absv[k], two_omega, px, py, pz, t);
   zeta[k] = z;
@@ -375,9 +378,11 @@ __global__ void pack_strat_kernel(const double* __restrict__ x, const double* __
 
 __global__ void strat_rel_vort_kernel(const double* __restrict__ absv,
                                       const double* __restrict__ x, int n, double two_omega,
-                                      double t, double* __restrict__ out) {
+                                      double t, double* __restrict__ out, const PackBounds pb) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
+  if (!TC_BC(pb.rec, BC_PACK_IN, k, pb.in_len)) return;
+  if (!TC_BC(pb.rec, BC_PACK_OUT, k, pb.out_len)) return;
   out[k] = strat_rel_vort(absv[k], two_omega, x[3 * (size_t)k], x[3 * (size_t)k + 1],
                           x[3 * (size_t)k + 2], t);
 }
@@ -385,9 +390,16 @@ __global__ void strat_rel_vort_kernel(const double* __restrict__ absv,
 int launch_pack_strat(tc_ctx* ctx, double t) {
   Rk4State& R = ctx->rk;
   if (R.nA <= 0) return TC_OK;
+  const long long in_len = (long long)std::min({R.x0A.bytes / (3 * sizeof(double)),
+                                                R.absA.bytes / sizeof(double),
+                                                R.areaA.bytes / sizeof(double)});
+  const long long out_len =
+      (long long)std::min(R.z0.bytes / sizeof(double), R.src.bytes / sizeof(double4));
+  const PackBounds pb{ctx->bc_rec, bc_extent(ctx, BC_PACK_IN, in_len),
+                      bc_extent(ctx, BC_PACK_OUT, out_len)};
   pack_strat_kernel<<<(R.nA + 255) / 256, 256, 0, ctx->stream>>>(
       R.x0A.as<double>(), R.absA.as<double>(), R.areaA.as<double>(), R.nA, 2.0 * ctx->omega, t,
-      R.z0.as<double>(), R.src.as<double4>());
+      R.z0.as<double>(), R.src.as<double4>(), pb);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
   return TC_OK;
@@ -396,8 +408,9 @@ int launch_pack_strat(tc_ctx* ctx, double t) {
 int launch_strat_rel_vort(tc_ctx* ctx, const double* abs_vort, const double* x, int n, double t,
                           double* out) {
   if (n <= 0) return TC_OK;
+  const PackBounds pb{ctx->bc_rec, bc_extent(ctx, BC_PACK_IN, n), bc_extent(ctx, BC_PACK_OUT, n)};
   strat_rel_vort_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(abs_vort, x, n,
-                                                                  2.0 * ctx->omega, t, out);
+                                                                  2.0 * ctx->omega, t, out, pb);
   TC_CUDA_TRY(cudaGetLastError());
   ctx->launches += 1;
   return TC_OK;
