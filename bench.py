@@ -145,9 +145,10 @@ class ClockSampler:
 def measured_peaks(device: int) -> dict:
     from thesiscode_b200 import _native as N
 
-    out = {}  # ffma, dfma: FMA/s; rcp32: MUFU reciprocals/s
+    out = {}  # ffma, dfma: FMA/s; rcp32: MUFU reciprocals/s; far_pairs: pairs/s
     for key, kind, iters in (("ffma", N.TC_PROBE_FFMA, 65536), ("dfma", N.TC_PROBE_DFMA, 32768),
-                             ("rcp32", N.TC_PROBE_RCP32, 16384)):
+                             ("rcp32", N.TC_PROBE_RCP32, 16384),
+                             ("far_pairs", N.TC_PROBE_FAR_PAIRS, 2048)):
         best = 0.0
         for _ in range(3):
             v = ctypes.c_double()
@@ -568,7 +569,15 @@ def run_ours(args):
                            "achieved": main["pair_interactions"] / max(main["pair_ms"] * 1e-3, 1e-30),
                            "peak": peaks["rcp32"], "unit": "reciprocals/s",
                            "frac": main["pair_interactions"] / max(main["pair_ms"] * 1e-3, 1e-30) / peaks["rcp32"],
-                           "peak_source": "measured live: MUFU reciprocal probe (tc_probe_peak)"}
+                           "peak_source": "measured live: MUFU reciprocal probe (tc_probe_peak)",
+                           # the kernel's own far-form step alone over a resident shared-memory
+                           # tile (no staging, far tests, flushes or near tiles): the ceiling of
+                           # the pair loop's instruction mix
+                           "pair_loop_ceiling": {
+                               "value": peaks["far_pairs"], "unit": "pairs/s",
+                               "frac": main["pair_interactions"] / max(main["pair_ms"] * 1e-3, 1e-30)
+                               / peaks["far_pairs"],
+                               "source": "measured live: tc_probe_peak TC_PROBE_FAR_PAIRS"}}
                           if args.precision == "fp32c" else None),
         "gpu_launches": main["launches"],
         "gpu_launches_note": "the library's own kernels (pack, Hilbert keys, pair, stage epilogue, KE finalize); "

@@ -75,6 +75,7 @@ extern "C" {
 #define TC_PROBE_RCP64 4
 #define TC_PROBE_DDIV 5
 #define TC_PROBE_F2F 6
+#define TC_PROBE_FAR_PAIRS 7 /* the FP32C pair loop's far step alone, pairs/s */
 
 typedef struct tc_ctx tc_ctx;
 

@@ -38,7 +38,7 @@ TC_VERTEX = 1
 TC_PASSIVE = 2
 # probes
 (TC_PROBE_FFMA, TC_PROBE_FFMA2, TC_PROBE_DFMA, TC_PROBE_RCP32, TC_PROBE_RCP64, TC_PROBE_DDIV,
- TC_PROBE_F2F) = range(7)
+ TC_PROBE_F2F, TC_PROBE_FAR_PAIRS) = range(8)
 # batched ensembles
 TC_BATCH_GRAPH = 1
 TC_BATCH_AUTOTUNE = 2
