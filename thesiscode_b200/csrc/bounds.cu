@@ -1,10 +1,13 @@
 // The checked build's violation records and their C ABI (tc_bounds_*).
 //
-// Each device has one record, shared by every context on that device. The
-// first context created there in the checked library allocates it (32 bytes,
-// kept until the process exits). Kernels receive the record's address in their
-// launch structures, so CUDA graphs captured earlier keep reporting into it.
-// The release library allocates no record and passes null.
+// Each device has one record, shared by every library context on that
+// device. The first library context created there allocates it (32 bytes).
+// The record is kept until the process exits, or until the device's CUDA
+// context is replaced (after cudaDeviceReset). The CUDA context's id is stored
+// with it, so a replaced context gets a new record rather than a dead address.
+// Kernels receive the record's address in their launch structures, so CUDA
+// graphs captured earlier keep reporting into it. The release library
+// allocates no record and passes null.
 #include <mutex>
 
 #include "tc_ctx.h"
@@ -13,6 +16,7 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_bounds_mu;
 tcb::BoundsRec* g_bounds[kMaxDevices] = {};
+unsigned long long g_bounds_ctx[kMaxDevices] = {};  // CUDA context id of each record
 }  // namespace
 
 namespace tcb {
@@ -23,14 +27,18 @@ int bounds_attach(tc_ctx* ctx) {
     tc_record_error("checked build: device %d has no violation record slot", ctx->device);
     return TC_ERR_ARG;
   }
+  const unsigned long long id = current_context_id();
   std::lock_guard<std::mutex> lock(g_bounds_mu);
   BoundsRec*& rec = g_bounds[ctx->device];
-  if (!rec) {
+  // a record of another (replaced) CUDA context is not freed: its memory went with that
+  // context (id 0: the driver cannot tell contexts apart, and the record is kept)
+  if (!rec || (id != 0 && g_bounds_ctx[ctx->device] != id)) {
     void* p = nullptr;
     TC_CUDA_TRY(cudaMalloc(&p, sizeof(BoundsRec)));
     TC_CUDA_TRY(cudaMemset(p, 0, sizeof(BoundsRec)));
     TC_CUDA_TRY(cudaDeviceSynchronize());
     rec = static_cast<BoundsRec*>(p);
+    g_bounds_ctx[ctx->device] = id;
   }
   ctx->bc_rec = rec;
 #else
@@ -50,9 +58,11 @@ extern "C" int tc_bounds_status(int device, long long rec[4], int reset) {
     return TC_ERR_ARG;
   }
   tcb::BoundsRec* d = nullptr;
+  unsigned long long owner = 0;
   {
     std::lock_guard<std::mutex> lock(g_bounds_mu);
     d = g_bounds[device];
+    owner = g_bounds_ctx[device];
   }
   if (!d) return TC_OK;  // release build, or no context on this device yet
   int rc = tc_set_device_checked(device);
@@ -60,6 +70,8 @@ extern "C" int tc_bounds_status(int device, long long rec[4], int reset) {
     tc_record_error("tc_bounds_status: device %d is not available", device);
     return rc;
   }
+  const unsigned long long id = tcb::current_context_id();
+  if (id != 0 && id != owner) return TC_OK;  // the record's CUDA context is gone
   TC_CUDA_TRY(cudaDeviceSynchronize());
   tcb::BoundsRec h{};
   TC_CUDA_TRY(cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost));

@@ -55,9 +55,11 @@ struct ScratchSlot {
 std::mutex g_scratch_mu;
 ScratchSlot g_scratch[kMaxDevices];
 
+}  // namespace
+
 // Unique id of the current context (cuCtxGetId, reached through the runtime so
 // the library links only libcudart); 0 when the driver cannot say.
-unsigned long long current_context_id() {
+unsigned long long tcb::current_context_id() {
   static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
   static PFN_cuCtxGetId_v12000 get_id = nullptr;
   static std::once_flag once;
@@ -81,13 +83,15 @@ unsigned long long current_context_id() {
   return id;
 }
 
+namespace {
+
 // Device address of g_noalloc_scratch on `device` (which must be current).
 int scratch_address(int device, void** out) {
   if (device < 0 || device >= kMaxDevices) {
     tc_record_error("tc_bs_velocity_device_noalloc: device %d out of range", device);
     return TC_ERR_ARG;
   }
-  const unsigned long long id = current_context_id();
+  const unsigned long long id = tcb::current_context_id();
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   ScratchSlot& s = g_scratch[device];
   // id 0 (unknown): look the address up on every call rather than trust a cached one

@@ -191,8 +191,11 @@ int launch_stage_epilogue(tc_ctx* ctx, int stage, double dt, const int range[6],
                           const double* partial = nullptr, long long row_nchunks_len = 0,
                           long long partial_len = 0);
 int resolve_slots(tc_ctx* ctx);
-// Checked build: points ctx->bc_rec at the device's violation record (allocated on first use).
+// Checked build: points ctx->bc_rec at the device's violation record (allocated on first use
+// in each CUDA context).
 int bounds_attach(tc_ctx* ctx);
+// Unique id of the current CUDA context; 0 when the driver cannot say.
+unsigned long long current_context_id();
 const PairVariant* variant(int precision, int id);
 int variant_count(int precision);
 int select_variant(tc_ctx* ctx, int precision, int id);
