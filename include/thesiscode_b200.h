@@ -236,6 +236,11 @@ int tc_reset_rk4(tc_ctx* ctx);
  * checksum) returns TC_ERR_ARG and leaves the context's state as it was. */
 int tc_rk4_save(tc_ctx* ctx, const char* path);
 int tc_rk4_restore(tc_ctx* ctx, const char* path);
+/* Validates a checkpoint file the way tc_rk4_restore does (no GPU needed) and
+ * reports its sizes, whether it holds a forced run, and its step count. Every
+ * output may be NULL. */
+int tc_rk4_checkpoint_info(const char* path, int* nA, int* nV, int* nQ, int* forced,
+                           long long* steps);
 /* Steps advanced since the state was loaded (tc_rk4_advance / tc_rk4_step),
  * counting those recorded in a restored checkpoint. */
 int tc_rk4_steps_done(tc_ctx* ctx, long long* steps);

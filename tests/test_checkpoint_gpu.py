@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from thesiscode_b200 import _native as N
-from thesiscode_b200 import configs
+from thesiscode_b200 import checkpoint, configs
 from thesiscode_b200.panel_velocity import Context
 
 pytestmark = pytest.mark.gpu
@@ -40,7 +40,14 @@ def test_restart_from_checkpoint_continues_bit_for_bit(prec, gpu, tmp_path):
     tke_a = ctx.rk4_advance(dt, first)
     path = tmp_path / "state.tcb"
     ctx.save_state(path)
+    saved = ctx.rk4_store(w.nA, w.nV, w.nQ)
     ctx.close()
+    # the file holds the documented layout (read back here, validated by the library's reader)
+    r = checkpoint.read(path)
+    assert r["steps"] == first and r["omega"] == w.omega and r["deltas"] == tuple(w.deltas)
+    for k, a in zip(("xA", "zetaA", "xV", "xQ"), saved):
+        np.testing.assert_array_equal(r[k], a)
+    np.testing.assert_array_equal(r["areaA"], w.areaA)
 
     ctx = Context(0, prec)  # default Omega and deltas: the checkpoint sets them
     ctx.restore_state(path)

@@ -138,6 +138,7 @@ SIGNATURES: dict[str, tuple] = {
     "tc_rk4_save": (c_int, [c_void_p, c_char_p]),
     "tc_rk4_restore": (c_int, [c_void_p, c_char_p]),
     "tc_rk4_steps_done": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
+    "tc_rk4_checkpoint_info": (c_int, [c_char_p, ip, ip, ip, ip, POINTER(ctypes.c_longlong)]),
     "tc_bounds_checked": (c_int, []),
     "tc_bounds_status": (c_int, [c_int, POINTER(ctypes.c_longlong), c_int]),
     "tc_bounds_cap": (c_int, [c_void_p, c_int, ctypes.c_longlong]),

@@ -125,14 +125,32 @@ extern "C" int tc_rk4_save(tc_ctx* ctx, const char* path) {
   return TC_OK;
 }
 
-extern "C" int tc_rk4_restore(tc_ctx* ctx, const char* path) {
-  if (!ctx || !path) return TC_ERR_ARG;
+// Reads and validates a checkpoint: magic, version, sizes against the file
+// length, checksum. On success *h is its header and bytes its whole content.
+static int read_checkpoint(const char* path, Header* h, std::vector<unsigned char>& bytes);
+
+extern "C" int tc_rk4_checkpoint_info(const char* path, int* nA, int* nV, int* nQ, int* forced,
+                                      long long* steps) {
+  if (!path) return TC_ERR_ARG;
+  Header h;
+  std::vector<unsigned char> bytes;
+  const int rc = read_checkpoint(path, &h, bytes);
+  if (rc) return rc;
+  if (nA) *nA = h.nA;
+  if (nV) *nV = h.nV;
+  if (nQ) *nQ = h.nQ;
+  if (forced) *forced = (int)(h.flags & 1u);
+  if (steps) *steps = h.steps;
+  return TC_OK;
+}
+
+static int read_checkpoint(const char* path, Header* hp, std::vector<unsigned char>& bytes) {
   FILE* f = fopen(path, "rb");
   if (!f) {
-    tc_record_error("tc_rk4_restore: cannot open %s", path);
+    tc_record_error("checkpoint: cannot open %s", path);
     return TC_ERR_ARG;
   }
-  std::vector<unsigned char> bytes;
+  bytes.clear();
   unsigned char chunk[1 << 16];
   size_t got;
   while ((got = fread(chunk, 1, sizeof(chunk), f)) > 0)
@@ -140,33 +158,46 @@ extern "C" int tc_rk4_restore(tc_ctx* ctx, const char* path) {
   fclose(f);
   Header h;
   if (bytes.size() < sizeof(Header) + sizeof(uint64_t)) {
-    tc_record_error("tc_rk4_restore: %s is too short for a checkpoint", path);
+    tc_record_error("checkpoint: %s is too short for a checkpoint", path);
     return TC_ERR_ARG;
   }
   memcpy(&h, bytes.data(), sizeof(Header));
   if (memcmp(h.magic, kMagic, sizeof(kMagic)) != 0 || h.version != kVersion || (h.flags & ~1u)) {
-    tc_record_error("tc_rk4_restore: %s is not a version-%u checkpoint", path, kVersion);
+    tc_record_error("checkpoint: %s is not a version-%u checkpoint", path, kVersion);
     return TC_ERR_ARG;
   }
   const bool forced = (h.flags & 1u) != 0;
   if (h.nA < 0 || h.nV < 0 || h.nQ < 0) {
-    tc_record_error("tc_rk4_restore: negative sizes in %s", path);
+    tc_record_error("checkpoint: negative sizes in %s", path);
     return TC_ERR_ARG;
   }
   const size_t nA = (size_t)h.nA, nV = (size_t)h.nV, nQ = (size_t)h.nQ;
   const size_t doubles = 3 * nA + nA + nA + 3 * nV + 3 * nQ + (forced ? nA + nV : 0);
   const size_t body = bytes.size() - sizeof(Header) - sizeof(uint64_t);
   if (body != doubles * sizeof(double)) {
-    tc_record_error("tc_rk4_restore: %s holds %zu bytes of arrays, its header asks for %zu", path,
+    tc_record_error("checkpoint: %s holds %zu bytes of arrays, its header asks for %zu", path,
                     body, doubles * sizeof(double));
     return TC_ERR_ARG;
   }
   uint64_t sum;
   memcpy(&sum, bytes.data() + bytes.size() - sizeof(sum), sizeof(sum));
   if (fnv1a(bytes.data(), bytes.size() - sizeof(sum)) != sum) {
-    tc_record_error("tc_rk4_restore: %s fails its checksum", path);
+    tc_record_error("checkpoint: %s fails its checksum", path);
     return TC_ERR_ARG;
   }
+  *hp = h;
+  return TC_OK;
+}
+
+extern "C" int tc_rk4_restore(tc_ctx* ctx, const char* path) {
+  if (!ctx || !path) return TC_ERR_ARG;
+  Header h;
+  std::vector<unsigned char> bytes;
+  int rc = read_checkpoint(path, &h, bytes);
+  if (rc) return rc;
+  const bool forced = (h.flags & 1u) != 0;
+  const size_t nA = (size_t)h.nA, nV = (size_t)h.nV, nQ = (size_t)h.nQ;
+  const size_t doubles = 3 * nA + nA + nA + 3 * nV + 3 * nQ + (forced ? nA + nV : 0);
   // the arrays, copied out of the byte buffer (which need not be 8-byte aligned)
   std::vector<double> a(doubles);
   memcpy(a.data(), bytes.data() + sizeof(Header), doubles * sizeof(double));
@@ -177,7 +208,7 @@ extern "C" int tc_rk4_restore(tc_ctx* ctx, const char* path) {
   const double* xQ = xV + 3 * nV;
   const double* absA = xQ + 3 * nQ;
   const double* absV = absA + nA;
-  int rc = tc_rk4_load(ctx, xA, zA, arA, h.nA, xV, h.nV, xQ, h.nQ, 0);
+  rc = tc_rk4_load(ctx, xA, zA, arA, h.nA, xV, h.nV, xQ, h.nQ, 0);
   if (rc) return rc;
   tcb::Rk4State& R = ctx->rk;
   if (forced) {
